@@ -1,0 +1,236 @@
+"""bia_3d_gpu_b200 -- the BIA pair step of bia_3d_gpu, rebuilt for B200 (sm_100a).
+
+Two layers, both backed only by libbia_b200.so (CUDA kernels; no CPU fallback):
+
+* the reference's Fortran-facing interface, same names and argument meaning:
+    find_dxyuv_kernel(METHOD, N, I, EPS, DT, ITR, dX, dY, dZ, dU, dV, dW, RXYZUVW, dXYZUVW)
+        bia/find_dXYUV_kernel.cu:526-561, as called from bia/bia.f90:135,138
+    invariance_gpu(N, eps_th, X, Y, Z, U, V, W) -> (KE, PE, Lx, Ly, Lz, Ua, Va, Wa, Xa, Ya, Za)
+        bia/invariance.cu:50-110, as called from bia/bia.f90:67-68
+  operating in place on host numpy float64 arrays;
+
+* BIASolver: whole steps on device-resident state (a (6, n) float64 CUDA tensor),
+  multi-step runs captured in a CUDA graph, host-buffer runs, device invariants.
+"""
+import ctypes
+
+import numpy as np
+
+from . import capi
+from .capi import (BIA_ERR_NONFINITE, BIA_OK, METHOD_ALG, METHOD_RKF, BiaConfig, BiaError,
+                   BiaStats, default_config)
+
+__all__ = ["find_dxyuv_kernel", "invariance_gpu", "BIASolver", "default_config", "BiaConfig",
+           "BiaError", "METHOD_ALG", "METHOD_RKF", "INVARIANT_NAMES"]
+
+INVARIANT_NAMES = ("KE", "PE", "Lx", "Ly", "Lz", "Ua", "Va", "Wa", "Xa", "Ya", "Za")
+
+_PD = ctypes.POINTER(ctypes.c_double)
+
+
+def _host_f64(a, n, name):
+    if not isinstance(a, np.ndarray) or a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise TypeError(f"{name} must be a C-contiguous float64 numpy array")
+    if a.size < n:
+        raise ValueError(f"{name} has {a.size} elements, need {n}")
+    return a.ctypes.data_as(_PD)
+
+
+def find_dxyuv_kernel(METHOD, N, I, EPS, DT, ITR, dX, dY, dZ, dU, dV, dW, RXYZUVW, dXYZUVW):
+    """Pair solve of particle I (1-based) against every j > I, on the GPU.
+
+    Mirrors find_dxyuv_kernel_ (bia/find_dXYUV_kernel.cu:526-561): RXYZUVW holds the
+    AoS relative state x_I - x_j, ..., w_I - w_j for all j (6N doubles); dXYZUVW
+    (6N doubles) receives the half-displacements; dX..dW are accumulated in place
+    (dX[I] += h_j, dX[j] -= h_j).  No drift is added.  Returns the status code
+    (0 ok, 2 when a pair gave a non-finite result); other failures raise BiaError.
+    """
+    L = capi.lib()
+    ptrs = [_host_f64(a, N, nm) for a, nm in ((dX, "dX"), (dY, "dY"), (dZ, "dZ"), (dU, "dU"),
+                                              (dV, "dV"), (dW, "dW"))]
+    p_rel = _host_f64(RXYZUVW, 6 * N, "RXYZUVW")
+    p_out = _host_f64(dXYZUVW, 6 * N, "dXYZUVW")
+    L.find_dxyuv_kernel_(int(METHOD), int(N), int(I), float(EPS), float(DT), int(ITR), *ptrs,
+                         p_rel, p_out)
+    st = L.bia_last_error()
+    if st not in (BIA_OK, BIA_ERR_NONFINITE):
+        raise BiaError(st, "find_dxyuv_kernel")
+    return st
+
+
+def invariance_gpu(N, eps_th, X, Y, Z, U, V, W):
+    """Invariants on the GPU (bia/invariance.cu:50-110): returns the tuple
+    (KE, PE, Lx, Ly, Lz, Ua, Va, Wa, Xa, Ya, Za) that the reference returns through
+    its scalar pointer arguments.  KE = sum |v|^2, PE = eps_th * sum_{i<j} 1/r_ij."""
+    L = capi.lib()
+    ins = [_host_f64(a, N, nm) for a, nm in ((X, "X"), (Y, "Y"), (Z, "Z"), (U, "U"), (V, "V"),
+                                             (W, "W"))]
+    outs = [ctypes.c_double(0.0) for _ in range(11)]
+    L.invariance_gpu_(int(N), float(eps_th), *ins, *[ctypes.byref(o) for o in outs])
+    st = L.bia_last_error()
+    if st != BIA_OK:
+        raise BiaError(st, "invariance_gpu")
+    return tuple(o.value for o in outs)
+
+
+def measure_fp64_peak(device=0):
+    """Measured FP64 FMA throughput of the device in TFLOP/s."""
+    out = ctypes.c_double(0.0)
+    capi.check(capi.lib().bia_measure_fp64_peak(int(device), ctypes.byref(out)),
+               "bia_measure_fp64_peak")
+    return out.value
+
+
+class BIASolver:
+    """Device-resident BIA steps through libbia_b200.so.
+
+    state: a (6, n) contiguous float64 CUDA tensor (x, y, z, u, v, w rows), updated in
+    place.  q: optional (n,) float64 CUDA tensor of charges (pair coupling
+    eps_th * q_i * q_j).  The solver launches on `stream` (a torch.cuda.Stream; default:
+    a new non-default stream, which allows CUDA-graph replay in run()).
+    """
+
+    def __init__(self, device=0, stream=None):
+        import torch
+        self._torch = torch
+        self.device = torch.device("cuda", device)
+        if stream is None:
+            stream = torch.cuda.Stream(device=self.device)
+        self.stream = stream
+        self._ctx = ctypes.c_void_p()
+        capi.check(capi.lib().bia_context_create(ctypes.byref(self._ctx), int(device),
+                                                 ctypes.c_void_p(stream.cuda_stream)),
+                   "bia_context_create")
+
+    def close(self):
+        if self._ctx:
+            capi.lib().bia_context_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- helpers ----------------------------------------------------------------------
+    def _check_state(self, state):
+        t = self._torch
+        if not (isinstance(state, t.Tensor) and state.is_cuda and state.dtype == t.float64 and
+                state.dim() == 2 and state.shape[0] == 6 and state.is_contiguous()):
+            raise TypeError("state must be a contiguous (6, n) float64 CUDA tensor")
+        return state.shape[1]
+
+    def _ptrs(self, state):
+        n = state.shape[1]
+        base = state.data_ptr()
+        return [ctypes.c_void_p(base + k * n * 8) for k in range(6)]
+
+    def _qptr(self, q, n):
+        if q is None:
+            return ctypes.c_void_p(None)
+        t = self._torch
+        if not (isinstance(q, t.Tensor) and q.is_cuda and q.dtype == t.float64 and
+                q.numel() == n and q.is_contiguous()):
+            raise TypeError("q must be a contiguous float64 CUDA tensor of n charges")
+        return ctypes.c_void_p(q.data_ptr())
+
+    def _enter(self):
+        """Order the solver's stream after work already queued on torch's current stream."""
+        cur = self._torch.cuda.current_stream(self.device)
+        if cur.cuda_stream != self.stream.cuda_stream:
+            self.stream.wait_stream(cur)
+        return cur
+
+    def _leave(self, cur):
+        """Make torch's current stream wait for the solver's launches."""
+        if cur.cuda_stream != self.stream.cuda_stream:
+            cur.wait_stream(self.stream)
+
+    @staticmethod
+    def _finish(st, stats, what):
+        if st not in (BIA_OK, BIA_ERR_NONFINITE):
+            raise BiaError(st, what)
+        return stats.as_dict()
+
+    # -- API --------------------------------------------------------------------------
+    def step(self, state, cfg, q=None, disp=None, stats=True):
+        """One BIA step (all pairs, reduction, drift, update).  disp: optional (6, n)
+        float64 CUDA tensor receiving dX..dW.  Returns the step's counters (this
+        synchronises) or None with stats=False."""
+        n = self._check_state(state)
+        dp = ctypes.c_void_p(disp.data_ptr()) if disp is not None else ctypes.c_void_p(None)
+        s = BiaStats()
+        cur = self._enter()
+        st = capi.lib().bia_step(self._ctx, ctypes.byref(cfg), n, *self._ptrs(state),
+                                 self._qptr(q, n), dp, ctypes.byref(s) if stats else None)
+        self._leave(cur)
+        if not stats:
+            capi.check(st, "bia_step")
+            return None
+        return self._finish(st, s, "bia_step")
+
+    def run(self, state, cfg, nsteps, q=None, graph=True, stats=True):
+        """nsteps steps; the step sequence is captured once in a CUDA graph and replayed."""
+        n = self._check_state(state)
+        s = BiaStats()
+        cur = self._enter()
+        st = capi.lib().bia_run(self._ctx, ctypes.byref(cfg), n, *self._ptrs(state),
+                                self._qptr(q, n), int(nsteps), int(bool(graph)),
+                                ctypes.byref(s) if stats else None)
+        self._leave(cur)
+        if not stats:
+            capi.check(st, "bia_run")
+            return None
+        return self._finish(st, s, "bia_run")
+
+    def run_host(self, state, cfg, nsteps, q=None):
+        """nsteps steps on a host (6, n) float64 numpy state, updated in place (the
+        host-to-device and device-to-host copies are part of the call)."""
+        if not (isinstance(state, np.ndarray) and state.dtype == np.float64 and
+                state.flags.c_contiguous and state.ndim == 2 and state.shape[0] == 6):
+            raise TypeError("state must be a C-contiguous (6, n) float64 numpy array")
+        n = state.shape[1]
+        base = state.ctypes.data
+        ptrs = [ctypes.c_void_p(base + k * n * 8) for k in range(6)]
+        qp = ctypes.c_void_p(None)
+        if q is not None:
+            q = np.ascontiguousarray(q, dtype=np.float64)
+            qp = ctypes.c_void_p(q.ctypes.data)
+        s = BiaStats()
+        st = capi.lib().bia_run_host(self._ctx, ctypes.byref(cfg), n, *ptrs, qp, int(nsteps),
+                                     ctypes.byref(s))
+        return self._finish(st, s, "bia_run_host")
+
+    def invariance(self, state, eps_th, q=None):
+        """Invariants of the device state (FP64, fixed-order reductions)."""
+        n = self._check_state(state)
+        out = (ctypes.c_double * 11)()
+        cur = self._enter()
+        st = capi.lib().bia_invariance(self._ctx, n, float(eps_th), *self._ptrs(state),
+                                       self._qptr(q, n), out)
+        self._leave(cur)
+        capi.check(st, "bia_invariance")
+        return dict(zip(INVARIANT_NAMES, list(out)))
+
+    def counters(self, reset=True):
+        """Counters summed over every step run with stats=False since the last reset."""
+        s = BiaStats()
+        st = capi.lib().bia_context_stats(self._ctx, ctypes.byref(s), int(bool(reset)))
+        return self._finish(st, s, "bia_context_stats")
+
+    def set_timing(self, on):
+        capi.check(capi.lib().bia_context_set_timing(self._ctx, int(bool(on))))
+
+    def kernel_ms(self):
+        """(summed duration in ms, launches) of the pair kernel since the last call."""
+        ms = ctypes.c_double(0.0)
+        cnt = ctypes.c_longlong(0)
+        capi.check(capi.lib().bia_context_kernel_ms(self._ctx, ctypes.byref(ms), ctypes.byref(cnt)))
+        return ms.value, cnt.value

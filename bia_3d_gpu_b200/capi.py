@@ -1,0 +1,123 @@
+"""ctypes binding of libbia_b200.so (declarations in include/bia_capi.h).
+
+The library is the product: every pair solve runs in its CUDA kernels.  Loading
+fails loudly when the library has not been built; there is no CPU fallback.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbia_b200.so")
+
+BIA_OK = 0
+BIA_ERR_INVALID_ARGUMENT = 1
+BIA_ERR_NONFINITE = 2
+BIA_ERR_NOT_CONVERGED = 3
+BIA_ERR_DEVICE_TIMEOUT = 4
+BIA_ERR_CUDA = 5
+BIA_ERR_OUT_OF_MEMORY = 6
+BIA_ERR_NO_DEVICE = 7
+
+METHOD_RKF = 0
+METHOD_ALG = 1
+
+
+class BiaConfig(ctypes.Structure):
+    _fields_ = [("method", ctypes.c_int), ("itr", ctypes.c_int), ("eps_th", ctypes.c_double),
+                ("dt", ctypes.c_double), ("err", ctypes.c_double),
+                ("rkf_relerr", ctypes.c_double), ("rkf_abserr", ctypes.c_double),
+                ("deterministic", ctypes.c_int)]
+
+
+STAT_FIELDS = ("hyperbola", "parabola", "ellipse", "degenerate", "rkf", "iterations",
+               "iter_hyperbola", "iter_ellipse", "iter_parabola", "rkf_steps", "nonconverged",
+               "bracket_exits", "nonfinite")
+
+
+class BiaStats(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_longlong) for name in STAT_FIELDS]
+
+    def as_dict(self):
+        return {name: int(getattr(self, name)) for name in STAT_FIELDS}
+
+
+class BiaError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        msg = status_string(status)
+        super().__init__(f"{what}: {msg} (status {status})" if what else msg)
+
+
+_lib = None
+_D = ctypes.c_double
+_I = ctypes.c_int
+_V = ctypes.c_void_p
+_PD = ctypes.POINTER(ctypes.c_double)
+
+
+def lib():
+    """Load libbia_b200.so; raises if it is missing (build it first)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: run `python -m bia_3d_gpu_b200.build` "
+                           "(the CUDA library is required; there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    L.bia_config_default.argtypes = [ctypes.POINTER(BiaConfig)]
+    L.bia_config_default.restype = None
+    L.bia_status_string.argtypes = [_I]
+    L.bia_status_string.restype = ctypes.c_char_p
+    L.bia_last_error.restype = _I
+    L.bia_context_create.argtypes = [ctypes.POINTER(_V), _I, _V]
+    L.bia_context_destroy.argtypes = [_V]
+    L.bia_context_set_stream.argtypes = [_V, _V]
+    L.bia_context_set_timing.argtypes = [_V, _I]
+    L.bia_context_kernel_ms.argtypes = [_V, _PD, ctypes.POINTER(ctypes.c_longlong)]
+    L.bia_step.argtypes = [_V, ctypes.POINTER(BiaConfig), _I] + [_V] * 8 + [ctypes.POINTER(BiaStats)]
+    L.bia_run.argtypes = ([_V, ctypes.POINTER(BiaConfig), _I] + [_V] * 7 +
+                          [_I, _I, ctypes.POINTER(BiaStats)])
+    L.bia_run_host.argtypes = ([_V, ctypes.POINTER(BiaConfig), _I] + [_V] * 7 +
+                               [_I, ctypes.POINTER(BiaStats)])
+    L.bia_invariance.argtypes = [_V, _I, _D] + [_V] * 7 + [_PD]
+    L.bia_measure_fp64_peak.argtypes = [_I, _PD]
+    L.bia_context_stats.argtypes = [_V, ctypes.POINTER(BiaStats), _I]
+    L.find_dxyuv_kernel_.argtypes = [_I, _I, _I, _D, _D, _I] + [_PD] * 8
+    L.find_dxyuv_kernel_.restype = None
+    L.invariance_gpu_.argtypes = [_I, _D] + [_PD] * 6 + [_PD] * 11
+    L.invariance_gpu_.restype = None
+    for name in ("bia_context_create", "bia_context_destroy", "bia_context_set_stream",
+                 "bia_context_set_timing", "bia_context_kernel_ms", "bia_step", "bia_run",
+                 "bia_run_host", "bia_invariance", "bia_measure_fp64_peak", "bia_context_stats"):
+        getattr(L, name).restype = _I
+    _lib = L
+    return L
+
+
+def status_string(status):
+    try:
+        return lib().bia_status_string(status).decode()
+    except RuntimeError:
+        return f"status {status}"
+
+
+def check(status, what=""):
+    if status != BIA_OK:
+        raise BiaError(status, what)
+
+
+def default_config(**overrides):
+    cfg = BiaConfig()
+    lib().bia_config_default(ctypes.byref(cfg))
+    for k, v in overrides.items():
+        if not hasattr(cfg, k):
+            raise AttributeError(f"bia_config has no field {k!r}")
+        setattr(cfg, k, v)
+    return cfg
+
+
+EXPORTED_SYMBOLS = ("bia_config_default", "bia_context_create", "bia_context_destroy",
+                    "bia_context_set_stream", "bia_context_set_timing", "bia_context_kernel_ms",
+                    "bia_step", "bia_run", "bia_run_host", "bia_invariance", "bia_status_string",
+                    "bia_measure_fp64_peak", "bia_context_stats",
+                    "bia_last_error", "find_dxyuv_kernel_", "invariance_gpu_")

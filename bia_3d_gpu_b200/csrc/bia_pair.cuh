@@ -1,0 +1,548 @@
+// bia_pair.cuh -- per-pair BIA solvers in FP64 for sm_100a.
+//
+// One unordered pair (i, j) with relative state r = x_i - x_j, g = v_i - v_j is
+// reduced to a planar two-body problem (bia/bia.f90:284-314), classified by its
+// energy (bia/bia.f90:156-166) and advanced over dt by the hyperbola, parabola or
+// ellipse solver (bia/find_hyperbola.f90, find_parabola.f90, find_ellipse.f90) or by
+// the per-pair RKF4(5) (bia/find_dXYUV_RKF.f90).  The result is the pair's
+// half-displacement h (bia/bia.f90:173-185): i receives +h, j receives -h.
+//
+// The formulas follow the reference's CPU path; CUDA's double-precision math
+// functions replace glibc's, and nvcc's FMA contraction is left on, so results agree
+// with the CPU oracle to rounding, not bit for bit.  The same deviations as the
+// oracle are taken where the reference is undefined (uninitialised theta_stock,
+// bracket exit without a result, zero |g| or |L|).
+#pragma once
+#include <cstdint>
+
+namespace bia {
+
+constexpr double kPi = 3.14159265358979323846264338327950288419716939937510582097494;
+
+enum PairClass { kHyperbola = 0, kParabola = 1, kEllipse = 2, kDegenerate = 3, kRkf = 4 };
+
+struct PairParams {
+    double dt;
+    double err;      // ERR, residual threshold for the not-converged count
+    double relerr;   // RKF tolerances
+    double abserr;
+    int itr;         // Newton cap ITR
+    int method;      // 0 RKF, 1 ALG
+};
+
+// Per-thread counters, reduced per warp before one atomic per counter.
+struct PairCounters {
+    int cls[5];
+    int it_hyp, it_ell, it_par;
+    int rkf_steps;
+    int nonconverged;
+    int bracket_exits;
+    int nonfinite;
+};
+
+__device__ __forceinline__ void counters_zero(PairCounters &c)
+{
+#pragma unroll
+    for (int k = 0; k < 5; k++) c.cls[k] = 0;
+    c.it_hyp = c.it_ell = c.it_par = c.rkf_steps = c.nonconverged = c.bracket_exits = c.nonfinite = 0;
+}
+
+// bia/bia.f90:284-314.  Returns true for a degenerate pair (|g| == 0 or |L| == 0):
+// then the frame is the line of motion and Y has a single nonzero position axis.
+__device__ __forceinline__ bool frame_xi_eta(const double r[3], const double g[3], double e_xi[3],
+                                             double e_eta[3], double Y[4])
+{
+    double gsq = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+    double gm = sqrt(gsq);
+    double L0 = r[1] * g[2] - r[2] * g[1];
+    double L1 = r[2] * g[0] - r[0] * g[2];
+    double L2 = r[0] * g[1] - r[1] * g[0];
+    double Lsq = L0 * L0 + L1 * L1 + L2 * L2;
+    if (gm == 0.0 || Lsq == 0.0) {
+        if (gm == 0.0) {
+            double rm = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+#pragma unroll
+            for (int k = 0; k < 3; k++) { e_xi[k] = r[k] / rm; e_eta[k] = 0.0; }
+            Y[0] = rm; Y[1] = 0.0; Y[2] = 0.0; Y[3] = 0.0;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 3; k++) { e_eta[k] = g[k] / gm; e_xi[k] = 0.0; }
+            Y[0] = 0.0;
+            Y[1] = r[0] * e_eta[0] + r[1] * e_eta[1] + r[2] * e_eta[2];
+            Y[2] = 0.0;
+            Y[3] = gm;
+        }
+        return true;
+    }
+    double Lm = sqrt(Lsq);
+    double ez0 = L0 / Lm, ez1 = L1 / Lm, ez2 = L2 / Lm;
+#pragma unroll
+    for (int k = 0; k < 3; k++) e_eta[k] = g[k] / gm;
+    e_xi[0] = e_eta[1] * ez2 - e_eta[2] * ez1;
+    e_xi[1] = e_eta[2] * ez0 - e_eta[0] * ez2;
+    e_xi[2] = e_eta[0] * ez1 - e_eta[1] * ez0;
+    Y[0] = r[0] * e_xi[0] + r[1] * e_xi[1] + r[2] * e_xi[2];
+    Y[2] = 0.0;
+    Y[1] = r[0] * e_eta[0] + r[1] * e_eta[1] + r[2] * e_eta[2];
+    Y[3] = gm;
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// bia/find_hyperbola.f90:1-166.  Returns the main-loop iteration count.
+// ---------------------------------------------------------------------------
+struct HypConsts {
+    double theta_0, tn_0, cs_0, sn_0, time_end_;
+};
+
+// bia/find_hyperbola.f90:149-165 find_theta, given sn_p and sn_m at theta_now.
+__device__ __forceinline__ double hyp_newton(const HypConsts &c, double theta_now, double sn_p,
+                                             double sn_m, double *error_)
+{
+    double sn_now, cs_now;
+    sincos(theta_now, &sn_now, &cs_now);
+    double D_inv = 1.0 / (cs_now - c.cs_0);
+    double e = c.tn_0 * sn_now * D_inv - c.time_end_ + log(sn_p / sn_m);
+    *error_ = e;
+    if (e == 0.0) return theta_now;
+    double dfdth = c.tn_0 * (1.0 - c.cs_0 * cs_now) * (D_inv * D_inv) + c.sn_0 / (2.0 * sn_p * sn_m);
+    return theta_now - e / dfdth;
+}
+
+__device__ __forceinline__ int hyperbola(double eps_th, double dt, int ITR, const double YZ[4],
+                                         double YN[4], double *error_end, int *bracket_exit)
+{
+    const double X_ini = YZ[0], Y_ini = YZ[1], U_ini = YZ[2], V_ini = YZ[3];
+    const double r_g = X_ini * U_ini + Y_ini * V_ini;
+    const double Lz = X_ini * V_ini - Y_ini * U_ini;
+    const double r = sqrt(X_ini * X_ini + Y_ini * Y_ini);
+    const double g2 = U_ini * U_ini + V_ini * V_ini;
+    const double W = g2 + 2.0 * eps_th / r;
+    const double g_0 = sqrt(W);
+    const double b_0 = eps_th / W;
+    const double b = fabs(Lz) / g_0;
+    HypConsts c;
+    c.theta_0 = atan2(fabs(Lz), b_0 * g_0);
+    const double den0 = sqrt(b_0 * b_0 * (g_0 * g_0) + Lz * Lz);
+    c.cs_0 = b_0 * g_0 / den0;
+    c.sn_0 = fabs(Lz) / den0;
+    c.tn_0 = fabs(Lz) / (b_0 * g_0);
+    const double arg = c.cs_0 + b * c.sn_0 / r;
+    double theta_ini = (fabs(arg) > 1.0) ? 1e-30 : acos(arg);
+    if (Lz * r_g < 0.0) theta_ini = -theta_ini;
+    double sn, cs;
+    sincos(theta_ini, &sn, &cs);
+    const double x = r * cs, y = r * sn;
+    const double g0_sn0 = (Lz > 0.0) ? g_0 / c.sn_0 : -g_0 / c.sn_0;
+    const double u = g0_sn0 * (c.cs_0 * sn);
+    const double v = g0_sn0 * (1.0 - c.cs_0 * cs);
+    const double den_a = sqrt((X_ini * X_ini + Y_ini * Y_ini) * (x * x + y * y));
+    const double cs_a = (x * X_ini + y * Y_ini) / den_a;
+    const double sn_a = (x * Y_ini - y * X_ini) / den_a;
+    const double sp_ini = sin((c.theta_0 + theta_ini) * 0.5);
+    const double sm_ini = sin((c.theta_0 - theta_ini) * 0.5);
+    const double time_ini = (c.tn_0 * sn / (cs - c.cs_0) + log(sp_ini / sm_ini)) * b_0 / g_0;
+    const double time_end = (Lz > 0.0) ? time_ini + dt : time_ini - dt;
+    c.time_end_ = time_end * g_0 / b_0;
+    const double theta_gss = 2.0 / kPi * c.theta_0 * atan(c.time_end_ / c.tn_0);
+
+    // two candidate starts (bia/find_hyperbola.f90:73-89)
+    double error_ini_, error_gss_;
+    const double th_ini_end = hyp_newton(c, theta_ini, sp_ini, sm_ini, &error_ini_);
+    const double sp_g = sin((c.theta_0 + theta_gss) * 0.5);
+    const double sm_g = sin((c.theta_0 - theta_gss) * 0.5);
+    const double th_gss_end = hyp_newton(c, theta_gss, sp_g, sm_g, &error_gss_);
+    double theta_end, error_;
+    if (fabs(error_gss_) > 10.0 * fabs(error_ini_)) {
+        theta_end = th_ini_end;
+        error_ = error_ini_;
+    } else {
+        theta_end = th_gss_end;
+        error_ = error_gss_;
+    }
+    // minimum-residual Newton loop with cycle detection (bia/find_hyperbola.f90:93-120)
+    double err_stock = error_;
+    double theta_stock = theta_end;
+    double hist[64];
+    int IR = 0;
+    *bracket_exit = 0;
+    while (IR < ITR) {
+        const double theta_now = theta_end;
+        const double sn_p = sin((c.theta_0 + theta_now) * 0.5);
+        const double sn_m = sin((c.theta_0 - theta_now) * 0.5);
+        if (sn_p * sn_m < 0.0) {
+            *bracket_exit = 1;
+            break;
+        }
+        theta_end = hyp_newton(c, theta_now, sn_p, sn_m, &error_);
+        IR++;
+        bool cycle = false;
+        for (int num = IR - 1; num >= 1; num--)
+            if (hist[num] == error_) { cycle = true; break; }
+        if (cycle) break;
+        hist[IR] = error_;
+        if (fabs(error_) < fabs(err_stock)) {
+            err_stock = error_ * b_0 / g_0;
+            theta_stock = theta_end;
+            if (fabs(err_stock) < 2e-16) break;
+        }
+    }
+    *error_end = error_ * b_0 / g_0;
+    double sn_end, cs_end;
+    sincos(theta_stock, &sn_end, &cs_end);
+    const double u_end = g0_sn0 * c.cs_0 * sn_end;
+    const double du_end = u_end - u;
+    const double v_end = g0_sn0 * (1.0 - c.cs_0 * cs_end);
+    const double dv_end = v_end - v;
+    const double r_end = b * c.sn_0 / (cs_end - c.cs_0);
+    YN[0] = r_end * (cs_end * cs_a - sn_end * sn_a);
+    YN[1] = r_end * (cs_end * sn_a + sn_end * cs_a);
+    YN[2] = YZ[2] + (du_end * cs_a - dv_end * sn_a);
+    YN[3] = YZ[3] + (du_end * sn_a + dv_end * cs_a);
+    return IR;
+}
+
+// ---------------------------------------------------------------------------
+// bia/find_ellipse.f90:1-157 (with its contained Newton).  Returns ir.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double f_sign(double a, double b) { return (b >= 0.0) ? fabs(a) : -fabs(a); }
+
+static __device__ __noinline__ int ellipse(double eps_th, double dt, int ITR, const double YZ[4],
+                                    double YN[4], double *error)
+{
+    const double X_ini = YZ[0], Y_ini = YZ[1], U_ini = YZ[2], V_ini = YZ[3];
+    const double g2_ini = U_ini * U_ini + V_ini * V_ini;
+    const double r_ini = sqrt(X_ini * X_ini + Y_ini * Y_ini);
+    const double W = g2_ini + 2.0 * eps_th / r_ini;
+    const double L = X_ini * V_ini - Y_ini * U_ini;
+    const double r_g_ini = X_ini * U_ini + Y_ini * V_ini;
+    const double g_a = f_sign(sqrt(-W), L);
+    const double a = eps_th / W;
+    const double b = L / g_a;
+    const double omega_a = g_a / a;
+    double ecc = sqrt((a * g_a) * (a * g_a) - L * L) / (a * g_a);
+    double xi_ini;
+    if (r_g_ini == 0.0) {
+        if (r_ini < a) {
+            xi_ini = 0.0;
+        } else if (r_ini == a) {
+            xi_ini = atan2(Y_ini, X_ini);
+            ecc = 0.0;
+        } else {
+            xi_ini = f_sign(kPi, L);
+        }
+    } else {
+        xi_ini = atan2(r_g_ini / g_a, a - r_ini);
+    }
+    double s_ini, c_ini;
+    sincos(xi_ini, &s_ini, &c_ini);
+    const double alpha = atan2(Y_ini, X_ini) - atan2(b * s_ini, a * (c_ini - ecc));
+    const double tau_ini = xi_ini - ecc * s_ini;
+    const double time_ini = tau_ini / omega_a;
+    const double time_end = time_ini + dt;
+    const double tau_end = omega_a * time_end;
+    *error = 0.0;
+    if (dt == 0.0) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) YN[k] = YZ[k];
+        return 0;
+    }
+    int ir = 0;
+    const double error_ini = tau_end - xi_ini + ecc * s_ini;
+    const double delta_ini = error_ini * (1.0 - ecc * c_ini);
+    double st, ct;
+    sincos(tau_end, &st, &ct);
+    double xi_2 = (ct < 0.9) ? tau_end : f_sign(kPi / 2, st);
+    double s2, c2;
+    sincos(xi_2, &s2, &c2);
+    double error_tm2 = tau_end - xi_2 + ecc * s2;
+    double delta_xi2 = error_tm2 / (1.0 - ecc * c2);
+    double xi = (fabs(error_ini) < fabs(error_tm2)) ? xi_2 + delta_ini : xi_2 + delta_xi2;
+    double xi_1 = __longlong_as_double(0x7ff8000000000000LL);  // unset: compares unequal
+    double error_tm1;
+    while (xi_1 != xi_2 && ir <= ITR) {
+        ir++;
+        xi_1 = xi;
+        double s1, c1;
+        sincos(xi_1, &s1, &c1);
+        error_tm1 = tau_end - xi_1 + ecc * s1;
+        xi = xi_1 + error_tm1 / (1.0 - ecc * c1);
+        if (error_tm1 == 0.0 || error_tm1 == error_tm2 || error_tm1 + error_tm2 == 0.0) {
+            *error = error_tm1;
+            break;
+        }
+        ir++;
+        xi_2 = xi;
+        sincos(xi_2, &s2, &c2);
+        error_tm2 = tau_end - xi_2 + ecc * s2;
+        delta_xi2 = error_tm2 / (1.0 - ecc * c2);
+        xi = xi_2 + delta_xi2;
+        if (error_tm2 == 0.0 || error_tm1 == error_tm2 || error_tm1 + error_tm2 == 0.0) {
+            *error = error_tm2;
+            break;
+        }
+    }
+    double sn_end, cs_end;
+    sincos(xi, &sn_end, &cs_end);
+    const double xx_end = a * (cs_end - ecc);
+    const double yy_end = b * sn_end;
+    const double rr_end = a * (1.0 - ecc * cs_end);
+    const double uu_end = -a * g_a * sn_end / rr_end;
+    const double vv_end = b * g_a * cs_end / rr_end;
+    double sn_alp, cs_alp;
+    sincos(alpha, &sn_alp, &cs_alp);
+    YN[0] = xx_end * cs_alp - yy_end * sn_alp;
+    YN[1] = xx_end * sn_alp + yy_end * cs_alp;
+    YN[2] = uu_end * cs_alp - vv_end * sn_alp;
+    YN[3] = uu_end * sn_alp + vv_end * cs_alp;
+    return ir;
+}
+
+// ---------------------------------------------------------------------------
+// bia/find_parabola.f90:1-143 (diagnostic prints dropped).  Returns iterations.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double par_time(double r_min, double g_max, double theta)
+{
+    double sn, cs;
+    sincos(theta, &sn, &cs);
+    return (2.0 + cs) * sn / ((1.0 + cs) * (1.0 + cs)) * 4.0 * r_min / (3.0 * g_max);
+}
+
+static __device__ __noinline__ int parabola(double eps_th, double DT, const double YZ[4], double YN[4],
+                                     double *error_time)
+{
+    constexpr int NI = 99;
+    double theta_Newton[NI + 1], error_Newton[NI + 1];
+    const double r_ini = sqrt(YZ[0] * YZ[0] + YZ[1] * YZ[1]);
+    const double r_dot_g = YZ[0] * YZ[2] + YZ[1] * YZ[3];
+    const double r_crs_g = YZ[0] * YZ[3] - YZ[1] * YZ[2];
+    const double g_max = -2.0 * eps_th / r_crs_g;
+    const double r_min = r_crs_g / g_max;
+    const double x_ini = 2.0 * r_min - r_ini;
+    const double y_ini = f_sign(2.0 * r_min * sqrt(r_ini / r_min - 1.0), r_dot_g);
+    const double theta_ini = atan2(y_ini, x_ini);
+    const double time_ini = par_time(r_min, g_max, theta_ini);
+    const double time_end = time_ini + DT;
+    const double t_ = 3.0 * g_max / (4.0 * r_min) * time_end;
+    const double sq = sqrt(1.0 + t_ * t_);
+    const double theta_gss = 2.0 * atan(pow(sq + t_, 1.0 / 3) - pow(sq - t_, 1.0 / 3));
+    double theta = theta_gss, err_tm_min = 1e99, thetamin = theta;
+    int i_min = 1, i;
+    for (i = 1; i <= NI; i++) {
+        const double err_tm = par_time(r_min, g_max, theta) - time_end;
+        error_Newton[i] = err_tm;
+        const double ch = cos(theta * 0.5);
+        const double ch2 = ch * ch;
+        const double dtheta = -err_tm / (r_min / (g_max * (ch2 * ch2)));
+        if (fabs(err_tm) < err_tm_min) {
+            err_tm_min = fabs(err_tm);
+            thetamin = theta;
+            i_min = i;
+        }
+        theta = theta + dtheta;
+        theta_Newton[i] = theta;
+        if (dtheta == 0.0) break;
+        if (theta - dtheta == theta) break;
+        bool cyc = false;
+        for (int j = 1; j <= i - 1; j++)
+            if (error_Newton[i] == error_Newton[j]) { cyc = true; break; }
+        if (cyc) { theta = theta_Newton[i_min]; break; }
+    }
+    if (i == NI + 1) theta = thetamin;
+    const double theta_end = theta;
+    double sn_b, cs_b;
+    sincos(theta_end * 0.5, &sn_b, &cs_b);
+    const double r_end = r_min / (cs_b * cs_b);
+    const double g_end = g_max * cs_b;
+    double st, ct;
+    sincos(theta_end, &st, &ct);
+    const double x_end = r_end * ct, y_end = r_end * st;
+    const double u_end = -g_end * sn_b, v_end = g_end * cs_b;
+    const double s1 = x_ini * YZ[1] - y_ini * YZ[0];
+    const double c1 = x_ini * YZ[0] + y_ini * YZ[1];
+    const double tmp = 1.0 / sqrt(s1 * s1 + c1 * c1);
+    const double sn_g = s1 * tmp, cs_g = c1 * tmp;
+    YN[0] = x_end * cs_g - y_end * sn_g;
+    YN[1] = x_end * sn_g + y_end * cs_g;
+    YN[2] = u_end * cs_g - v_end * sn_g;
+    YN[3] = u_end * sn_g + v_end * cs_g;
+    *error_time = time_end - par_time(r_min, g_max, theta_end);
+    return (i > NI) ? NI : i;
+}
+
+// ---------------------------------------------------------------------------
+// bia/find_dXYUV_RKF.f90:1-170: per-pair RKF4(5) with step doubling on the planar
+// relative equation r'' = eps r/|r|^3 (moon_2D).  Returns ier; YN = step-doubled
+// solution, *error = max of (yln - yhn)/31.
+// ---------------------------------------------------------------------------
+struct Fehlberg {
+    static constexpr double AL2 = 1.0 / 4, AL3 = 3.0 / 8, AL4 = 12.0 / 13, AL5 = 1.0, AL6 = 1.0 / 2;
+    static constexpr double B21 = 1.0 / 4;
+    static constexpr double B31 = 3.0 / 32, B32 = 9.0 / 32;
+    static constexpr double B41 = 1932.0 / 2197, B42 = -7200.0 / 2197, B43 = 7296.0 / 2197;
+    static constexpr double B51 = 439.0 / 216, B52 = -8.0, B53 = 3680.0 / 513, B54 = -845.0 / 4104;
+    static constexpr double B61 = -8.0 / 27, B62 = 2.0, B63 = -3544.0 / 2565, B64 = 1859.0 / 4104,
+                            B65 = -11.0 / 40;
+    static constexpr double GA1 = 16.0 / 135, GA3 = 6656.0 / 12825, GA4 = 28561.0 / 56430,
+                            GA5 = -9.0 / 50, GA6 = 2.0 / 55;
+    static constexpr double DA1 = 1.0 / 360, DA3 = -128.0 / 4275, DA4 = -2197.0 / 75240,
+                            DA5 = 1.0 / 50, DA6 = 2.0 / 55;
+};
+
+__device__ __forceinline__ void moon2d(double eps_th, const double Y[4], double F[4])
+{
+    const double rsq = Y[0] * Y[0] + Y[1] * Y[1];
+    const double aaa = eps_th / (rsq * sqrt(rsq));
+    F[0] = Y[2];
+    F[1] = Y[3];
+    F[2] = Y[0] * aaa;
+    F[3] = Y[1] * aaa;
+}
+
+// bia/find_dXYUV_RKF.f90:150-157 fehl on 4 equations; er written when want_er.
+__device__ __forceinline__ void fehl4(double eps_th, double h, const double y0[4], double yn[4],
+                                      double er[4], bool want_er)
+{
+    using F = Fehlberg;
+    double k1[4], k2[4], k3[4], k4[4], k5[4], k6[4], w[4];
+    moon2d(eps_th, y0, k1);
+#pragma unroll
+    for (int i = 0; i < 4; i++) w[i] = y0[i] + h * F::B21 * k1[i];
+    moon2d(eps_th, w, k2);
+#pragma unroll
+    for (int i = 0; i < 4; i++) w[i] = y0[i] + h * (F::B31 * k1[i] + F::B32 * k2[i]);
+    moon2d(eps_th, w, k3);
+#pragma unroll
+    for (int i = 0; i < 4; i++) w[i] = y0[i] + h * (F::B41 * k1[i] + F::B42 * k2[i] + F::B43 * k3[i]);
+    moon2d(eps_th, w, k4);
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+        w[i] = y0[i] + h * (F::B51 * k1[i] + F::B52 * k2[i] + F::B53 * k3[i] + F::B54 * k4[i]);
+    moon2d(eps_th, w, k5);
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+        w[i] = y0[i] + h * (F::B61 * k1[i] + F::B62 * k2[i] + F::B63 * k3[i] + F::B64 * k4[i] +
+                            F::B65 * k5[i]);
+    moon2d(eps_th, w, k6);
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+        yn[i] = y0[i] + h * (F::GA1 * k1[i] + F::GA3 * k3[i] + F::GA4 * k4[i] + F::GA5 * k5[i] +
+                             F::GA6 * k6[i]);
+    if (want_er) {
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+            er[i] = h * (F::DA1 * k1[i] + F::DA3 * k3[i] + F::DA4 * k4[i] + F::DA5 * k5[i] +
+                         F::DA6 * k6[i]);
+    }
+}
+
+static __device__ __noinline__ int rkf_pair(double eps_th, double xe, double relerr, double abserr,
+                                     const double YZ[4], double YN[4], double *error, int *nacc)
+{
+    const int itemax = 100000;
+    const double epsmin = 1e-15;
+    double yh0[4], yl0[4], yln[4], yhn[4], er[4], ymid[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) { yh0[i] = YZ[i]; yl0[i] = YZ[i]; yhn[i] = YZ[i]; }
+    double f0[4];
+    moon2d(eps_th, yl0, f0);
+    double toldy = 1.7976931348623157e308;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        if (f0[i] != 0.0) {
+            const double tol = relerr * fabs(yl0[i]) + abserr;
+            toldy = fmin(toldy, fabs(tol / f0[i]));
+        }
+    }
+    double h = (toldy == 1.7976931348623157e308) ? epsmin * xe : fmin(xe / 100.0, pow(toldy, 0.2));
+    double x = 0.0;
+    int ier = 10000, n = 0;
+    *error = 0.0;
+    for (int iter = 1; iter <= itemax; iter++) {
+        fehl4(eps_th, h, yl0, yln, er, true);
+        double erret = 0.0;
+        bool bad = false;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const double et = relerr / 2.0 * (fabs(yl0[i]) + fabs(yln[i])) + abserr;
+            if (et == 0.0) bad = true;
+            erret = fmax(erret, fabs(er[i]) / et);
+        }
+        if (bad) { ier = 20000; break; }
+        if (erret > 1.0) {
+            h = (erret >= 59049.0) ? 0.1 * h : 0.9 * h / pow(erret, 0.2);
+            if (h <= epsmin) { ier = 30000; break; }
+        } else if (x + h < xe) {
+            fehl4(eps_th, h * 0.5, yh0, ymid, er, false);
+            fehl4(eps_th, h * 0.5, ymid, yhn, er, false);
+            x = x + h;
+#pragma unroll
+            for (int i = 0; i < 4; i++) { yl0[i] = yln[i]; yh0[i] = yhn[i]; }
+            n++;
+            h = (erret <= 1.889568e-4) ? 5.0 * h : 0.9 * h / pow(erret, 0.2);
+        } else {
+            h = xe - x;
+            fehl4(eps_th, h, yl0, yln, er, true);
+            fehl4(eps_th, h * 0.5, yh0, ymid, er, false);
+            fehl4(eps_th, h * 0.5, ymid, yhn, er, false);
+            double m = (yln[0] - yhn[0]) / 31.0;
+#pragma unroll
+            for (int i = 1; i < 4; i++) m = fmax(m, (yln[i] - yhn[i]) / 31.0);
+            *error = m;
+            n++;
+            ier = 0;
+            break;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) YN[i] = yhn[i];
+    *nacc = n;
+    return ier;
+}
+
+// ---------------------------------------------------------------------------
+// One pair: frame, classification, solve, half-displacement (bia/bia.f90:141-191).
+// Returns the half-displacement in h[6] = (dX, dY, dZ, dU, dV, dW)/2 terms.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pair_halfdisp(const PairParams &P, double eps_ij, const double r[3],
+                                              const double g[3], double h[6], PairCounters &cnt)
+{
+    double e_xi[3], e_eta[3], YZ[4], YN[4];
+    double error = 0.0;
+    const bool degenerate = frame_xi_eta(r, g, e_xi, e_eta, YZ);
+    if (degenerate || P.method == 0) {
+        int nacc = 0;
+        rkf_pair(eps_ij, P.dt, P.relerr, P.abserr, YZ, YN, &error, &nacc);
+        cnt.cls[degenerate ? kDegenerate : kRkf]++;
+        cnt.rkf_steps += nacc;
+    } else {
+        const double r_ij = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+        const double E_ij = g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + 2.0 * eps_ij / r_ij;
+        if (E_ij > 0.0) {
+            int bx = 0;
+            cnt.it_hyp += hyperbola(eps_ij, P.dt, P.itr, YZ, YN, &error, &bx);
+            cnt.bracket_exits += bx;
+            cnt.cls[kHyperbola]++;
+        } else if (E_ij < 0.0) {
+            cnt.it_ell += ellipse(eps_ij, P.dt, P.itr, YZ, YN, &error);
+            cnt.cls[kEllipse]++;
+        } else {
+            cnt.it_par += parabola(eps_ij, P.dt, YZ, YN, &error);
+            cnt.cls[kParabola]++;
+        }
+    }
+    if (fabs(error) > P.err) cnt.nonconverged++;
+    const double dr_xi = YN[0] - YZ[0], dr_eta = YN[1] - YZ[1];
+    const double dg_xi = YN[2] - YZ[2], dg_eta = YN[3] - YZ[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        h[k] = (dr_xi * e_xi[k] + dr_eta * e_eta[k] - g[k] * P.dt) * 0.5;
+        h[3 + k] = (dg_xi * e_xi[k] + dg_eta * e_eta[k]) * 0.5;
+    }
+    bool finite = true;
+#pragma unroll
+    for (int k = 0; k < 6; k++) finite = finite && isfinite(h[k]);
+    if (!finite) cnt.nonfinite++;
+}
+
+}  // namespace bia

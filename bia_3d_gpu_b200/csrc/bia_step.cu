@@ -1,0 +1,561 @@
+// bia_step.cu -- the BIA pair step on B200: tile kernel, reduction, context and API.
+//
+// Work decomposition.  The pairs i<j form the upper triangle of an n x n matrix.  It
+// is cut into 32 x 32 warp-blocks (bi <= bj, 32-particle row and column blocks); one
+// warp owns one warp-block.  Lane l keeps its row particle i = 32*bi + l and its
+// column particle j = 32*bj + l in registers.  At rotation step k lane l pairs its
+// row with column slot (l + k) mod 32, fetched from that lane with a shuffle, so
+// every lane solves a different pair and the column slot's accumulator can be
+// handed back by a second shuffle from lane (l - k) mod 32.  Off-diagonal blocks take
+// 32 rotation steps (1024 pairs), diagonal blocks 16 (k = 1..15 on all lanes, k = 16
+// on lanes 0..15: the 496 pairs of the block once each; orientation does not matter
+// because the half-displacement is exactly antisymmetric under i <-> j).
+//
+// Reduction.  Each warp-block leaves 32 row sums and 32 column sums of the six
+// half-displacement components.  Deterministic mode writes them to a partial buffer
+// part[m][c][p] in which every (m, p) slot is written exactly once per step (row sums
+// of block (bi, bj) at m = bj, column sums at m = bi, the diagonal block's combined
+// sums at m = bi), and a second kernel adds the nb partials of each particle in a fixed
+// order, adds the drift u*dt and updates the state: the result is bitwise
+// reproducible.  Atomic mode adds the sums straight into an accumulator with FP64
+// atomics (no partial buffer; summation order varies between runs).
+//
+// Layout in HBM: state is SoA (x, y, z, u, v, w, optional q), FP64, n entries each;
+// partials are [nb][6][nb*32] FP64 (1.5 n^2 bytes); accumulators [6][nb*32].
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "bia_internal.cuh"
+#include "bia_pair.cuh"
+
+namespace bia {
+
+constexpr int kWarpsPerBlock = 8;
+constexpr int kThreads = kWarpsPerBlock * 32;
+
+struct StepArgs {
+    const double *x, *y, *z, *u, *v, *w, *q;
+    double *part;   // deterministic partials, or atomic accumulators
+    unsigned long long *stats;
+    long long nwb;  // number of warp-blocks = nb*(nb+1)/2
+    int n, nb, npad;
+    double eps_th;
+    PairParams P;
+};
+
+__device__ __forceinline__ void warp_block_coords(long long t, int &bi, int &bj)
+{
+    // t = bj*(bj+1)/2 + bi with 0 <= bi <= bj
+    long long c = (long long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while (c * (c + 1) / 2 > t) c--;
+    while ((c + 1) * (c + 2) / 2 <= t) c++;
+    bj = (int)c;
+    bi = (int)(t - c * (c + 1) / 2);
+}
+
+__device__ __forceinline__ void load_particle(const StepArgs &A, int p, double s[7])
+{
+    if (p < A.n) {
+        s[0] = A.x[p]; s[1] = A.y[p]; s[2] = A.z[p];
+        s[3] = A.u[p]; s[4] = A.v[p]; s[5] = A.w[p];
+        s[6] = A.q ? A.q[p] : 1.0;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 7; k++) s[k] = 0.0;
+    }
+}
+
+__device__ __forceinline__ void flush_counters(const PairCounters &c, unsigned long long *stats, int lane)
+{
+    const unsigned full = 0xffffffffu;
+    int vals[kNumStats] = {c.cls[0], c.cls[1], c.cls[2], c.cls[3], c.cls[4], c.it_hyp, c.it_ell,
+                           c.it_par, c.rkf_steps, c.nonconverged, c.bracket_exits, c.nonfinite};
+#pragma unroll
+    for (int k = 0; k < kNumStats; k++) {
+        int s = __reduce_add_sync(full, vals[k]);
+        if (lane == 0 && s != 0) atomicAdd(&stats[k], (unsigned long long)s);
+    }
+}
+
+template <bool kDeterministic>
+__global__ void __launch_bounds__(kThreads) bia_pair_tiles_kernel(const StepArgs A)
+{
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const long long t = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    if (t >= A.nwb) return;  // warp-uniform
+    int bi, bj;
+    warp_block_coords(t, bi, bj);
+    const int i = bi * 32 + lane;
+    const int jown = bj * 32 + lane;
+    double si[7], sj[7];
+    load_particle(A, i, si);
+    load_particle(A, jown, sj);
+
+    double racc[6] = {0, 0, 0, 0, 0, 0}, cacc[6] = {0, 0, 0, 0, 0, 0};
+    PairCounters cnt;
+    counters_zero(cnt);
+    const bool diag = (bi == bj);
+    const int k0 = diag ? 1 : 0;
+    const int k1 = diag ? 16 : 31;
+    for (int k = k0; k <= k1; k++) {
+        const int src = (lane + k) & 31;
+        double sc[7];
+#pragma unroll
+        for (int c = 0; c < 7; c++) sc[c] = __shfl_sync(full, sj[c], src);
+        const int j = bj * 32 + src;
+        const bool active = (!diag || k < 16 || lane < 16) && i < A.n && j < A.n;
+        double h[6] = {0, 0, 0, 0, 0, 0};
+        if (active) {
+            const double r[3] = {si[0] - sc[0], si[1] - sc[1], si[2] - sc[2]};
+            const double g[3] = {si[3] - sc[3], si[4] - sc[4], si[5] - sc[5]};
+            const double eps_ij = A.q ? A.eps_th * si[6] * sc[6] : A.eps_th;
+            pair_halfdisp(A.P, eps_ij, r, g, h, cnt);
+        }
+        const int back = (lane - k) & 31;
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            racc[c] += h[c];
+            cacc[c] += __shfl_sync(full, h[c], back);
+        }
+    }
+    flush_counters(cnt, A.stats, lane);
+
+    const size_t plane = (size_t)A.npad;
+    if (kDeterministic) {
+        if (diag) {
+            double *dst = A.part + (size_t)bi * 6 * plane;
+#pragma unroll
+            for (int c = 0; c < 6; c++) dst[c * plane + i] = racc[c] - cacc[c];
+        } else {
+            double *drow = A.part + (size_t)bj * 6 * plane;
+            double *dcol = A.part + (size_t)bi * 6 * plane;
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                drow[c * plane + i] = racc[c];
+                dcol[c * plane + jown] = -cacc[c];
+            }
+        }
+    } else {
+        if (diag) {
+#pragma unroll
+            for (int c = 0; c < 6; c++)
+                if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c] - cacc[c]);
+        } else {
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c]);
+                if (jown < A.n) atomicAdd(&A.part[c * plane + jown], -cacc[c]);
+            }
+        }
+    }
+}
+
+struct UpdateArgs {
+    double *x, *y, *z, *u, *v, *w;
+    const double *part;
+    double *disp;  // optional [6][n]
+    int n, nb, npad, nparts;  // nparts = nb (deterministic) or 1 (atomic)
+    double dt;
+};
+
+// Sum of the partials in fixed order, drift and state update (bia/bia.f90:194-204).
+__global__ void __launch_bounds__(256) bia_reduce_update_kernel(const UpdateArgs A)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= A.n) return;
+    const size_t plane = (size_t)A.npad;
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int m = 0; m < A.nparts; m++) {
+        const double *src = A.part + (size_t)m * 6 * plane + p;
+#pragma unroll
+        for (int c = 0; c < 6; c++) s[c] += src[c * plane];
+    }
+    const double u = A.u[p], v = A.v[p], w = A.w[p];
+    const double d[6] = {s[0] + u * A.dt, s[1] + v * A.dt, s[2] + w * A.dt, s[3], s[4], s[5]};
+    A.x[p] = A.x[p] + d[0];
+    A.y[p] = A.y[p] + d[1];
+    A.z[p] = A.z[p] + d[2];
+    A.u[p] = u + d[3];
+    A.v[p] = v + d[4];
+    A.w[p] = w + d[5];
+    if (A.disp) {
+#pragma unroll
+        for (int c = 0; c < 6; c++) A.disp[(size_t)c * A.n + p] = d[c];
+    }
+}
+
+// ----------------------------------------------------------------------------------
+static thread_local int g_last_error = BIA_OK;
+
+int set_last_error(int status)
+{
+    g_last_error = status;
+    return status;
+}
+
+int cuda_status(cudaError_t e)
+{
+    if (e == cudaSuccess) return BIA_OK;
+    if (e == cudaErrorMemoryAllocation) return BIA_ERR_OUT_OF_MEMORY;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return BIA_ERR_NO_DEVICE;
+    return BIA_ERR_CUDA;
+}
+
+static int num_blocks32(int n) { return (n + 31) / 32; }
+
+int ensure_step_buffers(bia_context *ctx, const bia_config *cfg, int n)
+{
+    const int nb = num_blocks32(n);
+    const size_t npad = (size_t)nb * 32;
+    cudaError_t e;
+    if (cfg->deterministic) {
+        e = ctx->part.reserve((size_t)nb * 6 * npad * sizeof(double));
+    } else {
+        e = ctx->acc.reserve(6 * npad * sizeof(double));
+    }
+    if (e != cudaSuccess) return cuda_status(e);
+    e = ctx->stats.reserve(kNumStats * sizeof(unsigned long long));
+    return cuda_status(e);
+}
+
+static int validate(const bia_config *cfg, int n, const void *x, const void *y, const void *z,
+                    const void *u, const void *v, const void *w)
+{
+    if (!cfg || n < 1 || !x || !y || !z || !u || !v || !w) return BIA_ERR_INVALID_ARGUMENT;
+    if (cfg->method != BIA_METHOD_ALG && cfg->method != BIA_METHOD_RKF) return BIA_ERR_INVALID_ARGUMENT;
+    if (cfg->itr < 1 || cfg->itr > 62) return BIA_ERR_INVALID_ARGUMENT;
+    // 32-bit particle indices and a warp-block count that fits the grid
+    if (n > (1 << 30)) return BIA_ERR_INVALID_ARGUMENT;
+    return BIA_OK;
+}
+
+static void record_event(bia_context *ctx)
+{
+    if (!ctx->timing) return;
+    if (ctx->ev_used == ctx->ev_cap) {
+        int cap = ctx->ev_cap ? ctx->ev_cap * 2 : 64;
+        cudaEvent_t *ev = (cudaEvent_t *)realloc(ctx->ev, sizeof(cudaEvent_t) * cap);
+        if (!ev) return;
+        for (int k = ctx->ev_cap; k < cap; k++) cudaEventCreate(&ev[k]);
+        ctx->ev = ev;
+        ctx->ev_cap = cap;
+    }
+    cudaEventRecord(ctx->ev[ctx->ev_used++], ctx->stream);
+}
+
+int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y, double *z,
+                 double *u, double *v, double *w, const double *q, double *disp)
+{
+    const int nb = num_blocks32(n);
+    StepArgs A;
+    A.x = x; A.y = y; A.z = z; A.u = u; A.v = v; A.w = w; A.q = q;
+    A.stats = (unsigned long long *)ctx->stats.ptr;
+    A.n = n;
+    A.nb = nb;
+    A.npad = nb * 32;
+    A.nwb = (long long)nb * (nb + 1) / 2;
+    A.eps_th = cfg->eps_th;
+    A.P.dt = cfg->dt;
+    A.P.err = cfg->err;
+    A.P.relerr = cfg->rkf_relerr;
+    A.P.abserr = cfg->rkf_abserr;
+    A.P.itr = cfg->itr;
+    A.P.method = cfg->method;
+    const long long grid = (A.nwb + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    UpdateArgs U;
+    U.x = x; U.y = y; U.z = z; U.u = u; U.v = v; U.w = w;
+    U.disp = disp;
+    U.n = n;
+    U.nb = nb;
+    U.npad = nb * 32;
+    U.dt = cfg->dt;
+    if (cfg->deterministic) {
+        A.part = (double *)ctx->part.ptr;
+        U.part = A.part;
+        U.nparts = nb;
+        record_event(ctx);
+        bia_pair_tiles_kernel<true><<<(unsigned)grid, kThreads, 0, ctx->stream>>>(A);
+        record_event(ctx);
+    } else {
+        A.part = (double *)ctx->acc.ptr;
+        U.part = A.part;
+        U.nparts = 1;
+        cudaMemsetAsync(A.part, 0, 6 * (size_t)A.npad * sizeof(double), ctx->stream);
+        record_event(ctx);
+        bia_pair_tiles_kernel<false><<<(unsigned)grid, kThreads, 0, ctx->stream>>>(A);
+        record_event(ctx);
+    }
+    bia_reduce_update_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(U);
+    return cuda_status(cudaGetLastError());
+}
+
+static void copy_stats(const unsigned long long *h, bia_stats *s)
+{
+    s->hyperbola = (long long)h[0];
+    s->parabola = (long long)h[1];
+    s->ellipse = (long long)h[2];
+    s->degenerate = (long long)h[3];
+    s->rkf = (long long)h[4];
+    s->iter_hyperbola = (long long)h[5];
+    s->iter_ellipse = (long long)h[6];
+    s->iter_parabola = (long long)h[7];
+    s->iterations = s->iter_hyperbola + s->iter_ellipse + s->iter_parabola;
+    s->rkf_steps = (long long)h[8];
+    s->nonconverged = (long long)h[9];
+    s->bracket_exits = (long long)h[10];
+    s->nonfinite = (long long)h[11];
+}
+
+static int fetch_stats(bia_context *ctx, bia_stats *stats)
+{
+    cudaError_t e = cudaMemcpyAsync(ctx->h_stats, ctx->stats.ptr, kNumStats * sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_status(e);
+    copy_stats(ctx->h_stats, stats);
+    return stats->nonfinite ? BIA_ERR_NONFINITE : BIA_OK;
+}
+
+}  // namespace bia
+
+using namespace bia;
+
+extern "C" {
+
+void bia_config_default(bia_config *cfg)
+{
+    if (!cfg) return;
+    cfg->method = BIA_METHOD_ALG;
+    cfg->itr = 18;
+    cfg->eps_th = -6e-7;
+    cfg->dt = 1.0;
+    cfg->err = 1e-12;
+    cfg->rkf_relerr = 0.0;
+    cfg->rkf_abserr = 1e-16;
+    cfg->deterministic = 1;
+}
+
+const char *bia_status_string(int status)
+{
+    switch (status) {
+    case BIA_OK: return "ok";
+    case BIA_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case BIA_ERR_NONFINITE: return "a pair produced a non-finite displacement";
+    case BIA_ERR_NOT_CONVERGED: return "solver did not converge";
+    case BIA_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
+    case BIA_ERR_CUDA: return "CUDA runtime error";
+    case BIA_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case BIA_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+    }
+}
+
+int bia_last_error(void) { return g_last_error; }
+
+int bia_context_create(bia_context **out, int device, void *stream)
+{
+    if (!out) return BIA_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) return BIA_ERR_NO_DEVICE;
+    if (device < 0 || device >= count) return BIA_ERR_INVALID_ARGUMENT;
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_status(e);
+    bia_context *ctx = new bia_context();
+    ctx->device = device;
+    ctx->stream = (cudaStream_t)stream;
+    e = cudaMallocHost((void **)&ctx->h_stats, kNumStats * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_inv, 64 * sizeof(double));
+    if (e == cudaSuccess) e = ctx->stats.reserve(kNumStats * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(ctx->stats.ptr, 0, kNumStats * sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        bia_context_destroy(ctx);
+        return cuda_status(e);
+    }
+    *out = ctx;
+    return BIA_OK;
+}
+
+int bia_context_destroy(bia_context *ctx)
+{
+    if (!ctx) return BIA_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    else cudaDeviceSynchronize();
+    if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+    if (ctx->graph) cudaGraphDestroy(ctx->graph);
+    for (int k = 0; k < ctx->ev_cap; k++) cudaEventDestroy(ctx->ev[k]);
+    free(ctx->ev);
+    ctx->part.release();
+    ctx->acc.release();
+    ctx->stats.release();
+    ctx->state.release();
+    ctx->inv.release();
+    if (ctx->h_stats) cudaFreeHost(ctx->h_stats);
+    if (ctx->h_inv) cudaFreeHost(ctx->h_inv);
+    delete ctx;
+    return BIA_OK;
+}
+
+int bia_context_set_stream(bia_context *ctx, void *stream)
+{
+    if (!ctx) return BIA_ERR_INVALID_ARGUMENT;
+    ctx->stream = (cudaStream_t)stream;
+    return BIA_OK;
+}
+
+int bia_context_set_timing(bia_context *ctx, int on)
+{
+    if (!ctx) return BIA_ERR_INVALID_ARGUMENT;
+    ctx->timing = on != 0;
+    ctx->ev_used = 0;
+    return BIA_OK;
+}
+
+int bia_context_stats(bia_context *ctx, bia_stats *stats, int reset)
+{
+    if (!ctx || !stats) return BIA_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    int st = fetch_stats(ctx, stats);
+    if (st != BIA_OK && st != BIA_ERR_NONFINITE) return st;
+    if (reset) {
+        cudaError_t e = cudaMemsetAsync(ctx->stats.ptr, 0, kNumStats * sizeof(unsigned long long), ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    return st;
+}
+
+int bia_context_kernel_ms(bia_context *ctx, double *ms, long long *launches)
+{
+    if (!ctx || !ms) return BIA_ERR_INVALID_ARGUMENT;
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_status(e);
+    double total = 0.0;
+    long long cnt = 0;
+    for (int k = 0; k + 1 < ctx->ev_used; k += 2) {
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, ctx->ev[k], ctx->ev[k + 1]) == cudaSuccess) {
+            total += t;
+            cnt++;
+        }
+    }
+    *ms = total;
+    if (launches) *launches = cnt;
+    ctx->ev_used = 0;
+    return BIA_OK;
+}
+
+int bia_step(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y, double *z,
+             double *u, double *v, double *w, const double *q, double *disp, bia_stats *stats)
+{
+    if (!ctx) return BIA_ERR_INVALID_ARGUMENT;
+    int st = validate(cfg, n, x, y, z, u, v, w);
+    if (st != BIA_OK) return st;
+    cudaSetDevice(ctx->device);
+    st = ensure_step_buffers(ctx, cfg, n);
+    if (st != BIA_OK) return st;
+    if (stats) {
+        cudaError_t e = cudaMemsetAsync(ctx->stats.ptr, 0, kNumStats * sizeof(unsigned long long), ctx->stream);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    st = enqueue_step(ctx, cfg, n, x, y, z, u, v, w, q, disp);
+    if (st != BIA_OK) return st;
+    if (stats) return fetch_stats(ctx, stats);
+    return BIA_OK;
+}
+
+int bia_run(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y, double *z,
+            double *u, double *v, double *w, const double *q, int nsteps, int use_graph,
+            bia_stats *stats)
+{
+    if (!ctx || nsteps < 0) return BIA_ERR_INVALID_ARGUMENT;
+    int st = validate(cfg, n, x, y, z, u, v, w);
+    if (st != BIA_OK) return st;
+    cudaSetDevice(ctx->device);
+    st = ensure_step_buffers(ctx, cfg, n);
+    if (st != BIA_OK) return st;
+    cudaError_t e = cudaSuccess;
+    if (stats) {
+        e = cudaMemsetAsync(ctx->stats.ptr, 0, kNumStats * sizeof(unsigned long long), ctx->stream);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    // a capturing stream needs a non-default stream; timing events are per launch, so
+    // graph replay is only used with timing off
+    if (use_graph && ctx->stream && !ctx->timing && nsteps > 0) {
+        GraphKey key;
+        key.n = n; key.nsteps = nsteps; key.method = cfg->method; key.itr = cfg->itr;
+        key.deterministic = cfg->deterministic; key.eps = cfg->eps_th; key.dt = cfg->dt;
+        key.err = cfg->err; key.relerr = cfg->rkf_relerr; key.abserr = cfg->rkf_abserr;
+        const void *p[7] = {x, y, z, u, v, w, q};
+        for (int k = 0; k < 7; k++) key.ptrs[k] = p[k];
+        if (!ctx->graph_exec || !(key == ctx->graph_key)) {
+            if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+            if (ctx->graph) cudaGraphDestroy(ctx->graph);
+            ctx->graph_exec = nullptr;
+            ctx->graph = nullptr;
+            e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return cuda_status(e);
+            int est = BIA_OK;
+            for (int s = 0; s < nsteps && est == BIA_OK; s++)
+                est = enqueue_step(ctx, cfg, n, x, y, z, u, v, w, q, nullptr);
+            e = cudaStreamEndCapture(ctx->stream, &ctx->graph);
+            if (est != BIA_OK) return est;
+            if (e != cudaSuccess) return cuda_status(e);
+            e = cudaGraphInstantiate(&ctx->graph_exec, ctx->graph, 0);
+            if (e != cudaSuccess) return cuda_status(e);
+            ctx->graph_key = key;
+        }
+        e = cudaGraphLaunch(ctx->graph_exec, ctx->stream);
+        if (e != cudaSuccess) return cuda_status(e);
+    } else {
+        for (int s = 0; s < nsteps; s++) {
+            st = enqueue_step(ctx, cfg, n, x, y, z, u, v, w, q, nullptr);
+            if (st != BIA_OK) return st;
+        }
+    }
+    if (stats) return fetch_stats(ctx, stats);
+    return cuda_status(cudaGetLastError());
+}
+
+int bia_run_host(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y, double *z,
+                 double *u, double *v, double *w, const double *q, int nsteps, bia_stats *stats)
+{
+    if (!ctx) return BIA_ERR_INVALID_ARGUMENT;
+    int st = validate(cfg, n, x, y, z, u, v, w);
+    if (st != BIA_OK) return st;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = ctx->state.reserve((size_t)7 * n * sizeof(double));
+    if (e != cudaSuccess) return cuda_status(e);
+    double *d = (double *)ctx->state.ptr;
+    double *host[6] = {x, y, z, u, v, w};
+    for (int k = 0; k < 6; k++) {
+        e = cudaMemcpyAsync(d + (size_t)k * n, host[k], n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    const double *dq = nullptr;
+    if (q) {
+        e = cudaMemcpyAsync(d + (size_t)6 * n, q, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) return cuda_status(e);
+        dq = d + (size_t)6 * n;
+    }
+    st = bia_run(ctx, cfg, n, d, d + n, d + 2 * (size_t)n, d + 3 * (size_t)n, d + 4 * (size_t)n,
+                 d + 5 * (size_t)n, dq, nsteps, 1, stats);
+    if (st != BIA_OK && st != BIA_ERR_NONFINITE) return st;
+    int st2 = st;
+    for (int k = 0; k < 6; k++) {
+        e = cudaMemcpyAsync(host[k], d + (size_t)k * n, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_status(e);
+    return st2;
+}
+
+}  // extern "C"

@@ -1,0 +1,144 @@
+/*
+ * bia_capi.h -- C ABI of libbia_b200.so, the B200 (sm_100a) BIA pair-step library.
+ *
+ * Two groups of entry points:
+ *
+ *  1. Drop-in replacements for the reference's Fortran-callable symbols.  Same
+ *     names, same gfortran calling convention (scalars by value through %VAL,
+ *     arrays as host pointers), same accumulate/overwrite semantics, void return.
+ *     Status of the last call on this host thread: bia_last_error().
+ *
+ *  2. A status-returning API with device-resident state owned by the caller or
+ *     by a bia_context (one per host thread, explicit CUDA stream).
+ *
+ * All arrays are FP64.  State arrays are structure-of-arrays: x, y, z, u, v, w,
+ * each of length n.  No function takes or returns a torch type.
+ */
+#ifndef BIA_CAPI_H
+#define BIA_CAPI_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------- */
+enum bia_status {
+    BIA_OK = 0,
+    BIA_ERR_INVALID_ARGUMENT = 1, /* bad n, NULL pointer, unknown method, ... */
+    BIA_ERR_NONFINITE = 2,        /* a pair produced a non-finite displacement */
+    BIA_ERR_NOT_CONVERGED = 3,    /* reserved: RKF step-size underflow / iteration limit */
+    BIA_ERR_DEVICE_TIMEOUT = 4,   /* a bounded device-side wait gave up */
+    BIA_ERR_CUDA = 5,             /* a CUDA runtime call failed */
+    BIA_ERR_OUT_OF_MEMORY = 6,
+    BIA_ERR_NO_DEVICE = 7
+};
+
+/* pair solver: the reference's METHOD argument (bia/bia.f90:134-139) */
+enum bia_method { BIA_METHOD_RKF = 0, BIA_METHOD_ALG = 1 };
+
+typedef struct bia_config {
+    int method;        /* BIA_METHOD_ALG (Kepler/Barker solve) or BIA_METHOD_RKF */
+    int itr;           /* Newton iteration cap, ITR = 18 (bia/bia.f90:52) */
+    double eps_th;     /* coupling of r'' = eps r/|r|^3 (bia/bia.f90:37); with charges q
+                          the pair coupling is eps_th * q_i * q_j */
+    double dt;         /* step length, time_end (bia/bia.f90:35) */
+    double err;        /* residual above which a pair counts as not converged, ERR = 1e-12 */
+    double rkf_relerr; /* per-pair RKF tolerances (bia/find_dXYUV_RKF.f90:4): 0 ... */
+    double rkf_abserr; /* ... and 1e-16 */
+    int deterministic; /* 1: fixed-order two-pass reduction (bitwise reproducible);
+                          0: FP64 atomics (no scratch, order varies run to run) */
+} bia_config;
+
+/* fills cfg with the reference's defaults: ALG, ITR 18, eps_th -6e-7, dt 1,
+   ERR 1e-12, RKF 0/1e-16, deterministic reduction */
+void bia_config_default(bia_config *cfg);
+
+/* per-step counters (pairs per branch of bia/bia.f90:158-166 and solver work) */
+typedef struct bia_stats {
+    long long hyperbola, parabola, ellipse, degenerate, rkf;
+    long long iterations;    /* Newton iterations, summed over ALG pairs */
+    long long iter_hyperbola, iter_ellipse, iter_parabola; /* the same split by branch */
+    long long rkf_steps;     /* accepted RKF steps, summed over RKF pairs */
+    long long nonconverged;  /* |residual| > cfg.err (bia/bia.f90:151,167) */
+    long long bracket_exits; /* hyperbola iterate left (-theta_0, theta_0) */
+    long long nonfinite;     /* pairs whose displacement was not finite */
+} bia_stats;
+
+typedef struct bia_context bia_context;
+
+/* Create a context on `device` that launches on `stream` (a cudaStream_t, NULL =
+   the legacy default stream).  The context owns scratch buffers, grown on demand. */
+int bia_context_create(bia_context **ctx, int device, void *stream);
+int bia_context_destroy(bia_context *ctx);
+int bia_context_set_stream(bia_context *ctx, void *stream);
+/* kernel timing: when on, the pair kernel's launches are bracketed by CUDA events on
+   the context's stream; bia_context_kernel_ms returns their summed duration and count
+   since the last reset (synchronises the stream). */
+int bia_context_set_timing(bia_context *ctx, int on);
+int bia_context_kernel_ms(bia_context *ctx, double *ms, long long *launches);
+
+/* Counters of every step enqueued on the context since the last reset (steps called
+   with stats == NULL add to them; a call with stats != NULL reports and clears its own
+   steps).  Synchronises the context's stream; reset != 0 clears them afterwards. */
+int bia_context_stats(bia_context *ctx, bia_stats *stats, int reset);
+
+/* One BIA step on device-resident SoA state (bia/bia.f90:126-204 as one launch
+   sequence): all pairs i<j, per-particle reduction, drift, and the update
+   X += dX, U += dU in place.  q: optional device array of n charges (NULL: eps_th
+   for every pair).  disp: optional device array [6][n] receiving dX..dW (drift
+   included, as in the .BIA record, bia/bia.f90:206).  stats: optional, host. */
+int bia_step(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y, double *z,
+             double *u, double *v, double *w, const double *q, double *disp, bia_stats *stats);
+
+/* nsteps BIA steps.  With use_graph != 0 the step sequence is captured once in a
+   CUDA graph and replayed.  stats (optional) are summed over the steps. */
+int bia_run(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y, double *z,
+            double *u, double *v, double *w, const double *q, int nsteps, int use_graph,
+            bia_stats *stats);
+
+/* Host-buffer form of bia_run: copies the host state (6 arrays of n) and charges to
+   the device, runs nsteps steps, copies the state back into the same host arrays. */
+int bia_run_host(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y,
+                 double *z, double *u, double *v, double *w, const double *q, int nsteps,
+                 bia_stats *stats);
+
+/* Invariants of device SoA state (bia/invariance.cu:50-110 semantics, FP64):
+   out[11] = {KE, PE, Lx, Ly, Lz, Ua, Va, Wa, Xa, Ya, Za} on the host.
+   KE = sum |v|^2, PE = eps_th * sum_{i<j} (q_i q_j) / r_ij. */
+int bia_invariance(bia_context *ctx, int n, double eps_th, const double *x, const double *y,
+                   const double *z, const double *u, const double *v, const double *w,
+                   const double *q, double out[11]);
+
+/* Measured FP64 FMA throughput of `device` in TFLOP/s (FMA = 2 flops): the roofline
+   denominator of the FP64-bound pair kernel. */
+int bia_measure_fp64_peak(int device, double *tflops);
+
+const char *bia_status_string(int status);
+/* status of the last drop-in call (find_dxyuv_kernel_, invariance_gpu_, rkf_c_) on this
+   host thread */
+int bia_last_error(void);
+
+/* ---- drop-in replacements of the reference's symbols ----------------------- */
+
+/* Replaces find_dxyuv_kernel_ (bia/find_dXYUV_kernel.cu:526-561), called from
+   bia/bia.f90:135,138.  For the fixed particle I (1-based) and every j > I it solves
+   the pair given by the host AoS array RXYZUVW[6N] of x_i-x_j, ..., w_i-w_j, writes
+   the half-displacements into the host array dXYZUVW[6j..6j+5] (entries j <= I are
+   set to 0), and accumulates them into the host arrays: dX[I] += h_j, dX[j] -= h_j
+   (likewise dY..dW).  No drift is added (the caller does, bia/bia.f90:194-196).
+   METHOD: 0 = RKF, 1 = ALG. */
+void find_dxyuv_kernel_(const int METHOD, const int N, const int I, const double EPS,
+                        const double DT, const int ITR, double *dX, double *dY, double *dZ,
+                        double *dU, double *dV, double *dW, double *RXYZUVW, double *dXYZUVW);
+
+/* Replaces invariance_gpu_ (bia/invariance.cu:50-110), called from bia/bia.f90:67-68:
+   host SoA arrays in, the 11 invariants out through scalar pointers. */
+void invariance_gpu_(const int N, const double eps_th, double *X, double *Y, double *Z,
+                     double *U, double *V, double *W, double *KE, double *PE, double *Lx,
+                     double *Ly, double *Lz, double *Ua, double *Va, double *Wa, double *Xa,
+                     double *Ya, double *Za);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BIA_CAPI_H */

@@ -1,0 +1,224 @@
+"""GPU parity: the CUDA pair step against the CPU oracle, through the C-ABI.
+
+Tolerances: global relative error ||X_gpu - X_oracle|| / ||X_oracle||
+<= 1e-12 for positions and velocities, and the per-particle maximum
+max|X_gpu - X_oracle| / max|X_oracle| <= 1e-12 at the workloads' step lengths.  At the
+reference fixture's dt = 1 the per-particle maximum is 1e-11 (see test_oracle.py: one
+pericentre pair is ill-conditioned in the reference algorithm itself).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from bia_3d_gpu_b200 import (BIASolver, METHOD_ALG, METHOD_RKF, default_config, find_dxyuv_kernel,
+                             initial, invariance_gpu)
+from conftest import max_rel_err, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_run(cuda, state, eps, dt, nsteps, q=None, method=METHOD_ALG, deterministic=1,
+            graph=False, disp=False):
+    t = cuda.tensor(state, dtype=cuda.float64, device="cuda").contiguous()
+    qt = cuda.tensor(q, dtype=cuda.float64, device="cuda") if q is not None else None
+    cfg = default_config(eps_th=eps, dt=dt, method=method, deterministic=deterministic)
+    d = cuda.zeros_like(t) if disp else None
+    with BIASolver() as s:
+        if graph:
+            stats = s.run(t, cfg, nsteps, q=qt, graph=True)
+        else:
+            stats = None
+            for _ in range(nsteps):
+                stats = s.step(t, cfg, q=qt, disp=d)
+        s.stream.synchronize()
+    out = t.cpu().numpy()
+    return (out, stats, d.cpu().numpy()) if disp else (out, stats)
+
+
+def oracle_run(state, eps, dt, nsteps, q=None, method=1):
+    s = state
+    st = None
+    for _ in range(nsteps):
+        s, _, st = oracle.bia_step(s, eps, dt, method=method, q=q)
+    return s, st
+
+
+def assert_parity(gpu, ref, tol_max=1e-12):
+    assert rel_err(gpu[:3], ref[:3]) <= 1e-12
+    assert rel_err(gpu[3:], ref[3:]) <= 1e-12
+    assert max_rel_err(gpu[:3], ref[:3]) <= tol_max
+    assert max_rel_err(gpu[3:], ref[3:]) <= tol_max
+
+
+def test_gravity_ball_matches_oracle(cuda):
+    s, eps = initial.gravity_ball(300, seed=21)
+    g, st = gpu_run(cuda, s, eps, 1e-4, 5)
+    r, rst = oracle_run(s, eps, 1e-4, 5)
+    assert_parity(g, r)
+    assert st["hyperbola"] + st["ellipse"] + st["parabola"] == 300 * 299 // 2
+    assert st["hyperbola"] == rst["hyperbola"] and st["ellipse"] == rst["ellipse"]
+    assert st["nonfinite"] == 0
+
+
+def test_coulomb_mixed_classes_match_oracle(cuda):
+    """Repulsive pairs on hyperbolae, attractive pairs mostly on ellipses."""
+    s, eps, q = initial.coulomb_cube(400, seed=22, dmin=1e-3)
+    g, st = gpu_run(cuda, s, eps, 1e-5, 3, q=q)
+    r, rst = oracle_run(s, eps, 1e-5, 3, q=q)
+    assert st["ellipse"] > 1000 and st["hyperbola"] > 1000
+    assert st["ellipse"] == rst["ellipse"]
+    assert_parity(g, r)
+
+
+def test_plummer_matches_oracle(cuda):
+    s, eps = initial.plummer(384, seed=23)
+    g, _ = gpu_run(cuda, s, eps, 1e-4, 4)
+    r, _ = oracle_run(s, eps, 1e-4, 4)
+    assert_parity(g, r)
+
+
+def test_rkf_mode_matches_oracle(cuda):
+    s, eps, q = initial.coulomb_cube(96, seed=24, dmin=1e-2)
+    g, st = gpu_run(cuda, s, eps, 1e-5, 2, q=q, method=METHOD_RKF)
+    r, rst = oracle_run(s, eps, 1e-5, 2, q=q, method=0)
+    assert st["rkf"] == 96 * 95 // 2 and st["rkf_steps"] == rst["rkf_steps"]
+    assert_parity(g, r)
+
+
+def test_reference_fixture_through_bia_step(cuda, golden, golden_ic):
+    """The .BIA record of the reference (dt = 1, eps_th = -6e-7) via the whole-step API."""
+    g, st, disp = gpu_run(cuda, golden_ic, -6e-7, 1.0, 1, disp=True)
+    ref_disp = golden["bia_disp_aos"].reshape(-1, 6).T
+    ref = golden_ic + ref_disp
+    assert_parity(g, ref, tol_max=1e-11)
+    assert np.abs(disp[3:] - ref_disp[3:]).max() <= 1e-14
+    o, _, _ = oracle.bia_step(golden_ic, -6e-7, 1.0)
+    assert_parity(g, o, tol_max=1e-11)
+
+
+def test_reference_fixture_through_dropin_row_entry(cuda, golden, golden_ic):
+    """bia/bia.f90:128-204 GPU branch restated over the drop-in find_dxyuv_kernel_."""
+    s = golden_ic
+    n = s.shape[1]
+    X, Y, Z, U, V, W = [np.ascontiguousarray(s[k]) for k in range(6)]
+    acc = [np.zeros(n) for _ in range(6)]
+    rel = np.zeros(6 * n)
+    out = np.zeros(6 * n)
+    for I in range(1, n + 1):
+        i = I - 1
+        for k, a in enumerate((X, Y, Z, U, V, W)):
+            rel[k::6] = a[i] - a
+        st = find_dxyuv_kernel(1, n, I, -6e-7, 1.0, 18, *acc, rel, out)
+        assert st == 0
+        assert np.all(out[: 6 * I] == 0)
+        acc[0][i] += U[i] * 1.0
+        acc[1][i] += V[i] * 1.0
+        acc[2][i] += W[i] * 1.0
+    disp = np.stack(acc)
+    ref_disp = golden["bia_disp_aos"].reshape(-1, 6).T
+    assert_parity(s + disp, s + ref_disp, tol_max=1e-11)
+
+
+def test_deterministic_mode_is_bitwise_reproducible(cuda):
+    s, eps, q = initial.coulomb_cube(700, seed=25)
+    a, _ = gpu_run(cuda, s, eps, 1e-5, 2, q=q)
+    b, _ = gpu_run(cuda, s, eps, 1e-5, 2, q=q)
+    assert np.array_equal(a, b)
+
+
+def test_atomic_mode_matches_deterministic(cuda):
+    s, eps = initial.gravity_ball(500, seed=26)
+    a, _ = gpu_run(cuda, s, eps, 1e-4, 2, deterministic=1)
+    b, _ = gpu_run(cuda, s, eps, 1e-4, 2, deterministic=0)
+    assert rel_err(b, a) <= 1e-15
+
+
+def test_graph_run_equals_stepwise(cuda):
+    s, eps = initial.plummer(600, seed=27)
+    a, sa = gpu_run(cuda, s, eps, 1e-4, 4, graph=True)
+    b, _ = gpu_run(cuda, s, eps, 1e-4, 4, graph=False)
+    assert np.array_equal(a, b)
+    assert sa["hyperbola"] + sa["ellipse"] == 4 * 600 * 599 // 2
+
+
+def test_host_buffer_run_equals_device_run(cuda):
+    s, eps, q = initial.coulomb_cube(300, seed=28)
+    h = s.copy()
+    cfg = default_config(eps_th=eps, dt=1e-5)
+    with BIASolver() as solver:
+        solver.run_host(h, cfg, 3, q=q)
+    d, _ = gpu_run(cuda, s, eps, 1e-5, 3, q=q, graph=True)
+    assert np.array_equal(h, d)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 31, 32, 33, 64, 65, 97])
+def test_ragged_sizes(cuda, n):
+    s, eps = initial.gravity_ball(n, seed=100 + n)
+    g, st = gpu_run(cuda, s, eps, 1e-3, 2)
+    r, _ = oracle_run(s, eps, 1e-3, 2)
+    assert_parity(g, r)
+    assert st["hyperbola"] + st["ellipse"] + st["parabola"] == n * (n - 1) // 2
+
+
+def test_degenerate_and_parabolic_pairs(cuda):
+    """g = 0 (cold start), r parallel to g, and an exactly parabolic pair."""
+    s = np.zeros((6, 4))
+    s[:3, 0] = (0, 0, 0)
+    s[:3, 1] = (4, 3, 0)        # |r| = 5 from particle 0
+    s[3:, 1] = (0, 0, 1)        # |g| = 1, W = 1 + 2 eps / 5 = 0 with eps = -2.5
+    s[:3, 2] = (-3, 0, 0)
+    s[3:, 2] = (-0.5, 0, 0)     # r parallel to g relative to particle 0
+    s[:3, 3] = (0, 7, 1)        # at rest with particle 0: g = 0
+    eps = -2.5
+    g, st = gpu_run(cuda, s, eps, 0.01, 1)
+    r, rst = oracle_run(s, eps, 0.01, 1)
+    assert st["parabola"] == rst["parabola"] == 1
+    assert st["degenerate"] == rst["degenerate"] >= 2
+    assert st["nonfinite"] == 0
+    assert_parity(g, r)
+
+
+def test_cold_start_all_degenerate(cuda):
+    s, eps = initial.cold_ball(200, seed=29)
+    g, st = gpu_run(cuda, s, eps, 5e-5, 1)
+    r, _ = oracle_run(s, eps, 5e-5, 1)
+    assert st["degenerate"] == 200 * 199 // 2
+    assert_parity(g, r)
+
+
+def test_nonfinite_input_is_reported(cuda):
+    s, eps = initial.gravity_ball(40, seed=30)
+    s[0, 5] = np.nan
+    _, st = gpu_run(cuda, s, eps, 1e-4, 1)
+    assert st["nonfinite"] >= 39
+
+
+def test_invalid_arguments_raise(cuda):
+    from bia_3d_gpu_b200 import BiaError
+    t = cuda.zeros((6, 8), dtype=cuda.float64, device="cuda")
+    with BIASolver() as s:
+        with pytest.raises(BiaError):
+            s.step(t, default_config(itr=0))
+        with pytest.raises(BiaError):
+            s.step(t, default_config(method=7))
+    with pytest.raises(TypeError):
+        BIASolver().step(t.float(), default_config())
+
+
+def test_invariance_matches_oracle(cuda, golden_ic):
+    s, eps, q = initial.coulomb_cube(1000, seed=31)
+    t = cuda.tensor(s, device="cuda")
+    qt = cuda.tensor(q, device="cuda")
+    with BIASolver() as solver:
+        got = solver.invariance(t, eps, q=qt)
+    ref = oracle.invariance(s, eps, q=q, quad=True)
+    for k in ("KE", "PE"):
+        assert abs(got[k] / ref[k] - 1) <= 1e-13, k
+    for k in ("Ua", "Va", "Wa", "Xa", "Ya", "Za", "Lx", "Ly", "Lz"):
+        assert abs(got[k] - ref[k]) <= 1e-12 * max(1.0, abs(ref[k])), k
+    # drop-in invariance_gpu_ on the fixture (bia/bia.f90:67-68 call shape)
+    X, Y, Z, U, V, W = [np.ascontiguousarray(golden_ic[k]) for k in range(6)]
+    vals = invariance_gpu(golden_ic.shape[1], -6e-7, X, Y, Z, U, V, W)
+    refq = oracle.invariance(golden_ic, -6e-7, quad=True)
+    for name, v in zip(("KE", "PE", "Lx", "Ly", "Lz", "Ua", "Va", "Wa", "Xa", "Ya", "Za"), vals):
+        assert abs(v - refq[name]) <= 1e-13 * max(1.0, abs(refq[name])), name
