@@ -49,6 +49,7 @@ FLOPS = {
     "ellipse": (447, 47),      # per pair, per Kepler Newton step
     "parabola": (429, 76),     # per pair, per Barker Newton step
     "rkf": (147, 758),         # per pair, per accepted RKF45 step (3 Fehlberg stages sets)
+    "universal": (145, 74),    # per pair, per universal-variable Newton iteration
 }
 
 # DRAM traffic per launch of bia_pair_tiles_kernel at the default workload, from the
@@ -56,12 +57,16 @@ FLOPS = {
 TRAFFIC_BYTES_PER_LAUNCH = None
 
 
-def pair_flops(stats):
+def pair_flops(stats, method):
     h, e, p, r = FLOPS["hyperbola"], FLOPS["ellipse"], FLOPS["parabola"], FLOPS["rkf"]
+    u = FLOPS["universal"]
+    deg_rkf = stats["degenerate"] if method == 0 else 0
+    deg_uv = stats["degenerate"] - deg_rkf
     return (stats["hyperbola"] * h[0] + stats["iter_hyperbola"] * h[1] +
             stats["ellipse"] * e[0] + stats["iter_ellipse"] * e[1] +
             stats["parabola"] * p[0] + stats["iter_parabola"] * p[1] +
-            (stats["rkf"] + stats["degenerate"]) * r[0] + stats["rkf_steps"] * r[1])
+            (stats["rkf"] + deg_rkf) * r[0] + stats["rkf_steps"] * r[1] +
+            (stats["universal"] + deg_uv) * u[0] + stats["iter_universal"] * u[1])
 
 
 def parse():
@@ -72,7 +77,7 @@ def parse():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="coulomb_cube_32768")
     ap.add_argument("--n", type=int, default=None, help="override the particle count")
-    ap.add_argument("--method", choices=("alg", "rkf"), default="alg")
+    ap.add_argument("--method", choices=("alg", "rkf", "universal"), default="alg")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -161,7 +166,7 @@ def run_reference(args, rank, world):
         return
     from bia_3d_gpu_b200 import initial
     state, eps, q, dt, steps_cfg = initial.make(args.workload, n=args.n)
-    method = 1 if args.method == "alg" else 0
+    method = {"rkf": 0, "alg": 1, "universal": 2}[args.method]
     steps = args.steps if args.steps is not None else steps_cfg
     per_step = max(0.5, min(3.0, 120.0 / max(1, steps + args.warmup)))
     for w in range(args.warmup):
@@ -214,7 +219,7 @@ def main():
     n = state.shape[1]
     pairs = n * (n - 1) // 2
     steps = args.steps if args.steps is not None else steps_cfg
-    method = 1 if args.method == "alg" else 0
+    method = {"rkf": 0, "alg": 1, "universal": 2}[args.method]
     cfg = default_config(eps_th=eps, dt=dt, method=method)
     dev = torch.device("cuda", local)
     solver = BIASolver(device=local)
@@ -289,7 +294,7 @@ def main():
                "wall_s": wall}
 
     # roofline of the pair kernel
-    flops_total = pair_flops(stats)
+    flops_total = pair_flops(stats, method)
     per_launch_flops = flops_total / max(kern_launches, 1)
     per_launch_s = kern_ms * 1e-3 / max(kern_launches, 1)
     peak = measure_fp64_peak(local)
@@ -322,7 +327,7 @@ def main():
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
             "gpu_launches": 2 * steps,
             "stats": {k: v for k, v in stats.items()},
-            "iterations_per_alg_pair": stats["iterations"] / max(
+            "iterations_per_classical_pair": stats["iterations"] / max(
                 1, stats["hyperbola"] + stats["ellipse"] + stats["parabola"]),
         }
         print(json.dumps(line), flush=True)

@@ -17,11 +17,12 @@ import ctypes
 import numpy as np
 
 from . import capi
-from .capi import (BIA_ERR_NONFINITE, BIA_OK, METHOD_ALG, METHOD_RKF, BiaConfig, BiaError,
-                   BiaStats, default_config)
+from .capi import (BIA_ERR_NONFINITE, BIA_OK, METHOD_ALG, METHOD_RKF, METHOD_UNIVERSAL,
+                   BiaConfig, BiaError, BiaStats, default_config)
 
 __all__ = ["find_dxyuv_kernel", "invariance_gpu", "BIASolver", "default_config", "BiaConfig",
-           "BiaError", "METHOD_ALG", "METHOD_RKF", "INVARIANT_NAMES"]
+           "BiaError", "METHOD_ALG", "METHOD_RKF", "METHOD_UNIVERSAL", "INVARIANT_NAMES",
+           "measure_fp64_peak"]
 
 INVARIANT_NAMES = ("KE", "PE", "Lx", "Ly", "Lz", "Ua", "Va", "Wa", "Xa", "Ya", "Za")
 

@@ -20,6 +20,7 @@ BIA_ERR_NO_DEVICE = 7
 
 METHOD_RKF = 0
 METHOD_ALG = 1
+METHOD_UNIVERSAL = 2
 
 
 class BiaConfig(ctypes.Structure):
@@ -29,9 +30,9 @@ class BiaConfig(ctypes.Structure):
                 ("deterministic", ctypes.c_int)]
 
 
-STAT_FIELDS = ("hyperbola", "parabola", "ellipse", "degenerate", "rkf", "iterations",
-               "iter_hyperbola", "iter_ellipse", "iter_parabola", "rkf_steps", "nonconverged",
-               "bracket_exits", "nonfinite")
+STAT_FIELDS = ("hyperbola", "parabola", "ellipse", "degenerate", "rkf", "universal",
+               "iterations", "iter_hyperbola", "iter_ellipse", "iter_parabola", "iter_universal",
+               "rkf_steps", "nonconverged", "bracket_exits", "fallbacks", "nonfinite")
 
 
 class BiaStats(ctypes.Structure):

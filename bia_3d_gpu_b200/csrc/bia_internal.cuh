@@ -9,10 +9,10 @@
 namespace bia {
 
 // device counters in the stats buffer: hyperbola, parabola, ellipse, degenerate, rkf,
-// iter_hyperbola, iter_ellipse, iter_parabola, rkf_steps, nonconverged, bracket_exits,
-// nonfinite
-constexpr int kNumStats = 12;
-constexpr int kStatNonfinite = 11;
+// universal, iter_hyperbola, iter_ellipse, iter_parabola, iter_universal, rkf_steps,
+// nonconverged, bracket_exits, fallbacks, nonfinite
+constexpr int kNumStats = 15;
+constexpr int kStatNonfinite = 14;
 
 struct DeviceBuffer {
     void *ptr = nullptr;

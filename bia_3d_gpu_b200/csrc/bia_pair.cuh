@@ -10,8 +10,11 @@
 // The formulas follow the reference's CPU path; CUDA's double-precision math
 // functions replace glibc's, and nvcc's FMA contraction is left on, so results agree
 // with the CPU oracle to rounding, not bit for bit.  The same deviations as the
-// oracle are taken where the reference is undefined (uninitialised theta_stock,
-// bracket exit without a result, zero |g| or |L|).
+// oracle are taken where the reference is undefined or fails in FP64: uninitialised
+// theta_stock, bracket exit without a result, iterations that end unconverged
+// (bracketed re-solve), and pairs with zero |g| or |L| or with |e^2 - 1| < 0.1 (the
+// classical parametrisations lose up to every digit there), which are advanced by a
+// universal-variable (Stumpff function) solver.
 #pragma once
 #include <cstdint>
 
@@ -19,7 +22,10 @@ namespace bia {
 
 constexpr double kPi = 3.14159265358979323846264338327950288419716939937510582097494;
 
-enum PairClass { kHyperbola = 0, kParabola = 1, kEllipse = 2, kDegenerate = 3, kRkf = 4 };
+enum PairClass { kHyperbola = 0, kParabola = 1, kEllipse = 2, kDegenerate = 3, kRkf = 4, kUniversal = 5 };
+
+// |e^2 - 1| below which ALG pairs use the universal-variable solver
+constexpr double kNearUnitEcc = 0.1;
 
 struct PairParams {
     double dt;
@@ -27,24 +33,26 @@ struct PairParams {
     double relerr;   // RKF tolerances
     double abserr;
     int itr;         // Newton cap ITR
-    int method;      // 0 RKF, 1 ALG
+    int method;      // 0 RKF, 1 ALG, 2 universal variables for every pair
 };
 
 // Per-thread counters, reduced per warp before one atomic per counter.
 struct PairCounters {
-    int cls[5];
-    int it_hyp, it_ell, it_par;
+    int cls[6];
+    int it_hyp, it_ell, it_par, it_uv;
     int rkf_steps;
     int nonconverged;
     int bracket_exits;
+    int fallbacks;
     int nonfinite;
 };
 
 __device__ __forceinline__ void counters_zero(PairCounters &c)
 {
 #pragma unroll
-    for (int k = 0; k < 5; k++) c.cls[k] = 0;
-    c.it_hyp = c.it_ell = c.it_par = c.rkf_steps = c.nonconverged = c.bracket_exits = c.nonfinite = 0;
+    for (int k = 0; k < 6; k++) c.cls[k] = 0;
+    c.it_hyp = c.it_ell = c.it_par = c.it_uv = 0;
+    c.rkf_steps = c.nonconverged = c.bracket_exits = c.fallbacks = c.nonfinite = 0;
 }
 
 // bia/bia.f90:284-314.  Returns true for a degenerate pair (|g| == 0 or |L| == 0):
@@ -109,8 +117,34 @@ __device__ __forceinline__ double hyp_newton(const HypConsts &c, double theta_no
     return theta_now - e / dfdth;
 }
 
+// Bracketed Newton-bisection on the same time equation, used only when the reference's
+// loop ends without a small residual.  The equation is monotonic on (-theta_0, theta_0):
+// increasing for repulsive pairs (tn_0 > 0), decreasing for attractive ones.
+static __device__ __noinline__ double hyp_safe(const HypConsts c, double x)
+{
+    double lo = -c.theta_0, hi = c.theta_0;
+    const double dir = (c.tn_0 > 0.0) ? 1.0 : -1.0;
+    if (!(x > lo && x < hi)) x = 0.0;
+    for (int it = 0; it < 400; it++) {
+        const double sp = sin((c.theta_0 + x) * 0.5), sm = sin((c.theta_0 - x) * 0.5);
+        double sn, cs;
+        sincos(x, &sn, &cs);
+        const double Dinv = 1.0 / (cs - c.cs_0);
+        const double f = c.tn_0 * sn * Dinv - c.time_end_ + log(sp / sm);
+        if (f == 0.0) break;
+        if (f * dir < 0.0) lo = x; else hi = x;
+        const double d = c.tn_0 * (1.0 - c.cs_0 * cs) * (Dinv * Dinv) + c.sn_0 / (2.0 * sp * sm);
+        double xn = x - f / d;
+        if (!(xn > lo && xn < hi)) xn = 0.5 * (lo + hi);
+        if (xn == x) break;
+        x = xn;
+    }
+    return x;
+}
+
 __device__ __forceinline__ int hyperbola(double eps_th, double dt, int ITR, const double YZ[4],
-                                         double YN[4], double *error_end, int *bracket_exit)
+                                         double YN[4], double *error_end, int *bracket_exit,
+                                         int *fallback)
 {
     const double X_ini = YZ[0], Y_ini = YZ[1], U_ini = YZ[2], V_ini = YZ[3];
     const double r_g = X_ini * U_ini + Y_ini * V_ini;
@@ -163,6 +197,7 @@ __device__ __forceinline__ int hyperbola(double eps_th, double dt, int ITR, cons
     // minimum-residual Newton loop with cycle detection (bia/find_hyperbola.f90:93-120)
     double err_stock = error_;
     double theta_stock = theta_end;
+    double best_res = fabs(error_);  // smallest dimensionless residual seen
     double hist[64];
     int IR = 0;
     *bracket_exit = 0;
@@ -181,6 +216,7 @@ __device__ __forceinline__ int hyperbola(double eps_th, double dt, int ITR, cons
             if (hist[num] == error_) { cycle = true; break; }
         if (cycle) break;
         hist[IR] = error_;
+        best_res = fmin(best_res, fabs(error_));
         if (fabs(error_) < fabs(err_stock)) {
             err_stock = error_ * b_0 / g_0;
             theta_stock = theta_end;
@@ -188,6 +224,11 @@ __device__ __forceinline__ int hyperbola(double eps_th, double dt, int ITR, cons
         }
     }
     *error_end = error_ * b_0 / g_0;
+    *fallback = 0;
+    if (!(best_res <= 1e-8 * (1.0 + fabs(c.time_end_)))) {  // the reference loop did not converge
+        theta_stock = hyp_safe(c, theta_stock);
+        *fallback = 1;
+    }
     double sn_end, cs_end;
     sincos(theta_stock, &sn_end, &cs_end);
     const double u_end = g0_sn0 * c.cs_0 * sn_end;
@@ -207,8 +248,29 @@ __device__ __forceinline__ int hyperbola(double eps_th, double dt, int ITR, cons
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double f_sign(double a, double b) { return (b >= 0.0) ? fabs(a) : -fabs(a); }
 
+// Bracketed Newton-bisection for Kepler's equation xi - e sin(xi) = M (root in
+// [M - |e|, M + |e|]), used only when the reference's iteration ends unconverged.
+static __device__ __noinline__ double kepler_safe(double M, double e, double x)
+{
+    const double ae = fabs(e);
+    double lo = M - ae, hi = M + ae;
+    if (!(x >= lo && x <= hi)) x = M;
+    for (int it = 0; it < 400; it++) {
+        double sx, cx;
+        sincos(x, &sx, &cx);
+        const double f = x - e * sx - M;
+        if (f == 0.0) break;
+        if (f < 0.0) lo = x; else hi = x;
+        double xn = x - f / (1.0 - e * cx);
+        if (!(xn > lo && xn < hi)) xn = 0.5 * (lo + hi);
+        if (xn == x) break;
+        x = xn;
+    }
+    return x;
+}
+
 static __device__ __noinline__ int ellipse(double eps_th, double dt, int ITR, const double YZ[4],
-                                    double YN[4], double *error)
+                                    double YN[4], double *error, int *fallback)
 {
     const double X_ini = YZ[0], Y_ini = YZ[1], U_ini = YZ[2], V_ini = YZ[3];
     const double g2_ini = U_ini * U_ini + V_ini * V_ini;
@@ -259,7 +321,8 @@ static __device__ __noinline__ int ellipse(double eps_th, double dt, int ITR, co
     double delta_xi2 = error_tm2 / (1.0 - ecc * c2);
     double xi = (fabs(error_ini) < fabs(error_tm2)) ? xi_2 + delta_ini : xi_2 + delta_xi2;
     double xi_1 = __longlong_as_double(0x7ff8000000000000LL);  // unset: compares unequal
-    double error_tm1;
+    double error_tm1 = error_tm2;
+    bool conv = false;
     while (xi_1 != xi_2 && ir <= ITR) {
         ir++;
         xi_1 = xi;
@@ -269,6 +332,7 @@ static __device__ __noinline__ int ellipse(double eps_th, double dt, int ITR, co
         xi = xi_1 + error_tm1 / (1.0 - ecc * c1);
         if (error_tm1 == 0.0 || error_tm1 == error_tm2 || error_tm1 + error_tm2 == 0.0) {
             *error = error_tm1;
+            conv = true;
             break;
         }
         ir++;
@@ -279,8 +343,15 @@ static __device__ __noinline__ int ellipse(double eps_th, double dt, int ITR, co
         xi = xi_2 + delta_xi2;
         if (error_tm2 == 0.0 || error_tm1 == error_tm2 || error_tm1 + error_tm2 == 0.0) {
             *error = error_tm2;
+            conv = true;
             break;
         }
+    }
+    if (xi_1 == xi_2) conv = true;
+    *fallback = 0;
+    if (!conv && !(fmin(fabs(error_tm1), fabs(error_tm2)) <= 1e-8 * (1.0 + fabs(tau_end)))) {
+        xi = kepler_safe(tau_end, ecc, xi);
+        *fallback = 1;
     }
     double sn_end, cs_end;
     sincos(xi, &sn_end, &cs_end);
@@ -501,43 +572,138 @@ static __device__ __noinline__ int rkf_pair(double eps_th, double xe, double rel
 }
 
 // ---------------------------------------------------------------------------
+// Universal-variable propagation of r'' = eps r/|r|^3 (mu = -eps) with Stumpff
+// functions (Danby, Fundamentals of Celestial Mechanics, 2nd ed., 6.7-6.9).  Uniformly
+// well conditioned for every conic and for radial or zero-velocity pairs; the
+// displacement from free motion is formed without cancellation:
+//   r(t) - r0 - v0 dt = -(mu/r0) s^2 c2 r0vec - mu s^3 c3 v0vec
+//   v(t) - v0         = -(mu/(r r0)) s c1 r0vec - (mu/r) s^2 c2 v0vec
+// with s the root of r0 s c1 + sigma0 s^2 c2 + mu s^3 c3 = dt (bracketed Newton).
+// No transcendental function is called: the Stumpff functions come from a series at
+// |x| <= 0.1 and the duplication formulas c0(4x) = 2c0^2 - 1, c1(4x) = c0 c1,
+// c2(4x) = c1^2/2, c3(4x) = (c2 + c0 c3)/4.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void stumpff(double x, double c[4])
+{
+    int n = 0;
+    while (fabs(x) > 0.1 && n < 200) { x *= 0.25; n++; }
+    // c2 = sum (-x)^j / (2+2j)!, c3 = sum (-x)^j / (3+2j)!, j = 0..10 (|x| <= 0.1)
+    double c2 = 1.0 / 620448401733239439360000.0;    // 1/24!
+    double c3 = 1.0 / 15511210043330985984000000.0;  // 1/25!
+    c2 = 1.0 / 20922789888000.0 - x * (1.0 / 6402373705728000.0 - x * (1.0 / 2432902008176640000.0 - x * (1.0 / 1124000727777607680000.0 - x * c2)));
+    c3 = 1.0 / 355687428096000.0 - x * (1.0 / 121645100408832000.0 - x * (1.0 / 51090942171709440000.0 - x * (1.0 / 25852016738884976640000.0 - x * c3)));
+    c2 = 0.5 - x * (1.0 / 24 - x * (1.0 / 720 - x * (1.0 / 40320 - x * (1.0 / 3628800 - x * (1.0 / 479001600 - x * (1.0 / 87178291200.0 - x * c2))))));
+    c3 = 1.0 / 6 - x * (1.0 / 120 - x * (1.0 / 5040 - x * (1.0 / 362880 - x * (1.0 / 39916800 - x * (1.0 / 6227020800.0 - x * (1.0 / 1307674368000.0 - x * c3))))));
+    double c1 = 1.0 - x * c3;
+    double c0 = 1.0 - x * c2;
+    for (; n > 0; n--) {
+        const double c3n = (c2 + c0 * c3) * 0.25;
+        const double c2n = c1 * c1 * 0.5;
+        const double c1n = c0 * c1;
+        const double c0n = 2.0 * c0 * c0 - 1.0;
+        c0 = c0n; c1 = c1n; c2 = c2n; c3 = c3n;
+    }
+    c[0] = c0; c[1] = c1; c[2] = c2; c[3] = c3;
+}
+
+__device__ __forceinline__ int uv_halfdisp(double eps_th, double dt, const double r[3], const double g[3],
+                                           double h[6])
+{
+    const double mu = -eps_th;
+    const double r0 = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    const double sig = r[0] * g[0] + r[1] * g[1] + r[2] * g[2];
+    const double v2 = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+    const double beta = 2.0 * mu / r0 - v2;
+#pragma unroll
+    for (int k = 0; k < 6; k++) h[k] = 0.0;
+    if (dt == 0.0) return 0;
+    double c[4];
+    double s = dt / r0;
+    s = s - sig * s * s / (2.0 * r0);
+    if (!(s > 0.0)) s = dt / r0;
+    double lo = 0.0, hi = -1.0;
+    int it;
+    for (it = 1; it <= 200; it++) {
+        stumpff(beta * s * s, c);
+        const double F = r0 * s * c[1] + sig * s * s * c[2] + mu * s * s * s * c[3] - dt;
+        const double Fp = r0 * c[0] + sig * s * c[1] + mu * s * s * c[2];
+        if (F == 0.0) break;
+        if (F < 0.0) lo = s; else hi = s;
+        double sn = s - F / Fp;
+        if (!(sn > lo) || (hi > 0.0 && !(sn < hi)) || !(Fp > 0.0)) sn = (hi > 0.0) ? 0.5 * (lo + hi) : 2.0 * s;
+        const double ds = sn - s;
+        s = sn;
+        if (fabs(ds) <= 4.0 * 2.220446049250313e-16 * fabs(s)) break;
+    }
+    stumpff(beta * s * s, c);
+    const double s2c2 = s * s * c[2], s3c3 = s * s * s * c[3];
+    const double rr = r0 * c[0] + sig * s * c[1] + mu * s2c2;
+    const double fm1 = -mu * s2c2 / r0;
+    const double gmdt = -mu * s3c3;
+    const double fdot = -mu * s * c[1] / (rr * r0);
+    const double gdm1 = -mu * s2c2 / rr;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        h[k] = (fm1 * r[k] + gmdt * g[k]) * 0.5;
+        h[3 + k] = (fdot * r[k] + gdm1 * g[k]) * 0.5;
+    }
+    return it;
+}
+
+// ---------------------------------------------------------------------------
 // One pair: frame, classification, solve, half-displacement (bia/bia.f90:141-191).
 // Returns the half-displacement in h[6] = (dX, dY, dZ, dU, dV, dW)/2 terms.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void pair_halfdisp(const PairParams &P, double eps_ij, const double r[3],
                                               const double g[3], double h[6], PairCounters &cnt)
 {
-    double e_xi[3], e_eta[3], YZ[4], YN[4];
-    double error = 0.0;
-    const bool degenerate = frame_xi_eta(r, g, e_xi, e_eta, YZ);
-    if (degenerate || P.method == 0) {
-        int nacc = 0;
-        rkf_pair(eps_ij, P.dt, P.relerr, P.abserr, YZ, YN, &error, &nacc);
-        cnt.cls[degenerate ? kDegenerate : kRkf]++;
-        cnt.rkf_steps += nacc;
+    if (P.method == 2) {
+        cnt.it_uv += uv_halfdisp(eps_ij, P.dt, r, g, h);
+        cnt.cls[kUniversal]++;
     } else {
-        const double r_ij = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-        const double E_ij = g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + 2.0 * eps_ij / r_ij;
-        if (E_ij > 0.0) {
-            int bx = 0;
-            cnt.it_hyp += hyperbola(eps_ij, P.dt, P.itr, YZ, YN, &error, &bx);
-            cnt.bracket_exits += bx;
-            cnt.cls[kHyperbola]++;
-        } else if (E_ij < 0.0) {
-            cnt.it_ell += ellipse(eps_ij, P.dt, P.itr, YZ, YN, &error);
-            cnt.cls[kEllipse]++;
+        double e_xi[3], e_eta[3], YZ[4], YN[4];
+        double error = 0.0;
+        const bool degenerate = frame_xi_eta(r, g, e_xi, e_eta, YZ);
+        bool done = false;
+        if (P.method == 0) {
+            int nacc = 0;
+            rkf_pair(eps_ij, P.dt, P.relerr, P.abserr, YZ, YN, &error, &nacc);
+            cnt.cls[degenerate ? kDegenerate : kRkf]++;
+            cnt.rkf_steps += nacc;
         } else {
-            cnt.it_par += parabola(eps_ij, P.dt, YZ, YN, &error);
-            cnt.cls[kParabola]++;
+            const double r_ij = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+            const double E_ij = g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + 2.0 * eps_ij / r_ij;
+            const double Lm = YZ[0] * YZ[3];
+            if (E_ij != 0.0 && (degenerate || fabs(E_ij) * (Lm * Lm) < kNearUnitEcc * (eps_ij * eps_ij))) {
+                cnt.it_uv += uv_halfdisp(eps_ij, P.dt, r, g, h);
+                cnt.cls[degenerate ? kDegenerate : kUniversal]++;
+                done = true;
+            } else if (E_ij > 0.0) {
+                int bx = 0, fb = 0;
+                cnt.it_hyp += hyperbola(eps_ij, P.dt, P.itr, YZ, YN, &error, &bx, &fb);
+                cnt.bracket_exits += bx;
+                cnt.fallbacks += fb;
+                cnt.cls[kHyperbola]++;
+            } else if (E_ij < 0.0) {
+                int fb = 0;
+                cnt.it_ell += ellipse(eps_ij, P.dt, P.itr, YZ, YN, &error, &fb);
+                cnt.fallbacks += fb;
+                cnt.cls[kEllipse]++;
+            } else {
+                cnt.it_par += parabola(eps_ij, P.dt, YZ, YN, &error);
+                cnt.cls[kParabola]++;
+            }
         }
-    }
-    if (fabs(error) > P.err) cnt.nonconverged++;
-    const double dr_xi = YN[0] - YZ[0], dr_eta = YN[1] - YZ[1];
-    const double dg_xi = YN[2] - YZ[2], dg_eta = YN[3] - YZ[3];
+        if (!done) {
+            if (fabs(error) > P.err) cnt.nonconverged++;
+            const double dr_xi = YN[0] - YZ[0], dr_eta = YN[1] - YZ[1];
+            const double dg_xi = YN[2] - YZ[2], dg_eta = YN[3] - YZ[3];
 #pragma unroll
-    for (int k = 0; k < 3; k++) {
-        h[k] = (dr_xi * e_xi[k] + dr_eta * e_eta[k] - g[k] * P.dt) * 0.5;
-        h[3 + k] = (dg_xi * e_xi[k] + dg_eta * e_eta[k]) * 0.5;
+            for (int k = 0; k < 3; k++) {
+                h[k] = (dr_xi * e_xi[k] + dr_eta * e_eta[k] - g[k] * P.dt) * 0.5;
+                h[3 + k] = (dg_xi * e_xi[k] + dg_eta * e_eta[k]) * 0.5;
+            }
+        }
     }
     bool finite = true;
 #pragma unroll

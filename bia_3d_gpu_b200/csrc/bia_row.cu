@@ -50,9 +50,9 @@ __global__ void __launch_bounds__(128) bia_row_kernel(const RowArgs A)
         for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(full, v, off);
         if (lane == 0 && v != 0.0) atomicAdd(&A.rowsum[c], v);
     }
-    int vals[kNumStats] = {cnt.cls[0], cnt.cls[1], cnt.cls[2], cnt.cls[3], cnt.cls[4], cnt.it_hyp,
-                           cnt.it_ell, cnt.it_par, cnt.rkf_steps, cnt.nonconverged,
-                           cnt.bracket_exits, cnt.nonfinite};
+    int vals[kNumStats] = {cnt.cls[0], cnt.cls[1], cnt.cls[2], cnt.cls[3], cnt.cls[4], cnt.cls[5],
+                           cnt.it_hyp, cnt.it_ell, cnt.it_par, cnt.it_uv, cnt.rkf_steps,
+                           cnt.nonconverged, cnt.bracket_exits, cnt.fallbacks, cnt.nonfinite};
 #pragma unroll
     for (int k = 0; k < kNumStats; k++) {
         int s = __reduce_add_sync(full, vals[k]);

@@ -72,8 +72,9 @@ __device__ __forceinline__ void load_particle(const StepArgs &A, int p, double s
 __device__ __forceinline__ void flush_counters(const PairCounters &c, unsigned long long *stats, int lane)
 {
     const unsigned full = 0xffffffffu;
-    int vals[kNumStats] = {c.cls[0], c.cls[1], c.cls[2], c.cls[3], c.cls[4], c.it_hyp, c.it_ell,
-                           c.it_par, c.rkf_steps, c.nonconverged, c.bracket_exits, c.nonfinite};
+    int vals[kNumStats] = {c.cls[0], c.cls[1], c.cls[2], c.cls[3], c.cls[4], c.cls[5],
+                           c.it_hyp, c.it_ell, c.it_par, c.it_uv, c.rkf_steps,
+                           c.nonconverged, c.bracket_exits, c.fallbacks, c.nonfinite};
 #pragma unroll
     for (int k = 0; k < kNumStats; k++) {
         int s = __reduce_add_sync(full, vals[k]);
@@ -227,7 +228,8 @@ static int validate(const bia_config *cfg, int n, const void *x, const void *y, 
                     const void *u, const void *v, const void *w)
 {
     if (!cfg || n < 1 || !x || !y || !z || !u || !v || !w) return BIA_ERR_INVALID_ARGUMENT;
-    if (cfg->method != BIA_METHOD_ALG && cfg->method != BIA_METHOD_RKF) return BIA_ERR_INVALID_ARGUMENT;
+    if (cfg->method != BIA_METHOD_ALG && cfg->method != BIA_METHOD_RKF && cfg->method != BIA_METHOD_UNIVERSAL)
+        return BIA_ERR_INVALID_ARGUMENT;
     if (cfg->itr < 1 || cfg->itr > 62) return BIA_ERR_INVALID_ARGUMENT;
     // 32-bit particle indices and a warp-block count that fits the grid
     if (n > (1 << 30)) return BIA_ERR_INVALID_ARGUMENT;
@@ -301,14 +303,17 @@ static void copy_stats(const unsigned long long *h, bia_stats *s)
     s->ellipse = (long long)h[2];
     s->degenerate = (long long)h[3];
     s->rkf = (long long)h[4];
-    s->iter_hyperbola = (long long)h[5];
-    s->iter_ellipse = (long long)h[6];
-    s->iter_parabola = (long long)h[7];
+    s->universal = (long long)h[5];
+    s->iter_hyperbola = (long long)h[6];
+    s->iter_ellipse = (long long)h[7];
+    s->iter_parabola = (long long)h[8];
+    s->iter_universal = (long long)h[9];
     s->iterations = s->iter_hyperbola + s->iter_ellipse + s->iter_parabola;
-    s->rkf_steps = (long long)h[8];
-    s->nonconverged = (long long)h[9];
-    s->bracket_exits = (long long)h[10];
-    s->nonfinite = (long long)h[11];
+    s->rkf_steps = (long long)h[10];
+    s->nonconverged = (long long)h[11];
+    s->bracket_exits = (long long)h[12];
+    s->fallbacks = (long long)h[13];
+    s->nonfinite = (long long)h[14];
 }
 
 static int fetch_stats(bia_context *ctx, bia_stats *stats)

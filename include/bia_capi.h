@@ -33,11 +33,14 @@ enum bia_status {
     BIA_ERR_NO_DEVICE = 7
 };
 
-/* pair solver: the reference's METHOD argument (bia/bia.f90:134-139) */
-enum bia_method { BIA_METHOD_RKF = 0, BIA_METHOD_ALG = 1 };
+/* pair solver: the reference's METHOD argument (bia/bia.f90:134-139), plus
+   BIA_METHOD_UNIVERSAL, which advances every pair with the universal-variable
+   (Stumpff function) solver that ALG uses for near-unit-eccentricity pairs */
+enum bia_method { BIA_METHOD_RKF = 0, BIA_METHOD_ALG = 1, BIA_METHOD_UNIVERSAL = 2 };
 
 typedef struct bia_config {
-    int method;        /* BIA_METHOD_ALG (Kepler/Barker solve) or BIA_METHOD_RKF */
+    int method;        /* BIA_METHOD_ALG (Kepler/Barker solve), BIA_METHOD_RKF or
+                          BIA_METHOD_UNIVERSAL */
     int itr;           /* Newton iteration cap, ITR = 18 (bia/bia.f90:52) */
     double eps_th;     /* coupling of r'' = eps r/|r|^3 (bia/bia.f90:37); with charges q
                           the pair coupling is eps_th * q_i * q_j */
@@ -56,11 +59,16 @@ void bia_config_default(bia_config *cfg);
 /* per-step counters (pairs per branch of bia/bia.f90:158-166 and solver work) */
 typedef struct bia_stats {
     long long hyperbola, parabola, ellipse, degenerate, rkf;
-    long long iterations;    /* Newton iterations, summed over ALG pairs */
+    long long universal;     /* pairs advanced by the universal-variable solver (ALG pairs
+                                with |e^2 - 1| < 0.1, or every pair of BIA_METHOD_UNIVERSAL);
+                                degenerate pairs (|g| = 0 or |L| = 0) are counted apart */
+    long long iterations;    /* Newton iterations, summed over the classical ALG branches */
     long long iter_hyperbola, iter_ellipse, iter_parabola; /* the same split by branch */
+    long long iter_universal; /* Newton iterations of the universal-variable solver */
     long long rkf_steps;     /* accepted RKF steps, summed over RKF pairs */
     long long nonconverged;  /* |residual| > cfg.err (bia/bia.f90:151,167) */
     long long bracket_exits; /* hyperbola iterate left (-theta_0, theta_0) */
+    long long fallbacks;     /* classical iteration ended unconverged: bracketed re-solve */
     long long nonfinite;     /* pairs whose displacement was not finite */
 } bia_stats;
 

@@ -22,8 +22,9 @@ _PD = ctypes.POINTER(ctypes.c_double)
 _PI = ctypes.POINTER(ctypes.c_int)
 _PL = ctypes.POINTER(ctypes.c_int64)
 
-STAT_NAMES = ("hyperbola", "parabola", "ellipse", "degenerate", "rkf",
-              "iterations", "rkf_steps", "nonconverged", "bracket_exits")
+STAT_NAMES = ("hyperbola", "parabola", "ellipse", "degenerate", "rkf", "universal",
+              "iterations", "rkf_steps", "nonconverged", "bracket_exits", "fallbacks",
+              "uv_iterations")
 
 
 def build():
@@ -44,9 +45,14 @@ def lib():
         L.oracle_particle_disp.argtypes = ([_I, _I, _D, _PD, _D, _I, _D, _D] + [_PD] * 6 +
                                            [_PI, _I, _PD, _I])
         L.oracle_pair_halfdisp.argtypes = [_I, _D, _D, _I, _D, _D, _PD, _PD, _PD, _PL]
-        L.oracle_find_hyperbola.argtypes = [_D, _D, _PD, _PD, _PD, _I, _PI]
+        L.oracle_pair_halfdisp_q.argtypes = L.oracle_pair_halfdisp.argtypes
+        L.oracle_bia_step_q.argtypes = L.oracle_bia_step.argtypes
+        L.oracle_particle_disp_q.argtypes = L.oracle_particle_disp.argtypes
+        L.oracle_bia_rows_omp_q.argtypes = L.oracle_bia_rows_omp.argtypes
+        L.oracle_bia_rows_omp_q.restype = ctypes.c_int64
+        L.oracle_find_hyperbola.argtypes = [_D, _D, _PD, _PD, _PD, _I, _PI, _PI]
         L.oracle_find_hyperbola.restype = _I
-        L.oracle_find_ellipse.argtypes = [_D, _D, _PD, _PD, _PD, _I]
+        L.oracle_find_ellipse.argtypes = [_D, _D, _PD, _PD, _PD, _I, _PI]
         L.oracle_find_ellipse.restype = _I
         L.oracle_find_parabola.argtypes = [_D, _D, _PD, _PD, _PD]
         L.oracle_find_parabola.restype = _I
@@ -70,18 +76,21 @@ def _c(a):
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
-def bia_step(state, eps_th, dt, method=1, q=None, itr=18, relerr=0.0, abserr=1e-16):
+def bia_step(state, eps_th, dt, method=1, q=None, itr=18, relerr=0.0, abserr=1e-16, quad=False):
     """One BIA step in the reference's pair order (bia/bia.f90:126-204).
 
     Returns (new_state, disp, stats) where disp = (dX..dW) including drift.
+    quad=True evaluates the same algorithm in __float128 (state stored in FP64 between
+    steps): the step without rounding noise.
     """
     s = np.array(state, dtype=np.float64, copy=True)
     n = s.shape[1]
     d = np.zeros((6, n))
     qq = _c(q) if q is not None else None
-    st = np.zeros(9, dtype=np.int64)
+    st = np.zeros(12, dtype=np.int64)
     rows = [np.ascontiguousarray(s[k]) for k in range(6)]
-    lib().oracle_bia_step(method, n, eps_th, _p(qq), dt, itr, relerr, abserr,
+    f = lib().oracle_bia_step_q if quad else lib().oracle_bia_step
+    f(method, n, eps_th, _p(qq), dt, itr, relerr, abserr,
                           *[_p(r) for r in rows], *[_p(d[k]) for k in range(6)],
                           st.ctypes.data_as(_PL))
     return np.stack(rows), d, dict(zip(STAT_NAMES, st.tolist()))
@@ -96,7 +105,7 @@ def bia_rows(state, eps_th, dt, rows, method=1, q=None, itr=18, relerr=0.0, abse
     r = np.ascontiguousarray(rows, dtype=np.int32)
     d = np.zeros((6, n))
     qq = _c(q) if q is not None else None
-    st = np.zeros(9, dtype=np.int64)
+    st = np.zeros(12, dtype=np.int64)
     cols = [np.ascontiguousarray(s[k]) for k in range(6)]
     pairs = lib().oracle_bia_rows_omp(method, n, eps_th, _p(qq), dt, itr, relerr, abserr,
                                       *[_p(c) for c in cols], r.ctypes.data_as(_PI), len(r),
@@ -106,7 +115,7 @@ def bia_rows(state, eps_th, dt, rows, method=1, q=None, itr=18, relerr=0.0, abse
 
 
 def particle_disp(state, eps_th, dt, sel, method=1, q=None, itr=18, relerr=0.0, abserr=1e-16,
-                  nthreads=0):
+                  nthreads=0, quad=False):
     """Full step displacement (dX..dW, drift included) of the particles in sel,
     summed over every other particle.  Returns (len(sel), 6)."""
     s = _c(state)
@@ -115,17 +124,19 @@ def particle_disp(state, eps_th, dt, sel, method=1, q=None, itr=18, relerr=0.0, 
     out = np.zeros((len(sl), 6))
     qq = _c(q) if q is not None else None
     cols = [np.ascontiguousarray(s[k]) for k in range(6)]
-    lib().oracle_particle_disp(method, n, eps_th, _p(qq), dt, itr, relerr, abserr,
+    f = lib().oracle_particle_disp_q if quad else lib().oracle_particle_disp
+    f(method, n, eps_th, _p(qq), dt, itr, relerr, abserr,
                                *[_p(c) for c in cols], sl.ctypes.data_as(_PI), len(sl), _p(out),
                                nthreads)
     return out
 
 
-def pair_halfdisp(r, g, eps_th, dt, method=1, itr=18, relerr=0.0, abserr=1e-16):
+def pair_halfdisp(r, g, eps_th, dt, method=1, itr=18, relerr=0.0, abserr=1e-16, quad=False):
     """Half-displacement h (6,) that bia.f90 adds to i and subtracts from j."""
     rr, gg, h = _c(r), _c(g), np.zeros(6)
-    st = np.zeros(9, dtype=np.int64)
-    lib().oracle_pair_halfdisp(method, eps_th, dt, itr, relerr, abserr, _p(rr), _p(gg), _p(h),
+    st = np.zeros(12, dtype=np.int64)
+    f = lib().oracle_pair_halfdisp_q if quad else lib().oracle_pair_halfdisp
+    f(method, eps_th, dt, itr, relerr, abserr, _p(rr), _p(gg), _p(h),
                                st.ctypes.data_as(_PL))
     return h, dict(zip(STAT_NAMES, st.tolist()))
 
@@ -137,16 +148,21 @@ def frame(r, g):
     return exi, eeta, ezeta, Y, bool(deg)
 
 
-def find_hyperbola(eps_th, dt, YZ, itr=18):
-    yz, yn, err, bx = _c(YZ), np.zeros(4), _D(0), _I(0)
+def find_hyperbola(eps_th, dt, YZ, itr=18, return_fallback=False):
+    yz, yn, err, bx, fb = _c(YZ), np.zeros(4), _D(0), _I(0), _I(0)
     it = lib().oracle_find_hyperbola(eps_th, dt, _p(yz), _p(yn), ctypes.byref(err), itr,
-                                     ctypes.byref(bx))
+                                     ctypes.byref(bx), ctypes.byref(fb))
+    if return_fallback:
+        return yn, err.value, it, fb.value
     return yn, err.value, it
 
 
-def find_ellipse(eps_th, dt, YZ, itr=18):
-    yz, yn, err = _c(YZ), np.zeros(4), _D(0)
-    it = lib().oracle_find_ellipse(eps_th, dt, _p(yz), _p(yn), ctypes.byref(err), itr)
+def find_ellipse(eps_th, dt, YZ, itr=18, return_fallback=False):
+    yz, yn, err, fb = _c(YZ), np.zeros(4), _D(0), _I(0)
+    it = lib().oracle_find_ellipse(eps_th, dt, _p(yz), _p(yn), ctypes.byref(err), itr,
+                                   ctypes.byref(fb))
+    if return_fallback:
+        return yn, err.value, it, fb.value
     return yn, err.value, it
 
 

@@ -26,7 +26,7 @@ def test_sampled_particles_match_oracle(cuda, name):
     new, disp, st = one_step(cuda, s, eps, dt, q)
     n = s.shape[1]
     assert st["nonfinite"] == 0
-    assert sum(st[k] for k in ("hyperbola", "ellipse", "parabola", "degenerate")) == n * (n - 1) // 2
+    assert sum(st[k] for k in ("hyperbola", "ellipse", "parabola", "degenerate", "universal")) == n * (n - 1) // 2
     sel = np.random.default_rng(7).choice(n, 48, replace=False)
     ref = oracle.particle_disp(s, eps, dt, sel, q=q)       # (48, 6)
     got = disp[:, sel].T
@@ -34,6 +34,10 @@ def test_sampled_particles_match_oracle(cuda, name):
     vscale = np.abs(s[3:]).max()
     assert np.abs(got[:, :3] - ref[:, :3]).max() <= 1e-12 * xscale
     assert np.abs(got[:, 3:] - ref[:, 3:]).max() <= 1e-12 * vscale
+    # and against the exact step on a few of them
+    refq = oracle.particle_disp(s, eps, dt, sel[:6], q=q, quad=True)
+    assert np.abs(got[:6, :3] - refq[:, :3]).max() <= 1e-13 * xscale
+    assert np.abs(got[:6, 3:] - refq[:, 3:]).max() <= 1e-13 * vscale
     # momentum: sum of all velocity kicks cancels pair by pair
     kick = disp[3:].sum(axis=1)
     assert np.abs(kick).max() <= 1e-12 * np.abs(disp[3:]).sum(axis=1).max()

@@ -1,7 +1,9 @@
 """Pins of the CPU oracle against the reference's own outputs and known answers.
 
 The oracle (oracle/bia_oracle.c) restates the reference's CPU path; these tests check
-it before it is trusted as the parity reference for the CUDA kernels:
+it before it is trusted as the parity reference for the CUDA kernels.  The same source
+is also evaluated in __float128 ("quad"): the BIA step without rounding noise, against
+which any FP64 implementation's rounding error is measured.  Pins:
   * the committed fixture OUT/0001332_10^0.{bbb,BIA,DIM} (reference run, N = 1332,
     eps_th = -6e-7, dt = 1; tests/golden/make_golden.py converts it);
   * per-branch identities every two-body solve must satisfy (energy W and angular
@@ -168,7 +170,8 @@ def test_pair_antisymmetry_bitwise():
 
 def test_degenerate_pairs_are_radial():
     """Zero relative velocity or r parallel to g: the reference divides by zero
-    (bia/bia.f90:295-296); the oracle integrates along the line of motion."""
+    (bia/bia.f90:295-296); the oracle advances them with the universal-variable solver,
+    which agrees with the per-pair RKF45 along the line of motion."""
     eps, dt = -0.5, 0.01
     r = np.array([1.0, 2.0, 2.0])
     h, st = oracle.pair_halfdisp(r, np.zeros(3), eps, dt)
@@ -211,3 +214,116 @@ def test_dim_oracle_conserves_energy_small():
     e0 = oracle.invariance(s, 2 * eps_dim, quad=True)
     e1 = oracle.invariance(yn.reshape(-1, 6).T, 2 * eps_dim, quad=True)
     assert abs((e1["KE"] + e1["PE"]) / (e0["KE"] + e0["PE"]) - 1) <= 1e-13
+
+
+# ---- quad-precision evaluation: rounding noise of the FP64 path ----------------------
+
+def test_fixture_fp64_vs_quad_sampled(golden, golden_ic):
+    """On the reference fixture (dt = 1) the FP64 path is within 1e-11 of max|X| of
+    the exact step on every sampled particle, including the pericentre pair of
+    particles 207/1086 (start angle from acos near 1, bia/find_hyperbola.f90:38), and
+    the reference's own record (its GPU run) is within the same band."""
+    sel = [0, 207, 1086, 557, 1244] + list(range(3, 1332, 97))
+    d = oracle.particle_disp(golden_ic, EPS_FIX, 1.0, sel)
+    qd = oracle.particle_disp(golden_ic, EPS_FIX, 1.0, sel, quad=True)
+    ref = golden["bia_disp_aos"].reshape(-1, 6).T[:, sel].T
+    scale = np.abs(golden_ic[:3]).max()
+    assert np.abs(d - qd)[:, :3].max() <= 1e-11 * scale
+    assert np.abs(ref - qd)[:, :3].max() <= 1e-11 * scale
+    assert np.abs(d - qd)[:, 3:].max() <= 1e-14
+
+
+@pytest.mark.parametrize("case", ["gravity", "coulomb", "plummer"])
+def test_fp64_step_within_1e13_of_quad(case):
+    """With the near-unit-eccentricity pairs on the universal-variable solver and the
+    unconverged iterations re-solved, the FP64 step is within 1e-13 of the exact step."""
+    from bia_3d_gpu_b200 import initial
+    if case == "gravity":
+        (s, eps), q, dt = initial.gravity_ball(160, seed=41), None, 1e-4
+    elif case == "coulomb":
+        s, eps, q = initial.coulomb_cube(160, seed=42)
+        dt = 1e-5
+    else:
+        (s, eps), q, dt = initial.plummer(160, seed=43), None, 1e-4
+    a, _, st = oracle.bia_step(s, eps, dt, q=q)
+    b, _, _ = oracle.bia_step(s, eps, dt, q=q, quad=True)
+    assert rel_err(a[:3], b[:3]) <= 1e-13 and max_rel_err(a[:3], b[:3]) <= 1e-13
+    assert rel_err(a[3:], b[3:]) <= 1e-13 and max_rel_err(a[3:], b[3:]) <= 1e-13
+
+
+def test_universal_variables_match_quad_classical():
+    """Universal-variable solver (FP64) against the classical formulas evaluated in quad:
+    agreement to 1e-12 of the displacement itself on random pairs of every class."""
+    rng = np.random.default_rng(8)
+    worst = 0.0
+    for _ in range(300):
+        eps = -10 ** rng.uniform(-4, 0.5) * rng.choice([1, 1, -1])
+        r = rng.standard_normal(3) * 10 ** rng.uniform(-1, 0.3)
+        g = rng.standard_normal(3) * 10 ** rng.uniform(-1.5, 0.5)
+        dt = 10 ** rng.uniform(-6, -1.5)
+        hq, _ = oracle.pair_halfdisp(r, g, eps, dt, quad=True)
+        hu, st = oracle.pair_halfdisp(r, g, eps, dt, method=2)
+        assert st["universal"] == 1
+        worst = max(worst, np.abs(hu - hq).max() / np.abs(hq).max())
+    assert worst <= 1e-12
+
+
+def test_near_parabolic_bound_pair_regression():
+    """A barely bound pair (W = -3.6e-5, eps = -2): the reference's ellipse formulas give a
+    displacement of 1e4 in dt = 1e-5; the guarded path matches the exact step."""
+    YZ = np.array([0.3191676, 0.61635585, 0.0, 2.40060326])
+    eps = -2.0
+    r_abs = np.hypot(YZ[0], YZ[1])
+    # set |g| so that W = g^2 + 2 eps / r = -3.6e-5
+    gm = np.sqrt(-2 * eps / r_abs - 3.6e-5)
+    r = np.array([YZ[0], YZ[1], 0.0])
+    g = np.array([0.0, gm, 0.0])
+    h, st = oracle.pair_halfdisp(r, g, eps, 1e-5)
+    hq, _ = oracle.pair_halfdisp(r, g, eps, 1e-5, quad=True)
+    hr, _ = oracle.pair_halfdisp(r, g, eps, 1e-5, method=0, quad=True)
+    assert st["universal"] == 1
+    assert np.abs(h - hq).max() <= 1e-12 * np.abs(hq).max()
+    assert np.abs(hq - hr).max() <= 1e-9 * np.abs(hq).max()
+
+
+def test_unconverged_ellipse_is_resolved():
+    """Pair (365, 179) of coulomb_cube(400, seed 22), a bound pair with e close to 1:
+    the reference's Kepler Newton starts from xi_2 + delta_ini (bia/find_ellipse.f90:
+    125-129) and ends at ITR unconverged with a displacement of order 10.  The raw
+    ellipse branch flags it and re-solves Kepler's equation by bisection-safeguarded
+    Newton; the whole pair path sends it to the universal-variable solver
+    (|e^2 - 1| < 0.1).  Both agree with the quad-precision per-pair RKF45."""
+    from bia_3d_gpu_b200 import initial
+    s, eps, q = initial.coulomb_cube(400, seed=22, dmin=1e-3)
+    r = s[:3, 365] - s[:3, 179]
+    g = s[3:, 365] - s[3:, 179]
+    e = eps * q[365] * q[179]
+    h, st = oracle.pair_halfdisp(r, g, e, 1e-5)
+    hr, _ = oracle.pair_halfdisp(r, g, e, 1e-5, method=0, quad=True)
+    assert st["universal"] == 1
+    assert np.abs(h - hr).max() <= 1e-9 * np.abs(hr).max()
+    _, _, _, YZ, _ = oracle.frame(r, g)
+    YN, _, it, fb = oracle.find_ellipse(e, 1e-5, YZ, return_fallback=True)
+    YR, _, ier, _ = oracle.find_dxyuv_rkf(e, 1e-5, YZ)
+    assert fb == 1 and ier == 0
+    assert np.abs(YN - YR).max() <= 1e-9 * np.abs(YZ).max()
+
+
+def test_attractive_hyperbola_bracket_fallback():
+    """An attractive hyperbola whose reference iterate leaves (-theta_0, theta_0)
+    (bia/find_hyperbola.f90:98-101): the raw hyperbola branch re-solves the time
+    equation by bracketed Newton (decreasing in theta for eps < 0) and matches the
+    per-pair RKF45; the pair path sends it to the universal-variable solver
+    (|e^2 - 1| = 0.03), which matches as well."""
+    r = np.array([0.05477136, 0.29190468, 0.0])
+    g = np.array([0.0, 4.50440845, 0.0])
+    eps, dt = -2.54, 0.0534
+    _, _, _, YZ, _ = oracle.frame(r, g)
+    YN, _, it, fb = oracle.find_hyperbola(eps, dt, YZ, return_fallback=True)
+    YR, _, ier, _ = oracle.find_dxyuv_rkf(eps, dt, YZ)
+    assert fb == 1 and ier == 0
+    assert np.abs(YN - YR).max() <= 1e-8 * np.abs(YZ).max()
+    h, st = oracle.pair_halfdisp(r, g, eps, dt)
+    hr, _ = oracle.pair_halfdisp(r, g, eps, dt, method=0, quad=True)
+    assert st["universal"] == 1
+    assert np.abs(h - hr).max() <= 1e-8 * np.abs(hr).max()
