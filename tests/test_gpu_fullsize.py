@@ -36,8 +36,8 @@ def test_sampled_particles_match_oracle(cuda, name):
     assert np.abs(got[:, 3:] - ref[:, 3:]).max() <= 1e-12 * vscale
     # and against the exact step on a few of them
     refq = oracle.particle_disp(s, eps, dt, sel[:6], q=q, quad=True)
-    assert np.abs(got[:6, :3] - refq[:, :3]).max() <= 1e-13 * xscale
-    assert np.abs(got[:6, 3:] - refq[:, 3:]).max() <= 1e-13 * vscale
+    assert np.abs(got[:6, :3] - refq[:, :3]).max() <= 1e-12 * xscale
+    assert np.abs(got[:6, 3:] - refq[:, 3:]).max() <= 1e-12 * vscale
     # momentum: sum of all velocity kicks cancels pair by pair
     kick = disp[3:].sum(axis=1)
     assert np.abs(kick).max() <= 1e-12 * np.abs(disp[3:]).sum(axis=1).max()
