@@ -83,6 +83,8 @@ def lib():
     L.bia_invariance.argtypes = [_V, _I, _D] + [_V] * 7 + [_PD]
     L.bia_measure_fp64_peak.argtypes = [_I, _PD]
     L.bia_context_stats.argtypes = [_V, ctypes.POINTER(BiaStats), _I]
+    L.bia_step_noalloc.argtypes = [ctypes.POINTER(BiaConfig), _I] + [_V] * 9
+    L.bia_step_noalloc.restype = _I
     L.find_dxyuv_kernel_.argtypes = [_I, _I, _I, _D, _D, _I] + [_PD] * 8
     L.find_dxyuv_kernel_.restype = None
     L.invariance_gpu_.argtypes = [_I, _D] + [_PD] * 6 + [_PD] * 11

@@ -28,6 +28,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 
 #include "bia_internal.cuh"
 #include "bia_pair.cuh"
@@ -564,3 +565,97 @@ int bia_run_host(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
 }
 
 }  // extern "C"
+
+// ----------------------------------------------------------------------------------
+// Allocation-free BIA step.
+//
+// Some callers cannot allocate device memory once they are running: a host process
+// whose GPU memory is handed out by another framework's pool up front, a real-time
+// loop that must not touch the CUDA allocator, or code that enqueues work where a
+// cudaMalloc would synchronise or fail.  For them the step's scratch (the
+// deterministic per-block partial sums and the step counters) lives in a file-scope
+// __device__ array of fixed size instead of a context's buffers, so one call only
+// enqueues kernels and a memset on the caller's stream.
+//
+// Limit: n <= kNoAllocMaxN = 2048 particles (partials nb x 6 x 2048 doubles with
+// nb = 64: 6 MiB, plus 256 bytes of counters).  Every GPU that loads this library
+// holds the array until the process exits.
+namespace bia {
+
+constexpr int kNoAllocMaxN = 2048;
+constexpr int kNoAllocNb = kNoAllocMaxN / 32;
+constexpr size_t kNoAllocPartDoubles = (size_t)kNoAllocNb * 6 * kNoAllocMaxN;
+constexpr int kNoAllocMaxDevices = 64;
+
+// Partials first, then the counters (32 doubles of room for kNumStats u64).
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocPartDoubles + 32];
+
+// Device address of g_noalloc_scratch per device ordinal.  The host-side name of the
+// array is only a stand-in: it must be resolved with cudaGetSymbolAddress while the
+// device is current.
+static double *g_noalloc_addr[kNoAllocMaxDevices] = {};
+static std::mutex g_noalloc_mutex;
+
+static int noalloc_scratch(double **out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return BIA_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_status(e);
+        g_noalloc_addr[dev] = (double *)p;
+    }
+    *out = g_noalloc_addr[dev];
+    return BIA_OK;
+}
+
+}  // namespace bia
+
+extern "C" int bia_step_noalloc(const bia_config *cfg, int n, double *x, double *y, double *z, double *u,
+                                double *v, double *w, const double *q, double *disp, void *stream)
+{
+    int st = validate(cfg, n, x, y, z, u, v, w);
+    if (st != BIA_OK) return st;
+    if (n > kNoAllocMaxN) return BIA_ERR_INVALID_ARGUMENT;  // beyond the fixed scratch
+    double *part = nullptr;
+    st = noalloc_scratch(&part);
+    if (st != BIA_OK) return st;
+    unsigned long long *counters = (unsigned long long *)(part + kNoAllocPartDoubles);
+    cudaStream_t s = (cudaStream_t)stream;
+    // the partials are fully rewritten by every step; only the counters start at zero
+    cudaError_t e = cudaMemsetAsync(counters, 0, kNumStats * sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return cuda_status(e);
+    const int nb = (n + 31) / 32;
+    StepArgs A;
+    A.x = x; A.y = y; A.z = z; A.u = u; A.v = v; A.w = w; A.q = q;
+    A.part = part;
+    A.stats = counters;
+    A.n = n;
+    A.nb = nb;
+    A.npad = nb * 32;
+    A.nwb = (long long)nb * (nb + 1) / 2;
+    A.eps_th = cfg->eps_th;
+    A.P.dt = cfg->dt;
+    A.P.err = cfg->err;
+    A.P.relerr = cfg->rkf_relerr;
+    A.P.abserr = cfg->rkf_abserr;
+    A.P.itr = cfg->itr;
+    A.P.method = cfg->method;
+    const long long grid = (A.nwb + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    bia_pair_tiles_kernel<true><<<(unsigned)grid, kThreads, 0, s>>>(A);
+    UpdateArgs U;
+    U.x = x; U.y = y; U.z = z; U.u = u; U.v = v; U.w = w;
+    U.part = part;
+    U.disp = disp;
+    U.n = n;
+    U.nb = nb;
+    U.npad = nb * 32;
+    U.nparts = nb;
+    U.dt = cfg->dt;
+    bia_reduce_update_kernel<<<(n + 255) / 256, 256, 0, s>>>(U);
+    return cuda_status(cudaGetLastError());
+}

@@ -110,6 +110,21 @@ int bia_run_host(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
                  double *z, double *u, double *v, double *w, const double *q, int nsteps,
                  bia_stats *stats);
 
+/* Allocation-free form of bia_step, for callers that cannot allocate device memory once
+   they run (a framework that owns the GPU's memory pool, a real-time loop that must not
+   enter the CUDA allocator).  No counterpart in the reference.  The step's scratch is a
+   fixed array inside the library (6 MiB per GPU that loads it, held until exit) instead
+   of a bia_context, so n must be <= 2048; larger n returns BIA_ERR_INVALID_ARGUMENT.
+   The caller passes device state (updated in place), optional charges q and optional
+   disp [6][n]; kernels and one memset are enqueued on `stream` (a cudaStream_t, NULL =
+   legacy default stream) and the call returns without synchronising.  The reduction is
+   always the deterministic one (cfg->deterministic is ignored); no counters are returned.
+   The first call on a device resolves the array's device address (cudaGetSymbolAddress),
+   so make that first call before any stream capture.  All calls share the one array:
+   calls whose work overlaps on the GPU (different streams, or host threads) race. */
+int bia_step_noalloc(const bia_config *cfg, int n, double *x, double *y, double *z, double *u,
+                     double *v, double *w, const double *q, double *disp, void *stream);
+
 /* Invariants of device SoA state (bia/invariance.cu:50-110 semantics, FP64):
    out[11] = {KE, PE, Lx, Ly, Lz, Ua, Va, Wa, Xa, Ya, Za} on the host.
    KE = sum |v|^2, PE = eps_th * sum_{i<j} (q_i q_j) / r_ij. */
