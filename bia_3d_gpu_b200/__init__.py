@@ -74,6 +74,35 @@ def invariance_gpu(N, eps_th, X, Y, Z, U, V, W):
     return tuple(o.value for o in outs)
 
 
+def rkf_c(neq, eps_th, X0, XE, YH0, INIT, RELERR, ABSERR):
+    """Direct-integration run on the GPU, mirroring rkf_c_ (dim/rkf_kernel.cu:194-495) as
+    called from dim/dim_3D.f90:30.  YH0: host AoS state (neq = 6n float64), updated to
+    the final state.  Returns a dict with YHN, ESE, NDE, IER, H, X0 (= XE), INIT."""
+    L = capi.lib()
+    n = int(neq)
+    x0 = ctypes.c_double(X0)
+    xe = ctypes.c_double(XE)
+    init = ctypes.c_int(INIT)
+    rel = ctypes.c_double(RELERR)
+    abs_ = ctypes.c_double(ABSERR)
+    nde = ctypes.c_int(0)
+    ier = ctypes.c_int(0)
+    h = ctypes.c_double(0.0)
+    yh0 = np.ascontiguousarray(YH0, dtype=np.float64)
+    outs = {k: np.zeros(n) for k in ("YHN", "ESE", "YL0", "YLN", "ERR")}
+    _host_f64(yh0, n, "YH0")
+    L.rkf_c_(n, float(eps_th), ctypes.byref(x0), ctypes.byref(xe), yh0.ctypes.data_as(_PD),
+             ctypes.byref(init), ctypes.byref(rel), ctypes.byref(abs_),
+             outs["YHN"].ctypes.data_as(_PD), outs["ESE"].ctypes.data_as(_PD), ctypes.byref(nde),
+             ctypes.byref(ier), ctypes.byref(h), outs["YL0"].ctypes.data_as(_PD),
+             outs["YLN"].ctypes.data_as(_PD), outs["ERR"].ctypes.data_as(_PD), None)
+    st = L.bia_last_error()
+    if st not in (BIA_OK, capi.BIA_ERR_NOT_CONVERGED):
+        raise BiaError(st, "rkf_c")
+    return dict(outs, NDE=nde.value, IER=ier.value, H=h.value, X0=x0.value, INIT=init.value,
+                YH0=yh0)
+
+
 def measure_fp64_peak(device=0):
     """Measured FP64 FMA throughput of the device in TFLOP/s."""
     out = ctypes.c_double(0.0)
@@ -226,6 +255,26 @@ class BIASolver:
         st = capi.lib().bia_context_stats(self._ctx, ctypes.byref(s), int(bool(reset)))
         return self._finish(st, s, "bia_context_stats")
 
+    def dim_integrate(self, state, eps_th, x0, xe, relerr=0.0, abserr=1e-16):
+        """Direct-integration reference solver (dim/rkf_kernel.cu) on the device state,
+        advanced in place from x0 to xe.  eps_th is the per-particle coupling of
+        dim/dim_3D.f90 (half the BIA pair coupling).  Returns the step counters."""
+        n = self._check_state(state)
+        st_ = capi.BiaDimStats()
+        cur = self._enter()
+        st = capi.lib().bia_dim_integrate(self._ctx, n, float(eps_th), ctypes.c_void_p(state.data_ptr()),
+                                          float(x0), float(xe), float(relerr), float(abserr),
+                                          ctypes.byref(st_))
+        self._leave(cur)
+        if st not in (BIA_OK, capi.BIA_ERR_NOT_CONVERGED):
+            raise BiaError(st, "bia_dim_integrate")
+        return st_.as_dict()
+
+    def ensemble(self, sizes, eps):
+        """An ensemble of independent systems (sizes[s] particles, pair coupling eps[s])
+        stored back to back; returns an Ensemble bound to this solver."""
+        return Ensemble(self, sizes, eps)
+
     def set_timing(self, on):
         capi.check(capi.lib().bia_context_set_timing(self._ctx, int(bool(on))))
 
@@ -235,3 +284,60 @@ class BIASolver:
         cnt = ctypes.c_longlong(0)
         capi.check(capi.lib().bia_context_kernel_ms(self._ctx, ctypes.byref(ms), ctypes.byref(cnt)))
         return ms.value, cnt.value
+
+
+class Ensemble:
+    """Independent systems of uneven size advanced together (bia_ensemble_*).  The state
+    is one (6, sum(sizes)) float64 CUDA tensor with the systems back to back."""
+
+    def __init__(self, solver, sizes, eps):
+        self.solver = solver
+        self.sizes = np.ascontiguousarray(sizes, dtype=np.int32)
+        self.eps = np.ascontiguousarray(eps, dtype=np.float64)
+        if self.sizes.shape != self.eps.shape:
+            raise ValueError("sizes and eps must have one entry per system")
+        self.nsys = int(self.sizes.size)
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)])
+        self._ens = ctypes.c_void_p()
+        capi.check(capi.lib().bia_ensemble_create(
+            solver._ctx, self.nsys, self.sizes.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+            self.eps.ctypes.data_as(_PD), ctypes.byref(self._ens)), "bia_ensemble_create")
+
+    def close(self):
+        if self._ens:
+            capi.lib().bia_ensemble_destroy(self._ens)
+            self._ens = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, state, cfg, nsteps, q=None, graph=True, stats=True):
+        s = self.solver
+        n = s._check_state(state)
+        if n != int(self.offsets[-1]):
+            raise ValueError("state does not hold sum(sizes) particles")
+        st_ = BiaStats()
+        cur = s._enter()
+        st = capi.lib().bia_ensemble_run(s._ctx, self._ens, ctypes.byref(cfg), *s._ptrs(state),
+                                         s._qptr(q, n), int(nsteps), int(bool(graph)),
+                                         ctypes.byref(st_) if stats else None)
+        s._leave(cur)
+        if not stats:
+            capi.check(st, "bia_ensemble_run")
+            return None
+        return s._finish(st, st_, "bia_ensemble_run")
+
+    def energy(self, state, q=None):
+        """(KE, PE) arrays per system: KE = sum |v|^2, PE = eps_s sum_{i<j} (q_i q_j)/r_ij."""
+        s = self.solver
+        n = s._check_state(state)
+        out = np.zeros(2 * self.nsys)
+        cur = s._enter()
+        st = capi.lib().bia_ensemble_energy(s._ctx, self._ens, *s._ptrs(state), s._qptr(q, n),
+                                            out.ctypes.data_as(_PD))
+        s._leave(cur)
+        capi.check(st, "bia_ensemble_energy")
+        return out[0::2].copy(), out[1::2].copy()

@@ -42,6 +42,15 @@ class BiaStats(ctypes.Structure):
         return {name: int(getattr(self, name)) for name in STAT_FIELDS}
 
 
+class BiaDimStats(ctypes.Structure):
+    _fields_ = [("accepted", ctypes.c_longlong), ("rejected", ctypes.c_longlong),
+                ("nde", ctypes.c_int), ("ier", ctypes.c_int), ("h_last", ctypes.c_double),
+                ("x_reached", ctypes.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class BiaError(RuntimeError):
     def __init__(self, status, what=""):
         self.status = status
@@ -85,6 +94,22 @@ def lib():
     L.bia_context_stats.argtypes = [_V, ctypes.POINTER(BiaStats), _I]
     L.bia_step_noalloc.argtypes = [ctypes.POINTER(BiaConfig), _I] + [_V] * 9
     L.bia_step_noalloc.restype = _I
+    L.bia_ensemble_create.argtypes = [_V, _I, ctypes.POINTER(ctypes.c_int), _PD, ctypes.POINTER(_V)]
+    L.bia_ensemble_destroy.argtypes = [_V]
+    L.bia_ensemble_particles.argtypes = [_V]
+    L.bia_ensemble_particles.restype = ctypes.c_longlong
+    L.bia_ensemble_run.argtypes = ([_V, _V, ctypes.POINTER(BiaConfig)] + [_V] * 7 +
+                                   [_I, _I, ctypes.POINTER(BiaStats)])
+    L.bia_ensemble_energy.argtypes = [_V, _V] + [_V] * 7 + [_PD]
+    for name in ("bia_ensemble_create", "bia_ensemble_destroy", "bia_ensemble_run",
+                 "bia_ensemble_energy"):
+        getattr(L, name).restype = _I
+    L.bia_dim_integrate.argtypes = [_V, _I, _D, _V, _D, _D, _D, _D, ctypes.POINTER(BiaDimStats)]
+    L.bia_dim_integrate.restype = _I
+    _PI = ctypes.POINTER(ctypes.c_int)
+    L.rkf_c_.argtypes = [_I, _D, _PD, _PD, _PD, _PI, _PD, _PD, _PD, _PD, _PI, _PI, _PD, _PD, _PD,
+                         _PD, _PD]
+    L.rkf_c_.restype = None
     L.find_dxyuv_kernel_.argtypes = [_I, _I, _I, _D, _D, _I] + [_PD] * 8
     L.find_dxyuv_kernel_.restype = None
     L.invariance_gpu_.argtypes = [_I, _D] + [_PD] * 6 + [_PD] * 11
@@ -122,5 +147,7 @@ def default_config(**overrides):
 EXPORTED_SYMBOLS = ("bia_config_default", "bia_context_create", "bia_context_destroy",
                     "bia_context_set_stream", "bia_context_set_timing", "bia_context_kernel_ms",
                     "bia_step", "bia_run", "bia_run_host", "bia_invariance", "bia_status_string",
-                    "bia_measure_fp64_peak", "bia_context_stats",
+                    "bia_measure_fp64_peak", "bia_context_stats", "bia_dim_integrate", "rkf_c_",
+                    "bia_ensemble_create", "bia_ensemble_destroy", "bia_ensemble_particles",
+                    "bia_ensemble_run", "bia_ensemble_energy",
                     "bia_last_error", "find_dxyuv_kernel_", "invariance_gpu_")

@@ -1,0 +1,373 @@
+// bia_ensemble.cu -- many independent BIA systems of uneven size in one launch per step.
+//
+// The systems are stored back to back in one set of SoA arrays: system s owns particles
+// [off[s], off[s] + n_s) and has pair coupling eps[s] (gravity: -2/n_s for G = 1 and
+// masses 1/n_s).  At creation the host lists every 32 x 32 warp-block of every system's
+// upper triangle as one work item (system, bi, bj); a step is then one launch of the pair
+// kernel over the whole item table -- the same per-warp-block code as the single-system
+// step (bia_tiles.cuh), so each system's result is identical to a bia_step of that system
+// alone -- plus one reduction launch over all particles.  bia_ensemble_run captures the
+// step sequence in a CUDA graph.  Per-system partial sums use the single-system layout at
+// offset part_off[s]: [nb_s][6][32 nb_s] doubles.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "bia_internal.cuh"
+#include "bia_pair.cuh"
+#include "bia_tiles.cuh"
+
+struct bia_ensemble {
+    int nsys = 0;
+    long long nparticles = 0, nitems = 0;
+    int *d_off = nullptr;              // [nsys + 1] particle offsets
+    int *d_psys = nullptr;             // [nparticles] system of each particle
+    long long *d_part_off = nullptr;   // [nsys] partial-buffer offsets (doubles)
+    long long *d_item_off = nullptr;   // [nsys + 1] first item of each system
+    double *d_eps = nullptr;           // [nsys]
+    uint2 *d_items = nullptr;          // [nitems] (system, bi | bj << 16)
+    double *d_part = nullptr;          // partial sums
+    double *d_scratch = nullptr;       // [nitems + nparticles] energy scratch
+    double *d_energy = nullptr;        // [2 nsys] KE, PE per system
+    size_t part_doubles = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    bia::GraphKey graph_key;
+};
+
+namespace bia {
+
+constexpr int kEnsWarps = 8;
+constexpr int kEnsThreads = kEnsWarps * 32;
+
+struct EnsArgs {
+    const double *x, *y, *z, *u, *v, *w, *q;
+    const int *off;
+    const long long *part_off;
+    const double *eps;
+    const uint2 *items;
+    long long nitems;
+    double *part;
+    unsigned long long *stats;
+    PairParams P;
+};
+
+template <int M>
+__global__ void __launch_bounds__(kEnsThreads, TileOccupancy<M>::kMinBlocks) ens_pair_tiles_kernel(const EnsArgs A)
+{
+    const int lane = threadIdx.x & 31;
+    const long long t = (long long)blockIdx.x * kEnsWarps + (threadIdx.x >> 5);
+    if (t >= A.nitems) return;  // warp-uniform
+    const uint2 it = A.items[t];
+    const int s = (int)it.x;
+    const int bi = (int)(it.y & 0xffffu), bj = (int)(it.y >> 16);
+    const int base = A.off[s];
+    const int n = A.off[s + 1] - base;
+    const double *q = A.q ? A.q + base : nullptr;
+    double racc[6], cacc[6];
+    PairCounters cnt;
+    warp_block_solve<M>(A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base, q, n,
+                            A.eps[s], A.P, bi, bj, lane, racc, cacc, cnt);
+    flush_counters(cnt, A.stats, lane);
+    const int nb = (n + 31) / 32;
+    write_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
+}
+
+struct EnsUpdateArgs {
+    double *x, *y, *z, *u, *v, *w;
+    const int *off, *psys;
+    const long long *part_off;
+    const double *part;
+    long long nparticles;
+    double dt;
+};
+
+// fixed-order partial sums, drift and update (bia/bia.f90:194-204), all systems at once
+__global__ void __launch_bounds__(256) ens_reduce_update_kernel(const EnsUpdateArgs A)
+{
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= A.nparticles) return;
+    const int s = A.psys[p];
+    const int base = A.off[s];
+    const int n = A.off[s + 1] - base;
+    const int nb = (n + 31) / 32;
+    const size_t plane = (size_t)nb * 32;
+    const double *src = A.part + A.part_off[s] + (p - base);
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int m = 0; m < nb; m++) {
+#pragma unroll
+        for (int c = 0; c < 6; c++) acc[c] += src[((size_t)m * 6 + c) * plane];
+    }
+    const double u = A.u[p], v = A.v[p], w = A.w[p];
+    A.x[p] = A.x[p] + (acc[0] + u * A.dt);
+    A.y[p] = A.y[p] + (acc[1] + v * A.dt);
+    A.z[p] = A.z[p] + (acc[2] + w * A.dt);
+    A.u[p] = u + acc[3];
+    A.v[p] = v + acc[4];
+    A.w[p] = w + acc[5];
+}
+
+// per-item pair sums sum (q_i q_j) / r_ij of each system (energy)
+__global__ void __launch_bounds__(kEnsThreads) ens_pe_items_kernel(const double *x, const double *y, const double *z,
+                                                                    const double *q, const int *off,
+                                                                    const uint2 *items, long long nitems,
+                                                                    double *out)
+{
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const long long t = (long long)blockIdx.x * kEnsWarps + (threadIdx.x >> 5);
+    if (t >= nitems) return;
+    const uint2 it = items[t];
+    const int s = (int)it.x;
+    const int bi = (int)(it.y & 0xffffu), bj = (int)(it.y >> 16);
+    const int base = off[s];
+    const int n = off[s + 1] - base;
+    const int i = bi * 32 + lane, jo = bj * 32 + lane;
+    const bool iv = i < n, jv = jo < n;
+    const double xi = iv ? x[base + i] : 0.0, yi = iv ? y[base + i] : 0.0, zi = iv ? z[base + i] : 0.0;
+    const double qi = (iv && q) ? q[base + i] : 1.0;
+    const double xj = jv ? x[base + jo] : 0.0, yj = jv ? y[base + jo] : 0.0, zj = jv ? z[base + jo] : 0.0;
+    const double qj = (jv && q) ? q[base + jo] : 1.0;
+    const bool diag = bi == bj;
+    double acc = 0.0;
+    for (int k = diag ? 1 : 0; k <= (diag ? 16 : 31); k++) {
+        const int src = (lane + k) & 31;
+        const double cx = __shfl_sync(full, xj, src), cy = __shfl_sync(full, yj, src);
+        const double cz = __shfl_sync(full, zj, src), cq = __shfl_sync(full, qj, src);
+        if ((!diag || k < 16 || lane < 16) && iv && bj * 32 + src < n) {
+            const double dx = xi - cx, dy = yi - cy, dz = zi - cz;
+            const double wgt = 1.0 / sqrt(dx * dx + dy * dy + dz * dz);
+            acc += q ? qi * cq * wgt : wgt;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(full, acc, o);
+    if (lane == 0) out[t] = acc;
+}
+
+// one block per system: KE = sum |v|^2 over its particles, PE = eps_s * (ordered sum of
+// its items' pair sums)
+__global__ void __launch_bounds__(256) ens_energy_kernel(const double *u, const double *v, const double *w,
+                                                         const int *off, const long long *item_off,
+                                                         const double *eps, const double *item_pe, double *energy)
+{
+    __shared__ double sh[2][256];
+    const int s = blockIdx.x;
+    double ke = 0.0, pe = 0.0;
+    for (int p = off[s] + threadIdx.x; p < off[s + 1]; p += blockDim.x) ke += u[p] * u[p] + v[p] * v[p] + w[p] * w[p];
+    for (long long t = item_off[s] + threadIdx.x; t < item_off[s + 1]; t += blockDim.x) pe += item_pe[t];
+    sh[0][threadIdx.x] = ke;
+    sh[1][threadIdx.x] = pe;
+    __syncthreads();
+    for (int k = 128; k > 0; k >>= 1) {
+        if (threadIdx.x < k) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + k];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + k];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        energy[2 * s] = sh[0][0];
+        energy[2 * s + 1] = eps[s] * sh[1][0];
+    }
+}
+
+static int ens_enqueue_step(bia_context *ctx, bia_ensemble *E, const bia_config *cfg, double *x, double *y,
+                            double *z, double *u, double *v, double *w, const double *q)
+{
+    EnsArgs A;
+    A.x = x; A.y = y; A.z = z; A.u = u; A.v = v; A.w = w; A.q = q;
+    A.off = E->d_off;
+    A.part_off = E->d_part_off;
+    A.eps = E->d_eps;
+    A.items = E->d_items;
+    A.nitems = E->nitems;
+    A.part = E->d_part;
+    A.stats = (unsigned long long *)ctx->stats.ptr;
+    A.P.dt = cfg->dt;
+    A.P.err = cfg->err;
+    A.P.relerr = cfg->rkf_relerr;
+    A.P.abserr = cfg->rkf_abserr;
+    A.P.itr = cfg->itr;
+    A.P.method = cfg->method;
+    const unsigned grid = (unsigned)((E->nitems + kEnsWarps - 1) / kEnsWarps);
+    switch (cfg->method) {
+    case BIA_METHOD_RKF: ens_pair_tiles_kernel<kMethodRkf><<<grid, kEnsThreads, 0, ctx->stream>>>(A); break;
+    case BIA_METHOD_UNIVERSAL:
+        ens_pair_tiles_kernel<kMethodUniversal><<<grid, kEnsThreads, 0, ctx->stream>>>(A);
+        break;
+    default: ens_pair_tiles_kernel<kMethodAlg><<<grid, kEnsThreads, 0, ctx->stream>>>(A); break;
+    }
+    EnsUpdateArgs U;
+    U.x = x; U.y = y; U.z = z; U.u = u; U.v = v; U.w = w;
+    U.off = E->d_off;
+    U.psys = E->d_psys;
+    U.part_off = E->d_part_off;
+    U.part = E->d_part;
+    U.nparticles = E->nparticles;
+    U.dt = cfg->dt;
+    ens_reduce_update_kernel<<<(unsigned)((E->nparticles + 255) / 256), 256, 0, ctx->stream>>>(U);
+    return cuda_status(cudaGetLastError());
+}
+
+static void ens_free(bia_ensemble *E)
+{
+    if (!E) return;
+    if (E->graph_exec) cudaGraphExecDestroy(E->graph_exec);
+    if (E->graph) cudaGraphDestroy(E->graph);
+    cudaFree(E->d_off);
+    cudaFree(E->d_psys);
+    cudaFree(E->d_part_off);
+    cudaFree(E->d_item_off);
+    cudaFree(E->d_eps);
+    cudaFree(E->d_items);
+    cudaFree(E->d_part);
+    cudaFree(E->d_scratch);
+    cudaFree(E->d_energy);
+    delete E;
+}
+
+}  // namespace bia
+
+using namespace bia;
+
+extern "C" int bia_ensemble_create(bia_context *ctx, int nsys, const int *sizes, const double *eps,
+                                   bia_ensemble **out)
+{
+    if (!ctx || !out || nsys < 1 || !sizes || !eps) return BIA_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    cudaSetDevice(ctx->device);
+    std::vector<int> off(nsys + 1, 0);
+    std::vector<long long> part_off(nsys), item_off(nsys + 1, 0);
+    size_t part = 0;
+    for (int s = 0; s < nsys; s++) {
+        if (sizes[s] < 1 || sizes[s] > 32 * 65535) return BIA_ERR_INVALID_ARGUMENT;
+        if ((long long)off[s] + sizes[s] > (1LL << 30)) return BIA_ERR_INVALID_ARGUMENT;
+        off[s + 1] = off[s] + sizes[s];
+        const long long nb = (sizes[s] + 31) / 32;
+        part_off[s] = (long long)part;
+        part += (size_t)nb * 6 * nb * 32;
+        item_off[s + 1] = item_off[s] + nb * (nb + 1) / 2;
+    }
+    const long long np = off[nsys], nitems = item_off[nsys];
+    std::vector<uint2> items((size_t)nitems);
+    for (int s = 0; s < nsys; s++) {
+        const int nb = (sizes[s] + 31) / 32;
+        long long t = item_off[s];
+        for (int bj = 0; bj < nb; bj++)
+            for (int bi = 0; bi <= bj; bi++) items[(size_t)t++] = make_uint2((unsigned)s, (unsigned)bi | ((unsigned)bj << 16));
+    }
+    std::vector<int> psys((size_t)np);
+    for (int s = 0; s < nsys; s++)
+        for (int p = off[s]; p < off[s + 1]; p++) psys[(size_t)p] = s;
+    bia_ensemble *E = new bia_ensemble();
+    E->nsys = nsys;
+    E->nparticles = np;
+    E->nitems = nitems;
+    E->part_doubles = part;
+    cudaError_t e = cudaSuccess;
+#define ENS_ALLOC(ptr, count)                                                        \
+    if (e == cudaSuccess) e = cudaMalloc((void **)&(ptr), sizeof(*(ptr)) * (size_t)(count))
+    ENS_ALLOC(E->d_off, nsys + 1);
+    ENS_ALLOC(E->d_psys, np);
+    ENS_ALLOC(E->d_part_off, nsys);
+    ENS_ALLOC(E->d_item_off, nsys + 1);
+    ENS_ALLOC(E->d_eps, nsys);
+    ENS_ALLOC(E->d_items, nitems);
+    ENS_ALLOC(E->d_part, part);
+    ENS_ALLOC(E->d_scratch, nitems);
+    ENS_ALLOC(E->d_energy, 2 * nsys);
+#undef ENS_ALLOC
+    if (e == cudaSuccess) e = cudaMemcpy(E->d_off, off.data(), sizeof(int) * (nsys + 1), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(E->d_psys, psys.data(), sizeof(int) * np, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(E->d_part_off, part_off.data(), sizeof(long long) * nsys, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(E->d_item_off, item_off.data(), sizeof(long long) * (nsys + 1), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(E->d_eps, eps, sizeof(double) * nsys, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(E->d_items, items.data(), sizeof(uint2) * nitems, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = ctx->stats.reserve(kNumStats * sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        ens_free(E);
+        return cuda_status(e);
+    }
+    *out = E;
+    return BIA_OK;
+}
+
+extern "C" int bia_ensemble_destroy(bia_ensemble *ens)
+{
+    ens_free(ens);
+    return BIA_OK;
+}
+
+extern "C" long long bia_ensemble_particles(const bia_ensemble *ens) { return ens ? ens->nparticles : 0; }
+
+extern "C" int bia_ensemble_run(bia_context *ctx, bia_ensemble *E, const bia_config *cfg, double *x, double *y,
+                                double *z, double *u, double *v, double *w, const double *q, int nsteps,
+                                int use_graph, bia_stats *stats)
+{
+    if (!ctx || !E || !cfg || !x || !y || !z || !u || !v || !w || nsteps < 0) return BIA_ERR_INVALID_ARGUMENT;
+    if (cfg->method != BIA_METHOD_ALG && cfg->method != BIA_METHOD_RKF && cfg->method != BIA_METHOD_UNIVERSAL)
+        return BIA_ERR_INVALID_ARGUMENT;
+    if (cfg->itr < 1 || cfg->itr > 62) return BIA_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaSuccess;
+    if (stats) {
+        e = cudaMemsetAsync(ctx->stats.ptr, 0, kNumStats * sizeof(unsigned long long), ctx->stream);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    if (use_graph && ctx->stream && nsteps > 0) {
+        GraphKey key;
+        key.n = (int)E->nparticles; key.nsteps = nsteps; key.method = cfg->method; key.itr = cfg->itr;
+        key.deterministic = 1; key.eps = 0.0; key.dt = cfg->dt; key.err = cfg->err;
+        key.relerr = cfg->rkf_relerr; key.abserr = cfg->rkf_abserr;
+        const void *p[7] = {x, y, z, u, v, w, q};
+        for (int k = 0; k < 7; k++) key.ptrs[k] = p[k];
+        if (!E->graph_exec || !(key == E->graph_key)) {
+            if (E->graph_exec) cudaGraphExecDestroy(E->graph_exec);
+            if (E->graph) cudaGraphDestroy(E->graph);
+            E->graph_exec = nullptr;
+            E->graph = nullptr;
+            e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return cuda_status(e);
+            int st = BIA_OK;
+            for (int s = 0; s < nsteps && st == BIA_OK; s++) st = ens_enqueue_step(ctx, E, cfg, x, y, z, u, v, w, q);
+            e = cudaStreamEndCapture(ctx->stream, &E->graph);
+            if (st != BIA_OK) return st;
+            if (e != cudaSuccess) return cuda_status(e);
+            e = cudaGraphInstantiate(&E->graph_exec, E->graph, 0);
+            if (e != cudaSuccess) return cuda_status(e);
+            E->graph_key = key;
+        }
+        e = cudaGraphLaunch(E->graph_exec, ctx->stream);
+        if (e != cudaSuccess) return cuda_status(e);
+    } else {
+        for (int s = 0; s < nsteps; s++) {
+            int st = ens_enqueue_step(ctx, E, cfg, x, y, z, u, v, w, q);
+            if (st != BIA_OK) return st;
+        }
+    }
+    if (stats) return bia_context_stats(ctx, stats, 0);
+    return cuda_status(cudaGetLastError());
+}
+
+extern "C" int bia_ensemble_energy(bia_context *ctx, bia_ensemble *E, const double *x, const double *y,
+                                   const double *z, const double *u, const double *v, const double *w,
+                                   const double *q, double *energy)
+{
+    if (!ctx || !E || !x || !y || !z || !u || !v || !w || !energy) return BIA_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    const unsigned grid = (unsigned)((E->nitems + kEnsWarps - 1) / kEnsWarps);
+    ens_pe_items_kernel<<<grid, kEnsThreads, 0, ctx->stream>>>(x, y, z, q, E->d_off, E->d_items, E->nitems,
+                                                               E->d_scratch);
+    ens_energy_kernel<<<E->nsys, 256, 0, ctx->stream>>>(u, v, w, E->d_off, E->d_item_off, E->d_eps, E->d_scratch,
+                                                        E->d_energy);
+    cudaError_t e = cudaMemcpyAsync(energy, E->d_energy, sizeof(double) * 2 * E->nsys, cudaMemcpyDeviceToHost,
+                                    ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    return cuda_status(e);
+}

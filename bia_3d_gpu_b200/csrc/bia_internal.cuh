@@ -63,6 +63,8 @@ struct bia_context {
     bia::DeviceBuffer stats;    // kNumStats unsigned long long
     bia::DeviceBuffer state;    // host-path staging: 7 arrays of n
     bia::DeviceBuffer inv;      // invariance partials
+    bia::DeviceBuffer dim;      // DIM integrator work arrays
+    double *h_dim = nullptr;    // pinned scalars of the DIM control loop
     unsigned long long *h_stats = nullptr;  // pinned
     double *h_inv = nullptr;                // pinned
     // kernel timing

@@ -22,6 +22,36 @@ namespace bia {
 
 constexpr double kPi = 3.14159265358979323846264338327950288419716939937510582097494;
 
+// Optional out-of-line FP64 math: each libm call site expands to a long instruction
+// sequence; routing the calls through one copy shrinks the code.  Measured on B200
+// (n = 32768, 3 CTAs/SM): out-of-line math and hyp_eval 204 ms (Coulomb, mixed orbit
+// classes) / 88 ms (Plummer, hyperbolae only) per step, everything inline 213 / 73 ms;
+// inline is the default.
+#ifndef BIA_NOINLINE_MATH
+#define BIA_NOINLINE_MATH 0
+#endif
+#if BIA_NOINLINE_MATH
+static __device__ __noinline__ void d_sincos(double x, double *s, double *c) { sincos(x, s, c); }
+static __device__ __noinline__ double d_log(double x) { return log(x); }
+static __device__ __noinline__ double d_atan2(double y, double x) { return atan2(y, x); }
+static __device__ __noinline__ double d_acos(double x) { return acos(x); }
+static __device__ __noinline__ double d_atan(double x) { return atan(x); }
+#else
+__device__ __forceinline__ void d_sincos(double x, double *s, double *c) { sincos(x, s, c); }
+__device__ __forceinline__ double d_log(double x) { return log(x); }
+__device__ __forceinline__ double d_atan2(double y, double x) { return atan2(y, x); }
+__device__ __forceinline__ double d_acos(double x) { return acos(x); }
+__device__ __forceinline__ double d_atan(double x) { return atan(x); }
+#endif
+#ifndef BIA_NOINLINE_HYPEVAL
+#define BIA_NOINLINE_HYPEVAL 0
+#endif
+#if BIA_NOINLINE_HYPEVAL
+#define BIA_HYPEVAL_INLINE static __device__ __noinline__
+#else
+#define BIA_HYPEVAL_INLINE __device__ __forceinline__
+#endif
+
 enum PairClass { kHyperbola = 0, kParabola = 1, kEllipse = 2, kDegenerate = 3, kRkf = 4, kUniversal = 5 };
 
 // |e^2 - 1| below which ALG pairs use the universal-variable solver
@@ -82,10 +112,10 @@ __device__ __forceinline__ bool frame_xi_eta(const double r[3], const double g[3
         }
         return true;
     }
-    double Lm = sqrt(Lsq);
-    double ez0 = L0 / Lm, ez1 = L1 / Lm, ez2 = L2 / Lm;
+    const double iL = 1.0 / sqrt(Lsq), ig = 1.0 / gm;
+    double ez0 = L0 * iL, ez1 = L1 * iL, ez2 = L2 * iL;
 #pragma unroll
-    for (int k = 0; k < 3; k++) e_eta[k] = g[k] / gm;
+    for (int k = 0; k < 3; k++) e_eta[k] = g[k] * ig;
     e_xi[0] = e_eta[1] * ez2 - e_eta[2] * ez1;
     e_xi[1] = e_eta[2] * ez0 - e_eta[0] * ez2;
     e_xi[2] = e_eta[0] * ez1 - e_eta[1] * ez0;
@@ -98,23 +128,32 @@ __device__ __forceinline__ bool frame_xi_eta(const double r[3], const double g[3
 
 // ---------------------------------------------------------------------------
 // bia/find_hyperbola.f90:1-166.  Returns the main-loop iteration count.
+//
+// The reference's time equation and Newton iteration in theta, evaluated through the
+// half angle: with (sh, ch) = sincos(theta/2) and (s0h, c0h) = sincos(theta_0/2),
+//   sin((theta_0 +- theta)/2) = s0h ch +- c0h sh,  sin theta = 2 sh ch,
+//   cos theta = 1 - 2 sh^2,  cos theta - cos theta_0 = 2 sin((theta_0+theta)/2) sin((theta_0-theta)/2),
+// so one sincos replaces the reference's sin, sin and sincos per evaluation, and the
+// denominator cos theta - cos theta_0 is a product instead of a difference.
 // ---------------------------------------------------------------------------
 struct HypConsts {
-    double theta_0, tn_0, cs_0, sn_0, time_end_;
+    double theta_0, tn_0, cs_0, sn_0, s0h, c0h, time_end_;
 };
 
-// bia/find_hyperbola.f90:149-165 find_theta, given sn_p and sn_m at theta_now.
-__device__ __forceinline__ double hyp_newton(const HypConsts &c, double theta_now, double sn_p,
-                                             double sn_m, double *error_)
+// find_theta (bia/find_hyperbola.f90:149-165): residual e and derivative d at theta;
+// sp, sm = sin((theta_0 +- theta)/2) for the bracket test.
+BIA_HYPEVAL_INLINE void hyp_eval(const HypConsts &c, double theta, double &e, double &d,
+                                         double &sp, double &sm)
 {
-    double sn_now, cs_now;
-    sincos(theta_now, &sn_now, &cs_now);
-    double D_inv = 1.0 / (cs_now - c.cs_0);
-    double e = c.tn_0 * sn_now * D_inv - c.time_end_ + log(sn_p / sn_m);
-    *error_ = e;
-    if (e == 0.0) return theta_now;
-    double dfdth = c.tn_0 * (1.0 - c.cs_0 * cs_now) * (D_inv * D_inv) + c.sn_0 / (2.0 * sn_p * sn_m);
-    return theta_now - e / dfdth;
+    double sh, ch;
+    d_sincos(0.5 * theta, &sh, &ch);
+    sp = c.s0h * ch + c.c0h * sh;
+    sm = c.s0h * ch - c.c0h * sh;
+    const double Dinv = 1.0 / (2.0 * sp * sm);
+    const double sn = 2.0 * sh * ch;
+    const double cs = 1.0 - 2.0 * sh * sh;
+    e = c.tn_0 * sn * Dinv - c.time_end_ + d_log(sp / sm);
+    d = c.tn_0 * (1.0 - c.cs_0 * cs) * (Dinv * Dinv) + c.sn_0 * Dinv;
 }
 
 // Bracketed Newton-bisection on the same time equation, used only when the reference's
@@ -126,14 +165,10 @@ static __device__ __noinline__ double hyp_safe(const HypConsts c, double x)
     const double dir = (c.tn_0 > 0.0) ? 1.0 : -1.0;
     if (!(x > lo && x < hi)) x = 0.0;
     for (int it = 0; it < 400; it++) {
-        const double sp = sin((c.theta_0 + x) * 0.5), sm = sin((c.theta_0 - x) * 0.5);
-        double sn, cs;
-        sincos(x, &sn, &cs);
-        const double Dinv = 1.0 / (cs - c.cs_0);
-        const double f = c.tn_0 * sn * Dinv - c.time_end_ + log(sp / sm);
+        double f, d, sp, sm;
+        hyp_eval(c, x, f, d, sp, sm);
         if (f == 0.0) break;
         if (f * dir < 0.0) lo = x; else hi = x;
-        const double d = c.tn_0 * (1.0 - c.cs_0 * cs) * (Dinv * Dinv) + c.sn_0 / (2.0 * sp * sm);
         double xn = x - f / d;
         if (!(xn > lo && xn < hi)) xn = 0.5 * (lo + hi);
         if (xn == x) break;
@@ -156,36 +191,43 @@ __device__ __forceinline__ int hyperbola(double eps_th, double dt, int ITR, cons
     const double b_0 = eps_th / W;
     const double b = fabs(Lz) / g_0;
     HypConsts c;
-    c.theta_0 = atan2(fabs(Lz), b_0 * g_0);
-    const double den0 = sqrt(b_0 * b_0 * (g_0 * g_0) + Lz * Lz);
-    c.cs_0 = b_0 * g_0 / den0;
-    c.sn_0 = fabs(Lz) / den0;
-    c.tn_0 = fabs(Lz) / (b_0 * g_0);
+    const double bg = b_0 * g_0;
+    c.theta_0 = d_atan2(fabs(Lz), bg);
+    const double den0 = 1.0 / sqrt(bg * bg + Lz * Lz);
+    c.cs_0 = bg * den0;
+    c.sn_0 = fabs(Lz) * den0;
+    c.tn_0 = fabs(Lz) / bg;
+    d_sincos(0.5 * c.theta_0, &c.s0h, &c.c0h);
     const double arg = c.cs_0 + b * c.sn_0 / r;
-    double theta_ini = (fabs(arg) > 1.0) ? 1e-30 : acos(arg);
+    double theta_ini = (fabs(arg) > 1.0) ? 1e-30 : d_acos(arg);
     if (Lz * r_g < 0.0) theta_ini = -theta_ini;
-    double sn, cs;
-    sincos(theta_ini, &sn, &cs);
+    // state and dimensionless time at theta_ini (bia/find_hyperbola.f90:46-64)
+    double sh, ch;
+    d_sincos(0.5 * theta_ini, &sh, &ch);
+    const double sp_i = c.s0h * ch + c.c0h * sh, sm_i = c.s0h * ch - c.c0h * sh;
+    const double Dinv_i = 1.0 / (2.0 * sp_i * sm_i);
+    const double sn = 2.0 * sh * ch, cs = 1.0 - 2.0 * sh * sh;
     const double x = r * cs, y = r * sn;
     const double g0_sn0 = (Lz > 0.0) ? g_0 / c.sn_0 : -g_0 / c.sn_0;
     const double u = g0_sn0 * (c.cs_0 * sn);
     const double v = g0_sn0 * (1.0 - c.cs_0 * cs);
-    const double den_a = sqrt((X_ini * X_ini + Y_ini * Y_ini) * (x * x + y * y));
-    const double cs_a = (x * X_ini + y * Y_ini) / den_a;
-    const double sn_a = (x * Y_ini - y * X_ini) / den_a;
-    const double sp_ini = sin((c.theta_0 + theta_ini) * 0.5);
-    const double sm_ini = sin((c.theta_0 - theta_ini) * 0.5);
-    const double time_ini = (c.tn_0 * sn / (cs - c.cs_0) + log(sp_ini / sm_ini)) * b_0 / g_0;
+    const double den_a = 1.0 / sqrt((X_ini * X_ini + Y_ini * Y_ini) * (x * x + y * y));
+    const double cs_a = (x * X_ini + y * Y_ini) * den_a;
+    const double sn_a = (x * Y_ini - y * X_ini) * den_a;
+    const double tau_ini = c.tn_0 * sn * Dinv_i + d_log(sp_i / sm_i);
+    const double time_ini = tau_ini * b_0 / g_0;
     const double time_end = (Lz > 0.0) ? time_ini + dt : time_ini - dt;
     c.time_end_ = time_end * g_0 / b_0;
-    const double theta_gss = 2.0 / kPi * c.theta_0 * atan(c.time_end_ / c.tn_0);
 
-    // two candidate starts (bia/find_hyperbola.f90:73-89)
-    double error_ini_, error_gss_;
-    const double th_ini_end = hyp_newton(c, theta_ini, sp_ini, sm_ini, &error_ini_);
-    const double sp_g = sin((c.theta_0 + theta_gss) * 0.5);
-    const double sm_g = sin((c.theta_0 - theta_gss) * 0.5);
-    const double th_gss_end = hyp_newton(c, theta_gss, sp_g, sm_g, &error_gss_);
+    // two candidate starts (bia/find_hyperbola.f90:71-89): one Newton step from theta_ini
+    // (its residual is known already) and one from the atan guess
+    const double error_ini_ = tau_ini - c.time_end_;
+    const double d_ini = c.tn_0 * (1.0 - c.cs_0 * cs) * (Dinv_i * Dinv_i) + c.sn_0 * Dinv_i;
+    const double th_ini_end = (error_ini_ == 0.0) ? theta_ini : theta_ini - error_ini_ / d_ini;
+    const double theta_gss = 2.0 / kPi * c.theta_0 * d_atan(c.time_end_ / c.tn_0);
+    double error_gss_, d_gss, spg, smg;
+    hyp_eval(c, theta_gss, error_gss_, d_gss, spg, smg);
+    const double th_gss_end = (error_gss_ == 0.0) ? theta_gss : theta_gss - error_gss_ / d_gss;
     double theta_end, error_;
     if (fabs(error_gss_) > 10.0 * fabs(error_ini_)) {
         theta_end = th_ini_end;
@@ -197,19 +239,20 @@ __device__ __forceinline__ int hyperbola(double eps_th, double dt, int ITR, cons
     // minimum-residual Newton loop with cycle detection (bia/find_hyperbola.f90:93-120)
     double err_stock = error_;
     double theta_stock = theta_end;
-    double best_res = fabs(error_);  // smallest dimensionless residual seen
+    double best_res = fabs(error_);
     double hist[64];
     int IR = 0;
     *bracket_exit = 0;
     while (IR < ITR) {
         const double theta_now = theta_end;
-        const double sn_p = sin((c.theta_0 + theta_now) * 0.5);
-        const double sn_m = sin((c.theta_0 - theta_now) * 0.5);
-        if (sn_p * sn_m < 0.0) {
+        double e, d, sp, sm;
+        hyp_eval(c, theta_now, e, d, sp, sm);
+        if (sp * sm < 0.0) {
             *bracket_exit = 1;
             break;
         }
-        theta_end = hyp_newton(c, theta_now, sn_p, sn_m, &error_);
+        error_ = e;
+        theta_end = (e == 0.0) ? theta_now : theta_now - e / d;
         IR++;
         bool cycle = false;
         for (int num = IR - 1; num >= 1; num--)
@@ -229,13 +272,15 @@ __device__ __forceinline__ int hyperbola(double eps_th, double dt, int ITR, cons
         theta_stock = hyp_safe(c, theta_stock);
         *fallback = 1;
     }
-    double sn_end, cs_end;
-    sincos(theta_stock, &sn_end, &cs_end);
+    // end state (bia/find_hyperbola.f90:126-142)
+    d_sincos(0.5 * theta_stock, &sh, &ch);
+    const double sn_end = 2.0 * sh * ch, cs_end = 1.0 - 2.0 * sh * sh;
+    const double sp_e = c.s0h * ch + c.c0h * sh, sm_e = c.s0h * ch - c.c0h * sh;
     const double u_end = g0_sn0 * c.cs_0 * sn_end;
     const double du_end = u_end - u;
     const double v_end = g0_sn0 * (1.0 - c.cs_0 * cs_end);
     const double dv_end = v_end - v;
-    const double r_end = b * c.sn_0 / (cs_end - c.cs_0);
+    const double r_end = b * c.sn_0 / (2.0 * sp_e * sm_e);
     YN[0] = r_end * (cs_end * cs_a - sn_end * sn_a);
     YN[1] = r_end * (cs_end * sn_a + sn_end * cs_a);
     YN[2] = YZ[2] + (du_end * cs_a - dv_end * sn_a);
@@ -257,7 +302,7 @@ static __device__ __noinline__ double kepler_safe(double M, double e, double x)
     if (!(x >= lo && x <= hi)) x = M;
     for (int it = 0; it < 400; it++) {
         double sx, cx;
-        sincos(x, &sx, &cx);
+        d_sincos(x, &sx, &cx);
         const double f = x - e * sx - M;
         if (f == 0.0) break;
         if (f < 0.0) lo = x; else hi = x;
@@ -288,17 +333,17 @@ static __device__ __noinline__ int ellipse(double eps_th, double dt, int ITR, co
         if (r_ini < a) {
             xi_ini = 0.0;
         } else if (r_ini == a) {
-            xi_ini = atan2(Y_ini, X_ini);
+            xi_ini = d_atan2(Y_ini, X_ini);
             ecc = 0.0;
         } else {
             xi_ini = f_sign(kPi, L);
         }
     } else {
-        xi_ini = atan2(r_g_ini / g_a, a - r_ini);
+        xi_ini = d_atan2(r_g_ini / g_a, a - r_ini);
     }
     double s_ini, c_ini;
-    sincos(xi_ini, &s_ini, &c_ini);
-    const double alpha = atan2(Y_ini, X_ini) - atan2(b * s_ini, a * (c_ini - ecc));
+    d_sincos(xi_ini, &s_ini, &c_ini);
+    const double alpha = d_atan2(Y_ini, X_ini) - d_atan2(b * s_ini, a * (c_ini - ecc));
     const double tau_ini = xi_ini - ecc * s_ini;
     const double time_ini = tau_ini / omega_a;
     const double time_end = time_ini + dt;
@@ -309,17 +354,17 @@ static __device__ __noinline__ int ellipse(double eps_th, double dt, int ITR, co
         for (int k = 0; k < 4; k++) YN[k] = YZ[k];
         return 0;
     }
+    // Kepler's equation tau_end = xi - e sin(xi) by the reference's Newton loop
+    // (bia/find_ellipse.f90:106-157).  Start: one Newton step from the initial anomaly
+    // xi_ini, whose residual is omega dt, instead of the reference's start from the mean
+    // anomaly (xi_2 + delta_ini, bia/find_ellipse.f90:116-129), which needs ~8 steps on
+    // average and fails outright for e near 1; the root is the same.
     int ir = 0;
     const double error_ini = tau_end - xi_ini + ecc * s_ini;
-    const double delta_ini = error_ini * (1.0 - ecc * c_ini);
-    double st, ct;
-    sincos(tau_end, &st, &ct);
-    double xi_2 = (ct < 0.9) ? tau_end : f_sign(kPi / 2, st);
-    double s2, c2;
-    sincos(xi_2, &s2, &c2);
-    double error_tm2 = tau_end - xi_2 + ecc * s2;
-    double delta_xi2 = error_tm2 / (1.0 - ecc * c2);
-    double xi = (fabs(error_ini) < fabs(error_tm2)) ? xi_2 + delta_ini : xi_2 + delta_xi2;
+    double xi_2 = xi_ini;
+    double error_tm2 = error_ini;
+    double s2, c2, delta_xi2;
+    double xi = xi_ini + error_ini / (1.0 - ecc * c_ini);
     double xi_1 = __longlong_as_double(0x7ff8000000000000LL);  // unset: compares unequal
     double error_tm1 = error_tm2;
     bool conv = false;
@@ -327,7 +372,7 @@ static __device__ __noinline__ int ellipse(double eps_th, double dt, int ITR, co
         ir++;
         xi_1 = xi;
         double s1, c1;
-        sincos(xi_1, &s1, &c1);
+        d_sincos(xi_1, &s1, &c1);
         error_tm1 = tau_end - xi_1 + ecc * s1;
         xi = xi_1 + error_tm1 / (1.0 - ecc * c1);
         if (error_tm1 == 0.0 || error_tm1 == error_tm2 || error_tm1 + error_tm2 == 0.0) {
@@ -337,7 +382,7 @@ static __device__ __noinline__ int ellipse(double eps_th, double dt, int ITR, co
         }
         ir++;
         xi_2 = xi;
-        sincos(xi_2, &s2, &c2);
+        d_sincos(xi_2, &s2, &c2);
         error_tm2 = tau_end - xi_2 + ecc * s2;
         delta_xi2 = error_tm2 / (1.0 - ecc * c2);
         xi = xi_2 + delta_xi2;
@@ -354,14 +399,14 @@ static __device__ __noinline__ int ellipse(double eps_th, double dt, int ITR, co
         *fallback = 1;
     }
     double sn_end, cs_end;
-    sincos(xi, &sn_end, &cs_end);
+    d_sincos(xi, &sn_end, &cs_end);
     const double xx_end = a * (cs_end - ecc);
     const double yy_end = b * sn_end;
     const double rr_end = a * (1.0 - ecc * cs_end);
     const double uu_end = -a * g_a * sn_end / rr_end;
     const double vv_end = b * g_a * cs_end / rr_end;
     double sn_alp, cs_alp;
-    sincos(alpha, &sn_alp, &cs_alp);
+    d_sincos(alpha, &sn_alp, &cs_alp);
     YN[0] = xx_end * cs_alp - yy_end * sn_alp;
     YN[1] = xx_end * sn_alp + yy_end * cs_alp;
     YN[2] = uu_end * cs_alp - vv_end * sn_alp;
@@ -630,10 +675,17 @@ __device__ __forceinline__ int uv_halfdisp(double eps_th, double dt, const doubl
         if (F == 0.0) break;
         if (F < 0.0) lo = s; else hi = s;
         double sn = s - F / Fp;
-        if (!(sn > lo) || (hi > 0.0 && !(sn < hi)) || !(Fp > 0.0)) sn = (hi > 0.0) ? 0.5 * (lo + hi) : 2.0 * s;
+        bool newton = true;
+        if (!(sn > lo) || (hi > 0.0 && !(sn < hi)) || !(Fp > 0.0)) {
+            sn = (hi > 0.0) ? 0.5 * (lo + hi) : 2.0 * s;
+            newton = false;
+        }
         const double ds = sn - s;
         s = sn;
         if (fabs(ds) <= 4.0 * 2.220446049250313e-16 * fabs(s)) break;
+        // Newton converges quadratically: after a step of relative size 1e-10 the next
+        // one would be below rounding, so s is final without another evaluation
+        if (newton && fabs(ds) <= 1e-10 * fabs(s)) break;
     }
     stumpff(beta * s * s, c);
     const double s2c2 = s * s * c[2], s3c3 = s * s * s * c[3];
@@ -654,37 +706,54 @@ __device__ __forceinline__ int uv_halfdisp(double eps_th, double dt, const doubl
 // One pair: frame, classification, solve, half-displacement (bia/bia.f90:141-191).
 // Returns the half-displacement in h[6] = (dX, dY, dZ, dU, dV, dW)/2 terms.
 // ---------------------------------------------------------------------------
+// ALG pair classes (bia/bia.f90:156-166 plus the guards): the branch each pair takes.
+enum AlgClass { kClsHyp = 0, kClsEll = 1, kClsUv = 2, kClsPar = 3, kClsDeg = 4 };
+
+// Branch of an ALG pair: E == 0 exactly keeps the reference's parabola branch; zero |g| or
+// |L| (degenerate) and |e^2 - 1| = |E| L^2 / eps^2 < 0.1 go to the universal-variable
+// solver; otherwise hyperbola (E > 0) or ellipse (E < 0).
+__device__ __forceinline__ int alg_classify(double eps_ij, const double r[3], const double g[3])
+{
+    const double gsq = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+    const double L0 = r[1] * g[2] - r[2] * g[1];
+    const double L1 = r[2] * g[0] - r[0] * g[2];
+    const double L2 = r[0] * g[1] - r[1] * g[0];
+    const double Lsq = L0 * L0 + L1 * L1 + L2 * L2;
+    const double r_ij = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    const double E_ij = gsq + 2.0 * eps_ij / r_ij;
+    if (E_ij == 0.0) return kClsPar;
+    if (gsq == 0.0 || Lsq == 0.0) return kClsDeg;
+    if (fabs(E_ij) * Lsq < kNearUnitEcc * (eps_ij * eps_ij)) return kClsUv;
+    return (E_ij > 0.0) ? kClsHyp : kClsEll;
+}
+
+// M: the compiled method (kMethodRkf, kMethodAlg, kMethodUniversal); each kernel is
+// instantiated per method so it carries only that method's code and registers.
+constexpr int kMethodRkf = 0, kMethodAlg = 1, kMethodUniversal = 2;
+
+template <int M>
 __device__ __forceinline__ void pair_halfdisp(const PairParams &P, double eps_ij, const double r[3],
                                               const double g[3], double h[6], PairCounters &cnt)
 {
-    if (P.method == 2) {
+    if (M == kMethodUniversal) {
         cnt.it_uv += uv_halfdisp(eps_ij, P.dt, r, g, h);
         cnt.cls[kUniversal]++;
-    } else {
-        double e_xi[3], e_eta[3], YZ[4], YN[4];
-        double error = 0.0;
-        const bool degenerate = frame_xi_eta(r, g, e_xi, e_eta, YZ);
-        bool done = false;
-        if (P.method == 0) {
-            int nacc = 0;
-            rkf_pair(eps_ij, P.dt, P.relerr, P.abserr, YZ, YN, &error, &nacc);
-            cnt.cls[degenerate ? kDegenerate : kRkf]++;
-            cnt.rkf_steps += nacc;
+    } else if (M == kMethodAlg) {
+        const int c = alg_classify(eps_ij, r, g);
+        if (c == kClsUv || c == kClsDeg) {
+            cnt.it_uv += uv_halfdisp(eps_ij, P.dt, r, g, h);
+            cnt.cls[c == kClsDeg ? kDegenerate : kUniversal]++;
         } else {
-            const double r_ij = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-            const double E_ij = g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + 2.0 * eps_ij / r_ij;
-            const double Lm = YZ[0] * YZ[3];
-            if (E_ij != 0.0 && (degenerate || fabs(E_ij) * (Lm * Lm) < kNearUnitEcc * (eps_ij * eps_ij))) {
-                cnt.it_uv += uv_halfdisp(eps_ij, P.dt, r, g, h);
-                cnt.cls[degenerate ? kDegenerate : kUniversal]++;
-                done = true;
-            } else if (E_ij > 0.0) {
+            double e_xi[3], e_eta[3], YZ[4], YN[4];
+            double error = 0.0;
+            frame_xi_eta(r, g, e_xi, e_eta, YZ);
+            if (c == kClsHyp) {
                 int bx = 0, fb = 0;
                 cnt.it_hyp += hyperbola(eps_ij, P.dt, P.itr, YZ, YN, &error, &bx, &fb);
                 cnt.bracket_exits += bx;
                 cnt.fallbacks += fb;
                 cnt.cls[kHyperbola]++;
-            } else if (E_ij < 0.0) {
+            } else if (c == kClsEll) {
                 int fb = 0;
                 cnt.it_ell += ellipse(eps_ij, P.dt, P.itr, YZ, YN, &error, &fb);
                 cnt.fallbacks += fb;
@@ -693,8 +762,6 @@ __device__ __forceinline__ void pair_halfdisp(const PairParams &P, double eps_ij
                 cnt.it_par += parabola(eps_ij, P.dt, YZ, YN, &error);
                 cnt.cls[kParabola]++;
             }
-        }
-        if (!done) {
             if (fabs(error) > P.err) cnt.nonconverged++;
             const double dr_xi = YN[0] - YZ[0], dr_eta = YN[1] - YZ[1];
             const double dg_xi = YN[2] - YZ[2], dg_eta = YN[3] - YZ[3];
@@ -703,6 +770,22 @@ __device__ __forceinline__ void pair_halfdisp(const PairParams &P, double eps_ij
                 h[k] = (dr_xi * e_xi[k] + dr_eta * e_eta[k] - g[k] * P.dt) * 0.5;
                 h[3 + k] = (dg_xi * e_xi[k] + dg_eta * e_eta[k]) * 0.5;
             }
+        }
+    } else {
+        double e_xi[3], e_eta[3], YZ[4], YN[4];
+        double error = 0.0;
+        const bool degenerate = frame_xi_eta(r, g, e_xi, e_eta, YZ);
+        int nacc = 0;
+        rkf_pair(eps_ij, P.dt, P.relerr, P.abserr, YZ, YN, &error, &nacc);
+        cnt.cls[degenerate ? kDegenerate : kRkf]++;
+        cnt.rkf_steps += nacc;
+        if (fabs(error) > P.err) cnt.nonconverged++;
+        const double dr_xi = YN[0] - YZ[0], dr_eta = YN[1] - YZ[1];
+        const double dg_xi = YN[2] - YZ[2], dg_eta = YN[3] - YZ[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            h[k] = (dr_xi * e_xi[k] + dr_eta * e_eta[k] - g[k] * P.dt) * 0.5;
+            h[3 + k] = (dg_xi * e_xi[k] + dg_eta * e_eta[k]) * 0.5;
         }
     }
     bool finite = true;

@@ -25,6 +25,7 @@ struct RowArgs {
     PairParams P;
 };
 
+template <int M>
 __global__ void __launch_bounds__(128) bia_row_kernel(const RowArgs A)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -36,7 +37,7 @@ __global__ void __launch_bounds__(128) bia_row_kernel(const RowArgs A)
         const double *s = A.rel + (size_t)6 * j;
         const double r[3] = {s[0], s[1], s[2]};
         const double g[3] = {s[3], s[4], s[5]};
-        pair_halfdisp(A.P, A.eps_th, r, g, h, cnt);
+        pair_halfdisp<M>(A.P, A.eps_th, r, g, h, cnt);
     }
     if (j < A.n) {
 #pragma unroll
@@ -129,7 +130,10 @@ extern "C" void find_dxyuv_kernel_(const int METHOD, const int N, const int I, c
     A.P.abserr = 1e-16;
     A.P.itr = ITR;
     A.P.method = METHOD;
-    bia_row_kernel<<<(N + 127) / 128, 128>>>(A);
+    if (METHOD == 0)
+        bia_row_kernel<kMethodRkf><<<(N + 127) / 128, 128>>>(A);
+    else
+        bia_row_kernel<kMethodAlg><<<(N + 127) / 128, 128>>>(A);
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpy(dXYZUVW, S.out.ptr, bytes, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(S.h_rowsum, d_rowsum, 6 * sizeof(double), cudaMemcpyDeviceToHost);

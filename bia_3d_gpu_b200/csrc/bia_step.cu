@@ -32,6 +32,7 @@
 
 #include "bia_internal.cuh"
 #include "bia_pair.cuh"
+#include "bia_tiles.cuh"
 
 namespace bia {
 
@@ -48,45 +49,9 @@ struct StepArgs {
     PairParams P;
 };
 
-__device__ __forceinline__ void warp_block_coords(long long t, int &bi, int &bj)
+template <bool kDeterministic, int M>
+__global__ void __launch_bounds__(kThreads, TileOccupancy<M>::kMinBlocks) bia_pair_tiles_kernel(const StepArgs A)
 {
-    // t = bj*(bj+1)/2 + bi with 0 <= bi <= bj
-    long long c = (long long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-    while (c * (c + 1) / 2 > t) c--;
-    while ((c + 1) * (c + 2) / 2 <= t) c++;
-    bj = (int)c;
-    bi = (int)(t - c * (c + 1) / 2);
-}
-
-__device__ __forceinline__ void load_particle(const StepArgs &A, int p, double s[7])
-{
-    if (p < A.n) {
-        s[0] = A.x[p]; s[1] = A.y[p]; s[2] = A.z[p];
-        s[3] = A.u[p]; s[4] = A.v[p]; s[5] = A.w[p];
-        s[6] = A.q ? A.q[p] : 1.0;
-    } else {
-#pragma unroll
-        for (int k = 0; k < 7; k++) s[k] = 0.0;
-    }
-}
-
-__device__ __forceinline__ void flush_counters(const PairCounters &c, unsigned long long *stats, int lane)
-{
-    const unsigned full = 0xffffffffu;
-    int vals[kNumStats] = {c.cls[0], c.cls[1], c.cls[2], c.cls[3], c.cls[4], c.cls[5],
-                           c.it_hyp, c.it_ell, c.it_par, c.it_uv, c.rkf_steps,
-                           c.nonconverged, c.bracket_exits, c.fallbacks, c.nonfinite};
-#pragma unroll
-    for (int k = 0; k < kNumStats; k++) {
-        int s = __reduce_add_sync(full, vals[k]);
-        if (lane == 0 && s != 0) atomicAdd(&stats[k], (unsigned long long)s);
-    }
-}
-
-template <bool kDeterministic>
-__global__ void __launch_bounds__(kThreads) bia_pair_tiles_kernel(const StepArgs A)
-{
-    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const long long t = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
     if (t >= A.nwb) return;  // warp-uniform
@@ -94,54 +59,15 @@ __global__ void __launch_bounds__(kThreads) bia_pair_tiles_kernel(const StepArgs
     warp_block_coords(t, bi, bj);
     const int i = bi * 32 + lane;
     const int jown = bj * 32 + lane;
-    double si[7], sj[7];
-    load_particle(A, i, si);
-    load_particle(A, jown, sj);
-
-    double racc[6] = {0, 0, 0, 0, 0, 0}, cacc[6] = {0, 0, 0, 0, 0, 0};
-    PairCounters cnt;
-    counters_zero(cnt);
     const bool diag = (bi == bj);
-    const int k0 = diag ? 1 : 0;
-    const int k1 = diag ? 16 : 31;
-    for (int k = k0; k <= k1; k++) {
-        const int src = (lane + k) & 31;
-        double sc[7];
-#pragma unroll
-        for (int c = 0; c < 7; c++) sc[c] = __shfl_sync(full, sj[c], src);
-        const int j = bj * 32 + src;
-        const bool active = (!diag || k < 16 || lane < 16) && i < A.n && j < A.n;
-        double h[6] = {0, 0, 0, 0, 0, 0};
-        if (active) {
-            const double r[3] = {si[0] - sc[0], si[1] - sc[1], si[2] - sc[2]};
-            const double g[3] = {si[3] - sc[3], si[4] - sc[4], si[5] - sc[5]};
-            const double eps_ij = A.q ? A.eps_th * si[6] * sc[6] : A.eps_th;
-            pair_halfdisp(A.P, eps_ij, r, g, h, cnt);
-        }
-        const int back = (lane - k) & 31;
-#pragma unroll
-        for (int c = 0; c < 6; c++) {
-            racc[c] += h[c];
-            cacc[c] += __shfl_sync(full, h[c], back);
-        }
-    }
+    double racc[6], cacc[6];
+    PairCounters cnt;
+    warp_block_solve<M>(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P, bi, bj, lane, racc, cacc, cnt);
     flush_counters(cnt, A.stats, lane);
 
     const size_t plane = (size_t)A.npad;
     if (kDeterministic) {
-        if (diag) {
-            double *dst = A.part + (size_t)bi * 6 * plane;
-#pragma unroll
-            for (int c = 0; c < 6; c++) dst[c * plane + i] = racc[c] - cacc[c];
-        } else {
-            double *drow = A.part + (size_t)bj * 6 * plane;
-            double *dcol = A.part + (size_t)bi * 6 * plane;
-#pragma unroll
-            for (int c = 0; c < 6; c++) {
-                drow[c * plane + i] = racc[c];
-                dcol[c * plane + jown] = -cacc[c];
-            }
-        }
+        write_partials(A.part, plane, bi, bj, lane, racc, cacc);
     } else {
         if (diag) {
 #pragma unroll
@@ -154,6 +80,22 @@ __global__ void __launch_bounds__(kThreads) bia_pair_tiles_kernel(const StepArgs
                 if (jown < A.n) atomicAdd(&A.part[c * plane + jown], -cacc[c]);
             }
         }
+    }
+}
+
+template <bool kDeterministic>
+static void launch_pair_tiles(const StepArgs &A, long long grid, cudaStream_t st)
+{
+    switch (A.P.method) {
+    case kMethodRkf:
+        bia_pair_tiles_kernel<kDeterministic, kMethodRkf><<<(unsigned)grid, kThreads, 0, st>>>(A);
+        break;
+    case kMethodUniversal:
+        bia_pair_tiles_kernel<kDeterministic, kMethodUniversal><<<(unsigned)grid, kThreads, 0, st>>>(A);
+        break;
+    default:
+        bia_pair_tiles_kernel<kDeterministic, kMethodAlg><<<(unsigned)grid, kThreads, 0, st>>>(A);
+        break;
     }
 }
 
@@ -282,7 +224,7 @@ int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
         U.part = A.part;
         U.nparts = nb;
         record_event(ctx);
-        bia_pair_tiles_kernel<true><<<(unsigned)grid, kThreads, 0, ctx->stream>>>(A);
+        launch_pair_tiles<true>(A, grid, ctx->stream);
         record_event(ctx);
     } else {
         A.part = (double *)ctx->acc.ptr;
@@ -290,7 +232,7 @@ int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
         U.nparts = 1;
         cudaMemsetAsync(A.part, 0, 6 * (size_t)A.npad * sizeof(double), ctx->stream);
         record_event(ctx);
-        bia_pair_tiles_kernel<false><<<(unsigned)grid, kThreads, 0, ctx->stream>>>(A);
+        launch_pair_tiles<false>(A, grid, ctx->stream);
         record_event(ctx);
     }
     bia_reduce_update_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(U);
@@ -403,6 +345,8 @@ int bia_context_destroy(bia_context *ctx)
     ctx->stats.release();
     ctx->state.release();
     ctx->inv.release();
+    ctx->dim.release();
+    if (ctx->h_dim) cudaFreeHost(ctx->h_dim);
     if (ctx->h_stats) cudaFreeHost(ctx->h_stats);
     if (ctx->h_inv) cudaFreeHost(ctx->h_inv);
     delete ctx;
@@ -646,7 +590,7 @@ extern "C" int bia_step_noalloc(const bia_config *cfg, int n, double *x, double 
     A.P.itr = cfg->itr;
     A.P.method = cfg->method;
     const long long grid = (A.nwb + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    bia_pair_tiles_kernel<true><<<(unsigned)grid, kThreads, 0, s>>>(A);
+    launch_pair_tiles<true>(A, grid, s);
     UpdateArgs U;
     U.x = x; U.y = y; U.z = z; U.u = u; U.v = v; U.w = w;
     U.part = part;

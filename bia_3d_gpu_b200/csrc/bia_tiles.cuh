@@ -1,0 +1,136 @@
+// bia_tiles.cuh -- one 32 x 32 warp-block of pairs, shared by the single-system step
+// (bia_step.cu) and the ensemble step (bia_ensemble.cu).
+//
+// Lane l keeps row particle 32*bi + l and column particle 32*bj + l in registers.  At
+// rotation step k it solves the pair (row l, column (l + k) mod 32), the column state
+// arriving by shuffle, and the column's half-displacement goes back by a second shuffle
+// from lane (l - k) mod 32, so every lane works on a different pair and both sums stay in
+// registers.  Off-diagonal blocks take 32 steps (1024 pairs); diagonal blocks 16 (k =
+// 1..15 on all lanes, k = 16 on lanes 0..15: each of the 496 pairs once; orientation does
+// not matter because the half-displacement is exactly antisymmetric under i <-> j).
+#pragma once
+#include <mutex>
+
+#include "bia_internal.cuh"
+#include "bia_pair.cuh"
+
+namespace bia {
+
+// Resident CTAs per SM each method's kernel is compiled for (register budget
+// 65536 / (256 threads * blocks)): ALG 3 and universal 3 (<= 85 registers), measured
+// fastest on the mixed-class Coulomb workload.
+#ifndef BIA_ALG_MIN_BLOCKS
+#define BIA_ALG_MIN_BLOCKS 3
+#endif
+#ifndef BIA_UV_MIN_BLOCKS
+#define BIA_UV_MIN_BLOCKS 3
+#endif
+template <int M> struct TileOccupancy { static constexpr int kMinBlocks = 1; };
+template <> struct TileOccupancy<kMethodAlg> { static constexpr int kMinBlocks = BIA_ALG_MIN_BLOCKS; };
+template <> struct TileOccupancy<kMethodUniversal> { static constexpr int kMinBlocks = BIA_UV_MIN_BLOCKS; };
+
+__device__ __forceinline__ void warp_block_coords(long long t, int &bi, int &bj)
+{
+    // t = bj*(bj+1)/2 + bi with 0 <= bi <= bj
+    long long c = (long long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while (c * (c + 1) / 2 > t) c--;
+    while ((c + 1) * (c + 2) / 2 <= t) c++;
+    bj = (int)c;
+    bi = (int)(t - c * (c + 1) / 2);
+}
+
+__device__ __forceinline__ void load_particle(const double *x, const double *y, const double *z,
+                                              const double *u, const double *v, const double *w,
+                                              const double *q, int n, int p, double s[7])
+{
+    if (p < n) {
+        s[0] = x[p]; s[1] = y[p]; s[2] = z[p];
+        s[3] = u[p]; s[4] = v[p]; s[5] = w[p];
+        s[6] = q ? q[p] : 1.0;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 7; k++) s[k] = 0.0;
+    }
+}
+
+__device__ __forceinline__ void flush_counters(const PairCounters &c, unsigned long long *stats, int lane)
+{
+    const unsigned full = 0xffffffffu;
+    int vals[kNumStats] = {c.cls[0], c.cls[1], c.cls[2], c.cls[3], c.cls[4], c.cls[5],
+                           c.it_hyp, c.it_ell, c.it_par, c.it_uv, c.rkf_steps,
+                           c.nonconverged, c.bracket_exits, c.fallbacks, c.nonfinite};
+#pragma unroll
+    for (int k = 0; k < kNumStats; k++) {
+        int s = __reduce_add_sync(full, vals[k]);
+        if (lane == 0 && s != 0) atomicAdd(&stats[k], (unsigned long long)s);
+    }
+}
+
+// Pairs of warp-block (bi, bj) of the system whose particles are x[0..n) etc.: row sums
+// racc (particle 32 bi + lane) and column sums cacc (particle 32 bj + lane) of the pair
+// half-displacements h (row receives +h, column -h: the caller writes -cacc).
+template <int M>
+__device__ __forceinline__ void warp_block_solve(const double *x, const double *y, const double *z,
+                                                 const double *u, const double *v, const double *w,
+                                                 const double *q, int n, double eps_th, const PairParams &P,
+                                                 int bi, int bj, int lane, double racc[6], double cacc[6],
+                                                 PairCounters &cnt)
+{
+    const unsigned full = 0xffffffffu;
+    const int i = bi * 32 + lane;
+    double si[7], sj[7];
+    load_particle(x, y, z, u, v, w, q, n, i, si);
+    load_particle(x, y, z, u, v, w, q, n, bj * 32 + lane, sj);
+#pragma unroll
+    for (int c = 0; c < 6; c++) racc[c] = cacc[c] = 0.0;
+    counters_zero(cnt);
+    const bool diag = (bi == bj);
+    const int k0 = diag ? 1 : 0;
+    const int k1 = diag ? 16 : 31;
+    for (int k = k0; k <= k1; k++) {
+        const int src = (lane + k) & 31;
+        double sc[7];
+#pragma unroll
+        for (int c = 0; c < 7; c++) sc[c] = __shfl_sync(full, sj[c], src);
+        const int j = bj * 32 + src;
+        const bool active = (!diag || k < 16 || lane < 16) && i < n && j < n;
+        double h[6] = {0, 0, 0, 0, 0, 0};
+        if (active) {
+            const double r[3] = {si[0] - sc[0], si[1] - sc[1], si[2] - sc[2]};
+            const double g[3] = {si[3] - sc[3], si[4] - sc[4], si[5] - sc[5]};
+            const double eps_ij = q ? eps_th * si[6] * sc[6] : eps_th;
+            pair_halfdisp<M>(P, eps_ij, r, g, h, cnt);
+        }
+        const int back = (lane - k) & 31;
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            racc[c] += h[c];
+            cacc[c] += __shfl_sync(full, h[c], back);
+        }
+    }
+}
+
+// Deterministic partial layout part[m][c][p] (plane = padded particle count): row sums
+// of block (bi, bj) at m = bj, column sums at m = bi, the diagonal block's combined sums
+// at m = bi; each (m, p) slot is written once per step.
+__device__ __forceinline__ void write_partials(double *part, size_t plane, int bi, int bj, int lane,
+                                               const double racc[6], const double cacc[6])
+{
+    const int i = bi * 32 + lane;
+    const int j = bj * 32 + lane;
+    if (bi == bj) {
+        double *dst = part + (size_t)bi * 6 * plane;
+#pragma unroll
+        for (int c = 0; c < 6; c++) dst[c * plane + i] = racc[c] - cacc[c];
+    } else {
+        double *drow = part + (size_t)bj * 6 * plane;
+        double *dcol = part + (size_t)bi * 6 * plane;
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            drow[c * plane + i] = racc[c];
+            dcol[c * plane + j] = -cacc[c];
+        }
+    }
+}
+
+}  // namespace bia

@@ -1,0 +1,465 @@
+// dim_rkf.cu -- the direct-integration (DIM) FP64 reference solver on the device.
+//
+// Rebuilds dim/rkf_kernel.cu: all 6n equations y' = (v, a) with the direct-sum
+// acceleration a_i = eps sum_j (r_i - r_j) / (|r_ij|^2 + 1e-99)^{3/2}
+// (dim/rkf_kernel.cu:29-53) integrated from x0 to xe by the Fehlberg 4(5) pair with
+// step doubling and the reference's adaptive control (dim/rkf_kernel.cu:194-495):
+// the "low" track advances by one step h with the embedded error estimate, the "high"
+// track by two steps h/2; a step is accepted when max_i |er_i| / et_i <= 1.
+//
+// Differences from the reference, none of which changes the scheme:
+//  * the state stays on the device for the whole integration; per attempted step the
+//    host reads one double (the error norm) instead of copying the 11*6n work array
+//    both ways (dim/rkf_kernel.cu:290-292,485-489);
+//  * the acceleration sum over j is split into 8 fixed chunks whose partial sums are
+//    added in order (deterministic; the association differs from the reference's single
+//    running sum by rounding only);
+//  * errors set IER (10000 too many steps, 20000 zero tolerance, 30000 step underflow)
+//    and return instead of calling exit(0) (dim/rkf_kernel.cu:298-315,491-494).
+// Layout: SoA, component-major, 6 arrays of n (x, y, z, u, v, w).
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+
+#include "bia_internal.cuh"
+
+namespace bia {
+
+constexpr int kDimChunks = 8;
+constexpr int kDimParticlesPerBlock = 32;
+
+// Fehlberg coefficients (dim/rkf_kernel.cu:161-168); stage s (1..5) forms
+// w_s = y0 + h * sum_m B[s][m] k_m, the 6th line forms yn with GA, the 7th er with DA.
+__constant__ double c_fehl[7][6] = {
+    {1.0 / 4, 0, 0, 0, 0, 0},
+    {3.0 / 32, 9.0 / 32, 0, 0, 0, 0},
+    {1932.0 / 2197, -7200.0 / 2197, 7296.0 / 2197, 0, 0, 0},
+    {439.0 / 216, -8.0, 3680.0 / 513, -845.0 / 4104, 0, 0},
+    {-8.0 / 27, 2.0, -3544.0 / 2565, 1859.0 / 4104, -11.0 / 40, 0},
+    {16.0 / 135, 0, 6656.0 / 12825, 28561.0 / 56430, -9.0 / 50, 2.0 / 55},
+    {1.0 / 360, 0, -128.0 / 4275, -2197.0 / 75240, 1.0 / 50, 2.0 / 55},
+};
+
+// k_out = (v, a)(y_in).  Block: 32 particles x 8 j-chunks; the chunk partial sums are
+// added in chunk order.
+__global__ void __launch_bounds__(kDimParticlesPerBlock * kDimChunks) dim_accel_kernel(
+    int n, double eps, const double *__restrict__ yin, double *__restrict__ kout)
+{
+    __shared__ double part[kDimChunks][3][kDimParticlesPerBlock];
+    const int lane = threadIdx.x % kDimParticlesPerBlock;
+    const int chunk = threadIdx.x / kDimParticlesPerBlock;
+    const int i = blockIdx.x * kDimParticlesPerBlock + lane;
+    const double *X = yin, *Y = yin + n, *Z = yin + 2 * (size_t)n;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    if (i < n) {
+        const double xi = X[i], yi = Y[i], zi = Z[i];
+        const int per = (n + kDimChunks - 1) / kDimChunks;
+        const int j0 = chunk * per;
+        const int j1 = min(n, j0 + per);
+        for (int j = j0; j < j1; j++) {
+            const double xij = xi - X[j], yij = yi - Y[j], zij = zi - Z[j];
+            const double rsq = xij * xij + yij * yij + zij * zij + 1e-99;
+            const double eee = eps / (rsq * sqrt(rsq));
+            ax += xij * eee;
+            ay += yij * eee;
+            az += zij * eee;
+        }
+    }
+    part[chunk][0][lane] = ax;
+    part[chunk][1][lane] = ay;
+    part[chunk][2][lane] = az;
+    __syncthreads();
+    if (chunk == 0 && i < n) {
+        double s[3] = {0.0, 0.0, 0.0};
+        for (int c = 0; c < kDimChunks; c++)
+            for (int d = 0; d < 3; d++) s[d] += part[c][d][lane];
+        kout[i] = yin[3 * (size_t)n + i];
+        kout[(size_t)n + i] = yin[4 * (size_t)n + i];
+        kout[2 * (size_t)n + i] = yin[5 * (size_t)n + i];
+        kout[3 * (size_t)n + i] = s[0];
+        kout[4 * (size_t)n + i] = s[1];
+        kout[5 * (size_t)n + i] = s[2];
+    }
+}
+
+// out = y0 + h * sum_{m < nk} c_fehl[row][m] k_m  (row 0..5), or er = h * sum (row 6)
+__global__ void __launch_bounds__(256) dim_combine_kernel(int len, int row, int nk, bool add_y0,
+                                                          const double *__restrict__ hdev,
+                                                          const double *__restrict__ y0,
+                                                          const double *__restrict__ k, double *__restrict__ out)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= len) return;
+    const double h = *hdev;
+    double acc;
+    if (row == 0) {
+        acc = h * c_fehl[0][0] * k[e];  // (h * B21) * k1, dim/rkf_kernel.cu:82
+    } else {
+        acc = 0.0;
+        for (int m = 0; m < nk; m++) acc += c_fehl[row][m] * k[(size_t)m * len + e];
+        acc = h * acc;
+    }
+    out[e] = add_y0 ? y0[e] + acc : acc;
+}
+
+// per-block max of |er| / et with et = relerr (|yl0| + |yln|) / 2 + abserr; a zero et
+// is flagged by a negative result
+__global__ void __launch_bounds__(256) dim_errnorm_kernel(int len, double relerr, double abserr,
+                                                          const double *__restrict__ yl0,
+                                                          const double *__restrict__ yln,
+                                                          const double *__restrict__ er, double *__restrict__ blockmax)
+{
+    __shared__ double sh[256];
+    double m = 0.0;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < len; e += gridDim.x * blockDim.x) {
+        const double et = relerr * (fabs(yl0[e]) + fabs(yln[e])) / 2 + abserr;
+        if (et == 0.0) m = -1.0e300;
+        else if (m >= 0.0) m = fmax(m, fabs(er[e]) / et);
+    }
+    sh[threadIdx.x] = m;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            const double a = sh[threadIdx.x], b = sh[threadIdx.x + s];
+            sh[threadIdx.x] = (a < 0.0 || b < 0.0) ? -1.0e300 : fmax(a, b);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) blockmax[blockIdx.x] = sh[0];
+}
+
+// min over i with |k1_i| > 0 of |(relerr |y_i| + abserr) / k1_i| (initial step size,
+// dim/rkf_kernel.cu:248-261); +inf when no k1_i is nonzero
+__global__ void __launch_bounds__(256) dim_toldy_kernel(int len, double relerr, double abserr,
+                                                        const double *__restrict__ y, const double *__restrict__ k1,
+                                                        double *__restrict__ blockmin)
+{
+    __shared__ double sh[256];
+    double m = INFINITY;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < len; e += gridDim.x * blockDim.x) {
+        if (fabs(k1[e]) > 0.0) m = fmin(m, fabs((relerr * fabs(y[e]) + abserr) / k1[e]));
+    }
+    sh[threadIdx.x] = m;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] = fmin(sh[threadIdx.x], sh[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) blockmin[blockIdx.x] = sh[0];
+}
+
+__global__ void dim_final_reduce_kernel(int count, bool take_max, const double *__restrict__ in, double *out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double m = take_max ? 0.0 : INFINITY;
+    for (int b = 0; b < count; b++) {
+        const double v = in[b];
+        if (take_max) m = (m < 0.0 || v < 0.0) ? -1.0e300 : fmax(m, v);
+        else m = fmin(m, v);
+    }
+    *out = m;
+}
+
+__global__ void __launch_bounds__(256) dim_esterr_kernel(int len, const double *__restrict__ yln,
+                                                         const double *__restrict__ yhn, double *__restrict__ ese)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < len) ese[e] = (yln[e] - yhn[e]) / 31;
+}
+
+constexpr int kDimReduceBlocks = 148;
+
+// Device buffers of one integration: 6n doubles each for yl0, yln, yh0, yhm, yhn, er, w
+// and 6 x 6n for k1..k6; plus reduction scratch and the step size.
+struct DimBuffers {
+    double *yl0, *yln, *yh0, *yhm, *yhn, *er, *w, *k, *red, *h, *scal;
+};
+
+struct DimRun {
+    int n, len;
+    double eps, relerr, abserr;
+    cudaStream_t st;
+    DimBuffers B;
+    double *h_pinned;  // [0] h to upload, [1] reduction result read back
+};
+
+static unsigned grid_of(int len) { return (unsigned)((len + 255) / 256); }
+
+// One Fehlberg step of size *hdev from y0: yn and (want_er) er (dim/rkf_kernel.cu fehl).
+static cudaError_t dim_fehl(const DimRun &R, const double *y0, double *yn, bool want_er)
+{
+    const int n = R.n, len = R.len;
+    const unsigned ga = (unsigned)((n + kDimParticlesPerBlock - 1) / kDimParticlesPerBlock);
+    const unsigned threads = kDimParticlesPerBlock * kDimChunks;
+    double *k = R.B.k;
+    dim_accel_kernel<<<ga, threads, 0, R.st>>>(n, R.eps, y0, k);
+    for (int s = 0; s < 5; s++) {
+        dim_combine_kernel<<<grid_of(len), 256, 0, R.st>>>(len, s, s + 1, true, R.B.h, y0, k, R.B.w);
+        dim_accel_kernel<<<ga, threads, 0, R.st>>>(n, R.eps, R.B.w, k + (size_t)(s + 1) * len);
+    }
+    dim_combine_kernel<<<grid_of(len), 256, 0, R.st>>>(len, 5, 6, true, R.B.h, y0, k, yn);
+    if (want_er) dim_combine_kernel<<<grid_of(len), 256, 0, R.st>>>(len, 6, 6, false, R.B.h, y0, k, R.B.er);
+    return cudaGetLastError();
+}
+
+static cudaError_t set_h(const DimRun &R, double h)
+{
+    R.h_pinned[0] = h;
+    return cudaMemcpyAsync(R.B.h, R.h_pinned, sizeof(double), cudaMemcpyHostToDevice, R.st);
+}
+
+static cudaError_t read_scalar(const DimRun &R, double *out)
+{
+    cudaError_t e = cudaMemcpyAsync(R.h_pinned + 1, R.B.scal, sizeof(double), cudaMemcpyDeviceToHost, R.st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(R.st);
+    if (e == cudaSuccess) *out = R.h_pinned[1];
+    return e;
+}
+
+// The adaptive loop of dim/rkf_kernel.cu:194-495 (INIT = 1 computes the first step).
+// y (device SoA 6n) holds the state at *x0 on entry and the high track at xe on exit;
+// ese (optional device 6n) the final (yln - yhn)/31.  Returns ier.
+static int dim_integrate(DimRun &R, double *y, double *x0, double xe, int init, double *H, int *nde,
+                         long long *accepted, long long *rejected, double *ese, int *status)
+{
+    const double EPSMIN = 1e-15;
+    const int ITEMAX = 10000;
+    const size_t bytes = (size_t)R.len * sizeof(double);
+    cudaError_t e;
+    *status = BIA_OK;
+#define DIM_CHECK(x)                          \
+    do {                                      \
+        e = (x);                              \
+        if (e != cudaSuccess) {               \
+            *status = cuda_status(e);         \
+            return 0;                         \
+        }                                     \
+    } while (0)
+    DIM_CHECK(cudaMemcpyAsync(R.B.yh0, y, bytes, cudaMemcpyDeviceToDevice, R.st));
+    DIM_CHECK(cudaMemcpyAsync(R.B.yl0, y, bytes, cudaMemcpyDeviceToDevice, R.st));
+    *nde = 0;
+    if (init == 1) {
+        const unsigned ga = (unsigned)((R.n + kDimParticlesPerBlock - 1) / kDimParticlesPerBlock);
+        dim_accel_kernel<<<ga, kDimParticlesPerBlock * kDimChunks, 0, R.st>>>(R.n, R.eps, R.B.yl0, R.B.k);
+        dim_toldy_kernel<<<kDimReduceBlocks, 256, 0, R.st>>>(R.len, R.relerr, R.abserr, R.B.yl0, R.B.k, R.B.red);
+        dim_final_reduce_kernel<<<1, 32, 0, R.st>>>(kDimReduceBlocks, false, R.B.red, R.B.scal);
+        double toldy = 0.0;
+        DIM_CHECK(read_scalar(R, &toldy));
+        *H = std::isinf(toldy) ? EPSMIN * (xe - *x0) : fmin((xe - *x0) / 100e0, pow(toldy, 0.2));
+        *nde = 1;
+    }
+    double X = *x0;
+    int ier = 10000;
+    for (int iter = 0; iter < ITEMAX; iter++) {
+        DIM_CHECK(set_h(R, *H));
+        DIM_CHECK(dim_fehl(R, R.B.yl0, R.B.yln, true));
+        *nde += 6;
+        dim_errnorm_kernel<<<kDimReduceBlocks, 256, 0, R.st>>>(R.len, R.relerr, R.abserr, R.B.yl0, R.B.yln,
+                                                                 R.B.er, R.B.red);
+        dim_final_reduce_kernel<<<1, 32, 0, R.st>>>(kDimReduceBlocks, true, R.B.red, R.B.scal);
+        double erret = 0.0;
+        DIM_CHECK(read_scalar(R, &erret));
+        if (erret < 0.0) {
+            ier = 20000;
+            break;
+        }
+        if (erret > 1) {
+            (*rejected)++;
+            if (erret >= 59049) *H *= 0.1;
+            else *H *= 0.9 / pow(erret, 0.2);
+            if (*H <= EPSMIN) {
+                ier = 30000;
+                break;
+            }
+        } else if (X + *H < xe) {
+            // two half steps on the high track (fhstep, dim/rkf_kernel.cu:318-362)
+            DIM_CHECK(set_h(R, *H / 2));
+            DIM_CHECK(dim_fehl(R, R.B.yh0, R.B.yhm, false));
+            DIM_CHECK(dim_fehl(R, R.B.yhm, R.B.yhn, false));
+            *nde += 12;
+            X += *H;
+            *x0 = X;
+            DIM_CHECK(cudaMemcpyAsync(R.B.yl0, R.B.yln, bytes, cudaMemcpyDeviceToDevice, R.st));
+            DIM_CHECK(cudaMemcpyAsync(R.B.yh0, R.B.yhn, bytes, cudaMemcpyDeviceToDevice, R.st));
+            (*accepted)++;
+            if (erret <= 1.889568e-4) *H *= 5.0;
+            else *H *= 0.9 / pow(erret, 0.2);
+        } else {
+            // last step to xe (dim/rkf_kernel.cu:386-483)
+            *H = xe - X;
+            DIM_CHECK(set_h(R, *H));
+            DIM_CHECK(dim_fehl(R, R.B.yl0, R.B.yln, true));
+            DIM_CHECK(set_h(R, *H / 2));
+            DIM_CHECK(dim_fehl(R, R.B.yh0, R.B.yhm, false));
+            DIM_CHECK(dim_fehl(R, R.B.yhm, R.B.yhn, false));
+            *nde += 18;
+            if (ese) dim_esterr_kernel<<<grid_of(R.len), 256, 0, R.st>>>(R.len, R.B.yln, R.B.yhn, ese);
+            DIM_CHECK(cudaMemcpyAsync(y, R.B.yhn, bytes, cudaMemcpyDeviceToDevice, R.st));
+            DIM_CHECK(cudaMemcpyAsync(R.B.yl0, R.B.yln, bytes, cudaMemcpyDeviceToDevice, R.st));
+            *x0 = xe;
+            (*accepted)++;
+            ier = 0;
+            break;
+        }
+    }
+    if (ier != 0) {  // leave the last accepted high-track state in y
+        DIM_CHECK(cudaMemcpyAsync(y, R.B.yh0, bytes, cudaMemcpyDeviceToDevice, R.st));
+    }
+    DIM_CHECK(cudaStreamSynchronize(R.st));
+#undef DIM_CHECK
+    return ier;
+}
+
+static size_t dim_buffer_doubles(int n)
+{
+    const size_t len = (size_t)6 * n;
+    return 7 * len + 6 * len + kDimReduceBlocks + 8;
+}
+
+static void dim_carve(double *base, int n, DimBuffers &B)
+{
+    const size_t len = (size_t)6 * n;
+    B.yl0 = base;
+    B.yln = base + len;
+    B.yh0 = base + 2 * len;
+    B.yhm = base + 3 * len;
+    B.yhn = base + 4 * len;
+    B.er = base + 5 * len;
+    B.w = base + 6 * len;
+    B.k = base + 7 * len;
+    B.red = base + 13 * len;
+    B.h = B.red + kDimReduceBlocks;
+    B.scal = B.h + 1;
+}
+
+struct DimDropIn {
+    bool ready = false;
+    DeviceBuffer buf, state;
+    double *h_pinned = nullptr;
+};
+static thread_local DimDropIn g_dim;
+
+}  // namespace bia
+
+using namespace bia;
+
+extern "C" int bia_dim_integrate(bia_context *ctx, int n, double eps_th, double *y, double x0, double xe,
+                                 double relerr, double abserr, bia_dim_stats *stats)
+{
+    if (!ctx || n < 1 || !y || !(xe > x0)) return BIA_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = ctx->dim.reserve(dim_buffer_doubles(n) * sizeof(double));
+    if (e != cudaSuccess) return cuda_status(e);
+    if (!ctx->h_dim) {
+        e = cudaMallocHost((void **)&ctx->h_dim, 4 * sizeof(double));
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    DimRun R;
+    R.n = n;
+    R.len = 6 * n;
+    R.eps = eps_th;
+    R.relerr = relerr;
+    R.abserr = abserr;
+    R.st = ctx->stream;
+    R.h_pinned = ctx->h_dim;
+    dim_carve((double *)ctx->dim.ptr, n, R.B);
+    double X = x0, H = 0.0;
+    int nde = 0, status = BIA_OK;
+    long long acc = 0, rej = 0;
+    const int ier = dim_integrate(R, y, &X, xe, 1, &H, &nde, &acc, &rej, nullptr, &status);
+    if (stats) {
+        stats->accepted = acc;
+        stats->rejected = rej;
+        stats->nde = nde;
+        stats->ier = ier;
+        stats->h_last = H;
+        stats->x_reached = X;
+    }
+    if (status != BIA_OK) return status;
+    return ier == 0 ? BIA_OK : BIA_ERR_NOT_CONVERGED;
+}
+
+// Drop-in for rkf_c_ (dim/rkf_kernel.cu:194-495), called from dim/dim_3D.f90:30 as
+// RKF_C(%VAL(NEQ), %VAL(eps_th), X0, XE, Y0, INIT, RELERR, ABSERR, YN, ESTERR, NDE, IER,
+// WK0, WK1, WK2, WK3, WK4).  Host arrays are AoS (x, y, z, u, v, w per particle).
+extern "C" void rkf_c_(const int neq, const double eps_th, double *X0, double *XE, double *YH0, int *INIT,
+                       const double *RELERR, const double *ABSERR, double *YHN, double *ESE, int *NDE, int *IER,
+                       double *H, double *YL0, double *YLN, double *ERR, double *WRK)
+{
+    (void)WRK;
+    if (neq < 6 || neq % 6 || !X0 || !XE || !YH0 || !INIT || !RELERR || !ABSERR || !YHN || !ESE || !NDE ||
+        !IER || !H || !YL0 || !YLN || !ERR || !(*XE > *X0)) {
+        set_last_error(BIA_ERR_INVALID_ARGUMENT);
+        return;
+    }
+    const int n = neq / 6;
+    DimDropIn &S = g_dim;
+    cudaError_t e = cudaSuccess;
+    if (!S.ready) {
+        e = cudaMallocHost((void **)&S.h_pinned, 4 * sizeof(double));
+        if (e != cudaSuccess) {
+            set_last_error(cuda_status(e));
+            return;
+        }
+        S.ready = true;
+    }
+    if ((e = S.buf.reserve(dim_buffer_doubles(n) * sizeof(double))) != cudaSuccess ||
+        (e = S.state.reserve((size_t)2 * neq * sizeof(double))) != cudaSuccess) {
+        set_last_error(cuda_status(e));
+        return;
+    }
+    double *dy = (double *)S.state.ptr;       // SoA state
+    double *dese = dy + neq;                  // SoA esterr
+    // AoS host -> SoA device
+    double *tmp = (double *)malloc(sizeof(double) * neq);
+    if (!tmp) {
+        set_last_error(BIA_ERR_OUT_OF_MEMORY);
+        return;
+    }
+    for (int i = 0; i < n; i++)
+        for (int c = 0; c < 6; c++) tmp[(size_t)c * n + i] = YH0[6 * (size_t)i + c];
+    e = cudaMemcpy(dy, tmp, sizeof(double) * neq, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        free(tmp);
+        set_last_error(cuda_status(e));
+        return;
+    }
+    DimRun R;
+    R.n = n;
+    R.len = neq;
+    R.eps = eps_th;
+    R.relerr = *RELERR;
+    R.abserr = *ABSERR;
+    R.st = 0;
+    R.h_pinned = S.h_pinned;
+    dim_carve((double *)S.buf.ptr, n, R.B);
+    int nde = 0, status = BIA_OK;
+    long long acc = 0, rej = 0;
+    const int init = *INIT;
+    const int ier = dim_integrate(R, dy, X0, *XE, init, H, &nde, &acc, &rej, dese, &status);
+    if (init == 1) *INIT = 2;
+    *NDE = nde;
+    *IER = ier;
+    if (status == BIA_OK) {
+        // SoA device -> AoS host: YHN (high track), YL0 / YLN (low track), ESE, ERR
+        double *outs[4] = {YHN, YLN, ESE, ERR};
+        const double *srcs[4] = {dy, R.B.yl0, dese, R.B.er};
+        for (int o = 0; o < 4 && e == cudaSuccess; o++) {
+            if (ier != 0 && o == 2) continue;
+            e = cudaMemcpy(tmp, srcs[o], sizeof(double) * neq, cudaMemcpyDeviceToHost);
+            if (e == cudaSuccess)
+                for (int i = 0; i < n; i++)
+                    for (int c = 0; c < 6; c++) outs[o][6 * (size_t)i + c] = tmp[(size_t)c * n + i];
+        }
+        if (e == cudaSuccess) {
+            memcpy(YL0, YLN, sizeof(double) * neq);  // after the last step YL0 = YLN
+            if (ier == 0) memcpy(YH0, YHN, sizeof(double) * neq);
+        }
+        status = cuda_status(e);
+    }
+    free(tmp);
+    set_last_error(status != BIA_OK ? status : (ier == 0 ? BIA_OK : BIA_ERR_NOT_CONVERGED));
+}

@@ -136,6 +136,44 @@ int bia_invariance(bia_context *ctx, int n, double eps_th, const double *x, cons
    denominator of the FP64-bound pair kernel. */
 int bia_measure_fp64_peak(int device, double *tflops);
 
+/* Ensemble of independent systems of uneven size (no counterpart in the reference, which
+   runs one system).  The systems are stored back to back in one set of device SoA arrays:
+   system s owns particles [off_s, off_s + sizes[s]) with off_s = sizes[0] + ... +
+   sizes[s-1], and has pair coupling eps[s] (times q_i q_j when charges are given).
+   Create once (host arrays sizes[nsys], eps[nsys]); every step is one pair-kernel launch
+   over all systems' 32 x 32 blocks plus one reduction launch, and each system's result
+   equals a bia_step of that system alone (same per-block code and summation order). */
+typedef struct bia_ensemble bia_ensemble;
+int bia_ensemble_create(bia_context *ctx, int nsys, const int *sizes, const double *eps,
+                        bia_ensemble **ens);
+int bia_ensemble_destroy(bia_ensemble *ens);
+long long bia_ensemble_particles(const bia_ensemble *ens);
+/* nsteps steps of every system (cfg->eps_th is ignored: each system has its own eps);
+   with use_graph != 0 and a non-default stream the sequence is captured in a CUDA graph */
+int bia_ensemble_run(bia_context *ctx, bia_ensemble *ens, const bia_config *cfg, double *x,
+                     double *y, double *z, double *u, double *v, double *w, const double *q,
+                     int nsteps, int use_graph, bia_stats *stats);
+/* per-system KE and PE (energy[2 s] = sum |v|^2, energy[2 s + 1] = eps_s sum (q_i q_j)/r_ij),
+   host array of 2 nsys doubles; synchronises */
+int bia_ensemble_energy(bia_context *ctx, bia_ensemble *ens, const double *x, const double *y,
+                        const double *z, const double *u, const double *v, const double *w,
+                        const double *q, double *energy);
+
+/* Direct-integration (DIM) reference solver: rebuilds rkf_c_ (dim/rkf_kernel.cu:194-495).
+   y: device state, 6 arrays of n (x, y, z, u, v, w), advanced in place from x0 to xe with
+   a_i = eps_th * sum_j (r_i - r_j) / (|r_ij|^2 + 1e-99)^{3/2} (per-particle coupling as in
+   dim/dim_3D.f90:9, i.e. half the BIA pair coupling) by adaptive RKF4(5) with step
+   doubling (the returned state is the two-half-step track).  BIA_ERR_NOT_CONVERGED when
+   ier != 0 (then y holds the last accepted state). */
+typedef struct bia_dim_stats {
+    long long accepted, rejected; /* steps */
+    int nde;                      /* derivative evaluations, as the reference's NDE */
+    int ier;                      /* 0, 10000 (too many steps), 20000, 30000 (step underflow) */
+    double h_last, x_reached;
+} bia_dim_stats;
+int bia_dim_integrate(bia_context *ctx, int n, double eps_th, double *y, double x0, double xe,
+                      double relerr, double abserr, bia_dim_stats *stats);
+
 const char *bia_status_string(int status);
 /* status of the last drop-in call (find_dxyuv_kernel_, invariance_gpu_, rkf_c_) on this
    host thread */
@@ -160,6 +198,17 @@ void invariance_gpu_(const int N, const double eps_th, double *X, double *Y, dou
                      double *U, double *V, double *W, double *KE, double *PE, double *Lx,
                      double *Ly, double *Lz, double *Ua, double *Va, double *Wa, double *Xa,
                      double *Ya, double *Za);
+
+/* Replaces rkf_c_ (dim/rkf_kernel.cu:194-495), called from dim/dim_3D.f90:30 as
+   RKF_C(%VAL(NEQ), %VAL(eps_th), X0, XE, Y0, INIT, RELERR, ABSERR, YN, ESTERR, NDE, IER,
+   WK0, WK1, WK2, WK3, WK4): host AoS state YH0[neq] at *X0 is integrated to *XE on the
+   device; YHN receives the result, ESE (yln - yhn)/31, NDE the derivative evaluations,
+   IER 0 / 10000 / 20000 / 30000, *H the last step, *X0 = *XE, *INIT = 2, YH0 and YL0 the
+   final tracks, YLN and ERR the last low-track state and error.  On trouble it returns
+   with IER set instead of calling exit(0); WRK is not written. */
+void rkf_c_(const int neq, const double eps_th, double *X0, double *XE, double *YH0, int *INIT,
+            const double *RELERR, const double *ABSERR, double *YHN, double *ESE, int *NDE,
+            int *IER, double *H, double *YL0, double *YLN, double *ERR, double *WRK);
 
 #ifdef __cplusplus
 }

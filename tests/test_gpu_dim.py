@@ -1,0 +1,65 @@
+"""The direct-integration (DIM) reference solver on the GPU (dim/rkf_kernel.cu rebuilt).
+
+Checks: against the oracle's CPU restatement of rkf_c_ on small lattices (same adaptive
+step sequence, final state to 1e-12), against the reference's own DIM run committed as
+OUT/0001332_10^0.DIM (N = 1332, eps_th = -3e-7, 0 -> 1; its adaptive trajectory of
+particle 1 in OUT/0001332.DIM has 239 time levels), energy conservation in quad
+precision (the reference reports dE/E0 = 1.33e-15 for this run, README.md:41), and the
+rkf_c_ drop-in on host arrays.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from bia_3d_gpu_b200 import BIASolver, initial, rkf_c
+from conftest import max_rel_err, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _dim_gpu(cuda, s, eps, x0, xe):
+    t = cuda.tensor(s, device="cuda")
+    with BIASolver() as solver:
+        st = solver.dim_integrate(t, eps, x0, xe)
+        solver.stream.synchronize()
+    return t.cpu().numpy(), st
+
+
+@pytest.mark.parametrize("NL,eps,xe", [(1, -3e-3, 1.0), (2, -1e-3, 0.5)])
+def test_dim_matches_oracle_small(cuda, NL, eps, xe):
+    s, _ = initial.lattice(NL=NL, seed=7)
+    g, st = _dim_gpu(cuda, s, eps, 0.0, xe)
+    y0 = np.ascontiguousarray(s.T).reshape(-1)
+    yn, ier, nacc, nde = oracle.dim_rkf(y0, eps, 0.0, xe)
+    r = yn.reshape(-1, 6).T
+    assert ier == 0 and st["ier"] == 0
+    assert st["accepted"] == nacc and st["nde"] == nde
+    assert rel_err(g[:3], r[:3]) <= 1e-12 and max_rel_err(g[:3], r[:3]) <= 1e-12
+    assert rel_err(g[3:], r[3:]) <= 1e-12 and max_rel_err(g[3:], r[3:]) <= 1e-12
+
+
+def test_dim_matches_reference_run(cuda, golden, golden_ic):
+    g, st = _dim_gpu(cuda, golden_ic, golden["eps_dim"].item(), 0.0, 1.0)
+    ref = golden["dim_final_aos"].reshape(-1, 6).T
+    assert st["ier"] == 0 and st["x_reached"] == 1.0
+    # the reference wrote one trajectory line per accepted step plus the initial one
+    assert st["accepted"] == golden["dim_p1_traj"].shape[0] - 1
+    assert rel_err(g[:3], ref[:3]) <= 1e-12 and max_rel_err(g[:3], ref[:3]) <= 1e-12
+    assert rel_err(g[3:], ref[3:]) <= 1e-12
+    # particle 1's final line (dim/dim_3D.f90:31, 17 significant digits)
+    assert np.abs(g[:, 0] - golden["dim_p1"][1:]).max() <= 1e-13
+    e0 = oracle.invariance(golden_ic, 2 * golden["eps_dim"].item(), quad=True)
+    e1 = oracle.invariance(g, 2 * golden["eps_dim"].item(), quad=True)
+    assert abs((e1["KE"] + e1["PE"]) / (e0["KE"] + e0["PE"]) - 1) <= 1e-14
+
+
+def test_rkf_c_dropin(cuda):
+    s, _ = initial.lattice(NL=1, seed=9)
+    y0 = np.ascontiguousarray(s.T).reshape(-1)
+    yh0 = y0.copy()  # rkf_c_ overwrites YH0 with the final state, as the reference does
+    out = rkf_c(yh0.size, -3e-3, 0.0, 1.0, yh0, 1, 0.0, 1e-16)
+    yn, ier, nacc, nde = oracle.dim_rkf(y0, -3e-3, 0.0, 1.0)
+    assert out["IER"] == 0 and out["X0"] == 1.0 and out["INIT"] == 2 and out["NDE"] == nde
+    assert np.abs(out["YHN"] - yn).max() <= 1e-12 * np.abs(yn).max()
+    assert np.array_equal(out["YH0"], out["YHN"])
+    assert np.all(np.isfinite(out["ESE"])) and np.abs(out["ESE"]).max() < 1e-12

@@ -1,0 +1,73 @@
+"""Ensemble engine: independent systems of uneven size in one launch per step.
+
+Each system's result must equal a bia_step of that system alone (same per-block code,
+same summation order, so bitwise), and the per-system energies must match the oracle's
+quad-precision invariants (bia/Invariance_QPU.f90 per system).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from bia_3d_gpu_b200 import BIASolver, METHOD_UNIVERSAL, default_config, initial
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [1, 5, 31, 32, 33, 64, 100, 150, 257]
+
+
+def _systems(seed=0):
+    rng = np.random.default_rng(seed)
+    states, eps = [], []
+    for k, n in enumerate(SIZES):
+        s, e = initial.plummer(n, seed=100 + k) if n > 1 else (rng.standard_normal((6, 1)), -2.0)
+        states.append(s)
+        eps.append(-2.0 / n if n > 1 else e)
+    return states, np.array(eps)
+
+
+@pytest.mark.parametrize("method", [1, METHOD_UNIVERSAL])
+def test_ensemble_equals_single_system_steps(cuda, method):
+    states, eps = _systems()
+    whole = cuda.tensor(np.concatenate(states, axis=1), device="cuda")
+    with BIASolver() as solver:
+        ens = solver.ensemble(SIZES, eps)
+        cfg = default_config(dt=1e-3, method=method)
+        st = ens.run(whole, cfg, 3, graph=True)
+        solver.stream.synchronize()
+        got = whole.cpu().numpy()
+        total = sum(n * (n - 1) // 2 for n in SIZES)
+        assert sum(st[k] for k in ("hyperbola", "ellipse", "parabola", "universal", "degenerate")) == 3 * total
+        off = 0
+        for s, e, n in zip(states, eps, SIZES):
+            t = cuda.tensor(s, device="cuda")
+            for _ in range(3):
+                solver.step(t, default_config(eps_th=e, dt=1e-3, method=method), stats=False)
+            solver.stream.synchronize()
+            assert np.array_equal(got[:, off:off + n], t.cpu().numpy()), n
+            off += n
+        ens.close()
+
+
+def test_ensemble_matches_oracle_and_energy(cuda):
+    states, eps = _systems(1)
+    whole = cuda.tensor(np.concatenate(states, axis=1), device="cuda")
+    with BIASolver() as solver:
+        ens = solver.ensemble(SIZES, eps)
+        ke, pe = ens.energy(whole)
+        for k, (s, e) in enumerate(zip(states, eps)):
+            ref = oracle.invariance(s, e, quad=True)
+            assert abs(ke[k] - ref["KE"]) <= 1e-13 * max(1.0, abs(ref["KE"]))
+            assert abs(pe[k] - ref["PE"]) <= 1e-13 * max(1e-300, abs(ref["PE"]))
+        ens.run(whole, default_config(dt=1e-3), 2, graph=False)
+        solver.stream.synchronize()
+        got = whole.cpu().numpy()
+        ens.close()
+    off = 0
+    for s, e, n in zip(states, eps, SIZES):
+        r = s
+        for _ in range(2):
+            r, _, _ = oracle.bia_step(r, e, 1e-3)
+        g = got[:, off:off + n]
+        scale = max(np.abs(r[:3]).max(), 1e-300)
+        assert np.abs(g[:3] - r[:3]).max() <= 1e-12 * scale, n
+        off += n
