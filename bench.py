@@ -20,6 +20,14 @@ JSON line is printed by rank 0.
   cpu_baseline  the CPU oracle (a C restatement of the reference's CPU path), OpenMP
             on all host cores, on a seeded sample of rows i (all j > i) of the workload
 
+Other workloads (own JSON line each):
+  --workload plummer_ensemble_4096  4096 independent Plummer systems, N_s uniform in
+            [32, 1024] (seeded), eps_s = -2/N_s, dt = 1e-4, 200 steps captured in one CUDA
+            graph: systems-steps/s, pair-updates/s and per-system energy drift
+  --workload dim_lattice_1332  the direct-integration reference solver (dim/rkf_kernel.cu
+            rebuilt) on a seeded 1332-particle lattice, eps = -3e-7, t = 0 -> 1 (the
+            reference's own DIM run of this size took 2.946 s on a TITAN V, README.md:41)
+
 --impl reference times the reference's CPU implementation of the path: its Fortran
 sources cannot be compiled on this image (no Fortran compiler), so the C restatement
 runs in its place, on all host cores, a bounded row sample per step.
@@ -79,8 +87,11 @@ def parse():
     ap.add_argument("--n", type=int, default=None, help="override the particle count")
     ap.add_argument("--method", choices=("alg", "rkf", "universal"), default="alg")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--systems", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-universal", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true")
     return ap.parse_args()
 
 
@@ -194,6 +205,130 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def _init_dist(world):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def _max_over_ranks(dist, value, dev):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_ensemble(args, rank, world, local):
+    """4096 independent Plummer systems of uneven size, 200 steps in
+    one CUDA graph (one pair-kernel launch per step over all systems)."""
+    import torch
+
+    from bia_3d_gpu_b200 import BIASolver, default_config, initial
+    dist = _init_dist(world)
+    dev = torch.device("cuda", local)
+    nsys = args.systems
+    sizes = initial.ensemble_sizes(nsys, 32, 1024, seed=4)
+    states = [initial.plummer(int(n), seed=10000 + k)[0] for k, n in enumerate(sizes)]
+    eps = -2.0 / sizes.astype(np.float64)
+    host = np.ascontiguousarray(np.concatenate(states, axis=1))
+    steps = args.steps if args.steps is not None else 200
+    dt = 1e-4
+    method = {"rkf": 0, "alg": 1, "universal": 2}[args.method]
+    cfg = default_config(dt=dt, method=method)
+    pairs = int(sum(int(n) * (int(n) - 1) // 2 for n in sizes))
+    solver = BIASolver(device=local)
+    ens = solver.ensemble(sizes, eps)
+    d = torch.tensor(host, device=dev)
+    ke0, pe0 = ens.energy(d)
+    with torch.cuda.stream(solver.stream):
+        ens.run(d, cfg, args.warmup, graph=False, stats=False)     # warm-up (untimed)
+    d.copy_(torch.tensor(host, device=dev))
+    ens.run(d, cfg, steps, graph=True, stats=False)              # capture the graph
+    d.copy_(torch.tensor(host, device=dev))
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    e0.record(solver.stream)
+    st = ens.run(d, cfg, steps, graph=True, stats=False)
+    e1.record(solver.stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = _max_over_ranks(dist, e0.elapsed_time(e1), dev)
+    stats = solver.counters(reset=True)
+    ke1, pe1 = ens.energy(d)
+    drift = np.abs((ke1 + pe1) / (ke0 + pe0) - 1)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "BIA ensemble systems-steps/s (plain FP64 step)",
+            "value": world * nsys * steps / (ms * 1e-3), "unit": "systems-steps/s",
+            "pair_updates_per_s": world * pairs * steps / (ms * 1e-3), "n_gpus": world,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": "plummer_ensemble_4096", "systems": nsys,
+                       "n_min": int(sizes.min()), "n_max": int(sizes.max()),
+                       "particles": int(sizes.sum()), "pairs_per_step": pairs, "dt": dt,
+                       "method": args.method, "graph": True,
+                       "l2": "per-step working set (partials %.1f GB) exceeds the 126 MB L2"
+                             % (sum(6 * 32 * ((int(n) + 31) // 32) ** 2 for n in sizes) * 8e-9),
+                       "parallelism": f"replicas x{world}"},
+            "energy_drift": {"max": float(drift.max()), "median": float(np.median(drift)),
+                             "p99": float(np.quantile(drift, 0.99))},
+            "clocks": clocks, "gpu_launches": 2 * steps,
+            "stats": stats}), flush=True)
+    ens.close()
+    solver.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_dim(args, rank, world, local):
+    """The direct-integration reference solver on the reference's DIM run shape."""
+    import torch
+
+    from bia_3d_gpu_b200 import BIASolver, initial
+    dist = _init_dist(world)
+    dev = torch.device("cuda", local)
+    s, _ = initial.lattice(NL=5, seed=0)
+    eps = -3e-7
+    solver = BIASolver(device=local)
+    d = torch.tensor(s, device=dev)
+    solver.dim_integrate(d, eps, 0.0, 0.05)                       # warm-up (untimed)
+    d.copy_(torch.tensor(s, device=dev))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    st = solver.dim_integrate(d, eps, 0.0, 1.0)
+    torch.cuda.synchronize()
+    wall = _max_over_ranks(dist, time.perf_counter() - t0, dev)
+    inv0 = solver.invariance(torch.tensor(s, device=dev), 2 * eps)
+    inv1 = solver.invariance(d, 2 * eps)
+    e0, e1 = inv0["KE"] + inv0["PE"], inv1["KE"] + inv1["PE"]
+    if rank == 0:
+        print(json.dumps({
+            "metric": "DIM RKF45 wall-clock, t = 0 -> 1", "value": wall, "unit": "s",
+            "n_gpus": world, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lattice)",
+            "config": {"workload": "dim_lattice_1332", "n": s.shape[1], "eps_th": eps,
+                       "relerr": 0.0, "abserr": 1e-16},
+            "accepted_steps": st["accepted"], "rejected_steps": st["rejected"],
+            "derivative_evaluations": st["nde"], "energy_error": e1 / e0 - 1,
+            "reference_published": {"value": 2.946, "unit": "s", "hardware": "TITAN V",
+                                    "source": "README.md:41"}}), flush=True)
+    solver.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -208,6 +343,12 @@ def main():
     from bia_3d_gpu_b200 import BIASolver, default_config, initial, measure_fp64_peak
 
     torch.cuda.set_device(local)
+    if args.workload == "plummer_ensemble_4096":
+        run_ensemble(args, rank, world, local)
+        return
+    if args.workload == "dim_lattice_1332":
+        run_dim(args, rank, world, local)
+        return
     dist = None
     if world > 1:
         import datetime
@@ -306,6 +447,87 @@ def main():
                 "flops_per_launch": per_launch_flops, "kernel_ms_per_launch": per_launch_s * 1e3,
                 "kernel": "bia_pair_tiles_kernel<true>"}
 
+    # the same workload advanced by the universal-variable method (every pair on the
+    # Stumpff-function solver): timing, and its distance from the ALG run after K steps
+    universal = None
+    if method == 1 and not args.no_universal:
+        cfg_u = default_config(eps_th=eps, dt=dt, method=2)
+        u_state = torch.tensor(state, device=dev)
+        a_state = torch.tensor(state, device=dev)
+        with torch.cuda.stream(stream):
+            solver.step(u_state, cfg_u, q=d_q, stats=False)
+            u_state.copy_(torch.tensor(state, device=dev))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            barrier()
+            e0.record(stream)
+            solver.run(u_state, cfg_u, steps, q=d_q, graph=True, stats=False)
+            e1.record(stream)
+            barrier()
+            u_ms = e0.elapsed_time(e1)
+            solver.run(a_state, cfg, steps, q=d_q, graph=True, stats=False)
+            barrier()
+        ua, aa = u_state.cpu().numpy(), a_state.cpu().numpy()
+        if dist is not None:
+            t = torch.tensor([u_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            u_ms = float(t.item())
+        universal = {"value": world * steps * pairs / (u_ms * 1e-3), "unit": "pair-updates/s",
+                     "ms_per_step": u_ms / steps, "graph": True,
+                     "rel_pos_diff_vs_alg": float(np.linalg.norm(ua[:3] - aa[:3]) /
+                                                  np.linalg.norm(aa[:3])),
+                     "rel_vel_diff_vs_alg": float(np.linalg.norm(ua[3:] - aa[3:]) /
+                                                  np.linalg.norm(aa[3:]))}
+
+    # the reference's own GPU pair kernel (bia/find_dXYUV_kernel.cu built for sm_100a by
+    # oracle/build_ref.sh) on a seeded row sample of a global-coupling workload
+    # (plummer_32768: the reference has one eps for all pairs, so no Coulomb charges),
+    # through its per-particle entry with its own per-call allocation and copies
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        import oracle
+        if oracle.ref_gpu_available():
+            ps, peps, _, pdt, _ = initial.make("plummer_32768")
+            pn = ps.shape[1]
+            rows = np.random.default_rng(5).choice(np.arange(2, pn + 1), 256, replace=False)
+            oracle.ref_gpu_rows(ps, peps, pdt, rows[:4])
+            t0 = time.perf_counter()
+            oracle.ref_gpu_rows(ps, peps, pdt, rows)
+            el = time.perf_counter() - t0
+            rpairs = int(sum(pn - r for r in rows))
+            # ours through the same per-row drop-in entry (host buffers, one row per call)
+            from bia_3d_gpu_b200 import find_dxyuv_kernel
+            acc = [np.zeros(pn) for _ in range(6)]
+            rel, out = np.zeros(6 * pn), np.zeros(6 * pn)
+
+            def _our_rows(rr):
+                for r_ in rr:
+                    for k_ in range(6):
+                        rel[k_::6] = ps[k_, r_ - 1] - ps[k_]
+                    find_dxyuv_kernel(1, pn, int(r_), peps, pdt, 18, *acc, rel, out)
+
+            _our_rows(rows[:4])
+            t0 = time.perf_counter()
+            _our_rows(rows)
+            el_ours = time.perf_counter() - t0
+            pt = torch.tensor(ps, device=dev)
+            pcfg = default_config(eps_th=peps, dt=pdt)
+            with torch.cuda.stream(stream):
+                solver.step(pt, pcfg, stats=False)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(3):
+                    solver.step(pt, pcfg, stats=False)
+                e1.record(stream)
+            torch.cuda.synchronize()
+            ref_gpu = {"workload": "plummer_32768", "unit": "pair-updates/s",
+                       "reference_kernel": rpairs / el,
+                       "ours_dropin_rows": rpairs / el_ours,
+                       "ours_alg": 3 * (pn * (pn - 1) // 2) / (e0.elapsed_time(e1) * 1e-3),
+                       "sample": f"{len(rows)} seeded rows I through find_dxyuv_kernel_ (reference, "
+                                 f"and ours as reference_kernel / ours_dropin_rows; ours_alg "
+                                 f"is the whole-step kernel path), "
+                                 f"{rpairs} pairs, {el:.2f} s wall"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, sample = cpu_sample(state, eps, q, dt, method, args.cpu_seconds)
@@ -325,7 +547,7 @@ def main():
                        "l2": "256 MB buffer written between timed steps (untimed)",
                        "parallelism": f"replicas x{world}"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-            "gpu_launches": 2 * steps,
+            "gpu_launches": 2 * steps, "universal": universal, "reference_gpu_kernel": ref_gpu,
             "stats": {k: v for k, v in stats.items()},
             "iterations_per_classical_pair": stats["iterations"] / max(
                 1, stats["hyperbola"] + stats["ellipse"] + stats["parabola"]),

@@ -201,3 +201,40 @@ def dim_rkf(y0_aos, eps_th, x0, xe, relerr=0.0, abserr=1e-16):
     ier = lib().oracle_dim_rkf(n, eps_th, x0, xe, _p(y0), relerr, abserr, _p(yn),
                                ctypes.byref(nacc), ctypes.byref(nde))
     return yn, ier, nacc.value, nde.value
+
+
+# ---- the reference's own GPU code, built from its sources by oracle/build_ref.sh ----------
+_REF_PATH = os.path.join(_HERE, "_ref", "libref_bia.so")
+_ref = None
+
+
+def ref_gpu_available():
+    return os.path.exists(_REF_PATH)
+
+
+def ref_gpu_lib():
+    """The reference's find_dxyuv_kernel_ / invariance_gpu_ compiled for sm_100a."""
+    global _ref
+    if _ref is None:
+        L = ctypes.CDLL(_REF_PATH)
+        L.find_dxyuv_kernel_.argtypes = [_I, _I, _I, _D, _D, _I] + [_PD] * 8
+        L.find_dxyuv_kernel_.restype = None
+        _ref = L
+    return _ref
+
+
+def ref_gpu_rows(state, eps_th, dt, rows, itr=18):
+    """The reference's GPU branch of bia/bia.f90:128-140 for the given 1-based rows I
+    (ALG method only): returns the accumulated pair sums (6, n), no drift."""
+    L = ref_gpu_lib()
+    s = _c(state)
+    n = s.shape[1]
+    acc = [np.zeros(n) for _ in range(6)]
+    rel = np.zeros(6 * n)
+    out = np.zeros(6 * n)
+    for I in rows:
+        i = I - 1
+        for k in range(6):
+            rel[k::6] = s[k, i] - s[k]
+        L.find_dxyuv_kernel_(1, n, int(I), eps_th, dt, itr, *[_p(a) for a in acc], _p(rel), _p(out))
+    return np.stack(acc)
