@@ -314,8 +314,16 @@ static __device__ __noinline__ double kepler_safe(double M, double e, double x)
     return x;
 }
 
-static __device__ __noinline__ int ellipse(double eps_th, double dt, int ITR, const double YZ[4],
-                                    double YN[4], double *error, int *fallback)
+#ifndef BIA_INLINE_ELLIPSE
+#define BIA_INLINE_ELLIPSE 0
+#endif
+#if BIA_INLINE_ELLIPSE
+#define BIA_ELLIPSE_LINKAGE __device__ __forceinline__
+#else
+#define BIA_ELLIPSE_LINKAGE static __device__ __noinline__
+#endif
+BIA_ELLIPSE_LINKAGE int ellipse(double eps_th, double dt, int ITR, const double YZ[4], double YN[4],
+                                double *error, int *fallback)
 {
     const double X_ini = YZ[0], Y_ini = YZ[1], U_ini = YZ[2], V_ini = YZ[3];
     const double g2_ini = U_ini * U_ini + V_ini * V_ini;
@@ -651,6 +659,10 @@ __device__ __forceinline__ void stumpff(double x, double c[4])
     c[0] = c0; c[1] = c1; c[2] = c2; c[3] = c3;
 }
 
+// iteration cap of the universal-variable solver; a pair that reaches it is counted as
+// not converged
+constexpr int kUvItMax = 200;
+
 __device__ __forceinline__ int uv_halfdisp(double eps_th, double dt, const double r[3], const double g[3],
                                            double h[6])
 {
@@ -666,26 +678,35 @@ __device__ __forceinline__ int uv_halfdisp(double eps_th, double dt, const doubl
     double s = dt / r0;
     s = s - sig * s * s / (2.0 * r0);
     if (!(s > 0.0)) s = dt / r0;
-    double lo = 0.0, hi = -1.0;
+    // Safeguarded Newton on F(s) = t(s) - dt, F' = r(s) > 0, with the bracket [lo, hi]
+    // (F(0) = -dt < 0; hi < 0 until an upper bound is seen).  A Newton step that leaves
+    // the bracket, or is not below half the step before last, is replaced by bisection,
+    // so the bracket at least halves every two iterations: on hyperbolic branches Newton
+    // from far above the root moves only ~1/sqrt(-beta) per step.
+    double lo = 0.0, hi = -1.0, dx = 1e300, dxold = 1e300;
     int it;
-    for (it = 1; it <= 200; it++) {
+    for (it = 1; it <= kUvItMax; it++) {
         stumpff(beta * s * s, c);
         const double F = r0 * s * c[1] + sig * s * s * c[2] + mu * s * s * s * c[3] - dt;
         const double Fp = r0 * c[0] + sig * s * c[1] + mu * s * s * c[2];
         if (F == 0.0) break;
-        if (F < 0.0) lo = s; else hi = s;
-        double sn = s - F / Fp;
-        bool newton = true;
-        if (!(sn > lo) || (hi > 0.0 && !(sn < hi)) || !(Fp > 0.0)) {
-            sn = (hi > 0.0) ? 0.5 * (lo + hi) : 2.0 * s;
-            newton = false;
+        const double step = F / Fp;
+        if (Fp > 0.0 && fabs(step) <= 4.0 * 2.220446049250313e-16 * fabs(s)) {
+            s = s - step;  // converged: the remaining correction is a few ulps
+            break;
         }
-        const double ds = sn - s;
+        if (F < 0.0) lo = s; else hi = s;  // a NaN F (overflow far above the root) lowers hi
+        double sn = s - step;
+        const bool newton = (Fp > 0.0) && (sn > lo) && (hi < 0.0 || sn < hi) &&
+                            (hi < 0.0 || fabs(step) <= 0.5 * dxold);
+        if (!newton) sn = (hi > 0.0) ? 0.5 * (lo + hi) : 2.0 * s;
+        dxold = dx;
+        dx = fabs(sn - s);
         s = sn;
-        if (fabs(ds) <= 4.0 * 2.220446049250313e-16 * fabs(s)) break;
+        if (dx <= 4.0 * 2.220446049250313e-16 * fabs(s)) break;  // bracket collapsed
         // Newton converges quadratically: after a step of relative size 1e-10 the next
         // one would be below rounding, so s is final without another evaluation
-        if (newton && fabs(ds) <= 1e-10 * fabs(s)) break;
+        if (newton && dx <= 1e-10 * fabs(s)) break;
     }
     stumpff(beta * s * s, c);
     const double s2c2 = s * s * c[2], s3c3 = s * s * s * c[3];
@@ -731,19 +752,90 @@ __device__ __forceinline__ int alg_classify(double eps_ij, const double r[3], co
 // instantiated per method so it carries only that method's code and registers.
 constexpr int kMethodRkf = 0, kMethodAlg = 1, kMethodUniversal = 2;
 
+__device__ __forceinline__ void count_nonfinite(const double h[6], PairCounters &cnt)
+{
+    bool finite = true;
+#pragma unroll
+    for (int k = 0; k < 6; k++) finite = finite && isfinite(h[k]);
+    if (!finite) cnt.nonfinite++;
+}
+
+// Half-displacement from the in-plane solution: h = ((dr . e - g dt) / 2, (dg . e) / 2)
+// (bia/bia.f90:170-191).
+__device__ __forceinline__ void compose_halfdisp(const PairParams &P, const double g[3], const double e_xi[3],
+                                                 const double e_eta[3], const double YZ[4],
+                                                 const double YN[4], double h[6])
+{
+    const double dr_xi = YN[0] - YZ[0], dr_eta = YN[1] - YZ[1];
+    const double dg_xi = YN[2] - YZ[2], dg_eta = YN[3] - YZ[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        h[k] = (dr_xi * e_xi[k] + dr_eta * e_eta[k] - g[k] * P.dt) * 0.5;
+        h[3 + k] = (dg_xi * e_xi[k] + dg_eta * e_eta[k]) * 0.5;
+    }
+}
+
+// ALG pair whose class C is known (kClsHyp, kClsEll or kClsPar): frame, conic solver,
+// half-displacement (bia/bia.f90:141-191).
+template <int C>
+__device__ __forceinline__ void alg_conic_pair(const PairParams &P, double eps_ij, const double r[3],
+                                               const double g[3], double h[6], PairCounters &cnt)
+{
+    double e_xi[3], e_eta[3], YZ[4], YN[4];
+    double error = 0.0;
+    frame_xi_eta(r, g, e_xi, e_eta, YZ);
+    if (C == kClsHyp) {
+        int bx = 0, fb = 0;
+        cnt.it_hyp += hyperbola(eps_ij, P.dt, P.itr, YZ, YN, &error, &bx, &fb);
+        cnt.bracket_exits += bx;
+        cnt.fallbacks += fb;
+        cnt.cls[kHyperbola]++;
+    } else if (C == kClsEll) {
+        int fb = 0;
+        cnt.it_ell += ellipse(eps_ij, P.dt, P.itr, YZ, YN, &error, &fb);
+        cnt.fallbacks += fb;
+        cnt.cls[kEllipse]++;
+    } else {
+        cnt.it_par += parabola(eps_ij, P.dt, YZ, YN, &error);
+        cnt.cls[kParabola]++;
+    }
+    if (fabs(error) > P.err) cnt.nonconverged++;
+    compose_halfdisp(P, g, e_xi, e_eta, YZ, YN, h);
+    count_nonfinite(h, cnt);
+}
+
+// ALG pair of the rare classes (parabola, degenerate, near-unit eccentricity): c is
+// alg_classify's answer for it.
+__device__ __forceinline__ void alg_rare_pair(const PairParams &P, double eps_ij, const double r[3],
+                                              const double g[3], double h[6], PairCounters &cnt, int c)
+{
+    if (c == kClsPar) {
+        alg_conic_pair<kClsPar>(P, eps_ij, r, g, h, cnt);
+    } else {
+        const int it = uv_halfdisp(eps_ij, P.dt, r, g, h);
+        cnt.it_uv += it;
+        if (it > kUvItMax) cnt.nonconverged++;
+        cnt.cls[c == kClsDeg ? kDegenerate : kUniversal]++;
+        count_nonfinite(h, cnt);
+    }
+}
+
 template <int M>
 __device__ __forceinline__ void pair_halfdisp(const PairParams &P, double eps_ij, const double r[3],
                                               const double g[3], double h[6], PairCounters &cnt)
 {
     if (M == kMethodUniversal) {
-        cnt.it_uv += uv_halfdisp(eps_ij, P.dt, r, g, h);
+        const int it = uv_halfdisp(eps_ij, P.dt, r, g, h);
+        cnt.it_uv += it;
+        if (it > kUvItMax) cnt.nonconverged++;
         cnt.cls[kUniversal]++;
+        count_nonfinite(h, cnt);
     } else if (M == kMethodAlg) {
         const int c = alg_classify(eps_ij, r, g);
         if (c == kClsUv || c == kClsDeg) {
-            cnt.it_uv += uv_halfdisp(eps_ij, P.dt, r, g, h);
-            cnt.cls[c == kClsDeg ? kDegenerate : kUniversal]++;
+            alg_rare_pair(P, eps_ij, r, g, h, cnt, c);
         } else {
+            // one copy of the frame and composition for the three conic branches
             double e_xi[3], e_eta[3], YZ[4], YN[4];
             double error = 0.0;
             frame_xi_eta(r, g, e_xi, e_eta, YZ);
@@ -763,13 +855,8 @@ __device__ __forceinline__ void pair_halfdisp(const PairParams &P, double eps_ij
                 cnt.cls[kParabola]++;
             }
             if (fabs(error) > P.err) cnt.nonconverged++;
-            const double dr_xi = YN[0] - YZ[0], dr_eta = YN[1] - YZ[1];
-            const double dg_xi = YN[2] - YZ[2], dg_eta = YN[3] - YZ[3];
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                h[k] = (dr_xi * e_xi[k] + dr_eta * e_eta[k] - g[k] * P.dt) * 0.5;
-                h[3 + k] = (dg_xi * e_xi[k] + dg_eta * e_eta[k]) * 0.5;
-            }
+            compose_halfdisp(P, g, e_xi, e_eta, YZ, YN, h);
+            count_nonfinite(h, cnt);
         }
     } else {
         double e_xi[3], e_eta[3], YZ[4], YN[4];
@@ -780,18 +867,9 @@ __device__ __forceinline__ void pair_halfdisp(const PairParams &P, double eps_ij
         cnt.cls[degenerate ? kDegenerate : kRkf]++;
         cnt.rkf_steps += nacc;
         if (fabs(error) > P.err) cnt.nonconverged++;
-        const double dr_xi = YN[0] - YZ[0], dr_eta = YN[1] - YZ[1];
-        const double dg_xi = YN[2] - YZ[2], dg_eta = YN[3] - YZ[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            h[k] = (dr_xi * e_xi[k] + dr_eta * e_eta[k] - g[k] * P.dt) * 0.5;
-            h[3 + k] = (dg_xi * e_xi[k] + dg_eta * e_eta[k]) * 0.5;
-        }
+        compose_halfdisp(P, g, e_xi, e_eta, YZ, YN, h);
+        count_nonfinite(h, cnt);
     }
-    bool finite = true;
-#pragma unroll
-    for (int k = 0; k < 6; k++) finite = finite && isfinite(h[k]);
-    if (!finite) cnt.nonfinite++;
 }
 
 }  // namespace bia

@@ -66,6 +66,114 @@ __device__ __forceinline__ void flush_counters(const PairCounters &c, unsigned l
     }
 }
 
+// Class-compacted ALG warp-block.  A warp that walks the 32 rotation steps together runs
+// the hyperbola, ellipse and universal-variable code at nearly every step, because almost
+// every step has lanes of each class.  Here each lane first classifies its own pairs (one
+// bit per rotation offset k in a mask per class), then the warp runs the hyperbola
+// pairs, the ellipse pairs and the rare classes as three loops, each lane taking its next
+// pair of that class: every loop turn is one class on all busy lanes, and the number of
+// turns is the largest per-lane count of that class instead of 32.  Column states and
+// column sums live in this warp's slice of shared memory; lanes that hit the same column
+// in one turn add their h in lane order (__match_any_sync groups), so the column sums
+// have a fixed order for given inputs and the step stays bitwise reproducible.
+#ifndef BIA_ALG_COMPACT
+#define BIA_ALG_COMPACT 1
+#endif
+constexpr int kTileWarps = 8;              // warps per CTA of every kernel using warp-blocks
+constexpr int kTileSmemDoubles = 13 * 32;  // per warp: column state [7][32], sums [6][32]
+
+template <int C>
+__device__ __forceinline__ void compact_class_loop(unsigned m, const double si[7], const double *ws,
+                                                   double *wacc, int lane, bool has_q, double eps_th,
+                                                   const PairParams &P, double racc[6], PairCounters &cnt)
+{
+    const unsigned full = 0xffffffffu;
+    const unsigned lt = (1u << lane) - 1u;
+    for (;;) {
+        const bool busy = (m != 0u);
+        const unsigned bm = __ballot_sync(full, busy);
+        if (bm == 0u) break;
+        if (busy) {
+            const int k = __ffs(m) - 1;
+            m &= m - 1u;
+            const int j = (lane + k) & 31;
+            double sc[7];
+#pragma unroll
+            for (int c = 0; c < 7; c++) sc[c] = ws[c * 32 + j];
+            const double r[3] = {si[0] - sc[0], si[1] - sc[1], si[2] - sc[2]};
+            const double g[3] = {si[3] - sc[3], si[4] - sc[4], si[5] - sc[5]};
+            const double eps_ij = has_q ? eps_th * si[6] * sc[6] : eps_th;
+            double h[6];
+            if (C == kClsUv) {
+                alg_rare_pair(P, eps_ij, r, g, h, cnt, alg_classify(eps_ij, r, g));
+            } else {
+                alg_conic_pair<C>(P, eps_ij, r, g, h, cnt);
+            }
+#pragma unroll
+            for (int c = 0; c < 6; c++) racc[c] += h[c];
+            const unsigned grp = __match_any_sync(bm, j);
+            const int rank = __popc(grp & lt);
+            const int turns = (int)__reduce_max_sync(bm, (unsigned)__popc(grp));
+            for (int t = 0; t < turns; t++) {
+                if (rank == t) {
+#pragma unroll
+                    for (int c = 0; c < 6; c++) wacc[c * 32 + j] += h[c];
+                }
+                __syncwarp(bm);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void warp_block_solve_compact(const double *x, const double *y, const double *z,
+                                                         const double *u, const double *v, const double *w,
+                                                         const double *q, int n, double eps_th,
+                                                         const PairParams &P, int bi, int bj, int lane,
+                                                         double racc[6], double cacc[6], PairCounters &cnt)
+{
+    __shared__ double s_tile[kTileWarps][kTileSmemDoubles];
+    double *ws = s_tile[(threadIdx.x >> 5) % kTileWarps];
+    double *wacc = ws + 7 * 32;
+    const int i = bi * 32 + lane;
+    double si[7], sj[7];
+    load_particle(x, y, z, u, v, w, q, n, i, si);
+    load_particle(x, y, z, u, v, w, q, n, bj * 32 + lane, sj);
+#pragma unroll
+    for (int c = 0; c < 7; c++) ws[c * 32 + lane] = sj[c];
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+        wacc[c * 32 + lane] = 0.0;
+        racc[c] = 0.0;
+    }
+    counters_zero(cnt);
+    __syncwarp();
+    const bool diag = (bi == bj);
+    const int k0 = diag ? 1 : 0;
+    const int k1 = diag ? 16 : 31;
+    unsigned mh = 0u, me = 0u, mr = 0u;
+    for (int k = k0; k <= k1; k++) {
+        const int src = (lane + k) & 31;
+        const int j = bj * 32 + src;
+        if ((!diag || k < 16 || lane < 16) && i < n && j < n) {
+            const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
+            const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
+            const double eps_ij = q ? eps_th * si[6] * ws[6 * 32 + src] : eps_th;
+            const int c = alg_classify(eps_ij, r, g);
+            const unsigned bit = 1u << k;
+            if (c == kClsHyp) mh |= bit;
+            else if (c == kClsEll) me |= bit;
+            else mr |= bit;
+        }
+    }
+    compact_class_loop<kClsHyp>(mh, si, ws, wacc, lane, q != nullptr, eps_th, P, racc, cnt);
+    compact_class_loop<kClsEll>(me, si, ws, wacc, lane, q != nullptr, eps_th, P, racc, cnt);
+    compact_class_loop<kClsUv>(mr, si, ws, wacc, lane, q != nullptr, eps_th, P, racc, cnt);
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
+    __syncwarp();  // the slice is reused by this warp's next block
+}
+
 // Pairs of warp-block (bi, bj) of the system whose particles are x[0..n) etc.: row sums
 // racc (particle 32 bi + lane) and column sums cacc (particle 32 bj + lane) of the pair
 // half-displacements h (row receives +h, column -h: the caller writes -cacc).
@@ -76,6 +184,10 @@ __device__ __forceinline__ void warp_block_solve(const double *x, const double *
                                                  int bi, int bj, int lane, double racc[6], double cacc[6],
                                                  PairCounters &cnt)
 {
+    if (M == kMethodAlg && BIA_ALG_COMPACT) {
+        warp_block_solve_compact(x, y, z, u, v, w, q, n, eps_th, P, bi, bj, lane, racc, cacc, cnt);
+        return;
+    }
     const unsigned full = 0xffffffffu;
     const int i = bi * 32 + lane;
     double si[7], sj[7];

@@ -259,3 +259,18 @@ def test_invariance_matches_oracle(cuda, golden_ic):
     refq = oracle.invariance(golden_ic, -6e-7, quad=True)
     for name, v in zip(("KE", "PE", "Lx", "Ly", "Lz", "Ua", "Va", "Wa", "Xa", "Ya", "Za"), vals):
         assert abs(v - refq[name]) <= 1e-13 * max(1.0, abs(refq[name])), name
+
+
+@pytest.mark.parametrize("method", [METHOD_ALG, METHOD_UNIVERSAL])
+def test_near_radial_pair_far_above_start_guess(cuda, method):
+    """Two particles a few microns apart closing at 543 of their 563 relative speed: the
+    universal-variable start guess lies far above the root on a hyperbolic branch, where
+    plain Newton crawls.  The step must converge and match the quad-precision oracle."""
+    s = np.zeros((6, 2))
+    s[:3, 0] = [-4.064577389883972e-06, 7.483568417843145e-06, -9.615181365080216e-06]
+    s[3:, 0] = [95.72878999340595, -231.02576430088004, 504.2191870037502]
+    g, st = gpu_run(cuda, s, -2.0, 1e-5, 1, method=method)
+    r, _ = oracle_run(s, -2.0, 1e-5, 1, method=method, quad=True)
+    assert st["nonconverged"] == 0 and st["nonfinite"] == 0
+    assert st["iter_universal"] < 60
+    assert_parity(g, r)

@@ -327,3 +327,21 @@ def test_attractive_hyperbola_bracket_fallback():
     hr, _ = oracle.pair_halfdisp(r, g, eps, dt, method=0, quad=True)
     assert st["universal"] == 1
     assert np.abs(h - hr).max() <= 1e-8 * np.abs(hr).max()
+
+
+def test_universal_variables_converge_from_far_above_root():
+    """A near-radial attractive pair a few microns apart, approaching at 543 of its 563
+    relative speed (from the Coulomb cube after 39 steps): the second-order start guess
+    lies 5000x above the root on a hyperbolic branch, where a Newton step moves s by only
+    1/sqrt(-beta) ~ 0.014.  Plain Newton stopped at the iteration cap with a position
+    displacement of 1e76; the safeguarded iteration (bisection when Newton stalls) must
+    converge and agree with the quad-precision solve."""
+    r = np.array([-4.064577389883972e-06, 7.483568417843145e-06, -9.615181365080216e-06])
+    g = np.array([95.72878999340595, -231.02576430088004, 504.2191870037502])
+    for method in (1, 2):
+        h, st = oracle.pair_halfdisp(r, g, -2.0, 1e-5, method=method)
+        hq, _ = oracle.pair_halfdisp(r, g, -2.0, 1e-5, method=method, quad=True)
+        assert st["nonconverged"] == 0 and st["uv_iterations"] < 60
+        assert np.abs(h[:3] - hq[:3]).max() <= 1e-12 * np.abs(g).max() * 1e-5
+        assert np.abs(h[3:] - hq[3:]).max() <= 1e-12 * np.abs(g).max()
+        assert np.abs(h[:3]).max() < np.abs(g).max() * 1e-5
