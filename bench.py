@@ -60,9 +60,13 @@ FLOPS = {
     "universal": (145, 74),    # per pair, per universal-variable Newton iteration
 }
 
-# DRAM traffic per launch of bia_pair_tiles_kernel at the default workload, from the
-# ncu capture summarised in profiles/ (None until captured).
-TRAFFIC_BYTES_PER_LAUNCH = None
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the ALG pair
+# kernel at coulomb_cube_32768: one ncu capture of bia_pair_phase_kernel at n = 16384
+# (100.5 MB read + 3169.5 MB written, 1.342e8 pairs) scaled by the pairs per launch
+# (x 4.0001); both the partial sums and the local-memory traffic grow with the pairs.
+TRAFFIC_PAIRS_MEASURED = 16384 * 16383 // 2
+TRAFFIC_BYTES_MEASURED = 100.488e6 + 3169.538e6
+TRAFFIC_WORKLOAD = "coulomb_cube_32768"
 
 
 def pair_flops(stats, method):
@@ -437,7 +441,12 @@ def main():
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 6 * n * 8,
                "wall_s": wall}
 
-    # roofline of the pair kernel
+    # roofline of the pair kernel (the ALG step takes the phase-locked kernel once there are
+    # two or more of its 32-warp CTAs per SM, as bia_step.cu decides)
+    nb_blocks = (n + 31) // 32
+    nwb = nb_blocks * (nb_blocks + 1) // 2
+    phase = method == 1 and (nwb + 31) // 32 >= 2 * torch.cuda.get_device_properties(dev).multi_processor_count
+    kernel_name = "bia_pair_phase_kernel<true>" if phase else "bia_pair_tiles_kernel<true>"
     flops_total = pair_flops(stats, method)
     per_launch_flops = flops_total / max(kern_launches, 1)
     per_launch_s = kern_ms * 1e-3 / max(kern_launches, 1)
@@ -445,10 +454,13 @@ def main():
     achieved = per_launch_flops / per_launch_s / 1e12
     roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak if peak else None,
-                "traffic": TRAFFIC_BYTES_PER_LAUNCH,
+                "traffic": (TRAFFIC_BYTES_MEASURED * pairs / TRAFFIC_PAIRS_MEASURED
+                            if args.workload == TRAFFIC_WORKLOAD and method == 1 else None),
+                "traffic_note": "ncu capture at n = 16384 scaled by pairs per launch",
+                "algorithmic_bytes_per_launch": nb_blocks * 6 * n * 8 + 6 * n * 8,
                 "peak_source": "measured live: bia_measure_fp64_peak DFMA loop on this GPU",
                 "flops_per_launch": per_launch_flops, "kernel_ms_per_launch": per_launch_s * 1e3,
-                "kernel": "bia_pair_tiles_kernel<true>"}
+                "kernel": kernel_name}
 
     # the same workload advanced by the universal-variable method (every pair on the
     # Stumpff-function solver): K steps timed as one graph launch, and the distance of one

@@ -14,6 +14,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "bia_internal.cuh"
@@ -74,6 +75,58 @@ __global__ void __launch_bounds__(kEnsThreads, TileOccupancy<M>::kMinBlocks) ens
     flush_counters(cnt, A.stats, lane);
     const int nb = (n + 31) / 32;
     write_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
+}
+
+// Phase-locked ALG variant of ens_pair_tiles_kernel (see phase_block_solve): one CTA of
+// kPhaseWarps warps per SM, each warp on one item; bitwise the same results.
+__global__ void __launch_bounds__(kPhaseWarps * 32, kPhaseMinBlocks) ens_pair_phase_kernel(const EnsArgs A)
+{
+    extern __shared__ double phase_smem[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const long long t = (long long)blockIdx.x * kPhaseWarps + warp;
+    const bool live = t < A.nitems;
+    int s = 0, bi = 0, bj = 0;
+    if (live) {
+        const uint2 it = A.items[t];
+        s = (int)it.x;
+        bi = (int)(it.y & 0xffffu);
+        bj = (int)(it.y >> 16);
+    }
+    const int base = A.off[s];
+    const int n = A.off[s + 1] - base;
+    const double *q = A.q ? A.q + base : nullptr;
+    double racc[6], cacc[6];
+    PairCounters cnt;
+    phase_block_solve(A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base, q, n, A.eps[s],
+                      A.P, bi, bj, lane, live, phase_smem + warp * kTileSmemDoubles, racc, cacc, cnt);
+    if (!live) return;  // warp-uniform; no barrier follows
+    flush_counters(cnt, A.stats, lane);
+    const int nb = (n + 31) / 32;
+    write_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
+}
+
+// Once per device (the current one): dynamic shared memory opt-in of the phase-locked
+// ensemble kernel and the SM count; 0 when the set-up failed (8-warp kernel used).
+static int ens_phase_setup()
+{
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static int sms_of[kMaxDevices] = {};
+    static bool done_of[kMaxDevices] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 0;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!done_of[dev]) {
+        int sms = 0;
+        bool ok = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(ens_pair_phase_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        kPhaseSmemBytes) == cudaSuccess;
+        if (!ok) cudaGetLastError();
+        sms_of[dev] = ok ? sms : 0;
+        done_of[dev] = true;
+    }
+    return sms_of[dev];
 }
 
 struct EnsUpdateArgs {
@@ -199,7 +252,15 @@ static int ens_enqueue_step(bia_context *ctx, bia_ensemble *E, const bia_config 
     case BIA_METHOD_UNIVERSAL:
         ens_pair_tiles_kernel<kMethodUniversal><<<grid, kEnsThreads, 0, ctx->stream>>>(A);
         break;
-    default: ens_pair_tiles_kernel<kMethodAlg><<<grid, kEnsThreads, 0, ctx->stream>>>(A); break;
+    default: {
+        const long long pgrid = (E->nitems + kPhaseWarps - 1) / kPhaseWarps;
+        const int sms = BIA_PHASE_WARPS > 0 ? ens_phase_setup() : 0;
+        if (sms > 0 && pgrid >= 2LL * sms)
+            ens_pair_phase_kernel<<<(unsigned)pgrid, kPhaseWarps * 32, kPhaseSmemBytes, ctx->stream>>>(A);
+        else
+            ens_pair_tiles_kernel<kMethodAlg><<<grid, kEnsThreads, 0, ctx->stream>>>(A);
+        break;
+    }
     }
     EnsUpdateArgs U;
     U.x = x; U.y = y; U.z = z; U.u = u; U.v = v; U.w = w;

@@ -83,9 +83,80 @@ __global__ void __launch_bounds__(kThreads, TileOccupancy<M>::kMinBlocks) bia_pa
     }
 }
 
+// Phase-locked ALG step kernel (see phase_block_solve): one CTA of kPhaseWarps warps per
+// SM, each warp on one warp-block.
+template <bool kDeterministic>
+__global__ void __launch_bounds__(kPhaseWarps * 32, kPhaseMinBlocks) bia_pair_phase_kernel(const StepArgs A)
+{
+    extern __shared__ double phase_smem[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const long long t = (long long)blockIdx.x * kPhaseWarps + warp;
+    const bool live = t < A.nwb;
+    int bi = 0, bj = 0;
+    if (live) warp_block_coords(t, bi, bj);
+    double racc[6], cacc[6];
+    PairCounters cnt;
+    phase_block_solve(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P, bi, bj, lane, live,
+                      phase_smem + warp * kTileSmemDoubles, racc, cacc, cnt);
+    if (!live) return;  // warp-uniform; no barrier follows
+    flush_counters(cnt, A.stats, lane);
+    const int i = bi * 32 + lane;
+    const int jown = bj * 32 + lane;
+    const size_t plane = (size_t)A.npad;
+    if (kDeterministic) {
+        write_partials(A.part, plane, bi, bj, lane, racc, cacc);
+    } else if (bi == bj) {
+#pragma unroll
+        for (int c = 0; c < 6; c++)
+            if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c] - cacc[c]);
+    } else {
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c]);
+            if (jown < A.n) atomicAdd(&A.part[c * plane + jown], -cacc[c]);
+        }
+    }
+}
+
+// Once per device (the current one): opt the phase-locked kernels in to their dynamic
+// shared memory and read the SM count.  Returns the SM count, 0 when the set-up failed
+// (the caller then launches the 8-warp kernel).
+static int phase_kernel_setup()
+{
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static int sms_of[kMaxDevices] = {};
+    static bool done_of[kMaxDevices] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 0;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!done_of[dev]) {
+        int sms = 0;
+        bool ok = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(bia_pair_phase_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        kPhaseSmemBytes) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(bia_pair_phase_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        kPhaseSmemBytes) == cudaSuccess;
+        if (!ok) cudaGetLastError();  // clear; the 8-warp kernel is used instead
+        sms_of[dev] = ok ? sms : 0;
+        done_of[dev] = true;
+    }
+    return sms_of[dev];
+}
+
 template <bool kDeterministic>
 static void launch_pair_tiles(const StepArgs &A, long long grid, cudaStream_t st)
 {
+    if (BIA_PHASE_WARPS > 0 && A.P.method == kMethodAlg) {
+        const long long pgrid = (A.nwb + kPhaseWarps - 1) / kPhaseWarps;
+        const int sms = phase_kernel_setup();
+        // below two CTAs per SM the 8-warp kernel keeps more SMs busy
+        if (sms > 0 && pgrid >= 2LL * sms) {
+            bia_pair_phase_kernel<kDeterministic><<<(unsigned)pgrid, kPhaseWarps * 32, kPhaseSmemBytes, st>>>(A);
+            return;
+        }
+    }
     switch (A.P.method) {
     case kMethodRkf:
         bia_pair_tiles_kernel<kDeterministic, kMethodRkf><<<(unsigned)grid, kThreads, 0, st>>>(A);

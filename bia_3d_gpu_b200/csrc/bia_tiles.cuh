@@ -125,32 +125,32 @@ __device__ __forceinline__ void compact_class_loop(unsigned m, const double si[7
     }
 }
 
-__device__ __forceinline__ void warp_block_solve_compact(const double *x, const double *y, const double *z,
-                                                         const double *u, const double *v, const double *w,
-                                                         const double *q, int n, double eps_th,
-                                                         const PairParams &P, int bi, int bj, int lane,
-                                                         double racc[6], double cacc[6], PairCounters &cnt)
+// Loads of a compacted warp-block and classification of its pairs: the column states go
+// to the warp's shared slice ws (sums zeroed), si receives the row particle, and the class
+// masks (bit k: the pair with column (lane + k) mod 32) are returned in mh, me, mr.
+// live == false leaves every mask empty (a warp without a block that still joins the
+// barriers of a phase-locked CTA).
+__device__ __forceinline__ void compact_prepare(const double *x, const double *y, const double *z,
+                                                const double *u, const double *v, const double *w,
+                                                const double *q, int n, double eps_th, int bi, int bj,
+                                                int lane, bool live, double *ws, double si[7],
+                                                unsigned &mh, unsigned &me, unsigned &mr)
 {
-    __shared__ double s_tile[kTileWarps][kTileSmemDoubles];
-    double *ws = s_tile[(threadIdx.x >> 5) % kTileWarps];
     double *wacc = ws + 7 * 32;
     const int i = bi * 32 + lane;
-    double si[7], sj[7];
+    double sj[7];
     load_particle(x, y, z, u, v, w, q, n, i, si);
     load_particle(x, y, z, u, v, w, q, n, bj * 32 + lane, sj);
 #pragma unroll
     for (int c = 0; c < 7; c++) ws[c * 32 + lane] = sj[c];
 #pragma unroll
-    for (int c = 0; c < 6; c++) {
-        wacc[c * 32 + lane] = 0.0;
-        racc[c] = 0.0;
-    }
-    counters_zero(cnt);
+    for (int c = 0; c < 6; c++) wacc[c * 32 + lane] = 0.0;
     __syncwarp();
+    mh = me = mr = 0u;
+    if (!live) return;
     const bool diag = (bi == bj);
     const int k0 = diag ? 1 : 0;
     const int k1 = diag ? 16 : 31;
-    unsigned mh = 0u, me = 0u, mr = 0u;
     for (int k = k0; k <= k1; k++) {
         const int src = (lane + k) & 31;
         const int j = bj * 32 + src;
@@ -165,13 +165,72 @@ __device__ __forceinline__ void warp_block_solve_compact(const double *x, const 
             else mr |= bit;
         }
     }
-    compact_class_loop<kClsHyp>(mh, si, ws, wacc, lane, q != nullptr, eps_th, P, racc, cnt);
-    compact_class_loop<kClsEll>(me, si, ws, wacc, lane, q != nullptr, eps_th, P, racc, cnt);
-    compact_class_loop<kClsUv>(mr, si, ws, wacc, lane, q != nullptr, eps_th, P, racc, cnt);
+}
+
+__device__ __forceinline__ void warp_block_solve_compact(const double *x, const double *y, const double *z,
+                                                         const double *u, const double *v, const double *w,
+                                                         const double *q, int n, double eps_th,
+                                                         const PairParams &P, int bi, int bj, int lane,
+                                                         double racc[6], double cacc[6], PairCounters &cnt)
+{
+    __shared__ double s_tile[kTileWarps][kTileSmemDoubles];
+    double *ws = s_tile[(threadIdx.x >> 5) % kTileWarps];
+    double si[7];
+    unsigned mh, me, mr;
+    compact_prepare(x, y, z, u, v, w, q, n, eps_th, bi, bj, lane, true, ws, si, mh, me, mr);
+#pragma unroll
+    for (int c = 0; c < 6; c++) racc[c] = 0.0;
+    counters_zero(cnt);
+    compact_class_loop<kClsHyp>(mh, si, ws, ws + 7 * 32, lane, q != nullptr, eps_th, P, racc, cnt);
+    compact_class_loop<kClsEll>(me, si, ws, ws + 7 * 32, lane, q != nullptr, eps_th, P, racc, cnt);
+    compact_class_loop<kClsUv>(mr, si, ws, ws + 7 * 32, lane, q != nullptr, eps_th, P, racc, cnt);
     __syncwarp();
 #pragma unroll
-    for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
+    for (int c = 0; c < 6; c++) cacc[c] = ws[(7 + c) * 32 + lane];
     __syncwarp();  // the slice is reused by this warp's next block
+}
+
+// Phase-locked CTAs: kPhaseWarps warps, one warp-block each.  After the classification
+// every warp of the CTA runs the hyperbola loop, then (barrier) the ellipse loop, then
+// (barrier) the rare classes, so the SM fetches one solver's instructions at a time: the
+// mixed-class ALG step is bound by instruction fetch when the warps of one SM sit in
+// different solvers (measured on B200, Coulomb N = 32768: 218 ms per step with 8-warp
+// CTAs, 122 ms phase-locked with 32 warps).  Same per-block arithmetic and order as
+// warp_block_solve_compact, so the results are bitwise equal.  Every thread of the CTA
+// must call it (warps without a block pass live = false); ws is the warp's slice of
+// kTileSmemDoubles doubles.
+#ifndef BIA_PHASE_WARPS
+#define BIA_PHASE_WARPS 32  // 0: never use the phase-locked kernels
+#endif
+#ifndef BIA_PHASE_MIN_BLOCKS
+#define BIA_PHASE_MIN_BLOCKS 1
+#endif
+constexpr int kPhaseWarps = BIA_PHASE_WARPS > 0 ? BIA_PHASE_WARPS : 8;
+constexpr int kPhaseMinBlocks = BIA_PHASE_MIN_BLOCKS;
+constexpr int kPhaseSmemBytes = kPhaseWarps * kTileSmemDoubles * (int)sizeof(double);
+
+__device__ __forceinline__ void phase_block_solve(const double *x, const double *y, const double *z,
+                                                  const double *u, const double *v, const double *w,
+                                                  const double *q, int n, double eps_th, const PairParams &P,
+                                                  int bi, int bj, int lane, bool live, double *ws,
+                                                  double racc[6], double cacc[6], PairCounters &cnt)
+{
+    double si[7];
+    unsigned mh, me, mr;
+    counters_zero(cnt);
+#pragma unroll
+    for (int c = 0; c < 6; c++) racc[c] = 0.0;
+    compact_prepare(x, y, z, u, v, w, q, n, eps_th, bi, bj, lane, live, ws, si, mh, me, mr);
+    const bool hq = q != nullptr;
+    __syncthreads();
+    compact_class_loop<kClsHyp>(mh, si, ws, ws + 7 * 32, lane, hq, eps_th, P, racc, cnt);
+    __syncthreads();
+    compact_class_loop<kClsEll>(me, si, ws, ws + 7 * 32, lane, hq, eps_th, P, racc, cnt);
+    __syncthreads();
+    compact_class_loop<kClsUv>(mr, si, ws, ws + 7 * 32, lane, hq, eps_th, P, racc, cnt);
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < 6; c++) cacc[c] = ws[(7 + c) * 32 + lane];
 }
 
 // Pairs of warp-block (bi, bj) of the system whose particles are x[0..n) etc.: row sums

@@ -71,3 +71,33 @@ def test_ensemble_matches_oracle_and_energy(cuda):
         scale = max(np.abs(r[:3]).max(), 1e-300)
         assert np.abs(g[:3] - r[:3]).max() <= 1e-12 * scale, n
         off += n
+
+
+def test_large_ensemble_phase_locked_equals_single_steps(cuda):
+    """Enough warp-blocks (about 20000) for the phase-locked ALG ensemble kernel: every
+    system still equals its own single-system step bitwise."""
+    rng = np.random.default_rng(5)
+    sizes = [int(x) for x in rng.integers(32, 320, 700)]
+    states, eps = [], []
+    for k, n in enumerate(sizes):
+        s, e, q = initial.coulomb_cube(n, seed=1000 + k, dmin=1e-2)
+        s[:3] *= 0.3
+        states.append(s)
+        eps.append(-2.0 / n)
+    eps = np.array(eps)
+    items = sum((n + 31) // 32 * ((n + 31) // 32 + 1) // 2 for n in sizes)
+    assert items > 2 * 148 * 32
+    whole = cuda.tensor(np.concatenate(states, axis=1), device="cuda")
+    with BIASolver() as solver:
+        ens = solver.ensemble(sizes, eps)
+        ens.run(whole, default_config(dt=1e-4), 1, graph=False)
+        solver.stream.synchronize()
+        got = whole.cpu().numpy()
+        off = 0
+        for s, e, n in zip(states, eps, sizes):
+            t = cuda.tensor(s, device="cuda")
+            solver.step(t, default_config(eps_th=e, dt=1e-4), stats=False)
+            solver.stream.synchronize()
+            assert np.array_equal(got[:, off:off + n], t.cpu().numpy()), n
+            off += n
+        ens.close()

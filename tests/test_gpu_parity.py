@@ -274,3 +274,21 @@ def test_near_radial_pair_far_above_start_guess(cuda, method):
     assert st["nonconverged"] == 0 and st["nonfinite"] == 0
     assert st["iter_universal"] < 60
     assert_parity(g, r)
+
+
+def test_phase_locked_kernel_modes_agree(cuda):
+    """N = 8192 takes the phase-locked ALG kernel (more than two 32-warp CTAs per SM):
+    deterministic mode is bitwise reproducible, atomic mode agrees to rounding, and
+    sampled particles match the oracle."""
+    s, eps, q = initial.coulomb_cube(8192, seed=27)
+    a, st, da = gpu_run(cuda, s, eps, 1e-5, 1, q=q, disp=True)
+    b, _ = gpu_run(cuda, s, eps, 1e-5, 1, q=q)
+    c, _ = gpu_run(cuda, s, eps, 1e-5, 1, q=q, deterministic=0)
+    assert np.array_equal(a, b)
+    assert rel_err(c, a) <= 1e-15
+    assert total_pairs(st) == 8192 * 8191 // 2 and st["ellipse"] > 0 and st["universal"] > 0
+    sel = np.random.default_rng(3).choice(8192, 24, replace=False)
+    ref = oracle.particle_disp(s, eps, 1e-5, sel, q=q)
+    got = da[:, sel].T
+    assert np.abs(got[:, :3] - ref[:, :3]).max() <= 1e-12 * np.abs(s[:3]).max()
+    assert np.abs(got[:, 3:] - ref[:, 3:]).max() <= 1e-12 * np.abs(s[3:]).max()
