@@ -2,22 +2,27 @@
 """Benchmark of the BIA pair step: pair-updates/s on one or more B200s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload coulomb_cube_32768] [--method alg|rkf]
+                    [--workload plummer_32768] [--method learned|alg|universal|rkf]
 
 A step is one BIA step of the workload (all N(N-1)/2 pairs, reduction, drift and state
-update).  Default workload: the plain FP64 BIA step of the Coulomb system, N = 32768,
-charges +-1, unit cube, Maxwellian sigma = 1, dt = 1e-5 (seeded synthetic input).  One
-JSON line is printed by rank 0.
+update).  Default: the learned mixed-precision form (METHOD_LEARNED) on the Plummer sphere,
+N = 32768, G = M = 1, equal masses, dt = 1e-4 (seeded synthetic input), beside the plain
+FP64 form (the reference's ALG algorithm) timed the same way in the same run.  One JSON
+line is printed by rank 0.
 
-  value     pair-updates/s with the state resident in HBM: K steps, each bracketed by
-            CUDA events on the solver's stream, an untimed 256 MB L2 flush between steps
+  value     pair-updates/s with the state resident in HBM: K steps, each from the seeded
+            state, each bracketed by CUDA events on the solver's stream, an untimed 256 MB
+            L2 flush between steps
   e2e       the same through the host-buffer call (bia_run_host): every step copies the
-            state and charges from pinned host memory and the state back
-  roofline  FP64 roofline of the dominant kernel (bia_pair_tiles_kernel): algorithmic
-            FP64 flops per launch (per-branch counts of this run times the per-pair flop
-            model below) over the kernel's event-timed duration, against the DFMA peak
-            measured on the same GPU by bia_measure_fp64_peak
-  cpu_baseline  the CPU oracle (a C restatement of the reference's CPU path), OpenMP
+            state (and charges) from pinned host memory and the state back
+  plain_fp64  the plain FP64 ALG form on the same workload, its speed-up ratio, and the
+            one-step distance of the measured form from it (global relative, positions and
+            velocities)
+  roofline  FP64 roofline of the dominant kernel: algorithmic FP64 flops per launch
+            (per-branch counts of this run times the per-pair flop model below) over the
+            kernel's event-timed duration, against the DFMA peak measured on the same GPU
+            by bia_measure_fp64_peak
+  cpu_baseline  the CPU oracle (a C restatement of the reference's CPU ALG path), OpenMP
             on all host cores, on a seeded sample of rows i (all j > i) of the workload
 
 Other workloads (own JSON line each):
@@ -58,7 +63,11 @@ FLOPS = {
     "parabola": (429, 76),     # per pair, per Barker Newton step
     "rkf": (147, 758),         # per pair, per accepted RKF45 step (3 Fehlberg stages sets)
     "universal": (145, 74),    # per pair, per universal-variable Newton iteration
+    "learned": (330, 0),       # per learned pair: elements, FP64 Halley step, composition
 }
+# BF16 tensor-core flops per learned pair: 2 x (16 x 64 + 64 x 64 + 64 x 64) multiply-adds
+LEARNED_TENSOR_FLOPS = 2 * (16 * 64 + 64 * 64 + 64 * 64)
+METHODS = {"rkf": 0, "alg": 1, "universal": 2, "learned": 3}
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the ALG pair
 # kernel at coulomb_cube_32768: one ncu capture of bia_pair_phase_kernel at n = 16384
@@ -70,8 +79,14 @@ TRAFFIC_WORKLOAD = "coulomb_cube_32768"
 
 
 def pair_flops(stats, method):
+    """Algorithmic FP64 flops of the counted pairs (learned pairs: their FP64 part; a
+    learned pair that fell back is also counted with the universal-variable iterations
+    it ran)."""
     h, e, p, r = FLOPS["hyperbola"], FLOPS["ellipse"], FLOPS["parabola"], FLOPS["rkf"]
     u = FLOPS["universal"]
+    if method == 3:
+        return (stats["learned"] * FLOPS["learned"][0] + stats["universal"] * u[0] +
+                stats["degenerate"] * u[0] + stats["iter_universal"] * u[1])
     deg_rkf = stats["degenerate"] if method == 0 else 0
     deg_uv = stats["degenerate"] - deg_rkf
     return (stats["hyperbola"] * h[0] + stats["iter_hyperbola"] * h[1] +
@@ -87,15 +102,16 @@ def parse():
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", default="coulomb_cube_32768")
+    ap.add_argument("--workload", default="plummer_32768")
     ap.add_argument("--n", type=int, default=None, help="override the particle count")
-    ap.add_argument("--method", choices=("alg", "rkf", "universal"), default="alg")
+    ap.add_argument("--method", choices=("learned", "alg", "rkf", "universal"), default="learned")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--systems", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-universal", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run")
     return ap.parse_args()
 
 
@@ -181,7 +197,8 @@ def run_reference(args, rank, world):
         return
     from bia_3d_gpu_b200 import initial
     state, eps, q, dt, steps_cfg = initial.make(args.workload, n=args.n)
-    method = {"rkf": 0, "alg": 1, "universal": 2}[args.method]
+    # the reference has no learned form: its CPU ALG path is the reference arm for it too
+    method = {"rkf": 0, "alg": 1, "universal": 2, "learned": 1}[args.method]
     steps = args.steps if args.steps is not None else steps_cfg
     per_step = max(0.5, min(3.0, 120.0 / max(1, steps + args.warmup)))
     for w in range(args.warmup):
@@ -194,7 +211,7 @@ def run_reference(args, rank, world):
     value = float(np.median(rates))
     n = state.shape[1]
     line = {
-        "metric": "BIA pair-updates/s (plain FP64 step)", "impl": "reference",
+        "metric": metric_name(args.method), "impl": "reference",
         "value": value, "unit": "pair-updates/s", "n_gpus": world, "steps": steps,
         "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
@@ -207,6 +224,12 @@ def run_reference(args, rank, world):
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def metric_name(method):
+    if method == "learned":
+        return "BIA pair-updates/s: learned-guess form vs plain FP64, at <=1e-12 pos. error"
+    return "BIA pair-updates/s (plain FP64 step)"
 
 
 def _init_dist(world):
@@ -364,10 +387,11 @@ def main():
     n = state.shape[1]
     pairs = n * (n - 1) // 2
     steps = args.steps if args.steps is not None else steps_cfg
-    method = {"rkf": 0, "alg": 1, "universal": 2}[args.method]
+    method = METHODS[args.method]
     cfg = default_config(eps_th=eps, dt=dt, method=method)
     dev = torch.device("cuda", local)
     solver = BIASolver(device=local)
+    solver.load_heads()
     stream = solver.stream
     d_init = torch.tensor(state, device=dev)
     d_state = d_init.clone()
@@ -380,37 +404,46 @@ def main():
             dist.barrier()
             torch.cuda.synchronize()
 
-    # warm-up (untimed): kernels loaded, buffers allocated
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            solver.step(d_state, cfg, q=d_q, stats=False)
-    solver.counters(reset=True)
-    solver.set_timing(True)
-    solver.kernel_ms()
-
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(steps)]
-    sampler = ClockSampler(local)
-    barrier()
-    sampler.start()
-    with torch.cuda.stream(stream):
-        for k in range(steps):
-            d_state.copy_(d_init)              # untimed: every step starts from the seeded state
-            flush.zero_()                      # untimed L2 flush (256 MB > 126 MB L2)
-            ev[k][0].record(stream)
-            solver.step(d_state, cfg, q=d_q, stats=False)
-            ev[k][1].record(stream)
-    barrier()
-    clocks = sampler.stop()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    total_ms = float(sum(step_ms))
-    kern_ms, kern_launches = solver.kernel_ms()
-    solver.set_timing(False)
-    stats = solver.counters(reset=True)
-    if dist is not None:
-        t = torch.tensor([total_ms], device=dev)
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        return float(t.item())
+
+    def timed_steps(c, k_steps, sample_clocks=False):
+        """k_steps steps of config c, each from the seeded state (untimed device copy) after
+        an untimed L2 flush, each bracketed by CUDA events on the solver's stream.  Returns
+        (total ms, clocks, counters, (kernel ms, kernel launches))."""
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                d_state.copy_(d_init)
+                solver.step(d_state, c, q=d_q, stats=False)
+        solver.counters(reset=True)
+        solver.set_timing(True)
+        solver.kernel_ms()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(k_steps)]
+        sampler = ClockSampler(local) if sample_clocks else None
+        barrier()
+        if sampler:
+            sampler.start()
+        with torch.cuda.stream(stream):
+            for k in range(k_steps):
+                d_state.copy_(d_init)              # untimed: every step starts from the seeded state
+                flush.zero_()                      # untimed L2 flush (256 MB > 126 MB L2)
+                ev[k][0].record(stream)
+                solver.step(d_state, c, q=d_q, stats=False)
+                ev[k][1].record(stream)
+        barrier()
+        clk = sampler.stop() if sampler else None
+        total = float(sum(a.elapsed_time(b) for a, b in ev))
+        kern = solver.kernel_ms()
+        solver.set_timing(False)
+        counters = solver.counters(reset=True)
+        return max_over_ranks(total), clk, counters, kern
+
+    total_ms, clocks, stats, (kern_ms, kern_launches) = timed_steps(cfg, steps, sample_clocks=True)
     value = world * steps * pairs / (total_ms * 1e-3)
 
     # end-to-end through the host-buffer call with pinned host memory
@@ -431,52 +464,73 @@ def main():
         e1.record(stream)
         barrier()
         wall = time.perf_counter() - t0
-        e2e_ms = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([e2e_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1))
         h2d = 6 * n * 8 + (n * 8 if q is not None else 0)
         e2e = {"value": world * steps * pairs / (e2e_ms * 1e-3), "unit": "pair-updates/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 6 * n * 8,
                "wall_s": wall}
 
-    # roofline of the pair kernel (the ALG step takes the phase-locked kernel once there are
-    # two or more of its 32-warp CTAs per SM, as bia_step.cu decides)
+    # roofline of the pair kernel: the learned kernel for the learned form; the ALG step
+    # takes the phase-locked kernel once there are two or more of its 32-warp CTAs per SM
+    # (as bia_step.cu decides)
     nb_blocks = (n + 31) // 32
     nwb = nb_blocks * (nb_blocks + 1) // 2
-    phase = method == 1 and (nwb + 31) // 32 >= 2 * torch.cuda.get_device_properties(dev).multi_processor_count
-    kernel_name = "bia_pair_phase_kernel<true>" if phase else "bia_pair_tiles_kernel<true>"
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    if method == 3:
+        kernel_name = "bia_pair_learned_kernel<true>"
+    elif method == 1 and (nwb + 31) // 32 >= 2 * sms:
+        kernel_name = "bia_pair_phase_kernel<true>"
+    else:
+        kernel_name = "bia_pair_tiles_kernel<true>"
     flops_total = pair_flops(stats, method)
     per_launch_flops = flops_total / max(kern_launches, 1)
     per_launch_s = kern_ms * 1e-3 / max(kern_launches, 1)
     peak = measure_fp64_peak(local)
     achieved = per_launch_flops / per_launch_s / 1e12
+    traffic = None
+    if args.workload == TRAFFIC_WORKLOAD and method == 1:
+        traffic = TRAFFIC_BYTES_MEASURED * pairs / TRAFFIC_PAIRS_MEASURED
     roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak if peak else None,
-                "traffic": (TRAFFIC_BYTES_MEASURED * pairs / TRAFFIC_PAIRS_MEASURED
-                            if args.workload == TRAFFIC_WORKLOAD and method == 1 else None),
-                "traffic_note": "ncu capture at n = 16384 scaled by pairs per launch",
+                "frac": achieved / peak if peak else None, "traffic": traffic,
+                "traffic_note": "ncu capture of the ALG kernel at n = 16384 on coulomb_cube, "
+                                "scaled by pairs per launch" if traffic else None,
                 "algorithmic_bytes_per_launch": nb_blocks * 6 * n * 8 + 6 * n * 8,
                 "peak_source": "measured live: bia_measure_fp64_peak DFMA loop on this GPU",
                 "flops_per_launch": per_launch_flops, "kernel_ms_per_launch": per_launch_s * 1e3,
                 "kernel": kernel_name}
+    if method == 3:
+        roofline["bf16_tensor_flops_per_launch"] = stats["learned"] * LEARNED_TENSOR_FLOPS / max(kern_launches, 1)
+
+    # the plain FP64 form (the reference's ALG algorithm) on the same workload, timed the
+    # same way, and the distance of one step of the measured form from one plain step
+    plain = None
+    if method != 1 and not args.no_plain:
+        cfg_p = default_config(eps_th=eps, dt=dt, method=1)
+        p_ms, _, p_stats, _ = timed_steps(cfg_p, steps)
+        a_state = d_init.clone()
+        b_state = d_init.clone()
+        with torch.cuda.stream(stream):
+            solver.step(a_state, cfg_p, q=d_q, stats=False)
+            solver.step(b_state, cfg, q=d_q, stats=False)
+        barrier()
+        aa, bb = a_state.cpu().numpy(), b_state.cpu().numpy()
+        solver.counters(reset=True)
+        plain = {"method": "alg", "value": world * steps * pairs / (p_ms * 1e-3),
+                 "ms_per_step": p_ms / steps, "speedup_of_measured_form": (p_ms / total_ms),
+                 "one_step_rel_pos_err_vs_plain": float(np.linalg.norm(bb[:3] - aa[:3]) /
+                                                        np.linalg.norm(aa[:3])),
+                 "one_step_rel_vel_err_vs_plain": float(np.linalg.norm(bb[3:] - aa[3:]) /
+                                                        np.linalg.norm(aa[3:])),
+                 "newton_iterations_per_classical_pair": p_stats["iterations"] / max(
+                     1, p_stats["hyperbola"] + p_stats["ellipse"] + p_stats["parabola"])}
 
     # the same workload advanced by the universal-variable method (every pair on the
-    # Stumpff-function solver): K steps timed as one graph launch, and the distance of one
-    # universal-variable step from one ALG step, both from the seeded state
+    # Stumpff-function solver): K steps timed as one graph launch
     universal = None
-    if method == 1 and not args.no_universal:
+    if method != 2 and not args.no_universal:
         cfg_u = default_config(eps_th=eps, dt=dt, method=2)
         u_state = d_init.clone()
-        a_state = d_init.clone()
         with torch.cuda.stream(stream):
-            solver.step(u_state, cfg_u, q=d_q, stats=False)
-            solver.step(a_state, cfg, q=d_q, stats=False)
-            barrier()
-            ua, aa = u_state.cpu().numpy(), a_state.cpu().numpy()
-            solver.counters(reset=True)
-            u_state.copy_(d_init)
             solver.run(u_state, cfg_u, 1, q=d_q, graph=True, stats=False)  # warm graph
             u_state.copy_(d_init)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -485,19 +539,10 @@ def main():
             solver.run(u_state, cfg_u, steps, q=d_q, graph=True, stats=False)
             e1.record(stream)
             barrier()
-            u_ms = e0.elapsed_time(e1)
-            ust = solver.counters(reset=True)
-        if dist is not None:
-            t = torch.tensor([u_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            u_ms = float(t.item())
-        dpos = np.linalg.norm(ua[:3] - aa[:3]) / np.linalg.norm(aa[:3] - state[:3])
+        u_ms = max_over_ranks(e0.elapsed_time(e1))
+        ust = solver.counters(reset=True)
         universal = {"value": world * steps * pairs / (u_ms * 1e-3), "unit": "pair-updates/s",
-                     "ms_per_step": u_ms / steps, "graph": True,
-                     "one_step_rel_disp_diff_vs_alg": float(dpos),
-                     "one_step_rel_vel_diff_vs_alg": float(np.linalg.norm(ua[3:] - aa[3:]) /
-                                                           np.linalg.norm(aa[3:])),
-                     "nonconverged": ust["nonconverged"]}
+                     "ms_per_step": u_ms / steps, "graph": True, "nonconverged": ust["nonconverged"]}
 
     # the reference's own GPU pair kernel (bia/find_dXYUV_kernel.cu built for sm_100a by
     # oracle/build_ref.sh) on a seeded row sample of a global-coupling workload
@@ -551,7 +596,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, cores, sample = cpu_sample(state, eps, q, dt, method, args.cpu_seconds)
+        v, cores, sample = cpu_sample(state, eps, q, dt, 1 if method == 3 else method, args.cpu_seconds)
         cpu = {"value": v, "unit": "pair-updates/s", "cores": cores, "kind": "port",
                "sample": sample}
 
@@ -559,18 +604,23 @@ def main():
         dist.barrier()
     if rank == 0:
         line = {
-            "metric": "BIA pair-updates/s (plain FP64 step)", "value": value,
+            "metric": metric_name(args.method), "value": value,
             "unit": "pair-updates/s", "n_gpus": world, "steps": steps, "warmup": args.warmup,
             "ms_per_step": total_ms / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "config": {"workload": args.workload, "n": n, "pairs_per_step": pairs, "dt": dt,
                        "method": args.method, "reduction": "deterministic",
+                       "precision": ("heads: BF16 operands, FP32 accumulation; first correction "
+                                     "FP32; final step, composition and sums FP64"
+                                     if method == 3 else "FP64"),
                        "l2": "256 MB buffer written between timed steps (untimed)",
                        "state": "reset to the seeded state before every timed step (untimed "
                                 "device copy; the e2e loop copies it into the host buffer)",
                        "parallelism": f"replicas x{world}"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-            "gpu_launches": 2 * steps, "universal": universal, "reference_gpu_kernel": ref_gpu,
+            "gpu_launches": 2 * steps, "plain_fp64": plain, "universal": universal,
+            "reference_gpu_kernel": ref_gpu,
+            "learned_pair_fraction": stats["learned"] / max(1, steps * pairs) if method == 3 else None,
             "stats": {k: v for k, v in stats.items()},
             "iterations_per_classical_pair": stats["iterations"] / max(
                 1, stats["hyperbola"] + stats["ellipse"] + stats["parabola"]),

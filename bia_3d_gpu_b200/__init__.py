@@ -13,16 +13,20 @@ Two layers, both backed only by libbia_b200.so (CUDA kernels; no CPU fallback):
   multi-step runs captured in a CUDA graph, host-buffer runs, device invariants.
 """
 import ctypes
+import os
 
 import numpy as np
 
 from . import capi
-from .capi import (BIA_ERR_NONFINITE, BIA_OK, METHOD_ALG, METHOD_RKF, METHOD_UNIVERSAL,
-                   BiaConfig, BiaError, BiaStats, default_config)
+from .capi import (BIA_ERR_NONFINITE, BIA_OK, METHOD_ALG, METHOD_LEARNED, METHOD_RKF,
+                   METHOD_UNIVERSAL, BiaConfig, BiaError, BiaStats, default_config)
 
 __all__ = ["find_dxyuv_kernel", "invariance_gpu", "BIASolver", "default_config", "BiaConfig",
-           "BiaError", "METHOD_ALG", "METHOD_RKF", "METHOD_UNIVERSAL", "INVARIANT_NAMES",
-           "measure_fp64_peak"]
+           "BiaError", "METHOD_ALG", "METHOD_RKF", "METHOD_UNIVERSAL", "METHOD_LEARNED",
+           "INVARIANT_NAMES", "measure_fp64_peak", "HEADS_PATH"]
+
+# the trained heads of BIA_METHOD_LEARNED (bia_3d_gpu_b200/train_heads.py writes them)
+HEADS_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "learned_heads.bin")
 
 INVARIANT_NAMES = ("KE", "PE", "Lx", "Ly", "Lz", "Ua", "Va", "Wa", "Xa", "Ya", "Za")
 
@@ -269,6 +273,26 @@ class BIASolver:
         if st not in (BIA_OK, capi.BIA_ERR_NOT_CONVERGED):
             raise BiaError(st, "bia_dim_integrate")
         return st_.as_dict()
+
+    def load_heads(self, path=None):
+        """Load the learned heads (learned_heads.bin) for METHOD_LEARNED steps."""
+        blob = open(path or HEADS_PATH, "rb").read()
+        capi.check(capi.lib().bia_context_set_heads(self._ctx, blob, len(blob)), "bia_context_set_heads")
+
+    def head_eval(self, head, inputs, out):
+        """Evaluate learned head `head` (0 elliptic, 1 hyperbolic) on the tensor cores:
+        inputs (n, 2) float32 CUDA tensor -> out (n,) float32 CUDA tensor."""
+        t = self._torch
+        if inputs.dtype != t.float32 or out.dtype != t.float32 or not inputs.is_contiguous():
+            raise ValueError("inputs and out must be contiguous float32 CUDA tensors")
+        n = inputs.shape[0]
+        if inputs.shape != (n, 2) or out.shape != (n,):
+            raise ValueError("inputs must be (n, 2) and out (n,)")
+        cur = self._enter()
+        st = capi.lib().bia_learned_head_eval(self._ctx, int(head), int(n), ctypes.c_void_p(inputs.data_ptr()),
+                                              ctypes.c_void_p(out.data_ptr()))
+        self._leave(cur)
+        capi.check(st, "bia_learned_head_eval")
 
     def ensemble(self, sizes, eps):
         """An ensemble of independent systems (sizes[s] particles, pair coupling eps[s])

@@ -21,6 +21,7 @@ BIA_ERR_NO_DEVICE = 7
 METHOD_RKF = 0
 METHOD_ALG = 1
 METHOD_UNIVERSAL = 2
+METHOD_LEARNED = 3
 
 
 class BiaConfig(ctypes.Structure):
@@ -32,7 +33,8 @@ class BiaConfig(ctypes.Structure):
 
 STAT_FIELDS = ("hyperbola", "parabola", "ellipse", "degenerate", "rkf", "universal",
                "iterations", "iter_hyperbola", "iter_ellipse", "iter_parabola", "iter_universal",
-               "rkf_steps", "nonconverged", "bracket_exits", "fallbacks", "nonfinite")
+               "rkf_steps", "nonconverged", "bracket_exits", "fallbacks", "nonfinite",
+               "learned", "learned_fallbacks", "learned_coarse", "timeouts")
 
 
 class BiaStats(ctypes.Structure):
@@ -104,6 +106,10 @@ def lib():
     for name in ("bia_ensemble_create", "bia_ensemble_destroy", "bia_ensemble_run",
                  "bia_ensemble_energy"):
         getattr(L, name).restype = _I
+    L.bia_context_set_heads.argtypes = [_V, ctypes.c_char_p, ctypes.c_size_t]
+    L.bia_context_set_heads.restype = _I
+    L.bia_learned_head_eval.argtypes = [_V, _I, _I, _V, _V]
+    L.bia_learned_head_eval.restype = _I
     L.bia_dim_integrate.argtypes = [_V, _I, _D, _V, _D, _D, _D, _D, ctypes.POINTER(BiaDimStats)]
     L.bia_dim_integrate.restype = _I
     _PI = ctypes.POINTER(ctypes.c_int)
@@ -150,4 +156,5 @@ EXPORTED_SYMBOLS = ("bia_config_default", "bia_context_create", "bia_context_des
                     "bia_measure_fp64_peak", "bia_context_stats", "bia_dim_integrate", "rkf_c_",
                     "bia_ensemble_create", "bia_ensemble_destroy", "bia_ensemble_particles",
                     "bia_ensemble_run", "bia_ensemble_energy",
+                    "bia_context_set_heads", "bia_learned_head_eval",
                     "bia_last_error", "find_dxyuv_kernel_", "invariance_gpu_")

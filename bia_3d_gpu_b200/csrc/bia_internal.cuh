@@ -11,8 +11,9 @@ namespace bia {
 // device counters in the stats buffer: hyperbola, parabola, ellipse, degenerate, rkf,
 // universal, iter_hyperbola, iter_ellipse, iter_parabola, iter_universal, rkf_steps,
 // nonconverged, bracket_exits, fallbacks, nonfinite
-constexpr int kNumStats = 15;
+constexpr int kNumStats = 19;
 constexpr int kStatNonfinite = 14;
+constexpr int kStatTimeouts = 18;  // tensor-core waits that gave up
 
 struct DeviceBuffer {
     void *ptr = nullptr;
@@ -71,6 +72,9 @@ struct bia_context {
     bool timing = false;
     cudaEvent_t *ev = nullptr;
     int ev_cap = 0, ev_used = 0;
+    // learned heads (BIA_METHOD_LEARNED), 2 records of learned_heads.bin
+    bia::DeviceBuffer heads;
+    bool heads_loaded = false;
     // graph cache
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;

@@ -75,6 +75,8 @@ struct PairCounters {
     int bracket_exits;
     int fallbacks;
     int nonfinite;
+    int learned, learned_fallbacks, learned_coarse;  // BIA_METHOD_LEARNED
+    int timeouts;
 };
 
 __device__ __forceinline__ void counters_zero(PairCounters &c)
@@ -83,6 +85,30 @@ __device__ __forceinline__ void counters_zero(PairCounters &c)
     for (int k = 0; k < 6; k++) c.cls[k] = 0;
     c.it_hyp = c.it_ell = c.it_par = c.it_uv = 0;
     c.rkf_steps = c.nonconverged = c.bracket_exits = c.fallbacks = c.nonfinite = 0;
+    c.learned = c.learned_fallbacks = c.learned_coarse = c.timeouts = 0;
+}
+
+#ifndef BIA_DIRECT_HALF_SINES
+#define BIA_DIRECT_HALF_SINES 0
+#endif
+#ifndef BIA_STRICT_SETUP
+#define BIA_STRICT_SETUP 0
+#endif
+#ifndef BIA_REF_END_STATE
+#define BIA_REF_END_STATE 1
+#endif
+// Uncontracted IEEE operations, in the oracle's (the reference's) order: the frame and the
+// hyperbola's start angle acos(cs_0 + b sn_0 / r) are ill-conditioned near pericentre
+// (d theta / d arg ~ 1 / sqrt(1 - arg)), so an ulp of difference in the argument becomes
+// up to ~1e-10 of displacement; these values are formed exactly as the CPU path forms
+// them (no fused multiply-add, divisions instead of reciprocals).
+__device__ __forceinline__ double m_(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double a_(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double s_(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double d_(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double dot3_(const double a[3], const double b[3])
+{
+    return a_(a_(m_(a[0], b[0]), m_(a[1], b[1])), m_(a[2], b[2]));
 }
 
 // bia/bia.f90:284-314.  Returns true for a degenerate pair (|g| == 0 or |L| == 0):
@@ -90,38 +116,51 @@ __device__ __forceinline__ void counters_zero(PairCounters &c)
 __device__ __forceinline__ bool frame_xi_eta(const double r[3], const double g[3], double e_xi[3],
                                              double e_eta[3], double Y[4])
 {
-    double gsq = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
-    double gm = sqrt(gsq);
-    double L0 = r[1] * g[2] - r[2] * g[1];
-    double L1 = r[2] * g[0] - r[0] * g[2];
-    double L2 = r[0] * g[1] - r[1] * g[0];
-    double Lsq = L0 * L0 + L1 * L1 + L2 * L2;
+    const double gsq = dot3_(g, g);
+    const double gm = __dsqrt_rn(gsq);
+    double L[3];
+    L[0] = s_(m_(r[1], g[2]), m_(r[2], g[1]));
+    L[1] = s_(m_(r[2], g[0]), m_(r[0], g[2]));
+    L[2] = s_(m_(r[0], g[1]), m_(r[1], g[0]));
+    const double Lsq = dot3_(L, L);
     if (gm == 0.0 || Lsq == 0.0) {
         if (gm == 0.0) {
-            double rm = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+            const double rm = __dsqrt_rn(dot3_(r, r));
 #pragma unroll
-            for (int k = 0; k < 3; k++) { e_xi[k] = r[k] / rm; e_eta[k] = 0.0; }
+            for (int k = 0; k < 3; k++) { e_xi[k] = d_(r[k], rm); e_eta[k] = 0.0; }
             Y[0] = rm; Y[1] = 0.0; Y[2] = 0.0; Y[3] = 0.0;
         } else {
 #pragma unroll
-            for (int k = 0; k < 3; k++) { e_eta[k] = g[k] / gm; e_xi[k] = 0.0; }
+            for (int k = 0; k < 3; k++) { e_eta[k] = d_(g[k], gm); e_xi[k] = 0.0; }
             Y[0] = 0.0;
-            Y[1] = r[0] * e_eta[0] + r[1] * e_eta[1] + r[2] * e_eta[2];
+            Y[1] = dot3_(r, e_eta);
             Y[2] = 0.0;
             Y[3] = gm;
         }
         return true;
     }
-    const double iL = 1.0 / sqrt(Lsq), ig = 1.0 / gm;
-    double ez0 = L0 * iL, ez1 = L1 * iL, ez2 = L2 * iL;
+    double ez[3];
+#if BIA_STRICT_SETUP
+    const double Lm = __dsqrt_rn(Lsq);
 #pragma unroll
-    for (int k = 0; k < 3; k++) e_eta[k] = g[k] * ig;
-    e_xi[0] = e_eta[1] * ez2 - e_eta[2] * ez1;
-    e_xi[1] = e_eta[2] * ez0 - e_eta[0] * ez2;
-    e_xi[2] = e_eta[0] * ez1 - e_eta[1] * ez0;
-    Y[0] = r[0] * e_xi[0] + r[1] * e_xi[1] + r[2] * e_xi[2];
+    for (int k = 0; k < 3; k++) {
+        e_eta[k] = d_(g[k], gm);
+        ez[k] = d_(L[k], Lm);
+    }
+#else
+    const double iL = 1.0 / sqrt(Lsq), ig = 1.0 / gm;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        e_eta[k] = g[k] * ig;
+        ez[k] = L[k] * iL;
+    }
+#endif
+    e_xi[0] = s_(m_(e_eta[1], ez[2]), m_(e_eta[2], ez[1]));
+    e_xi[1] = s_(m_(e_eta[2], ez[0]), m_(e_eta[0], ez[2]));
+    e_xi[2] = s_(m_(e_eta[0], ez[1]), m_(e_eta[1], ez[0]));
+    Y[0] = dot3_(r, e_xi);
     Y[2] = 0.0;
-    Y[1] = r[0] * e_eta[0] + r[1] * e_eta[1] + r[2] * e_eta[2];
+    Y[1] = dot3_(r, e_eta);
     Y[3] = gm;
     return false;
 }
@@ -140,6 +179,20 @@ struct HypConsts {
     double theta_0, tn_0, cs_0, sn_0, s0h, c0h, time_end_;
 };
 
+// sin((theta_0 +- theta)/2) from the half angles.  Near theta = +-theta_0 (far along an
+// asymptote) the difference of products cancels, so below 0.25 the sine of the small half
+// angle is taken directly, as the reference computes it (bia/find_hyperbola.f90:157-158).
+__device__ __forceinline__ void half_sines(const HypConsts &c, double theta, double sh, double ch, double &sp,
+                                          double &sm)
+{
+    sp = c.s0h * ch + c.c0h * sh;
+    sm = c.s0h * ch - c.c0h * sh;
+#if BIA_DIRECT_HALF_SINES
+    if (fabs(sm) < 0.25) sm = sin(0.5 * (c.theta_0 - theta));
+    if (fabs(sp) < 0.25) sp = sin(0.5 * (c.theta_0 + theta));
+#endif
+}
+
 // find_theta (bia/find_hyperbola.f90:149-165): residual e and derivative d at theta;
 // sp, sm = sin((theta_0 +- theta)/2) for the bracket test.
 BIA_HYPEVAL_INLINE void hyp_eval(const HypConsts &c, double theta, double &e, double &d,
@@ -147,8 +200,7 @@ BIA_HYPEVAL_INLINE void hyp_eval(const HypConsts &c, double theta, double &e, do
 {
     double sh, ch;
     d_sincos(0.5 * theta, &sh, &ch);
-    sp = c.s0h * ch + c.c0h * sh;
-    sm = c.s0h * ch - c.c0h * sh;
+    half_sines(c, theta, sh, ch, sp, sm);
     const double Dinv = 1.0 / (2.0 * sp * sm);
     const double sn = 2.0 * sh * ch;
     const double cs = 1.0 - 2.0 * sh * sh;
@@ -182,6 +234,26 @@ __device__ __forceinline__ int hyperbola(double eps_th, double dt, int ITR, cons
                                          int *fallback)
 {
     const double X_ini = YZ[0], Y_ini = YZ[1], U_ini = YZ[2], V_ini = YZ[3];
+#if BIA_STRICT_SETUP
+    // up to the start angle: the oracle's operations and order (see m_ above)
+    const double r_g = a_(m_(X_ini, U_ini), m_(Y_ini, V_ini));
+    const double Lz = s_(m_(X_ini, V_ini), m_(Y_ini, U_ini));
+    const double r = __dsqrt_rn(a_(m_(X_ini, X_ini), m_(Y_ini, Y_ini)));
+    const double g2 = a_(m_(U_ini, U_ini), m_(V_ini, V_ini));
+    const double W = a_(g2, d_(m_(2.0, eps_th), r));
+    const double g_0 = __dsqrt_rn(W);
+    const double b_0 = d_(eps_th, W);
+    const double b = d_(fabs(Lz), g_0);
+    HypConsts c;
+    const double bg = m_(b_0, g_0);
+    c.theta_0 = d_atan2(fabs(Lz), bg);
+    const double den0 = __dsqrt_rn(a_(m_(m_(b_0, b_0), m_(g_0, g_0)), m_(Lz, Lz)));
+    c.cs_0 = d_(bg, den0);
+    c.sn_0 = d_(fabs(Lz), den0);
+    c.tn_0 = d_(fabs(Lz), bg);
+    d_sincos(0.5 * c.theta_0, &c.s0h, &c.c0h);
+    const double arg = a_(c.cs_0, d_(m_(b, c.sn_0), r));
+#else
     const double r_g = X_ini * U_ini + Y_ini * V_ini;
     const double Lz = X_ini * V_ini - Y_ini * U_ini;
     const double r = sqrt(X_ini * X_ini + Y_ini * Y_ini);
@@ -193,19 +265,35 @@ __device__ __forceinline__ int hyperbola(double eps_th, double dt, int ITR, cons
     HypConsts c;
     const double bg = b_0 * g_0;
     c.theta_0 = d_atan2(fabs(Lz), bg);
-    const double den0 = 1.0 / sqrt(bg * bg + Lz * Lz);
-    c.cs_0 = bg * den0;
-    c.sn_0 = fabs(Lz) * den0;
+    const double den0 = sqrt(b_0 * b_0 * (g_0 * g_0) + Lz * Lz);
+    c.cs_0 = bg / den0;
+    c.sn_0 = fabs(Lz) / den0;
     c.tn_0 = fabs(Lz) / bg;
     d_sincos(0.5 * c.theta_0, &c.s0h, &c.c0h);
     const double arg = c.cs_0 + b * c.sn_0 / r;
+#endif
     double theta_ini = (fabs(arg) > 1.0) ? 1e-30 : d_acos(arg);
     if (Lz * r_g < 0.0) theta_ini = -theta_ini;
     // state and dimensionless time at theta_ini (bia/find_hyperbola.f90:46-64)
     double sh, ch;
     d_sincos(0.5 * theta_ini, &sh, &ch);
-    const double sp_i = c.s0h * ch + c.c0h * sh, sm_i = c.s0h * ch - c.c0h * sh;
+    double sp_i, sm_i;
+    half_sines(c, theta_ini, sh, ch, sp_i, sm_i);
     const double Dinv_i = 1.0 / (2.0 * sp_i * sm_i);
+#if BIA_REF_END_STATE
+    // the start position and the end state take sin and cos of the full angle, as the
+    // reference does: the end position is a difference of two positions of magnitude r,
+    // and only the same formula at both ends keeps their rounding from adding a bias
+    double sn, cs;
+    d_sincos(theta_ini, &sn, &cs);
+    const double x = r * cs, y = r * sn;
+    const double g0_sn0 = (Lz > 0.0) ? g_0 / c.sn_0 : -g_0 / c.sn_0;
+    const double u = g0_sn0 * (c.cs_0 * sn);
+    const double v = g0_sn0 * (1.0 - c.cs_0 * cs);
+    const double den_a = sqrt((X_ini * X_ini + Y_ini * Y_ini) * (x * x + y * y));
+    const double cs_a = (x * X_ini + y * Y_ini) / den_a;
+    const double sn_a = (x * Y_ini - y * X_ini) / den_a;
+#else
     const double sn = 2.0 * sh * ch, cs = 1.0 - 2.0 * sh * sh;
     const double x = r * cs, y = r * sn;
     const double g0_sn0 = (Lz > 0.0) ? g_0 / c.sn_0 : -g_0 / c.sn_0;
@@ -214,6 +302,7 @@ __device__ __forceinline__ int hyperbola(double eps_th, double dt, int ITR, cons
     const double den_a = 1.0 / sqrt((X_ini * X_ini + Y_ini * Y_ini) * (x * x + y * y));
     const double cs_a = (x * X_ini + y * Y_ini) * den_a;
     const double sn_a = (x * Y_ini - y * X_ini) * den_a;
+#endif
     const double tau_ini = c.tn_0 * sn * Dinv_i + d_log(sp_i / sm_i);
     const double time_ini = tau_ini * b_0 / g_0;
     const double time_end = (Lz > 0.0) ? time_ini + dt : time_ini - dt;
@@ -273,14 +362,21 @@ __device__ __forceinline__ int hyperbola(double eps_th, double dt, int ITR, cons
         *fallback = 1;
     }
     // end state (bia/find_hyperbola.f90:126-142)
+#if BIA_REF_END_STATE
+    double sn_end, cs_end;
+    d_sincos(theta_stock, &sn_end, &cs_end);
+    const double r_end = b * c.sn_0 / (cs_end - c.cs_0);
+#else
     d_sincos(0.5 * theta_stock, &sh, &ch);
     const double sn_end = 2.0 * sh * ch, cs_end = 1.0 - 2.0 * sh * sh;
-    const double sp_e = c.s0h * ch + c.c0h * sh, sm_e = c.s0h * ch - c.c0h * sh;
+    double sp_e, sm_e;
+    half_sines(c, theta_stock, sh, ch, sp_e, sm_e);
+    const double r_end = b * c.sn_0 / (2.0 * sp_e * sm_e);
+#endif
     const double u_end = g0_sn0 * c.cs_0 * sn_end;
     const double du_end = u_end - u;
     const double v_end = g0_sn0 * (1.0 - c.cs_0 * cs_end);
     const double dv_end = v_end - v;
-    const double r_end = b * c.sn_0 / (2.0 * sp_e * sm_e);
     YN[0] = r_end * (cs_end * cs_a - sn_end * sn_a);
     YN[1] = r_end * (cs_end * sn_a + sn_end * cs_a);
     YN[2] = YZ[2] + (du_end * cs_a - dv_end * sn_a);
@@ -663,32 +759,48 @@ __device__ __forceinline__ void stumpff(double x, double c[4])
 // not converged
 constexpr int kUvItMax = 200;
 
-__device__ __forceinline__ int uv_halfdisp(double eps_th, double dt, const double r[3], const double g[3],
-                                           double h[6])
+// The universal-variable pair in pieces (prepare, start, iterate, compose) so that other
+// solvers can supply their own start; uv_halfdisp chains them.
+struct UvPair {
+    double mu, r0, sig, beta;
+};
+
+__device__ __forceinline__ UvPair uv_prepare(double eps_th, const double r[3], const double g[3])
 {
-    const double mu = -eps_th;
-    const double r0 = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-    const double sig = r[0] * g[0] + r[1] * g[1] + r[2] * g[2];
+    UvPair p;
+    p.mu = -eps_th;
+    p.r0 = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    p.sig = r[0] * g[0] + r[1] * g[1] + r[2] * g[2];
     const double v2 = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
-    const double beta = 2.0 * mu / r0 - v2;
-#pragma unroll
-    for (int k = 0; k < 6; k++) h[k] = 0.0;
-    if (dt == 0.0) return 0;
+    p.beta = 2.0 * p.mu / p.r0 - v2;
+    return p;
+}
+
+// second-order Taylor start s(dt) = dt/r0 - sig dt^2 / (2 r0^3)
+__device__ __forceinline__ double uv_start(const UvPair &p, double dt)
+{
+    double s = dt / p.r0;
+    s = s - p.sig * s * s / (2.0 * p.r0);
+    if (!(s > 0.0)) s = dt / p.r0;
+    return s;
+}
+
+// Safeguarded Newton on F(s) = t(s) - dt, F' = r(s) > 0, with the bracket [lo, hi]
+// (F(0) = -dt < 0; hi < 0 until an upper bound is seen).  A Newton step that leaves the
+// bracket, or is not below half the step before last, is replaced by bisection, so the
+// bracket at least halves every two iterations: on hyperbolic branches Newton from far
+// above the root moves only ~1/sqrt(-beta) per step.  Returns the iterations
+// (kUvItMax + 1 when the cap was reached).
+__device__ __forceinline__ int uv_iterate(const UvPair &p, double dt, double &s_io)
+{
     double c[4];
-    double s = dt / r0;
-    s = s - sig * s * s / (2.0 * r0);
-    if (!(s > 0.0)) s = dt / r0;
-    // Safeguarded Newton on F(s) = t(s) - dt, F' = r(s) > 0, with the bracket [lo, hi]
-    // (F(0) = -dt < 0; hi < 0 until an upper bound is seen).  A Newton step that leaves
-    // the bracket, or is not below half the step before last, is replaced by bisection,
-    // so the bracket at least halves every two iterations: on hyperbolic branches Newton
-    // from far above the root moves only ~1/sqrt(-beta) per step.
+    double s = s_io;
     double lo = 0.0, hi = -1.0, dx = 1e300, dxold = 1e300;
     int it;
     for (it = 1; it <= kUvItMax; it++) {
-        stumpff(beta * s * s, c);
-        const double F = r0 * s * c[1] + sig * s * s * c[2] + mu * s * s * s * c[3] - dt;
-        const double Fp = r0 * c[0] + sig * s * c[1] + mu * s * s * c[2];
+        stumpff(p.beta * s * s, c);
+        const double F = p.r0 * s * c[1] + p.sig * s * s * c[2] + p.mu * s * s * s * c[3] - dt;
+        const double Fp = p.r0 * c[0] + p.sig * s * c[1] + p.mu * s * s * c[2];
         if (F == 0.0) break;
         const double step = F / Fp;
         if (Fp > 0.0 && fabs(step) <= 4.0 * 2.220446049250313e-16 * fabs(s)) {
@@ -708,18 +820,52 @@ __device__ __forceinline__ int uv_halfdisp(double eps_th, double dt, const doubl
         // one would be below rounding, so s is final without another evaluation
         if (newton && dx <= 1e-10 * fabs(s)) break;
     }
-    stumpff(beta * s * s, c);
+    s_io = s;
+    return it;
+}
+
+// One Halley step on the same equation from s: returns the step ds (s_new = s - ds).
+// F'' = dr/ds = sig c0 + (mu - beta r0) s c1.
+__device__ __forceinline__ double uv_halley_step(const UvPair &p, double dt, double s)
+{
+    double c[4];
+    stumpff(p.beta * s * s, c);
+    const double F = p.r0 * s * c[1] + p.sig * s * s * c[2] + p.mu * s * s * s * c[3] - dt;
+    const double Fp = p.r0 * c[0] + p.sig * s * c[1] + p.mu * s * s * c[2];
+    const double Fpp = p.sig * c[0] + (p.mu - p.beta * p.r0) * s * c[1];
+    return F * Fp / (Fp * Fp - 0.5 * F * Fpp);
+}
+
+// Half-displacement from the solved s: f - 1, g - dt, f', g' - 1 from the Stumpff
+// functions (no cancellation at small s).
+__device__ __forceinline__ void uv_compose(const UvPair &p, double s, const double r[3], const double g[3],
+                                           double h[6])
+{
+    double c[4];
+    stumpff(p.beta * s * s, c);
     const double s2c2 = s * s * c[2], s3c3 = s * s * s * c[3];
-    const double rr = r0 * c[0] + sig * s * c[1] + mu * s2c2;
-    const double fm1 = -mu * s2c2 / r0;
-    const double gmdt = -mu * s3c3;
-    const double fdot = -mu * s * c[1] / (rr * r0);
-    const double gdm1 = -mu * s2c2 / rr;
+    const double rr = p.r0 * c[0] + p.sig * s * c[1] + p.mu * s2c2;
+    const double fm1 = -p.mu * s2c2 / p.r0;
+    const double gmdt = -p.mu * s3c3;
+    const double fdot = -p.mu * s * c[1] / (rr * p.r0);
+    const double gdm1 = -p.mu * s2c2 / rr;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         h[k] = (fm1 * r[k] + gmdt * g[k]) * 0.5;
         h[3 + k] = (fdot * r[k] + gdm1 * g[k]) * 0.5;
     }
+}
+
+__device__ __forceinline__ int uv_halfdisp(double eps_th, double dt, const double r[3], const double g[3],
+                                           double h[6])
+{
+#pragma unroll
+    for (int k = 0; k < 6; k++) h[k] = 0.0;
+    if (dt == 0.0) return 0;
+    const UvPair p = uv_prepare(eps_th, r, g);
+    double s = uv_start(p, dt);
+    const int it = uv_iterate(p, dt, s);
+    uv_compose(p, s, r, g, h);
     return it;
 }
 
@@ -750,7 +896,7 @@ __device__ __forceinline__ int alg_classify(double eps_ij, const double r[3], co
 
 // M: the compiled method (kMethodRkf, kMethodAlg, kMethodUniversal); each kernel is
 // instantiated per method so it carries only that method's code and registers.
-constexpr int kMethodRkf = 0, kMethodAlg = 1, kMethodUniversal = 2;
+constexpr int kMethodRkf = 0, kMethodAlg = 1, kMethodUniversal = 2, kMethodLearned = 3;
 
 __device__ __forceinline__ void count_nonfinite(const double h[6], PairCounters &cnt)
 {

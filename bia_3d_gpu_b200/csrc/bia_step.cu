@@ -31,8 +31,10 @@
 #include <mutex>
 
 #include "bia_internal.cuh"
+#include "bia_learned.cuh"
 #include "bia_pair.cuh"
 #include "bia_tiles.cuh"
+#include "mlp_tc.cuh"
 
 namespace bia {
 
@@ -47,6 +49,7 @@ struct StepArgs {
     int n, nb, npad;
     double eps_th;
     PairParams P;
+    const MlpHead *heads;  // BIA_METHOD_LEARNED
 };
 
 template <bool kDeterministic, int M>
@@ -170,6 +173,222 @@ static void launch_pair_tiles(const StepArgs &A, long long grid, cudaStream_t st
     }
 }
 
+
+// ---------------------------------------------------------------------------------------
+// Learned mixed-precision step kernel (BIA_METHOD_LEARNED): 8 warps, one warp-block each,
+// two CTAs per SM.  Each lane classifies its pairs (hyperbolic head, elliptic head, plain),
+// then the CTA runs turns in lockstep, first for the hyperbolic head, then for the
+// elliptic one: every thread takes its next pair of that head (or an idle row), the CTA
+// evaluates the head for its 256 rows on the tensor cores (mlp_tc.cuh), and each thread
+// finishes its pair (FP32 correction, FP64 Halley step, composition).  The plain pairs
+// follow per warp with the universal-variable solver.  Column sums in the warp's shared
+// slice, added in lane order per turn as in the phase-locked kernel: deterministic.
+constexpr int kLearnedWarps = kMlpThreads / 32;
+constexpr size_t kLearnedSmemBytes = 1024 + sizeof(MlpSmem) + (size_t)kLearnedWarps * kTileSmemDoubles * sizeof(double);
+
+__device__ __forceinline__ void add_column(double *wacc, int j, const double h[6], unsigned bm, int lane)
+{
+    const unsigned grp = __match_any_sync(bm, j);
+    const int rank = __popc(grp & ((1u << lane) - 1u));
+    const int turns = (int)__reduce_max_sync(bm, (unsigned)__popc(grp));
+    for (int t = 0; t < turns; t++) {
+        if (rank == t) {
+#pragma unroll
+            for (int c = 0; c < 6; c++) wacc[c * 32 + j] += h[c];
+        }
+        __syncwarp(bm);
+    }
+}
+
+template <bool kDeterministic>
+__global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const StepArgs A)
+{
+    extern __shared__ uint8_t learned_smem_raw[];
+    uint8_t *base = (uint8_t *)(((uintptr_t)learned_smem_raw + 1023) & ~(uintptr_t)1023);
+    MlpSmem &S = *reinterpret_cast<MlpSmem *>(base);
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    double *ws = reinterpret_cast<double *>(base + sizeof(MlpSmem)) + warp * kTileSmemDoubles;
+    double *wacc = ws + 7 * 32;
+    const long long t = (long long)blockIdx.x * kLearnedWarps + warp;
+    const bool live = t < A.nwb;
+    int bi = 0, bj = 0;
+    if (live) warp_block_coords(t, bi, bj);
+    mlp_setup(S, A.heads);
+    uint32_t phase = 0;
+    PairCounters cnt;
+    counters_zero(cnt);
+    double si[7], racc[6];
+#pragma unroll
+    for (int c = 0; c < 6; c++) racc[c] = 0.0;
+    const double dt = A.P.dt;
+    const int n = A.n;
+    const bool hq = A.q != nullptr;
+    {
+        double sj[7];
+        load_particle(A.x, A.y, A.z, A.u, A.v, A.w, A.q, n, bi * 32 + lane, si);
+        load_particle(A.x, A.y, A.z, A.u, A.v, A.w, A.q, n, bj * 32 + lane, sj);
+#pragma unroll
+        for (int c = 0; c < 7; c++) ws[c * 32 + lane] = sj[c];
+#pragma unroll
+        for (int c = 0; c < 6; c++) wacc[c * 32 + lane] = 0.0;
+        __syncwarp();
+    }
+    const int i = bi * 32 + lane;
+    const bool diag = (bi == bj);
+    unsigned mh = 0u, me = 0u, mr = 0u;
+    if (live) {
+        const int k0 = diag ? 1 : 0, k1 = diag ? 16 : 31;
+        for (int k = k0; k <= k1; k++) {
+            const int src = (lane + k) & 31;
+            if ((!diag || k < 16 || lane < 16) && i < n && bj * 32 + src < n) {
+                const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
+                const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
+                const double eps_ij = hq ? A.eps_th * si[6] * ws[6 * 32 + src] : A.eps_th;
+                LearnedPair L;
+                learned_prepare(eps_ij, dt, r, g, L);
+                const unsigned bit = 1u << k;
+                if (L.kind == kLearnedHyp) mh |= bit;
+                else if (L.kind == kLearnedEll) me |= bit;
+                else mr |= bit;
+            }
+        }
+    }
+    bool timed_out = false;
+    for (int pass = 0; pass < 2; pass++) {
+        const int head = pass == 0 ? kHeadHyp : kHeadEll;
+        unsigned m = pass == 0 ? mh : me;
+        if (threadIdx.x == 0) S.turns = 0;
+        __syncthreads();
+        atomicMax(&S.turns, __popc(m));
+        __syncthreads();
+        const int nturns = S.turns;
+        for (int turn = 0; turn < nturns; turn++) {
+            const bool busy = (m != 0u);
+            int j = 0;
+            double r[3] = {0, 0, 0}, g[3] = {0, 0, 0}, eps_ij = 0.0;
+            LearnedPair L;
+            L.x0 = L.x1 = 0.0f;
+            if (busy) {
+                const int k = __ffs(m) - 1;
+                m &= m - 1u;
+                j = (lane + k) & 31;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    r[c] = si[c] - ws[c * 32 + j];
+                    g[c] = si[3 + c] - ws[(3 + c) * 32 + j];
+                }
+                eps_ij = hq ? A.eps_th * si[6] * ws[6 * 32 + j] : A.eps_th;
+                learned_prepare(eps_ij, dt, r, g, L);
+            }
+            bool ok;
+            const float y = mlp_eval_cta(S, head, L.x0, L.x1, phase, ok);
+            if (!ok) timed_out = true;
+            const unsigned bm = __ballot_sync(0xffffffffu, busy);
+            if (busy) {
+                double h[6];
+                bool coarse = true;
+                const bool done = ok && learned_finish(L, dt, y, r, g, h, coarse);
+                cnt.learned++;
+                if (coarse) cnt.learned_coarse++;
+                if (!done) {
+                    cnt.learned_fallbacks++;
+                    const int it = uv_halfdisp(eps_ij, dt, r, g, h);
+                    cnt.it_uv += it;
+                    if (it > kUvItMax) cnt.nonconverged++;
+                }
+                cnt.cls[head == kHeadEll ? kEllipse : kHyperbola]++;
+                count_nonfinite(h, cnt);
+#pragma unroll
+                for (int c = 0; c < 6; c++) racc[c] += h[c];
+                add_column(wacc, j, h, bm, lane);
+            }
+        }
+    }
+    if (timed_out && threadIdx.x == 0) cnt.timeouts++;
+    // plain pairs: the universal-variable solver, per warp
+    for (;;) {
+        const bool busy = (mr != 0u);
+        const unsigned bm = __ballot_sync(0xffffffffu, busy);
+        if (bm == 0u) break;
+        if (busy) {
+            const int k = __ffs(mr) - 1;
+            mr &= mr - 1u;
+            const int j = (lane + k) & 31;
+            double r[3], g[3], h[6];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                r[c] = si[c] - ws[c * 32 + j];
+                g[c] = si[3 + c] - ws[(3 + c) * 32 + j];
+            }
+            const double eps_ij = hq ? A.eps_th * si[6] * ws[6 * 32 + j] : A.eps_th;
+            const int it = uv_halfdisp(eps_ij, dt, r, g, h);
+            cnt.it_uv += it;
+            if (it > kUvItMax) cnt.nonconverged++;
+            cnt.cls[alg_classify(eps_ij, r, g) == kClsDeg ? kDegenerate : kUniversal]++;
+            count_nonfinite(h, cnt);
+#pragma unroll
+            for (int c = 0; c < 6; c++) racc[c] += h[c];
+            add_column(wacc, j, h, bm, lane);
+        }
+    }
+    __syncwarp();
+    double cacc[6];
+#pragma unroll
+    for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
+    mlp_teardown(S, phase);
+    if (timed_out && threadIdx.x == 0) {
+        // every thread of the CTA saw the timeout; count it with the CTA's first live warp
+        if (!live) atomicAdd(&A.stats[kStatTimeouts], 1ull);
+    }
+    if (!live) return;  // warp-uniform; no barrier follows
+    flush_counters(cnt, A.stats, lane);
+    const int jown = bj * 32 + lane;
+    const size_t plane = (size_t)A.npad;
+    if (kDeterministic) {
+        write_partials(A.part, plane, bi, bj, lane, racc, cacc);
+    } else if (diag) {
+#pragma unroll
+        for (int c = 0; c < 6; c++)
+            if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c] - cacc[c]);
+    } else {
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c]);
+            if (jown < A.n) atomicAdd(&A.part[c * plane + jown], -cacc[c]);
+        }
+    }
+}
+
+// Once per device: dynamic shared memory opt-in of the learned kernels (false on failure).
+static bool learned_kernel_setup()
+{
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static int state_of[kMaxDevices] = {};  // 0 unknown, 1 ok, 2 failed
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return false;
+    std::lock_guard<std::mutex> lk(mu);
+    if (state_of[dev] == 0) {
+        bool ok = cudaFuncSetAttribute(bia_pair_learned_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kLearnedSmemBytes) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(bia_pair_learned_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)kLearnedSmemBytes) == cudaSuccess;
+        if (!ok) cudaGetLastError();
+        state_of[dev] = ok ? 1 : 2;
+    }
+    return state_of[dev] == 1;
+}
+
+template <bool kDeterministic>
+static int launch_pair_learned(const StepArgs &A, cudaStream_t st)
+{
+    if (!learned_kernel_setup()) return BIA_ERR_CUDA;
+    const long long grid = (A.nwb + kLearnedWarps - 1) / kLearnedWarps;
+    bia_pair_learned_kernel<kDeterministic><<<(unsigned)grid, kMlpThreads, kLearnedSmemBytes, st>>>(A);
+    return BIA_OK;
+}
+
 struct UpdateArgs {
     double *x, *y, *z, *u, *v, *w;
     const double *part;
@@ -239,10 +458,12 @@ int ensure_step_buffers(bia_context *ctx, const bia_config *cfg, int n)
 }
 
 static int validate(const bia_config *cfg, int n, const void *x, const void *y, const void *z,
-                    const void *u, const void *v, const void *w)
+                    const void *u, const void *v, const void *w, const bia_context *ctx = nullptr)
 {
     if (!cfg || n < 1 || !x || !y || !z || !u || !v || !w) return BIA_ERR_INVALID_ARGUMENT;
-    if (cfg->method != BIA_METHOD_ALG && cfg->method != BIA_METHOD_RKF && cfg->method != BIA_METHOD_UNIVERSAL)
+    const bool learned_ok = cfg->method == BIA_METHOD_LEARNED && ctx && ctx->heads_loaded;
+    if (cfg->method != BIA_METHOD_ALG && cfg->method != BIA_METHOD_RKF && cfg->method != BIA_METHOD_UNIVERSAL &&
+        !learned_ok)
         return BIA_ERR_INVALID_ARGUMENT;
     if (cfg->itr < 1 || cfg->itr > 62) return BIA_ERR_INVALID_ARGUMENT;
     // 32-bit particle indices and a warp-block count that fits the grid
@@ -290,12 +511,17 @@ int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
     U.nb = nb;
     U.npad = nb * 32;
     U.dt = cfg->dt;
+    A.heads = (const MlpHead *)ctx->heads.ptr;
+    const bool learned = cfg->method == BIA_METHOD_LEARNED;
+    if (learned && !ctx->heads_loaded) return BIA_ERR_INVALID_ARGUMENT;
+    int st = BIA_OK;
     if (cfg->deterministic) {
         A.part = (double *)ctx->part.ptr;
         U.part = A.part;
         U.nparts = nb;
         record_event(ctx);
-        launch_pair_tiles<true>(A, grid, ctx->stream);
+        if (learned) st = launch_pair_learned<true>(A, ctx->stream);
+        else launch_pair_tiles<true>(A, grid, ctx->stream);
         record_event(ctx);
     } else {
         A.part = (double *)ctx->acc.ptr;
@@ -303,9 +529,11 @@ int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
         U.nparts = 1;
         cudaMemsetAsync(A.part, 0, 6 * (size_t)A.npad * sizeof(double), ctx->stream);
         record_event(ctx);
-        launch_pair_tiles<false>(A, grid, ctx->stream);
+        if (learned) st = launch_pair_learned<false>(A, ctx->stream);
+        else launch_pair_tiles<false>(A, grid, ctx->stream);
         record_event(ctx);
     }
+    if (st != BIA_OK) return st;
     bia_reduce_update_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(U);
     return cuda_status(cudaGetLastError());
 }
@@ -328,6 +556,10 @@ static void copy_stats(const unsigned long long *h, bia_stats *s)
     s->bracket_exits = (long long)h[12];
     s->fallbacks = (long long)h[13];
     s->nonfinite = (long long)h[14];
+    s->learned = (long long)h[15];
+    s->learned_fallbacks = (long long)h[16];
+    s->learned_coarse = (long long)h[17];
+    s->timeouts = (long long)h[18];
 }
 
 static int fetch_stats(bia_context *ctx, bia_stats *stats)
@@ -337,6 +569,7 @@ static int fetch_stats(bia_context *ctx, bia_stats *stats)
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return cuda_status(e);
     copy_stats(ctx->h_stats, stats);
+    if (stats->timeouts) return BIA_ERR_DEVICE_TIMEOUT;
     return stats->nonfinite ? BIA_ERR_NONFINITE : BIA_OK;
 }
 
@@ -401,6 +634,27 @@ int bia_context_create(bia_context **out, int device, void *stream)
     return BIA_OK;
 }
 
+int bia_context_set_heads(bia_context *ctx, const void *blob, size_t bytes)
+{
+    if (!ctx || !blob) return BIA_ERR_INVALID_ARGUMENT;
+    const size_t want = 16 + (size_t)kMlpHeads * sizeof(MlpHead);
+    if (bytes != want) return BIA_ERR_INVALID_ARGUMENT;
+    const unsigned char *b = (const unsigned char *)blob;
+    uint32_t version = 0, nheads = 0;
+    memcpy(&version, b + 8, 4);
+    memcpy(&nheads, b + 12, 4);
+    if (memcmp(b, "BIAHEAD1", 8) != 0 || version != 1 || nheads != (uint32_t)kMlpHeads)
+        return BIA_ERR_INVALID_ARGUMENT;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e == cudaSuccess) e = ctx->heads.reserve(kMlpHeads * sizeof(MlpHead));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ctx->heads.ptr, b + 16, kMlpHeads * sizeof(MlpHead), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = ctx->stream ? cudaStreamSynchronize(ctx->stream) : cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_status(e);
+    ctx->heads_loaded = true;
+    return BIA_OK;
+}
+
 int bia_context_destroy(bia_context *ctx)
 {
     if (!ctx) return BIA_OK;
@@ -413,6 +667,7 @@ int bia_context_destroy(bia_context *ctx)
     free(ctx->ev);
     ctx->part.release();
     ctx->acc.release();
+    ctx->heads.release();
     ctx->stats.release();
     ctx->state.release();
     ctx->inv.release();
@@ -477,7 +732,7 @@ int bia_step(bia_context *ctx, const bia_config *cfg, int n, double *x, double *
              double *u, double *v, double *w, const double *q, double *disp, bia_stats *stats)
 {
     if (!ctx) return BIA_ERR_INVALID_ARGUMENT;
-    int st = validate(cfg, n, x, y, z, u, v, w);
+    int st = validate(cfg, n, x, y, z, u, v, w, ctx);
     if (st != BIA_OK) return st;
     cudaSetDevice(ctx->device);
     st = ensure_step_buffers(ctx, cfg, n);
@@ -497,7 +752,7 @@ int bia_run(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y
             bia_stats *stats)
 {
     if (!ctx || nsteps < 0) return BIA_ERR_INVALID_ARGUMENT;
-    int st = validate(cfg, n, x, y, z, u, v, w);
+    int st = validate(cfg, n, x, y, z, u, v, w, ctx);
     if (st != BIA_OK) return st;
     cudaSetDevice(ctx->device);
     st = ensure_step_buffers(ctx, cfg, n);
@@ -549,7 +804,7 @@ int bia_run_host(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
                  double *u, double *v, double *w, const double *q, int nsteps, bia_stats *stats)
 {
     if (!ctx) return BIA_ERR_INVALID_ARGUMENT;
-    int st = validate(cfg, n, x, y, z, u, v, w);
+    int st = validate(cfg, n, x, y, z, u, v, w, ctx);
     if (st != BIA_OK) return st;
     cudaSetDevice(ctx->device);
     cudaError_t e = ctx->state.reserve((size_t)7 * n * sizeof(double));
@@ -673,4 +928,56 @@ extern "C" int bia_step_noalloc(const bia_config *cfg, int n, double *x, double 
     U.dt = cfg->dt;
     bia_reduce_update_kernel<<<(n + 255) / 256, 256, 0, s>>>(U);
     return cuda_status(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------------------
+// Head evaluation on its own (tests of the tensor-core network path).
+namespace bia {
+__global__ void __launch_bounds__(kMlpThreads, 1) bia_head_eval_kernel(const MlpHead *heads, int head, int n,
+                                                                      const float *in, float *out,
+                                                                      unsigned long long *timeouts)
+{
+    extern __shared__ uint8_t head_smem_raw[];
+    uint8_t *base = (uint8_t *)(((uintptr_t)head_smem_raw + 1023) & ~(uintptr_t)1023);
+    MlpSmem &S = *reinterpret_cast<MlpSmem *>(base);
+    mlp_setup(S, heads);
+    uint32_t phase = 0;
+    bool ok = true;
+    // the same number of rounds on every thread of the CTA (the MLP synchronises the CTA)
+    for (long long row0 = (long long)blockIdx.x * kMlpThreads; row0 < n && ok;
+         row0 += (long long)gridDim.x * kMlpThreads) {
+        const long long row = row0 + threadIdx.x;
+        const float x0 = row < n ? in[2 * row] : 0.0f;
+        const float x1 = row < n ? in[2 * row + 1] : 0.0f;
+        const float y = mlp_eval_cta(S, head, x0, x1, phase, ok);
+        if (row < n) out[row] = ok ? y : __int_as_float(0x7fc00000);
+    }
+    mlp_teardown(S, phase);
+    if (!ok && threadIdx.x == 0) atomicAdd(timeouts, 1ull);
+}
+}  // namespace bia
+
+int bia_learned_head_eval(bia_context *ctx, int head, int n, const float *in, float *out)
+{
+    if (!ctx || !in || !out || n < 1 || head < 0 || head >= kMlpHeads || !ctx->heads_loaded)
+        return set_last_error(BIA_ERR_INVALID_ARGUMENT);
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e == cudaSuccess) e = ctx->stats.reserve(kNumStats * sizeof(unsigned long long));
+    unsigned long long *timeouts = (unsigned long long *)ctx->stats.ptr + kStatTimeouts;
+    if (e == cudaSuccess) e = cudaMemsetAsync(timeouts, 0, sizeof(unsigned long long), ctx->stream);
+    if (e == cudaSuccess &&
+        cudaFuncSetAttribute(bia_head_eval_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(1024 + sizeof(MlpSmem))) != cudaSuccess)
+        e = cudaGetLastError();
+    if (e != cudaSuccess) return set_last_error(cuda_status(e));
+    int blocks = (n + kMlpThreads - 1) / kMlpThreads;
+    if (blocks > 4096) blocks = 4096;
+    bia_head_eval_kernel<<<blocks, kMlpThreads, 1024 + sizeof(MlpSmem), ctx->stream>>>(
+        (const MlpHead *)ctx->heads.ptr, head, n, in, out, timeouts);
+    e = cudaGetLastError();
+    unsigned long long h = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, timeouts, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = ctx->stream ? cudaStreamSynchronize(ctx->stream) : cudaDeviceSynchronize();
+    if (e != cudaSuccess) return set_last_error(cuda_status(e));
+    return set_last_error(h ? BIA_ERR_DEVICE_TIMEOUT : BIA_OK);
 }

@@ -1,0 +1,281 @@
+// mlp_tc.cuh -- the learned Kepler heads (MLP 2 -> 64 -> 64 -> 64 -> 1, ReLU) evaluated on
+// the 5th-generation tensor cores: BF16 operands in shared memory, FP32 accumulators in
+// tensor memory (TMEM), one thread issuing tcgen05.mma for the CTA.
+//
+// A CTA of kMlpThreads = 256 threads evaluates 256 rows (one per thread) per call: two
+// M = 128 tiles, N = 64, K = 16 for layer 1 (2 inputs padded with zeros) and K = 64 for
+// layers 2 and 3; layer 4 (64 -> 1) is a per-thread FP32 dot product.  Between layers each
+// thread reads its own accumulator row back with tcgen05.ld (warp w owns TMEM lanes
+// 32 (w mod 4) .. + 31 of tile w / 4), adds the bias, applies ReLU, rounds to BF16 and
+// writes the row as the next layer's A operand.
+//
+// Operand layout: K-major, no swizzle, the canonical arrangement of 8-row x 16-byte core
+// matrices: element (row, k) of a [rows][K] BF16 matrix sits at byte
+//     ((row / 8) * (K / 8) + k / 8) * 128 + (row % 8) * 16 + (k % 8) * 2,
+// so core matrices adjacent in K are 128 bytes apart (leading byte offset) and 8-row groups
+// are K * 16 bytes apart (stride byte offset).  One MMA covers K = 16 (two core matrices):
+// the descriptor start advances 256 bytes per K step.
+//
+// Completion: tcgen05.commit arrives on an mbarrier; every wait is bounded and a timeout
+// sets the CTA's abort flag (no further MMA is issued; the caller treats the guesses as
+// missing and reports BIA_ERR_DEVICE_TIMEOUT).
+#pragma once
+#include <cuda_bf16.h>
+
+#include <cstdint>
+
+namespace bia {
+
+constexpr int kMlpHidden = 64;
+constexpr int kMlpK1 = 16;
+constexpr int kMlpThreads = 256;
+
+// One head as stored in learned_heads.bin (after its 16-byte header): BF16 weights
+// output-major W[n][k], FP32 biases and the last layer.
+struct MlpHead {
+    uint16_t w1[kMlpHidden * kMlpK1];
+    uint16_t w2[kMlpHidden * kMlpHidden];
+    uint16_t w3[kMlpHidden * kMlpHidden];
+    float b1[kMlpHidden], b2[kMlpHidden], b3[kMlpHidden], w4[kMlpHidden], b4[4];
+};
+static_assert(sizeof(MlpHead) == 19472, "learned_heads.bin head record");
+constexpr int kMlpHeads = 2;  // 0 elliptic, 1 hyperbolic
+
+// Shared-memory image of both heads and the activation tiles (bytes, 1024-aligned parts).
+struct MlpSmem {
+    alignas(1024) uint8_t w1[kMlpHeads][kMlpHidden * kMlpK1 * 2];        // 2 x 2 KB
+    alignas(1024) uint8_t w2[kMlpHeads][kMlpHidden * kMlpHidden * 2];    // 2 x 8 KB
+    alignas(1024) uint8_t w3[kMlpHeads][kMlpHidden * kMlpHidden * 2];    // 2 x 8 KB
+    alignas(1024) uint8_t a1[kMlpThreads * kMlpK1 * 2];                  // 8 KB
+    alignas(1024) uint8_t a2[kMlpThreads * kMlpHidden * 2];              // 32 KB
+    float b1[kMlpHeads][kMlpHidden], b2[kMlpHeads][kMlpHidden], b3[kMlpHeads][kMlpHidden];
+    float w4[kMlpHeads][kMlpHidden], b4[kMlpHeads];
+    alignas(8) uint64_t mbar;
+    uint32_t tmem_base;
+    int abort;
+    int turns;  // scratch for CTA-wide turn counts of the callers
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ uint32_t kmajor_off(int row, int k, int K)
+{
+    return (uint32_t)((((row >> 3) * (K >> 3)) + (k >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+// tcgen05 shared-memory matrix descriptor: start, leading and stride byte offsets (>> 4),
+// descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t mma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// kind::f16 instruction descriptor: D F32, A and B BF16, both K-major, N = 64, M = 128.
+constexpr uint32_t kIdescBf16M128N64 =
+    (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
+        "l"(adesc), "l"(bdesc), "r"(kIdescBf16M128N64), "r"(accumulate));
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t *mbar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_addr(mbar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Bounded wait for the mbarrier phase with parity `phase` to complete; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t phase)
+{
+    const uint32_t a = smem_addr(mbar);
+    for (int it = 0; it < (1 << 22); it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(a), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// 16 consecutive FP32 accumulator columns of this thread's TMEM lane
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float v[16])
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b)
+{
+    const uint32_t lo = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a));
+    const uint32_t hi = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(b));
+    return lo | (hi << 16);
+}
+
+// Once per CTA (all threads): heads from global memory into the shared image, the constant
+// zero half of the layer-1 rows, the mbarrier, and the TMEM allocation (warp 0, 128
+// columns: two 128 x 64 FP32 accumulator tiles).
+__device__ __forceinline__ void mlp_setup(MlpSmem &S, const MlpHead *heads)
+{
+    const int tid = threadIdx.x;
+    for (int h = 0; h < kMlpHeads; h++) {
+        const MlpHead &H = heads[h];
+        for (int e = tid; e < kMlpHidden * kMlpK1; e += blockDim.x) {
+            const int n = e / kMlpK1, k = e % kMlpK1;
+            *(uint16_t *)(S.w1[h] + kmajor_off(n, k, kMlpK1)) = H.w1[e];
+        }
+        for (int e = tid; e < kMlpHidden * kMlpHidden; e += blockDim.x) {
+            const int n = e / kMlpHidden, k = e % kMlpHidden;
+            *(uint16_t *)(S.w2[h] + kmajor_off(n, k, kMlpHidden)) = H.w2[e];
+            *(uint16_t *)(S.w3[h] + kmajor_off(n, k, kMlpHidden)) = H.w3[e];
+        }
+        for (int e = tid; e < kMlpHidden; e += blockDim.x) {
+            S.b1[h][e] = H.b1[e];
+            S.b2[h][e] = H.b2[e];
+            S.b3[h][e] = H.b3[e];
+            S.w4[h][e] = H.w4[e];
+        }
+        if (tid == 0) S.b4[h] = H.b4[0];
+    }
+    // layer-1 rows: inputs in k = 0, 1; k = 2..15 stay zero
+    for (int e = tid; e < kMlpThreads * kMlpK1; e += blockDim.x)
+        *(uint16_t *)(S.a1 + kmajor_off(e / kMlpK1, e % kMlpK1, kMlpK1)) = 0;
+    if (tid == 0) {
+        S.abort = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();  // the .sync.aligned TMEM instructions need the whole warp converged
+    if ((tid >> 5) == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;" ::"r"(
+                         smem_addr(&S.tmem_base))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+}
+
+// Once per CTA at the end (all threads): free the TMEM columns.  After a timeout the MMA
+// group in flight is waited for once more (bounded) before the columns are released.
+__device__ __forceinline__ void mlp_teardown(MlpSmem &S, uint32_t phase)
+{
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (S.abort) mbar_wait(&S.mbar, phase);
+    __syncwarp();
+    if ((threadIdx.x >> 5) == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(S.tmem_base) : "memory");
+}
+
+// Layer MMAs of both 128-row tiles for one layer, issued by thread 0, then the bounded
+// wait of every thread.  Returns false (and sets S.abort) on a timeout.
+__device__ __forceinline__ bool mlp_layer(MlpSmem &S, const uint8_t *a, const uint8_t *w, int K, uint32_t &phase)
+{
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (S.abort) return false;  // uniform: read after the barrier
+    if (threadIdx.x == 0) {
+        const uint32_t sbo = (uint32_t)K * 16;
+        const uint32_t tile_bytes = 128u * (uint32_t)K * 2;
+        for (int t = 0; t < 2; t++) {
+            for (int ks = 0; ks < K / 16; ks++) {
+                const uint64_t ad = mma_desc(smem_addr(a) + t * tile_bytes + ks * 256, 128, sbo);
+                const uint64_t bd = mma_desc(smem_addr(w) + ks * 256, 128, sbo);
+                tc_mma(S.tmem_base + (uint32_t)(t * 64), ad, bd, ks > 0 ? 1u : 0u);
+            }
+        }
+        tc_commit(&S.mbar);
+    }
+    const bool ok = mbar_wait(&S.mbar, phase);
+    // every thread takes the same branch: a timeout anywhere aborts the CTA's MLP work
+    const int bad = __syncthreads_or(ok ? 0 : 1);
+    if (bad) {
+        if (threadIdx.x == 0) S.abort = 1;
+        return false;  // the phase stays: teardown waits for it once more
+    }
+    phase ^= 1u;
+    tc_fence_after();
+    return true;
+}
+
+// This thread's accumulator row of the last layer: + bias, ReLU; either written as BF16
+// into the next A tile (dst != nullptr) or dotted with w4 (returned).
+__device__ __forceinline__ float mlp_epilogue(MlpSmem &S, int head, const float *bias, uint8_t *dst)
+{
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const uint32_t taddr = S.tmem_base + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)((warp >> 2) * 64);
+    float dot = 0.0f;
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < kMlpHidden; c += 16) {
+        float v[16];
+        tc_ld16(taddr + (uint32_t)c, v);
+#pragma unroll
+        for (int j = 0; j < 16; j++) v[j] = fmaxf(v[j] + bias[c + j], 0.0f);
+        if (dst) {
+            uint4 lo, hi;
+            lo.x = pack_bf16(v[0], v[1]); lo.y = pack_bf16(v[2], v[3]);
+            lo.z = pack_bf16(v[4], v[5]); lo.w = pack_bf16(v[6], v[7]);
+            hi.x = pack_bf16(v[8], v[9]); hi.y = pack_bf16(v[10], v[11]);
+            hi.z = pack_bf16(v[12], v[13]); hi.w = pack_bf16(v[14], v[15]);
+            *(uint4 *)(dst + kmajor_off(tid, c, kMlpHidden)) = lo;
+            *(uint4 *)(dst + kmajor_off(tid, c + 8, kMlpHidden)) = hi;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; j++) dot = fmaf(v[j], S.w4[head][c + j], dot);
+        }
+    }
+    return dot + S.b4[head];
+}
+
+// The head's output for this thread's input row (x0, x1); every thread of the CTA calls it
+// with the same head.  ok (the same on every thread) is false when the tensor-core pipeline
+// timed out; the CTA then issues no more MMAs.
+__device__ __forceinline__ float mlp_eval_cta(MlpSmem &S, int head, float x0, float x1, uint32_t &phase, bool &ok)
+{
+    const int tid = threadIdx.x;
+    *(uint32_t *)(S.a1 + kmajor_off(tid, 0, kMlpK1)) = pack_bf16(x0, x1);
+    ok = false;
+    if (!mlp_layer(S, S.a1, S.w1[head], kMlpK1, phase)) return 0.0f;
+    mlp_epilogue(S, head, S.b1[head], S.a2);
+    if (!mlp_layer(S, S.a2, S.w2[head], kMlpHidden, phase)) return 0.0f;
+    mlp_epilogue(S, head, S.b2[head], S.a2);
+    if (!mlp_layer(S, S.a2, S.w3[head], kMlpHidden, phase)) return 0.0f;
+    ok = true;
+    return mlp_epilogue(S, head, S.b3[head], nullptr);
+}
+
+}  // namespace bia

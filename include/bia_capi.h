@@ -17,6 +17,8 @@
 #ifndef BIA_CAPI_H
 #define BIA_CAPI_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -36,7 +38,17 @@ enum bia_status {
 /* pair solver: the reference's METHOD argument (bia/bia.f90:134-139), plus
    BIA_METHOD_UNIVERSAL, which advances every pair with the universal-variable
    (Stumpff function) solver that ALG uses for near-unit-eccentricity pairs */
-enum bia_method { BIA_METHOD_RKF = 0, BIA_METHOD_ALG = 1, BIA_METHOD_UNIVERSAL = 2 };
+enum bia_method {
+    BIA_METHOD_RKF = 0,
+    BIA_METHOD_ALG = 1,
+    BIA_METHOD_UNIVERSAL = 2,
+    /* the learned mixed-precision form: attractive ellipses and hyperbolae inside a learned
+       head's domain start from the head's guess (BF16 tensor cores, FP32 accumulation), take
+       one FP32 Newton correction and one FP64 Halley step; every other pair, and any pair
+       whose FP64 step does not settle, takes the universal-variable solver.  Needs the heads
+       loaded with bia_context_set_heads. */
+    BIA_METHOD_LEARNED = 3
+};
 
 typedef struct bia_config {
     int method;        /* BIA_METHOD_ALG (Kepler/Barker solve), BIA_METHOD_RKF or
@@ -70,6 +82,11 @@ typedef struct bia_stats {
     long long bracket_exits; /* hyperbola iterate left (-theta_0, theta_0) */
     long long fallbacks;     /* classical iteration ended unconverged: bracketed re-solve */
     long long nonfinite;     /* pairs whose displacement was not finite */
+    long long learned;       /* BIA_METHOD_LEARNED: pairs started from a learned head */
+    long long learned_fallbacks; /* ... of which the FP64 step did not settle: plain solve */
+    long long learned_coarse;    /* ... whose head guess was > 1e-2 off in anomaly */
+    long long timeouts;      /* bounded tensor-core waits that gave up (the step returns
+                                BIA_ERR_DEVICE_TIMEOUT) */
 } bia_stats;
 
 typedef struct bia_context bia_context;
@@ -78,6 +95,14 @@ typedef struct bia_context bia_context;
    the legacy default stream).  The context owns scratch buffers, grown on demand. */
 int bia_context_create(bia_context **ctx, int device, void *stream);
 int bia_context_destroy(bia_context *ctx);
+/* Loads the two learned Kepler heads of BIA_METHOD_LEARNED from the bytes of
+   learned_heads.bin (bia_3d_gpu_b200/train_heads.py writes it: "BIAHEAD1", version 1,
+   2 heads of 19472 bytes).  No counterpart in the reference (the learned form is new). */
+int bia_context_set_heads(bia_context *ctx, const void *blob, size_t bytes);
+/* Evaluates one learned head (0 elliptic, 1 hyperbolic) on n rows of 2 FP32 inputs
+   (device arrays, in[2 n] -> out[n]) with the tensor-core kernels the learned step uses;
+   for tests of the network path.  No counterpart in the reference. */
+int bia_learned_head_eval(bia_context *ctx, int head, int n, const float *in, float *out);
 int bia_context_set_stream(bia_context *ctx, void *stream);
 /* kernel timing: when on, the pair kernel's launches are bracketed by CUDA events on
    the context's stream; bia_context_kernel_ms returns their summed duration and count

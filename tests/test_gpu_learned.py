@@ -1,0 +1,103 @@
+"""The learned mixed-precision form (BIA_METHOD_LEARNED) on the GPU.
+
+* The heads evaluated on the tensor cores (tcgen05, BF16 operands, FP32 accumulators in
+  tensor memory) agree with the numpy evaluation of the same BF16 network.
+* Learned steps match the FP64 oracle's ALG step to the plain form's bar (<= 1e-12
+  relative, positions and velocities) on mixed-class systems; pairs inside a head's domain
+  take the learned path, few of them fall back to the plain solver.
+* Deterministic mode is bitwise reproducible; the method is refused without heads.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from bia_3d_gpu_b200 import BIASolver, BiaError, METHOD_LEARNED, default_config, initial
+from bia_3d_gpu_b200 import train_heads as th
+from conftest import max_rel_err, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("head", [0, 1])
+def test_tensor_core_heads_match_numpy(cuda, head):
+    rng = np.random.default_rng(30 + head)
+    n = 5000  # not a multiple of the 256-row tile
+    x = rng.uniform(-1, 1, (n, 2)).astype(np.float32)
+    ref = th.head_forward(th.read_heads()[head], x)
+    xin = cuda.tensor(x, device="cuda")
+    out = cuda.empty(n, dtype=cuda.float32, device="cuda")
+    with BIASolver() as solver:
+        solver.load_heads()
+        solver.head_eval(head, xin, out)
+        solver.stream.synchronize()
+    got = out.cpu().numpy()
+    diff = np.abs(got - ref)
+    assert np.all(np.isfinite(got))
+    assert np.median(diff) <= 1e-5 and diff.max() <= 2e-3, (np.median(diff), diff.max())
+
+
+def _learned_vs_oracle(cuda, s, eps, dt, q=None, steps=1):
+    t = cuda.tensor(s, device="cuda")
+    qt = cuda.tensor(q, device="cuda") if q is not None else None
+    with BIASolver() as solver:
+        solver.load_heads()
+        st = None
+        for _ in range(steps):
+            st = solver.step(t, default_config(eps_th=eps, dt=dt, method=METHOD_LEARNED), q=qt)
+    g = t.cpu().numpy()
+    r = s
+    for _ in range(steps):
+        r, _, _ = oracle.bia_step(r, eps, dt, q=q)
+    return g, r, st
+
+
+def test_learned_coulomb_matches_oracle(cuda):
+    s, eps, q = initial.coulomb_cube(1500, seed=31, dmin=1e-2)
+    g, r, st = _learned_vs_oracle(cuda, s, eps, 1e-5, q=q, steps=2)
+    assert rel_err(g[:3], r[:3]) <= 1e-12 and rel_err(g[3:], r[3:]) <= 1e-12
+    assert max_rel_err(g[:3], r[:3]) <= 1e-12 and max_rel_err(g[3:], r[3:]) <= 1e-12
+    assert st["learned"] > 0.3 * 1500 * 1499 // 2
+    assert st["learned_fallbacks"] <= 0.01 * st["learned"]
+    assert st["nonfinite"] == 0 and st["timeouts"] == 0
+
+
+def test_learned_gravity_ball_matches_oracle(cuda):
+    s, eps = initial.gravity_ball(400, seed=32)
+    g, r, st = _learned_vs_oracle(cuda, s, eps, 1e-4, steps=3)
+    assert rel_err(g[:3], r[:3]) <= 1e-12 and rel_err(g[3:], r[3:]) <= 1e-12
+    assert max_rel_err(g[:3], r[:3]) <= 1e-12 and max_rel_err(g[3:], r[3:]) <= 1e-12
+    assert st["learned"] > 0 and st["nonfinite"] == 0 and st["timeouts"] == 0
+
+
+def test_learned_against_quad(cuda):
+    s, eps, q = initial.coulomb_cube(600, seed=33, dmin=1e-2)
+    t = cuda.tensor(s, device="cuda")
+    qt = cuda.tensor(q, device="cuda")
+    with BIASolver() as solver:
+        solver.load_heads()
+        solver.step(t, default_config(eps_th=eps, dt=1e-5, method=METHOD_LEARNED), q=qt)
+    g = t.cpu().numpy()
+    rq, _, _ = oracle.bia_step(s, eps, 1e-5, q=q, quad=True)
+    assert max_rel_err(g[:3], rq[:3]) <= 1e-13 and max_rel_err(g[3:], rq[3:]) <= 1e-13
+
+
+def test_learned_deterministic_and_atomic(cuda):
+    s, eps, q = initial.coulomb_cube(5000, seed=34)
+    outs = []
+    for det in (1, 1, 0):
+        t = cuda.tensor(s, device="cuda")
+        qt = cuda.tensor(q, device="cuda")
+        with BIASolver() as solver:
+            solver.load_heads()
+            solver.step(t, default_config(eps_th=eps, dt=1e-5, method=METHOD_LEARNED, deterministic=det), q=qt)
+        outs.append(t.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1])
+    assert rel_err(outs[2], outs[0]) <= 1e-15
+
+
+def test_learned_needs_heads(cuda):
+    s, eps = initial.gravity_ball(64, seed=35)
+    t = cuda.tensor(s, device="cuda")
+    with BIASolver() as solver:
+        with pytest.raises(BiaError):
+            solver.step(t, default_config(eps_th=eps, dt=1e-4, method=METHOD_LEARNED))
