@@ -101,6 +101,35 @@ __device__ __forceinline__ float sinhmx_f(float x)
     if (fabsf(x) < 0.5f) return x * x2 * (1.0f / 6.0f) * (1.0f + x2 * (1.0f / 20.0f) * (1.0f + x2 * (1.0f / 42.0f)));
     return sinhf(x) - x;
 }
+// sin x and 1 - cos x (FP32); below 0.5 from the series (no libm call, full relative
+// accuracy at the tiny increments of small time steps)
+__device__ __forceinline__ void sin_omc_f(float x, float &sn, float &omc)
+{
+    if (fabsf(x) < 0.5f) {
+        sn = x - xmsin_f(x);
+        const float h = 0.5f * x, h2 = h * h;
+        const float sh = h * (1.0f - h2 * (1.0f / 6.0f) * (1.0f - h2 * (1.0f / 20.0f)));
+        omc = 2.0f * sh * sh;
+    } else {
+        float c;
+        sincosf(x, &sn, &c);
+        omc = 1.0f - c;
+    }
+}
+// sinh x and cosh x - 1 (FP32), series below 0.5
+__device__ __forceinline__ void sinh_chm1_f(float x, float &sh, float &chm1)
+{
+    if (fabsf(x) < 0.5f) {
+        sh = x + sinhmx_f(x);
+        const float h = 0.5f * x, h2 = h * h;
+        const float s2 = h * (1.0f + h2 * (1.0f / 6.0f) * (1.0f + h2 * (1.0f / 20.0f)));
+        chm1 = 2.0f * s2 * s2;
+    } else {
+        const float e = expf(x), ei = 1.0f / e;
+        sh = 0.5f * (e - ei);
+        chm1 = 0.5f * (e + ei) - 1.0f;
+    }
+}
 
 // Anomaly guess of the head output y, then the FP32 correction: Newton on the difference
 // form, at most kLearnedFp32Steps steps, until a step is below 1e-6 of D.  (At small dt the
@@ -116,14 +145,13 @@ __device__ __forceinline__ float learned_first_correction(const LearnedPair &L, 
     for (steps = 1; steps <= kLearnedFp32Steps; steps++) {
         float F, Fp;
         if (L.kind == kLearnedEll) {
-            const float h = sinf(0.5f * D);
-            const float omc = 2.0f * h * h;  // 1 - cos D
+            float sn, omc;  // sin D, 1 - cos D
+            sin_omc_f(D, sn, omc);
             F = L.C0m * D + L.C0 * xmsin_f(D) + L.S0 * omc - L.dM;
-            Fp = L.C0m + L.C0 * omc + L.S0 * sinf(D);
+            Fp = L.C0m + L.C0 * omc + L.S0 * sn;
         } else {
-            const float h = sinhf(0.5f * D);
-            const float chm1 = 2.0f * h * h;  // cosh D - 1
-            const float sh = sinhf(D);
+            float sh, chm1;  // sinh D, cosh D - 1
+            sinh_chm1_f(D, sh, chm1);
             F = L.C0m * sh + L.S0 * chm1 + sinhmx_f(D) - L.dM;
             Fp = L.C0m * (chm1 + 1.0f) + L.S0 * sh + chm1;
         }

@@ -176,15 +176,20 @@ static void launch_pair_tiles(const StepArgs &A, long long grid, cudaStream_t st
 
 // ---------------------------------------------------------------------------------------
 // Learned mixed-precision step kernel (BIA_METHOD_LEARNED): 8 warps, one warp-block each,
-// two CTAs per SM.  Each lane classifies its pairs (hyperbolic head, elliptic head, plain),
-// then the CTA runs turns in lockstep, first for the hyperbolic head, then for the
-// elliptic one: every thread takes its next pair of that head (or an idle row), the CTA
-// evaluates the head for its 256 rows on the tensor cores (mlp_tc.cuh), and each thread
-// finishes its pair (FP32 correction, FP64 Halley step, composition).  The plain pairs
-// follow per warp with the universal-variable solver.  Column sums in the warp's shared
-// slice, added in lane order per turn as in the phase-locked kernel: deterministic.
+// two CTAs per SM, in three phases.
+//  1. Each lane classifies its pairs (hyperbolic head, elliptic head, plain) and writes the
+//     head inputs of its learned pairs into a CTA-wide row list in shared memory (packed
+//     BF16 pairs; hyperbolic rows first; offsets from a CTA scan of the per-lane counts).
+//  2. The CTA evaluates each head on its rows in full 256-row blocks on the tensor cores
+//     (mlp_tc.cuh) and writes each row's output over its input.
+//  3. Each warp finishes its learned pairs from the stored guesses (FP32 correction, FP64
+//     Halley step, composition; the plain solver where the FP64 step does not settle),
+//     then its plain pairs with the universal-variable solver, with no CTA barrier.
+// Column sums in the warp's shared slice, added in lane order per turn (deterministic).
 constexpr int kLearnedWarps = kMlpThreads / 32;
-constexpr size_t kLearnedSmemBytes = 1024 + sizeof(MlpSmem) + (size_t)kLearnedWarps * kTileSmemDoubles * sizeof(double);
+constexpr int kLearnedMaxRows = kLearnedWarps * 1024;
+constexpr size_t kLearnedTileBytes = (size_t)kLearnedWarps * kTileSmemDoubles * sizeof(double);
+constexpr size_t kLearnedSmemBytes = 1024 + sizeof(MlpSmem) + kLearnedTileBytes + kLearnedMaxRows * sizeof(uint32_t);
 
 __device__ __forceinline__ void add_column(double *wacc, int j, const double h[6], unsigned bm, int lane)
 {
@@ -200,21 +205,47 @@ __device__ __forceinline__ void add_column(double *wacc, int j, const double h[6
     }
 }
 
+// exclusive CTA-wide prefix sums of (a, b) over threads in thread order; totals returned
+__device__ __forceinline__ void cta_scan2(MlpSmem &S, int a, int b, int &oa, int &ob, int &ta, int &tb)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int ia = a, ib = b;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int xa = __shfl_up_sync(0xffffffffu, ia, d);
+        const int xb = __shfl_up_sync(0xffffffffu, ib, d);
+        if (lane >= d) { ia += xa; ib += xb; }
+    }
+    if (lane == 31) { S.wsum[0][warp] = ia; S.wsum[1][warp] = ib; }
+    __syncthreads();
+    int ba = 0, bb = 0;
+    ta = tb = 0;
+    for (int w = 0; w < kLearnedWarps; w++) {
+        if (w < warp) { ba += S.wsum[0][w]; bb += S.wsum[1][w]; }
+        ta += S.wsum[0][w];
+        tb += S.wsum[1][w];
+    }
+    oa = ba + ia - a;
+    ob = bb + ib - b;
+}
+
 template <bool kDeterministic>
 __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const StepArgs A)
 {
     extern __shared__ uint8_t learned_smem_raw[];
     uint8_t *base = (uint8_t *)(((uintptr_t)learned_smem_raw + 1023) & ~(uintptr_t)1023);
     MlpSmem &S = *reinterpret_cast<MlpSmem *>(base);
+    double *tiles = reinterpret_cast<double *>(base + sizeof(MlpSmem));
+    uint32_t *rows = reinterpret_cast<uint32_t *>(base + sizeof(MlpSmem) + kLearnedTileBytes);
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    double *ws = reinterpret_cast<double *>(base + sizeof(MlpSmem)) + warp * kTileSmemDoubles;
+    double *ws = tiles + warp * kTileSmemDoubles;
     double *wacc = ws + 7 * 32;
     const long long t = (long long)blockIdx.x * kLearnedWarps + warp;
     const bool live = t < A.nwb;
     int bi = 0, bj = 0;
     if (live) warp_block_coords(t, bi, bj);
-    mlp_setup(S, A.heads);
+    mlp_setup(S);
     uint32_t phase = 0;
     PairCounters cnt;
     counters_zero(cnt);
@@ -236,6 +267,8 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const 
     }
     const int i = bi * 32 + lane;
     const bool diag = (bi == bj);
+
+    // 1. classification and the head inputs
     unsigned mh = 0u, me = 0u, mr = 0u;
     if (live) {
         const int k0 = diag ? 1 : 0, k1 = diag ? 16 : 31;
@@ -254,41 +287,73 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const 
             }
         }
     }
+    int oh, oe, rh, re;
+    cta_scan2(S, __popc(mh), __popc(me), oh, oe, rh, re);
+    oe += rh;  // elliptic rows follow the hyperbolic ones
+    {
+        int ih = oh, ie = oe;
+        unsigned m = mh | me;
+        while (m) {
+            const int k = __ffs(m) - 1;
+            m &= m - 1u;
+            const int src = (lane + k) & 31;
+            const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
+            const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
+            const double eps_ij = hq ? A.eps_th * si[6] * ws[6 * 32 + src] : A.eps_th;
+            LearnedPair L;
+            learned_prepare(eps_ij, dt, r, g, L);
+            const uint32_t x01 = pack_bf16(L.x0, L.x1);
+            if ((mh >> k) & 1u) rows[ih++] = x01;
+            else rows[ie++] = x01;
+        }
+    }
+    __syncthreads();
+
+    // 2. the heads on the tensor cores, 256 rows per evaluation
     bool timed_out = false;
     for (int pass = 0; pass < 2; pass++) {
         const int head = pass == 0 ? kHeadHyp : kHeadEll;
-        unsigned m = pass == 0 ? mh : me;
-        if (threadIdx.x == 0) S.turns = 0;
-        __syncthreads();
-        atomicMax(&S.turns, __popc(m));
-        __syncthreads();
-        const int nturns = S.turns;
-        for (int turn = 0; turn < nturns; turn++) {
+        const int r0 = pass == 0 ? 0 : rh;
+        const int nr = pass == 0 ? rh : re;
+        if (nr == 0) continue;  // uniform
+        mlp_load_head(S, A.heads, head);
+        for (int b = 0; b < nr; b += kMlpThreads) {
+            const int row = b + (int)threadIdx.x;
+            const bool valid = row < nr;
+            const uint32_t x01 = valid ? rows[r0 + row] : 0u;
+            bool ok;
+            const float y = mlp_eval_cta(S, x01, phase, ok);
+            if (!ok) timed_out = true;
+            if (valid) rows[r0 + row] = __float_as_uint(ok ? y : __int_as_float(0x7fc00000));
+        }
+    }
+    __syncthreads();
+
+    // 3. learned pairs from their guesses, per warp
+    {
+        int ih = oh, ie = oe;
+        unsigned m = mh | me;
+        for (;;) {
             const bool busy = (m != 0u);
-            int j = 0;
-            double r[3] = {0, 0, 0}, g[3] = {0, 0, 0}, eps_ij = 0.0;
-            LearnedPair L;
-            L.x0 = L.x1 = 0.0f;
+            const unsigned bm = __ballot_sync(0xffffffffu, busy);
+            if (bm == 0u) break;
             if (busy) {
                 const int k = __ffs(m) - 1;
                 m &= m - 1u;
-                j = (lane + k) & 31;
+                const bool is_h = (mh >> k) & 1u;
+                const float y = __uint_as_float(rows[is_h ? ih++ : ie++]);
+                const int j = (lane + k) & 31;
+                double r[3], g[3], h[6];
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     r[c] = si[c] - ws[c * 32 + j];
                     g[c] = si[3 + c] - ws[(3 + c) * 32 + j];
                 }
-                eps_ij = hq ? A.eps_th * si[6] * ws[6 * 32 + j] : A.eps_th;
+                const double eps_ij = hq ? A.eps_th * si[6] * ws[6 * 32 + j] : A.eps_th;
+                LearnedPair L;
                 learned_prepare(eps_ij, dt, r, g, L);
-            }
-            bool ok;
-            const float y = mlp_eval_cta(S, head, L.x0, L.x1, phase, ok);
-            if (!ok) timed_out = true;
-            const unsigned bm = __ballot_sync(0xffffffffu, busy);
-            if (busy) {
-                double h[6];
                 bool coarse = true;
-                const bool done = ok && learned_finish(L, dt, y, r, g, h, coarse);
+                const bool done = learned_finish(L, dt, y, r, g, h, coarse);
                 cnt.learned++;
                 if (coarse) cnt.learned_coarse++;
                 if (!done) {
@@ -297,7 +362,7 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const 
                     cnt.it_uv += it;
                     if (it > kUvItMax) cnt.nonconverged++;
                 }
-                cnt.cls[head == kHeadEll ? kEllipse : kHyperbola]++;
+                cnt.cls[is_h ? kHyperbola : kEllipse]++;
                 count_nonfinite(h, cnt);
 #pragma unroll
                 for (int c = 0; c < 6; c++) racc[c] += h[c];
@@ -337,10 +402,7 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const 
 #pragma unroll
     for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
     mlp_teardown(S, phase);
-    if (timed_out && threadIdx.x == 0) {
-        // every thread of the CTA saw the timeout; count it with the CTA's first live warp
-        if (!live) atomicAdd(&A.stats[kStatTimeouts], 1ull);
-    }
+    if (timed_out && threadIdx.x == 0 && !live) atomicAdd(&A.stats[kStatTimeouts], 1ull);
     if (!live) return;  // warp-uniform; no barrier follows
     flush_counters(cnt, A.stats, lane);
     const int jown = bj * 32 + lane;
@@ -940,7 +1002,8 @@ __global__ void __launch_bounds__(kMlpThreads, 1) bia_head_eval_kernel(const Mlp
     extern __shared__ uint8_t head_smem_raw[];
     uint8_t *base = (uint8_t *)(((uintptr_t)head_smem_raw + 1023) & ~(uintptr_t)1023);
     MlpSmem &S = *reinterpret_cast<MlpSmem *>(base);
-    mlp_setup(S, heads);
+    mlp_setup(S);
+    mlp_load_head(S, heads, head);
     uint32_t phase = 0;
     bool ok = true;
     // the same number of rounds on every thread of the CTA (the MLP synchronises the CTA)
@@ -949,7 +1012,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1) bia_head_eval_kernel(const Mlp
         const long long row = row0 + threadIdx.x;
         const float x0 = row < n ? in[2 * row] : 0.0f;
         const float x1 = row < n ? in[2 * row + 1] : 0.0f;
-        const float y = mlp_eval_cta(S, head, x0, x1, phase, ok);
+        const float y = mlp_eval_cta(S, pack_bf16(x0, x1), phase, ok);
         if (row < n) out[row] = ok ? y : __int_as_float(0x7fc00000);
     }
     mlp_teardown(S, phase);

@@ -41,19 +41,21 @@ struct MlpHead {
 static_assert(sizeof(MlpHead) == 19472, "learned_heads.bin head record");
 constexpr int kMlpHeads = 2;  // 0 elliptic, 1 hyperbolic
 
-// Shared-memory image of both heads and the activation tiles (bytes, 1024-aligned parts).
+// Shared-memory image of one head and the activation tile (1024-aligned parts).  The
+// layer-1 rows (K = 16) live in the first 8 KB of the layer-2/3 tile: layer 1's MMA has
+// completed before the first epilogue overwrites them.
 struct MlpSmem {
-    alignas(1024) uint8_t w1[kMlpHeads][kMlpHidden * kMlpK1 * 2];        // 2 x 2 KB
-    alignas(1024) uint8_t w2[kMlpHeads][kMlpHidden * kMlpHidden * 2];    // 2 x 8 KB
-    alignas(1024) uint8_t w3[kMlpHeads][kMlpHidden * kMlpHidden * 2];    // 2 x 8 KB
-    alignas(1024) uint8_t a1[kMlpThreads * kMlpK1 * 2];                  // 8 KB
-    alignas(1024) uint8_t a2[kMlpThreads * kMlpHidden * 2];              // 32 KB
-    float b1[kMlpHeads][kMlpHidden], b2[kMlpHeads][kMlpHidden], b3[kMlpHeads][kMlpHidden];
-    float w4[kMlpHeads][kMlpHidden], b4[kMlpHeads];
+    alignas(1024) uint8_t w1[kMlpHidden * kMlpK1 * 2];        // 2 KB
+    alignas(1024) uint8_t w2[kMlpHidden * kMlpHidden * 2];    // 8 KB
+    alignas(1024) uint8_t w3[kMlpHidden * kMlpHidden * 2];    // 8 KB
+    alignas(1024) uint8_t a2[kMlpThreads * kMlpHidden * 2];   // 32 KB; a1 = a2
+    float b1[kMlpHidden], b2[kMlpHidden], b3[kMlpHidden], w4[kMlpHidden], b4;
     alignas(8) uint64_t mbar;
     uint32_t tmem_base;
     int abort;
-    int turns;  // scratch for CTA-wide turn counts of the callers
+    int turns;  // scratch for CTA-wide counts of the callers
+    int head;   // the head whose weights are loaded (-1: none)
+    int wsum[2][kMlpThreads / 32];  // per-warp totals of the callers' row scans
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
@@ -131,43 +133,46 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float v[16])
     for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
 }
 
+// (a, b) rounded to BF16 (nearest even), a in the low half: one paired conversion
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b)
 {
-    const uint32_t lo = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a));
-    const uint32_t hi = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(b));
-    return lo | (hi << 16);
+    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t *>(&v);
 }
 
-// Once per CTA (all threads): heads from global memory into the shared image, the constant
-// zero half of the layer-1 rows, the mbarrier, and the TMEM allocation (warp 0, 128
-// columns: two 128 x 64 FP32 accumulator tiles).
-__device__ __forceinline__ void mlp_setup(MlpSmem &S, const MlpHead *heads)
+// One head's weights from global memory into the shared image (all threads; the caller
+// synchronises before the next MMA: mlp_layer does).
+__device__ __forceinline__ void mlp_load_head(MlpSmem &S, const MlpHead *heads, int h)
 {
     const int tid = threadIdx.x;
-    for (int h = 0; h < kMlpHeads; h++) {
-        const MlpHead &H = heads[h];
-        for (int e = tid; e < kMlpHidden * kMlpK1; e += blockDim.x) {
-            const int n = e / kMlpK1, k = e % kMlpK1;
-            *(uint16_t *)(S.w1[h] + kmajor_off(n, k, kMlpK1)) = H.w1[e];
-        }
-        for (int e = tid; e < kMlpHidden * kMlpHidden; e += blockDim.x) {
-            const int n = e / kMlpHidden, k = e % kMlpHidden;
-            *(uint16_t *)(S.w2[h] + kmajor_off(n, k, kMlpHidden)) = H.w2[e];
-            *(uint16_t *)(S.w3[h] + kmajor_off(n, k, kMlpHidden)) = H.w3[e];
-        }
-        for (int e = tid; e < kMlpHidden; e += blockDim.x) {
-            S.b1[h][e] = H.b1[e];
-            S.b2[h][e] = H.b2[e];
-            S.b3[h][e] = H.b3[e];
-            S.w4[h][e] = H.w4[e];
-        }
-        if (tid == 0) S.b4[h] = H.b4[0];
+    const MlpHead &H = heads[h];
+    for (int e = tid; e < kMlpHidden * kMlpK1; e += blockDim.x)
+        *(uint16_t *)(S.w1 + kmajor_off(e / kMlpK1, e % kMlpK1, kMlpK1)) = H.w1[e];
+    for (int e = tid; e < kMlpHidden * kMlpHidden; e += blockDim.x) {
+        const int n = e / kMlpHidden, k = e % kMlpHidden;
+        *(uint16_t *)(S.w2 + kmajor_off(n, k, kMlpHidden)) = H.w2[e];
+        *(uint16_t *)(S.w3 + kmajor_off(n, k, kMlpHidden)) = H.w3[e];
     }
-    // layer-1 rows: inputs in k = 0, 1; k = 2..15 stay zero
-    for (int e = tid; e < kMlpThreads * kMlpK1; e += blockDim.x)
-        *(uint16_t *)(S.a1 + kmajor_off(e / kMlpK1, e % kMlpK1, kMlpK1)) = 0;
+    for (int e = tid; e < kMlpHidden; e += blockDim.x) {
+        S.b1[e] = H.b1[e];
+        S.b2[e] = H.b2[e];
+        S.b3[e] = H.b3[e];
+        S.w4[e] = H.w4[e];
+    }
+    if (tid == 0) {
+        S.b4 = H.b4[0];
+        S.head = h;
+    }
+}
+
+// Once per CTA (all threads): the mbarrier and the TMEM allocation (warp 0, 128 columns:
+// two 128 x 64 FP32 accumulator tiles).  No head is loaded yet.
+__device__ __forceinline__ void mlp_setup(MlpSmem &S)
+{
+    const int tid = threadIdx.x;
     if (tid == 0) {
         S.abort = 0;
+        S.head = -1;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.mbar)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -232,7 +237,7 @@ __device__ __forceinline__ bool mlp_layer(MlpSmem &S, const uint8_t *a, const ui
 
 // This thread's accumulator row of the last layer: + bias, ReLU; either written as BF16
 // into the next A tile (dst != nullptr) or dotted with w4 (returned).
-__device__ __forceinline__ float mlp_epilogue(MlpSmem &S, int head, const float *bias, uint8_t *dst)
+__device__ __forceinline__ float mlp_epilogue(MlpSmem &S, const float *bias, uint8_t *dst)
 {
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
@@ -255,27 +260,29 @@ __device__ __forceinline__ float mlp_epilogue(MlpSmem &S, int head, const float 
             *(uint4 *)(dst + kmajor_off(tid, c + 8, kMlpHidden)) = hi;
         } else {
 #pragma unroll
-            for (int j = 0; j < 16; j++) dot = fmaf(v[j], S.w4[head][c + j], dot);
+            for (int j = 0; j < 16; j++) dot = fmaf(v[j], S.w4[c + j], dot);
         }
     }
-    return dot + S.b4[head];
+    return dot + S.b4;
 }
 
-// The head's output for this thread's input row (x0, x1); every thread of the CTA calls it
-// with the same head.  ok (the same on every thread) is false when the tensor-core pipeline
-// timed out; the CTA then issues no more MMAs.
-__device__ __forceinline__ float mlp_eval_cta(MlpSmem &S, int head, float x0, float x1, uint32_t &phase, bool &ok)
+// The loaded head's output for this thread's input row, given as packed BF16 (x0 in the
+// low half); every thread of the CTA calls it.  ok (the same on every thread) is false
+// when the tensor-core pipeline timed out; the CTA then issues no more MMAs.
+__device__ __forceinline__ float mlp_eval_cta(MlpSmem &S, uint32_t x01_bf16, uint32_t &phase, bool &ok)
 {
     const int tid = threadIdx.x;
-    *(uint32_t *)(S.a1 + kmajor_off(tid, 0, kMlpK1)) = pack_bf16(x0, x1);
+    uint8_t *a1 = S.a2;  // layer-1 rows alias the layer-2 tile
+    *(uint4 *)(a1 + kmajor_off(tid, 0, kMlpK1)) = make_uint4(x01_bf16, 0u, 0u, 0u);
+    *(uint4 *)(a1 + kmajor_off(tid, 8, kMlpK1)) = make_uint4(0u, 0u, 0u, 0u);
     ok = false;
-    if (!mlp_layer(S, S.a1, S.w1[head], kMlpK1, phase)) return 0.0f;
-    mlp_epilogue(S, head, S.b1[head], S.a2);
-    if (!mlp_layer(S, S.a2, S.w2[head], kMlpHidden, phase)) return 0.0f;
-    mlp_epilogue(S, head, S.b2[head], S.a2);
-    if (!mlp_layer(S, S.a2, S.w3[head], kMlpHidden, phase)) return 0.0f;
+    if (!mlp_layer(S, a1, S.w1, kMlpK1, phase)) return 0.0f;
+    mlp_epilogue(S, S.b1, S.a2);
+    if (!mlp_layer(S, S.a2, S.w2, kMlpHidden, phase)) return 0.0f;
+    mlp_epilogue(S, S.b2, S.a2);
+    if (!mlp_layer(S, S.a2, S.w3, kMlpHidden, phase)) return 0.0f;
     ok = true;
-    return mlp_epilogue(S, head, S.b3[head], nullptr);
+    return mlp_epilogue(S, S.b3, nullptr);
 }
 
 }  // namespace bia
