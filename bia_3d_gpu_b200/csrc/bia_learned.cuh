@@ -42,6 +42,18 @@ struct LearnedPair {
     int kind;              // kLearnedPlain / kLearnedEll / kLearnedHyp
 };
 
+// Cheap first test: can the pair be in a head's domain?  ellipses (all of them: the
+// universal-variable guard leaves e^2 <= 0.9), and attractive hyperbolae with
+// e^2 - 1 = E L^2 / eps^2 <= 50^2 - 1.  learned_prepare makes the final decision.
+__device__ __forceinline__ bool learned_candidate(double eps_ij, double dt, const double r[3], const double g[3])
+{
+    double E, Lsq;
+    const int c = alg_classify(eps_ij, r, g, E, Lsq);
+    if (!(dt > 0.0) || !(eps_ij < 0.0)) return false;
+    if (c == kClsEll) return true;
+    return c == kClsHyp && E * Lsq <= (double)(kHypEMax * kHypEMax - 1.0f) * (eps_ij * eps_ij);
+}
+
 __device__ __forceinline__ void learned_prepare(double eps_ij, double dt, const double r[3], const double g[3],
                                                 LearnedPair &L)
 {

@@ -879,7 +879,8 @@ enum AlgClass { kClsHyp = 0, kClsEll = 1, kClsUv = 2, kClsPar = 3, kClsDeg = 4 }
 // Branch of an ALG pair: E == 0 exactly keeps the reference's parabola branch; zero |g| or
 // |L| (degenerate) and |e^2 - 1| = |E| L^2 / eps^2 < 0.1 go to the universal-variable
 // solver; otherwise hyperbola (E > 0) or ellipse (E < 0).
-__device__ __forceinline__ int alg_classify(double eps_ij, const double r[3], const double g[3])
+__device__ __forceinline__ int alg_classify(double eps_ij, const double r[3], const double g[3], double &E_out,
+                                            double &Lsq_out)
 {
     const double gsq = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
     const double L0 = r[1] * g[2] - r[2] * g[1];
@@ -888,10 +889,18 @@ __device__ __forceinline__ int alg_classify(double eps_ij, const double r[3], co
     const double Lsq = L0 * L0 + L1 * L1 + L2 * L2;
     const double r_ij = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
     const double E_ij = gsq + 2.0 * eps_ij / r_ij;
+    E_out = E_ij;
+    Lsq_out = Lsq;
     if (E_ij == 0.0) return kClsPar;
     if (gsq == 0.0 || Lsq == 0.0) return kClsDeg;
     if (fabs(E_ij) * Lsq < kNearUnitEcc * (eps_ij * eps_ij)) return kClsUv;
     return (E_ij > 0.0) ? kClsHyp : kClsEll;
+}
+
+__device__ __forceinline__ int alg_classify(double eps_ij, const double r[3], const double g[3])
+{
+    double E, Lsq;
+    return alg_classify(eps_ij, r, g, E, Lsq);
 }
 
 // M: the compiled method (kMethodRkf, kMethodAlg, kMethodUniversal); each kernel is

@@ -278,11 +278,15 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const 
                 const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
                 const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
                 const double eps_ij = hq ? A.eps_th * si[6] * ws[6 * 32 + src] : A.eps_th;
-                LearnedPair L;
-                learned_prepare(eps_ij, dt, r, g, L);
                 const unsigned bit = 1u << k;
-                if (L.kind == kLearnedHyp) mh |= bit;
-                else if (L.kind == kLearnedEll) me |= bit;
+                int kind = kLearnedPlain;
+                if (learned_candidate(eps_ij, dt, r, g)) {
+                    LearnedPair L;
+                    learned_prepare(eps_ij, dt, r, g, L);
+                    kind = L.kind;
+                }
+                if (kind == kLearnedHyp) mh |= bit;
+                else if (kind == kLearnedEll) me |= bit;
                 else mr |= bit;
             }
         }
@@ -329,8 +333,41 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const 
     }
     __syncthreads();
 
-    // 3. learned pairs from their guesses, per warp
-    {
+    // 3. learned pairs from their guesses, per warp.  A warp without learned pairs walks the
+    // rotation offsets instead (all its pairs plain; column sums by shuffle, no shared adds)
+    const bool warp_learned = __any_sync(0xffffffffu, (mh | me) != 0u);
+    double cacc[6];
+    if (!warp_learned) {
+        const unsigned full = 0xffffffffu;
+#pragma unroll
+        for (int c = 0; c < 6; c++) cacc[c] = 0.0;
+        const int k0 = diag ? 1 : 0, k1 = diag ? 16 : 31;
+        for (int k = k0; k <= k1; k++) {
+            const int src = (lane + k) & 31;
+            double h[6] = {0, 0, 0, 0, 0, 0};
+            if ((mr >> k) & 1u) {
+                double r[3], g[3];
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    r[c] = si[c] - ws[c * 32 + src];
+                    g[c] = si[3 + c] - ws[(3 + c) * 32 + src];
+                }
+                const double eps_ij = hq ? A.eps_th * si[6] * ws[6 * 32 + src] : A.eps_th;
+                const int it = uv_halfdisp(eps_ij, dt, r, g, h);
+                cnt.it_uv += it;
+                if (it > kUvItMax) cnt.nonconverged++;
+                cnt.cls[alg_classify(eps_ij, r, g) == kClsDeg ? kDegenerate : kUniversal]++;
+                count_nonfinite(h, cnt);
+            }
+            const int back = (lane - k) & 31;
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                racc[c] += h[c];
+                cacc[c] += __shfl_sync(full, h[c], back);
+            }
+        }
+        mr = 0u;
+    } else {
         int ih = oh, ie = oe;
         unsigned m = mh | me;
         for (;;) {
@@ -371,7 +408,7 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const 
         }
     }
     if (timed_out && threadIdx.x == 0) cnt.timeouts++;
-    // plain pairs: the universal-variable solver, per warp
+    // plain pairs: the universal-variable solver, per warp (mr is empty on rotation warps)
     for (;;) {
         const bool busy = (mr != 0u);
         const unsigned bm = __ballot_sync(0xffffffffu, busy);
@@ -397,10 +434,11 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const 
             add_column(wacc, j, h, bm, lane);
         }
     }
-    __syncwarp();
-    double cacc[6];
+    if (warp_learned) {
+        __syncwarp();
 #pragma unroll
-    for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
+        for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
+    }
     mlp_teardown(S, phase);
     if (timed_out && threadIdx.x == 0 && !live) atomicAdd(&A.stats[kStatTimeouts], 1ull);
     if (!live) return;  // warp-uniform; no barrier follows
