@@ -266,34 +266,54 @@ def run_ensemble(args, rank, world, local):
     host = np.ascontiguousarray(np.concatenate(states, axis=1))
     steps = args.steps if args.steps is not None else 200
     dt = 1e-4
-    method = {"rkf": 0, "alg": 1, "universal": 2}[args.method]
+    method = METHODS[args.method] if args.method != "learned" else 1
     cfg = default_config(dt=dt, method=method)
     pairs = int(sum(int(n) * (int(n) - 1) // 2 for n in sizes))
     solver = BIASolver(device=local)
+    solver.load_heads()
     ens = solver.ensemble(sizes, eps)
     d = torch.tensor(host, device=dev)
     ke0, pe0 = ens.energy(d)
-    with torch.cuda.stream(solver.stream):
-        ens.run(d, cfg, args.warmup, graph=False, stats=False)     # warm-up (untimed)
-    d.copy_(torch.tensor(host, device=dev))
-    ens.run(d, cfg, steps, graph=True, stats=False)              # capture the graph
-    d.copy_(torch.tensor(host, device=dev))
-    torch.cuda.synchronize()
-    sampler = ClockSampler(local)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
-    sampler.start()
-    e0.record(solver.stream)
-    st = ens.run(d, cfg, steps, graph=True, stats=False)
-    e1.record(solver.stream)
-    torch.cuda.synchronize()
-    clocks = sampler.stop()
-    ms = _max_over_ranks(dist, e0.elapsed_time(e1), dev)
-    stats = solver.counters(reset=True)
-    ke1, pe1 = ens.energy(d)
-    drift = np.abs((ke1 + pe1) / (ke0 + pe0) - 1)
+
+    def timed(c, sample_clocks):
+        """warm-up, graph capture, then the timed graph replay of `steps` steps from the
+        seeded state; returns (ms, clocks, counters, per-system energy drift)."""
+        with torch.cuda.stream(solver.stream):
+            ens.run(d, c, args.warmup, graph=False, stats=False)     # warm-up (untimed)
+        d.copy_(torch.tensor(host, device=dev))
+        ens.run(d, c, steps, graph=True, stats=False)              # capture the graph
+        d.copy_(torch.tensor(host, device=dev))
+        torch.cuda.synchronize()
+        solver.counters(reset=True)
+        sampler = ClockSampler(local) if sample_clocks else None
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.start()
+        e0.record(solver.stream)
+        ens.run(d, c, steps, graph=True, stats=False)
+        e1.record(solver.stream)
+        torch.cuda.synchronize()
+        clk = sampler.stop() if sampler else None
+        t_ms = _max_over_ranks(dist, e0.elapsed_time(e1), dev)
+        counters = solver.counters(reset=True)
+        ke1, pe1 = ens.energy(d)
+        dr = np.abs((ke1 + pe1) / (ke0 + pe0) - 1)
+        return t_ms, clk, counters, dr
+
+    ms, clocks, stats, drift = timed(cfg, True)
+    learned = None
+    if not args.no_plain and method == 1:
+        l_ms, _, l_stats, l_drift = timed(default_config(dt=dt, method=3), False)
+        learned = {"value": world * nsys * steps / (l_ms * 1e-3), "unit": "systems-steps/s",
+                   "pair_updates_per_s": world * pairs * steps / (l_ms * 1e-3),
+                   "ms_per_step": l_ms / steps, "speedup_vs_plain": ms / l_ms,
+                   "learned_pair_fraction": l_stats["learned"] / max(1, steps * pairs),
+                   "learned_fallbacks": l_stats["learned_fallbacks"],
+                   "energy_drift": {"max": float(l_drift.max()), "median": float(np.median(l_drift)),
+                                    "p99": float(np.quantile(l_drift, 0.99))}}
     if rank == 0:
         print(json.dumps({
             "metric": "BIA ensemble systems-steps/s (plain FP64 step)",
@@ -309,6 +329,7 @@ def run_ensemble(args, rank, world, local):
                        "l2": "per-step working set (partials %.1f GB) exceeds the 126 MB L2"
                              % (sum(6 * 32 * ((int(n) + 31) // 32) ** 2 for n in sizes) * 8e-9),
                        "parallelism": f"replicas x{world}"},
+            "learned": learned,
             "energy_drift": {"max": float(drift.max()), "median": float(np.median(drift)),
                              "p99": float(np.quantile(drift, 0.99))},
             "clocks": clocks, "gpu_launches": 2 * steps,
@@ -443,6 +464,12 @@ def main():
         counters = solver.counters(reset=True)
         return max_over_ranks(total), clk, counters, kern
 
+    # the ALG pair-kernel shape for this size, chosen by the autotuner on this GPU
+    tuned = None
+    if method == 1 or (method != 1 and not args.no_plain):
+        cfg_alg = default_config(eps_th=eps, dt=dt, method=1)
+        var, tms = solver.autotune(d_state, cfg_alg, q=d_q)
+        tuned = {"alg_shape": ("tiles8", "phase16", "phase32")[var], "ms": tms}
     total_ms, clocks, stats, (kern_ms, kern_launches) = timed_steps(cfg, steps, sample_clocks=True)
     value = world * steps * pairs / (total_ms * 1e-3)
 
@@ -478,8 +505,11 @@ def main():
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     if method == 3:
         kernel_name = "bia_pair_learned_kernel<true>"
+    elif method == 1 and tuned is not None:
+        kernel_name = {"tiles8": "bia_pair_tiles_kernel<true, 1>", "phase16": "bia_pair_phase_kernel<true, 16, 2>",
+                       "phase32": "bia_pair_phase_kernel<true, 32, 1>"}[tuned["alg_shape"]]
     elif method == 1 and (nwb + 31) // 32 >= 2 * sms:
-        kernel_name = "bia_pair_phase_kernel<true>"
+        kernel_name = "bia_pair_phase_kernel<true, 32, 1>"
     else:
         kernel_name = "bia_pair_tiles_kernel<true>"
     flops_total = pair_flops(stats, method)
@@ -616,7 +646,7 @@ def main():
                        "l2": "256 MB buffer written between timed steps (untimed)",
                        "state": "reset to the seeded state before every timed step (untimed "
                                 "device copy; the e2e loop copies it into the host buffer)",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"replicas x{world}", "autotuned": tuned},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
             "gpu_launches": 2 * steps, "plain_fp64": plain, "universal": universal,
             "reference_gpu_kernel": ref_gpu,

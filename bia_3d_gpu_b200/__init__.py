@@ -274,6 +274,20 @@ class BIASolver:
             raise BiaError(st, "bia_dim_integrate")
         return st_.as_dict()
 
+    def autotune(self, state, cfg, q=None):
+        """Time the pair-kernel shapes of cfg's method on this state (unchanged) and keep
+        the fastest for this size; returns (variant, {shape: ms})."""
+        n = self._check_state(state)
+        var = ctypes.c_int(-1)
+        ms = (ctypes.c_float * 3)()
+        cur = self._enter()
+        st = capi.lib().bia_context_autotune(self._ctx, ctypes.byref(cfg), n, *self._ptrs(state),
+                                             self._qptr(q, n), ctypes.byref(var), ms)
+        self._leave(cur)
+        capi.check(st, "bia_context_autotune")
+        names = ("tiles8", "phase16", "phase32")
+        return var.value, {names[k]: float(ms[k]) for k in range(3) if ms[k] >= 0}
+
     def load_heads(self, path=None):
         """Load the learned heads (learned_heads.bin) for METHOD_LEARNED steps."""
         blob = open(path or HEADS_PATH, "rb").read()

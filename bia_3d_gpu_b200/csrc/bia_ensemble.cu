@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "bia_internal.cuh"
+#include "bia_learned_block.cuh"
 #include "bia_pair.cuh"
 #include "bia_tiles.cuh"
 
@@ -54,6 +55,7 @@ struct EnsArgs {
     double *part;
     unsigned long long *stats;
     PairParams P;
+    const MlpHead *heads;  // BIA_METHOD_LEARNED
 };
 
 template <int M>
@@ -127,6 +129,54 @@ static int ens_phase_setup()
         done_of[dev] = true;
     }
     return sms_of[dev];
+}
+
+// Learned mixed-precision form over the item table (bia_learned_block.cuh): CTAs of
+// kLearnedWarps warps, one item each.
+__global__ void __launch_bounds__(kMlpThreads, 2) ens_pair_learned_kernel(const EnsArgs A)
+{
+    extern __shared__ uint8_t ens_learned_raw[];
+    const LearnedSmem M = learned_smem(ens_learned_raw);
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const long long t = (long long)blockIdx.x * kLearnedWarps + warp;
+    const bool live = t < A.nitems;
+    int s = 0, bi = 0, bj = 0;
+    if (live) {
+        const uint2 it = A.items[t];
+        s = (int)it.x;
+        bi = (int)(it.y & 0xffffu);
+        bj = (int)(it.y >> 16);
+    }
+    const int base = A.off[s];
+    const int n = A.off[s + 1] - base;
+    const LearnedBlockIn B = {A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base,
+                              A.q ? A.q + base : nullptr, n, A.eps[s], A.P.dt, A.heads};
+    double racc[6], cacc[6];
+    PairCounters cnt;
+    const bool timed_out = learned_block_solve(M, B, bi, bj, lane, live, racc, cacc, cnt);
+    if (timed_out && threadIdx.x == 0 && !live) atomicAdd(&A.stats[kStatTimeouts], 1ull);
+    if (!live) return;  // warp-uniform; no barrier follows
+    flush_counters(cnt, A.stats, lane);
+    const int nb = (n + 31) / 32;
+    write_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
+}
+
+static bool ens_learned_setup()
+{
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static int state_of[kMaxDevices] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return false;
+    std::lock_guard<std::mutex> lk(mu);
+    if (state_of[dev] == 0) {
+        const bool ok = cudaFuncSetAttribute(ens_pair_learned_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kLearnedSmemBytes) == cudaSuccess;
+        if (!ok) cudaGetLastError();
+        state_of[dev] = ok ? 1 : 2;
+    }
+    return state_of[dev] == 1;
 }
 
 struct EnsUpdateArgs {
@@ -246,8 +296,14 @@ static int ens_enqueue_step(bia_context *ctx, bia_ensemble *E, const bia_config 
     A.P.abserr = cfg->rkf_abserr;
     A.P.itr = cfg->itr;
     A.P.method = cfg->method;
+    A.heads = (const MlpHead *)ctx->heads.ptr;
     const unsigned grid = (unsigned)((E->nitems + kEnsWarps - 1) / kEnsWarps);
-    switch (cfg->method) {
+    if (cfg->method == BIA_METHOD_LEARNED) {
+        if (!ctx->heads_loaded || !ens_learned_setup()) return BIA_ERR_INVALID_ARGUMENT;
+        const unsigned lgrid = (unsigned)((E->nitems + kLearnedWarps - 1) / kLearnedWarps);
+        ens_pair_learned_kernel<<<lgrid, kMlpThreads, kLearnedSmemBytes, ctx->stream>>>(A);
+    } else {
+        switch (cfg->method) {
     case BIA_METHOD_RKF: ens_pair_tiles_kernel<kMethodRkf><<<grid, kEnsThreads, 0, ctx->stream>>>(A); break;
     case BIA_METHOD_UNIVERSAL:
         ens_pair_tiles_kernel<kMethodUniversal><<<grid, kEnsThreads, 0, ctx->stream>>>(A);
@@ -261,6 +317,7 @@ static int ens_enqueue_step(bia_context *ctx, bia_ensemble *E, const bia_config 
             ens_pair_tiles_kernel<kMethodAlg><<<grid, kEnsThreads, 0, ctx->stream>>>(A);
         break;
     }
+        }
     }
     EnsUpdateArgs U;
     U.x = x; U.y = y; U.z = z; U.u = u; U.v = v; U.w = w;
@@ -372,10 +429,13 @@ extern "C" int bia_ensemble_run(bia_context *ctx, bia_ensemble *E, const bia_con
                                 int use_graph, bia_stats *stats)
 {
     if (!ctx || !E || !cfg || !x || !y || !z || !u || !v || !w || nsteps < 0) return BIA_ERR_INVALID_ARGUMENT;
-    if (cfg->method != BIA_METHOD_ALG && cfg->method != BIA_METHOD_RKF && cfg->method != BIA_METHOD_UNIVERSAL)
+    const bool learned_ok = cfg->method == BIA_METHOD_LEARNED && ctx->heads_loaded;
+    if (cfg->method != BIA_METHOD_ALG && cfg->method != BIA_METHOD_RKF && cfg->method != BIA_METHOD_UNIVERSAL &&
+        !learned_ok)
         return BIA_ERR_INVALID_ARGUMENT;
     if (cfg->itr < 1 || cfg->itr > 62) return BIA_ERR_INVALID_ARGUMENT;
     cudaSetDevice(ctx->device);
+    if (learned_ok && !ens_learned_setup()) return BIA_ERR_CUDA;  // before any stream capture
     cudaError_t e = cudaSuccess;
     if (stats) {
         e = cudaMemsetAsync(ctx->stats.ptr, 0, kNumStats * sizeof(unsigned long long), ctx->stream);

@@ -72,6 +72,8 @@ struct bia_context {
     bool timing = false;
     cudaEvent_t *ev = nullptr;
     int ev_cap = 0, ev_used = 0;
+    // autotuned ALG pair-kernel shape per reduction mode and floor(log2 n); -1: default rule
+    int alg_tuned[2][32];
     // learned heads (BIA_METHOD_LEARNED), 2 records of learned_heads.bin
     bia::DeviceBuffer heads;
     bool heads_loaded = false;

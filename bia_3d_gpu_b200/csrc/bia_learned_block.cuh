@@ -1,0 +1,299 @@
+// bia_learned_block.cuh -- one warp-block of the learned mixed-precision form
+// (BIA_METHOD_LEARNED) for a CTA of kLearnedWarps warps, shared by the single-system step
+// (bia_step.cu) and the ensemble (bia_ensemble.cu).
+#pragma once
+#include "bia_learned.cuh"
+#include "bia_pair.cuh"
+#include "bia_tiles.cuh"
+#include "mlp_tc.cuh"
+
+namespace bia {
+
+// A learned CTA: 8 warps, one warp-block each, two CTAs per SM, in three phases.
+//  1. Each lane classifies its pairs (hyperbolic head, elliptic head, plain) and writes the
+//     head inputs of its learned pairs into a CTA-wide row list in shared memory (packed
+//     BF16 pairs; hyperbolic rows first; offsets from a CTA scan of the per-lane counts).
+//  2. The CTA evaluates each head on its rows in full 256-row blocks on the tensor cores
+//     (mlp_tc.cuh) and writes each row's output over its input.
+//  3. Each warp finishes its learned pairs from the stored guesses (FP32 correction, FP64
+//     Halley step, composition; the plain solver where the FP64 step does not settle),
+//     then its plain pairs with the universal-variable solver, with no CTA barrier.
+// Column sums in the warp's shared slice, added in lane order per turn (deterministic).
+constexpr int kLearnedWarps = kMlpThreads / 32;
+constexpr int kLearnedMaxRows = kLearnedWarps * 1024;
+constexpr size_t kLearnedTileBytes = (size_t)kLearnedWarps * kTileSmemDoubles * sizeof(double);
+constexpr size_t kLearnedSmemBytes = 1024 + sizeof(MlpSmem) + kLearnedTileBytes + kLearnedMaxRows * sizeof(uint32_t);
+
+__device__ __forceinline__ void add_column(double *wacc, int j, const double h[6], unsigned bm, int lane)
+{
+    const unsigned grp = __match_any_sync(bm, j);
+    const int rank = __popc(grp & ((1u << lane) - 1u));
+    const int turns = (int)__reduce_max_sync(bm, (unsigned)__popc(grp));
+    for (int t = 0; t < turns; t++) {
+        if (rank == t) {
+#pragma unroll
+            for (int c = 0; c < 6; c++) wacc[c * 32 + j] += h[c];
+        }
+        __syncwarp(bm);
+    }
+}
+
+// exclusive CTA-wide prefix sums of (a, b) over threads in thread order; totals returned
+__device__ __forceinline__ void cta_scan2(MlpSmem &S, int a, int b, int &oa, int &ob, int &ta, int &tb)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int ia = a, ib = b;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int xa = __shfl_up_sync(0xffffffffu, ia, d);
+        const int xb = __shfl_up_sync(0xffffffffu, ib, d);
+        if (lane >= d) { ia += xa; ib += xb; }
+    }
+    if (lane == 31) { S.wsum[0][warp] = ia; S.wsum[1][warp] = ib; }
+    __syncthreads();
+    int ba = 0, bb = 0;
+    ta = tb = 0;
+    for (int w = 0; w < kLearnedWarps; w++) {
+        if (w < warp) { ba += S.wsum[0][w]; bb += S.wsum[1][w]; }
+        ta += S.wsum[0][w];
+        tb += S.wsum[1][w];
+    }
+    oa = ba + ia - a;
+    ob = bb + ib - b;
+}
+
+
+// The system a warp-block belongs to: particles x..w[0, n) (and charges q), coupling eps_th.
+struct LearnedBlockIn {
+    const double *x, *y, *z, *u, *v, *w, *q;
+    int n;
+    double eps_th, dt;
+    const MlpHead *heads;
+};
+
+// Dynamic shared memory of a learned CTA: the MLP image, the warps' column tiles, the row
+// list; base aligned to 1024 bytes.
+struct LearnedSmem {
+    MlpSmem *mlp;
+    double *tiles;
+    uint32_t *rows;
+};
+__device__ __forceinline__ LearnedSmem learned_smem(uint8_t *raw)
+{
+    uint8_t *base = (uint8_t *)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
+    LearnedSmem L;
+    L.mlp = reinterpret_cast<MlpSmem *>(base);
+    L.tiles = reinterpret_cast<double *>(base + sizeof(MlpSmem));
+    L.rows = reinterpret_cast<uint32_t *>(base + sizeof(MlpSmem) + kLearnedTileBytes);
+    return L;
+}
+
+// Every thread of the CTA calls it (warps without a block pass live = false).  Returns the
+// row sums racc (particle 32 bi + lane), the column sums cacc (particle 32 bj + lane; the
+// caller writes -cacc) and the counters; true when the tensor-core pipeline timed out.
+__device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const LearnedBlockIn &B, int bi, int bj,
+                                                    int lane, bool live, double racc[6], double cacc[6],
+                                                    PairCounters &cnt)
+{
+    MlpSmem &S = *M.mlp;
+    const int warp = threadIdx.x >> 5;
+    double *ws = M.tiles + warp * kTileSmemDoubles;
+    double *wacc = ws + 7 * 32;
+    uint32_t *rows = M.rows;
+    mlp_setup(S);
+    uint32_t phase = 0;
+    counters_zero(cnt);
+    double si[7];
+#pragma unroll
+    for (int c = 0; c < 6; c++) racc[c] = 0.0;
+    const double dt = B.dt;
+    const int n = B.n;
+    const bool hq = B.q != nullptr;
+    {
+        double sj[7];
+        load_particle(B.x, B.y, B.z, B.u, B.v, B.w, B.q, n, bi * 32 + lane, si);
+        load_particle(B.x, B.y, B.z, B.u, B.v, B.w, B.q, n, bj * 32 + lane, sj);
+#pragma unroll
+        for (int c = 0; c < 7; c++) ws[c * 32 + lane] = sj[c];
+#pragma unroll
+        for (int c = 0; c < 6; c++) wacc[c * 32 + lane] = 0.0;
+        __syncwarp();
+    }
+    const int i = bi * 32 + lane;
+    const bool diag = (bi == bj);
+
+    // 1. classification and the head inputs
+    unsigned mh = 0u, me = 0u, mr = 0u;
+    if (live) {
+        const int k0 = diag ? 1 : 0, k1 = diag ? 16 : 31;
+        for (int k = k0; k <= k1; k++) {
+            const int src = (lane + k) & 31;
+            if ((!diag || k < 16 || lane < 16) && i < n && bj * 32 + src < n) {
+                const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
+                const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
+                const double eps_ij = hq ? B.eps_th * si[6] * ws[6 * 32 + src] : B.eps_th;
+                const unsigned bit = 1u << k;
+                int kind = kLearnedPlain;
+                if (learned_candidate(eps_ij, dt, r, g)) {
+                    LearnedPair L;
+                    learned_prepare(eps_ij, dt, r, g, L);
+                    kind = L.kind;
+                }
+                if (kind == kLearnedHyp) mh |= bit;
+                else if (kind == kLearnedEll) me |= bit;
+                else mr |= bit;
+            }
+        }
+    }
+    int oh, oe, rh, re;
+    cta_scan2(S, __popc(mh), __popc(me), oh, oe, rh, re);
+    oe += rh;  // elliptic rows follow the hyperbolic ones
+    {
+        int ih = oh, ie = oe;
+        unsigned m = mh | me;
+        while (m) {
+            const int k = __ffs(m) - 1;
+            m &= m - 1u;
+            const int src = (lane + k) & 31;
+            const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
+            const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
+            const double eps_ij = hq ? B.eps_th * si[6] * ws[6 * 32 + src] : B.eps_th;
+            LearnedPair L;
+            learned_prepare(eps_ij, dt, r, g, L);
+            const uint32_t x01 = pack_bf16(L.x0, L.x1);
+            if ((mh >> k) & 1u) rows[ih++] = x01;
+            else rows[ie++] = x01;
+        }
+    }
+    __syncthreads();
+
+    // 2. the heads on the tensor cores, 256 rows per evaluation
+    bool timed_out = false;
+    for (int pass = 0; pass < 2; pass++) {
+        const int head = pass == 0 ? kHeadHyp : kHeadEll;
+        const int r0 = pass == 0 ? 0 : rh;
+        const int nr = pass == 0 ? rh : re;
+        if (nr == 0) continue;  // uniform
+        mlp_load_head(S, B.heads, head);
+        for (int b = 0; b < nr; b += kMlpThreads) {
+            const int row = b + (int)threadIdx.x;
+            const bool valid = row < nr;
+            const uint32_t x01 = valid ? rows[r0 + row] : 0u;
+            bool ok;
+            const float y = mlp_eval_cta(S, x01, phase, ok);
+            if (!ok) timed_out = true;
+            if (valid) rows[r0 + row] = __float_as_uint(ok ? y : __int_as_float(0x7fc00000));
+        }
+    }
+    __syncthreads();
+
+    // 3. learned pairs from their guesses, per warp.  A warp without learned pairs walks the
+    // rotation offsets instead (all its pairs plain; column sums by shuffle, no shared adds)
+    const bool warp_learned = __any_sync(0xffffffffu, (mh | me) != 0u);
+    if (!warp_learned) {
+        const unsigned full = 0xffffffffu;
+#pragma unroll
+        for (int c = 0; c < 6; c++) cacc[c] = 0.0;
+        const int k0 = diag ? 1 : 0, k1 = diag ? 16 : 31;
+        for (int k = k0; k <= k1; k++) {
+            const int src = (lane + k) & 31;
+            double h[6] = {0, 0, 0, 0, 0, 0};
+            if ((mr >> k) & 1u) {
+                double r[3], g[3];
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    r[c] = si[c] - ws[c * 32 + src];
+                    g[c] = si[3 + c] - ws[(3 + c) * 32 + src];
+                }
+                const double eps_ij = hq ? B.eps_th * si[6] * ws[6 * 32 + src] : B.eps_th;
+                const int it = uv_halfdisp(eps_ij, dt, r, g, h);
+                cnt.it_uv += it;
+                if (it > kUvItMax) cnt.nonconverged++;
+                cnt.cls[alg_classify(eps_ij, r, g) == kClsDeg ? kDegenerate : kUniversal]++;
+                count_nonfinite(h, cnt);
+            }
+            const int back = (lane - k) & 31;
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                racc[c] += h[c];
+                cacc[c] += __shfl_sync(full, h[c], back);
+            }
+        }
+        mr = 0u;
+    } else {
+        int ih = oh, ie = oe;
+        unsigned m = mh | me;
+        for (;;) {
+            const bool busy = (m != 0u);
+            const unsigned bm = __ballot_sync(0xffffffffu, busy);
+            if (bm == 0u) break;
+            if (busy) {
+                const int k = __ffs(m) - 1;
+                m &= m - 1u;
+                const bool is_h = (mh >> k) & 1u;
+                const float y = __uint_as_float(rows[is_h ? ih++ : ie++]);
+                const int j = (lane + k) & 31;
+                double r[3], g[3], h[6];
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    r[c] = si[c] - ws[c * 32 + j];
+                    g[c] = si[3 + c] - ws[(3 + c) * 32 + j];
+                }
+                const double eps_ij = hq ? B.eps_th * si[6] * ws[6 * 32 + j] : B.eps_th;
+                LearnedPair L;
+                learned_prepare(eps_ij, dt, r, g, L);
+                bool coarse = true;
+                const bool done = learned_finish(L, dt, y, r, g, h, coarse);
+                cnt.learned++;
+                if (coarse) cnt.learned_coarse++;
+                if (!done) {
+                    cnt.learned_fallbacks++;
+                    const int it = uv_halfdisp(eps_ij, dt, r, g, h);
+                    cnt.it_uv += it;
+                    if (it > kUvItMax) cnt.nonconverged++;
+                }
+                cnt.cls[is_h ? kHyperbola : kEllipse]++;
+                count_nonfinite(h, cnt);
+#pragma unroll
+                for (int c = 0; c < 6; c++) racc[c] += h[c];
+                add_column(wacc, j, h, bm, lane);
+            }
+        }
+    }
+    if (timed_out && threadIdx.x == 0) cnt.timeouts++;
+    // plain pairs: the universal-variable solver, per warp (mr is empty on rotation warps)
+    for (;;) {
+        const bool busy = (mr != 0u);
+        const unsigned bm = __ballot_sync(0xffffffffu, busy);
+        if (bm == 0u) break;
+        if (busy) {
+            const int k = __ffs(mr) - 1;
+            mr &= mr - 1u;
+            const int j = (lane + k) & 31;
+            double r[3], g[3], h[6];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                r[c] = si[c] - ws[c * 32 + j];
+                g[c] = si[3 + c] - ws[(3 + c) * 32 + j];
+            }
+            const double eps_ij = hq ? B.eps_th * si[6] * ws[6 * 32 + j] : B.eps_th;
+            const int it = uv_halfdisp(eps_ij, dt, r, g, h);
+            cnt.it_uv += it;
+            if (it > kUvItMax) cnt.nonconverged++;
+            cnt.cls[alg_classify(eps_ij, r, g) == kClsDeg ? kDegenerate : kUniversal]++;
+            count_nonfinite(h, cnt);
+#pragma unroll
+            for (int c = 0; c < 6; c++) racc[c] += h[c];
+            add_column(wacc, j, h, bm, lane);
+        }
+    }
+    if (warp_learned) {
+        __syncwarp();
+#pragma unroll
+        for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
+    }
+    mlp_teardown(S, phase);
+    return timed_out;
+}
+
+}  // namespace bia

@@ -31,7 +31,7 @@
 #include <mutex>
 
 #include "bia_internal.cuh"
-#include "bia_learned.cuh"
+#include "bia_learned_block.cuh"
 #include "bia_pair.cuh"
 #include "bia_tiles.cuh"
 #include "mlp_tc.cuh"
@@ -86,15 +86,15 @@ __global__ void __launch_bounds__(kThreads, TileOccupancy<M>::kMinBlocks) bia_pa
     }
 }
 
-// Phase-locked ALG step kernel (see phase_block_solve): one CTA of kPhaseWarps warps per
-// SM, each warp on one warp-block.
-template <bool kDeterministic>
-__global__ void __launch_bounds__(kPhaseWarps * 32, kPhaseMinBlocks) bia_pair_phase_kernel(const StepArgs A)
+// Phase-locked ALG step kernel (see phase_block_solve): CTAs of kW warps, kMinB of them
+// per SM, each warp on one warp-block.
+template <bool kDeterministic, int kW, int kMinB>
+__global__ void __launch_bounds__(kW * 32, kMinB) bia_pair_phase_kernel(const StepArgs A)
 {
     extern __shared__ double phase_smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const long long t = (long long)blockIdx.x * kPhaseWarps + warp;
+    const long long t = (long long)blockIdx.x * kW + warp;
     const bool live = t < A.nwb;
     int bi = 0, bj = 0;
     if (live) warp_block_coords(t, bi, bj);
@@ -122,6 +122,17 @@ __global__ void __launch_bounds__(kPhaseWarps * 32, kPhaseMinBlocks) bia_pair_ph
     }
 }
 
+// ALG pair-kernel shapes the autotuner chooses from (bia_context_autotune):
+//   kVarTiles8    8-warp CTAs, per-warp class phases (bia_pair_tiles_kernel)
+//   kVarPhase16   phase-locked CTAs of 16 warps, 2 per SM (64 registers)
+//   kVarPhase32   phase-locked CTAs of 32 warps, 1 per SM (64 registers)
+// Without a tuned entry the step takes kVarPhase32 when it gives at least two CTAs per SM,
+// else kVarTiles8.
+enum AlgVariant { kVarTiles8 = 0, kVarPhase16 = 1, kVarPhase32 = 2, kVarCount = 3 };
+
+template <int kW>
+constexpr int phase_smem_bytes() { return kW * kTileSmemDoubles * (int)sizeof(double); }
+
 // Once per device (the current one): opt the phase-locked kernels in to their dynamic
 // shared memory and read the SM count.  Returns the SM count, 0 when the set-up failed
 // (the caller then launches the 8-warp kernel).
@@ -137,10 +148,14 @@ static int phase_kernel_setup()
     if (!done_of[dev]) {
         int sms = 0;
         bool ok = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess;
-        ok = ok && cudaFuncSetAttribute(bia_pair_phase_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        kPhaseSmemBytes) == cudaSuccess;
-        ok = ok && cudaFuncSetAttribute(bia_pair_phase_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        kPhaseSmemBytes) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(bia_pair_phase_kernel<true, 32, 1>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, phase_smem_bytes<32>()) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(bia_pair_phase_kernel<false, 32, 1>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, phase_smem_bytes<32>()) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(bia_pair_phase_kernel<true, 16, 2>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, phase_smem_bytes<16>()) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(bia_pair_phase_kernel<false, 16, 2>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, phase_smem_bytes<16>()) == cudaSuccess;
         if (!ok) cudaGetLastError();  // clear; the 8-warp kernel is used instead
         sms_of[dev] = ok ? sms : 0;
         done_of[dev] = true;
@@ -148,15 +163,36 @@ static int phase_kernel_setup()
     return sms_of[dev];
 }
 
-template <bool kDeterministic>
-static void launch_pair_tiles(const StepArgs &A, long long grid, cudaStream_t st)
+// The variant the step uses for this launch: the tuned one when given (>= 0), else the
+// default rule above.
+static int alg_variant_for(long long nwb, int tuned)
 {
-    if (BIA_PHASE_WARPS > 0 && A.P.method == kMethodAlg) {
-        const long long pgrid = (A.nwb + kPhaseWarps - 1) / kPhaseWarps;
-        const int sms = phase_kernel_setup();
-        // below two CTAs per SM the 8-warp kernel keeps more SMs busy
-        if (sms > 0 && pgrid >= 2LL * sms) {
-            bia_pair_phase_kernel<kDeterministic><<<(unsigned)pgrid, kPhaseWarps * 32, kPhaseSmemBytes, st>>>(A);
+    const int sms = phase_kernel_setup();
+    if (sms <= 0 || BIA_PHASE_WARPS == 0) return kVarTiles8;
+    if (tuned >= 0 && tuned < kVarCount) return tuned;
+    return ((nwb + 31) / 32 >= 2LL * sms) ? kVarPhase32 : kVarTiles8;
+}
+
+static int ilog2_bucket(int n)
+{
+    int b = 0;
+    while ((n >> (b + 1)) > 0 && b < 31) b++;
+    return b;
+}
+
+template <bool kDeterministic>
+static void launch_pair_tiles(const StepArgs &A, long long grid, cudaStream_t st, int tuned = -1)
+{
+    if (A.P.method == kMethodAlg) {
+        const int var = alg_variant_for(A.nwb, tuned);
+        if (var == kVarPhase32) {
+            bia_pair_phase_kernel<kDeterministic, 32, 1>
+                <<<(unsigned)((A.nwb + 31) / 32), 32 * 32, phase_smem_bytes<32>(), st>>>(A);
+            return;
+        }
+        if (var == kVarPhase16) {
+            bia_pair_phase_kernel<kDeterministic, 16, 2>
+                <<<(unsigned)((A.nwb + 15) / 16), 16 * 32, phase_smem_bytes<16>(), st>>>(A);
             return;
         }
     }
@@ -173,281 +209,31 @@ static void launch_pair_tiles(const StepArgs &A, long long grid, cudaStream_t st
     }
 }
 
-
-// ---------------------------------------------------------------------------------------
-// Learned mixed-precision step kernel (BIA_METHOD_LEARNED): 8 warps, one warp-block each,
-// two CTAs per SM, in three phases.
-//  1. Each lane classifies its pairs (hyperbolic head, elliptic head, plain) and writes the
-//     head inputs of its learned pairs into a CTA-wide row list in shared memory (packed
-//     BF16 pairs; hyperbolic rows first; offsets from a CTA scan of the per-lane counts).
-//  2. The CTA evaluates each head on its rows in full 256-row blocks on the tensor cores
-//     (mlp_tc.cuh) and writes each row's output over its input.
-//  3. Each warp finishes its learned pairs from the stored guesses (FP32 correction, FP64
-//     Halley step, composition; the plain solver where the FP64 step does not settle),
-//     then its plain pairs with the universal-variable solver, with no CTA barrier.
-// Column sums in the warp's shared slice, added in lane order per turn (deterministic).
-constexpr int kLearnedWarps = kMlpThreads / 32;
-constexpr int kLearnedMaxRows = kLearnedWarps * 1024;
-constexpr size_t kLearnedTileBytes = (size_t)kLearnedWarps * kTileSmemDoubles * sizeof(double);
-constexpr size_t kLearnedSmemBytes = 1024 + sizeof(MlpSmem) + kLearnedTileBytes + kLearnedMaxRows * sizeof(uint32_t);
-
-__device__ __forceinline__ void add_column(double *wacc, int j, const double h[6], unsigned bm, int lane)
-{
-    const unsigned grp = __match_any_sync(bm, j);
-    const int rank = __popc(grp & ((1u << lane) - 1u));
-    const int turns = (int)__reduce_max_sync(bm, (unsigned)__popc(grp));
-    for (int t = 0; t < turns; t++) {
-        if (rank == t) {
-#pragma unroll
-            for (int c = 0; c < 6; c++) wacc[c * 32 + j] += h[c];
-        }
-        __syncwarp(bm);
-    }
-}
-
-// exclusive CTA-wide prefix sums of (a, b) over threads in thread order; totals returned
-__device__ __forceinline__ void cta_scan2(MlpSmem &S, int a, int b, int &oa, int &ob, int &ta, int &tb)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int ia = a, ib = b;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const int xa = __shfl_up_sync(0xffffffffu, ia, d);
-        const int xb = __shfl_up_sync(0xffffffffu, ib, d);
-        if (lane >= d) { ia += xa; ib += xb; }
-    }
-    if (lane == 31) { S.wsum[0][warp] = ia; S.wsum[1][warp] = ib; }
-    __syncthreads();
-    int ba = 0, bb = 0;
-    ta = tb = 0;
-    for (int w = 0; w < kLearnedWarps; w++) {
-        if (w < warp) { ba += S.wsum[0][w]; bb += S.wsum[1][w]; }
-        ta += S.wsum[0][w];
-        tb += S.wsum[1][w];
-    }
-    oa = ba + ia - a;
-    ob = bb + ib - b;
-}
-
+// Learned mixed-precision step kernel (BIA_METHOD_LEARNED): see bia_learned_block.cuh.
 template <bool kDeterministic>
 __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const StepArgs A)
 {
     extern __shared__ uint8_t learned_smem_raw[];
-    uint8_t *base = (uint8_t *)(((uintptr_t)learned_smem_raw + 1023) & ~(uintptr_t)1023);
-    MlpSmem &S = *reinterpret_cast<MlpSmem *>(base);
-    double *tiles = reinterpret_cast<double *>(base + sizeof(MlpSmem));
-    uint32_t *rows = reinterpret_cast<uint32_t *>(base + sizeof(MlpSmem) + kLearnedTileBytes);
+    const LearnedSmem M = learned_smem(learned_smem_raw);
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    double *ws = tiles + warp * kTileSmemDoubles;
-    double *wacc = ws + 7 * 32;
     const long long t = (long long)blockIdx.x * kLearnedWarps + warp;
     const bool live = t < A.nwb;
     int bi = 0, bj = 0;
     if (live) warp_block_coords(t, bi, bj);
-    mlp_setup(S);
-    uint32_t phase = 0;
+    const LearnedBlockIn B = {A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P.dt, A.heads};
+    double racc[6], cacc[6];
     PairCounters cnt;
-    counters_zero(cnt);
-    double si[7], racc[6];
-#pragma unroll
-    for (int c = 0; c < 6; c++) racc[c] = 0.0;
-    const double dt = A.P.dt;
-    const int n = A.n;
-    const bool hq = A.q != nullptr;
-    {
-        double sj[7];
-        load_particle(A.x, A.y, A.z, A.u, A.v, A.w, A.q, n, bi * 32 + lane, si);
-        load_particle(A.x, A.y, A.z, A.u, A.v, A.w, A.q, n, bj * 32 + lane, sj);
-#pragma unroll
-        for (int c = 0; c < 7; c++) ws[c * 32 + lane] = sj[c];
-#pragma unroll
-        for (int c = 0; c < 6; c++) wacc[c * 32 + lane] = 0.0;
-        __syncwarp();
-    }
-    const int i = bi * 32 + lane;
-    const bool diag = (bi == bj);
-
-    // 1. classification and the head inputs
-    unsigned mh = 0u, me = 0u, mr = 0u;
-    if (live) {
-        const int k0 = diag ? 1 : 0, k1 = diag ? 16 : 31;
-        for (int k = k0; k <= k1; k++) {
-            const int src = (lane + k) & 31;
-            if ((!diag || k < 16 || lane < 16) && i < n && bj * 32 + src < n) {
-                const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
-                const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
-                const double eps_ij = hq ? A.eps_th * si[6] * ws[6 * 32 + src] : A.eps_th;
-                const unsigned bit = 1u << k;
-                int kind = kLearnedPlain;
-                if (learned_candidate(eps_ij, dt, r, g)) {
-                    LearnedPair L;
-                    learned_prepare(eps_ij, dt, r, g, L);
-                    kind = L.kind;
-                }
-                if (kind == kLearnedHyp) mh |= bit;
-                else if (kind == kLearnedEll) me |= bit;
-                else mr |= bit;
-            }
-        }
-    }
-    int oh, oe, rh, re;
-    cta_scan2(S, __popc(mh), __popc(me), oh, oe, rh, re);
-    oe += rh;  // elliptic rows follow the hyperbolic ones
-    {
-        int ih = oh, ie = oe;
-        unsigned m = mh | me;
-        while (m) {
-            const int k = __ffs(m) - 1;
-            m &= m - 1u;
-            const int src = (lane + k) & 31;
-            const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
-            const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
-            const double eps_ij = hq ? A.eps_th * si[6] * ws[6 * 32 + src] : A.eps_th;
-            LearnedPair L;
-            learned_prepare(eps_ij, dt, r, g, L);
-            const uint32_t x01 = pack_bf16(L.x0, L.x1);
-            if ((mh >> k) & 1u) rows[ih++] = x01;
-            else rows[ie++] = x01;
-        }
-    }
-    __syncthreads();
-
-    // 2. the heads on the tensor cores, 256 rows per evaluation
-    bool timed_out = false;
-    for (int pass = 0; pass < 2; pass++) {
-        const int head = pass == 0 ? kHeadHyp : kHeadEll;
-        const int r0 = pass == 0 ? 0 : rh;
-        const int nr = pass == 0 ? rh : re;
-        if (nr == 0) continue;  // uniform
-        mlp_load_head(S, A.heads, head);
-        for (int b = 0; b < nr; b += kMlpThreads) {
-            const int row = b + (int)threadIdx.x;
-            const bool valid = row < nr;
-            const uint32_t x01 = valid ? rows[r0 + row] : 0u;
-            bool ok;
-            const float y = mlp_eval_cta(S, x01, phase, ok);
-            if (!ok) timed_out = true;
-            if (valid) rows[r0 + row] = __float_as_uint(ok ? y : __int_as_float(0x7fc00000));
-        }
-    }
-    __syncthreads();
-
-    // 3. learned pairs from their guesses, per warp.  A warp without learned pairs walks the
-    // rotation offsets instead (all its pairs plain; column sums by shuffle, no shared adds)
-    const bool warp_learned = __any_sync(0xffffffffu, (mh | me) != 0u);
-    double cacc[6];
-    if (!warp_learned) {
-        const unsigned full = 0xffffffffu;
-#pragma unroll
-        for (int c = 0; c < 6; c++) cacc[c] = 0.0;
-        const int k0 = diag ? 1 : 0, k1 = diag ? 16 : 31;
-        for (int k = k0; k <= k1; k++) {
-            const int src = (lane + k) & 31;
-            double h[6] = {0, 0, 0, 0, 0, 0};
-            if ((mr >> k) & 1u) {
-                double r[3], g[3];
-#pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    r[c] = si[c] - ws[c * 32 + src];
-                    g[c] = si[3 + c] - ws[(3 + c) * 32 + src];
-                }
-                const double eps_ij = hq ? A.eps_th * si[6] * ws[6 * 32 + src] : A.eps_th;
-                const int it = uv_halfdisp(eps_ij, dt, r, g, h);
-                cnt.it_uv += it;
-                if (it > kUvItMax) cnt.nonconverged++;
-                cnt.cls[alg_classify(eps_ij, r, g) == kClsDeg ? kDegenerate : kUniversal]++;
-                count_nonfinite(h, cnt);
-            }
-            const int back = (lane - k) & 31;
-#pragma unroll
-            for (int c = 0; c < 6; c++) {
-                racc[c] += h[c];
-                cacc[c] += __shfl_sync(full, h[c], back);
-            }
-        }
-        mr = 0u;
-    } else {
-        int ih = oh, ie = oe;
-        unsigned m = mh | me;
-        for (;;) {
-            const bool busy = (m != 0u);
-            const unsigned bm = __ballot_sync(0xffffffffu, busy);
-            if (bm == 0u) break;
-            if (busy) {
-                const int k = __ffs(m) - 1;
-                m &= m - 1u;
-                const bool is_h = (mh >> k) & 1u;
-                const float y = __uint_as_float(rows[is_h ? ih++ : ie++]);
-                const int j = (lane + k) & 31;
-                double r[3], g[3], h[6];
-#pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    r[c] = si[c] - ws[c * 32 + j];
-                    g[c] = si[3 + c] - ws[(3 + c) * 32 + j];
-                }
-                const double eps_ij = hq ? A.eps_th * si[6] * ws[6 * 32 + j] : A.eps_th;
-                LearnedPair L;
-                learned_prepare(eps_ij, dt, r, g, L);
-                bool coarse = true;
-                const bool done = learned_finish(L, dt, y, r, g, h, coarse);
-                cnt.learned++;
-                if (coarse) cnt.learned_coarse++;
-                if (!done) {
-                    cnt.learned_fallbacks++;
-                    const int it = uv_halfdisp(eps_ij, dt, r, g, h);
-                    cnt.it_uv += it;
-                    if (it > kUvItMax) cnt.nonconverged++;
-                }
-                cnt.cls[is_h ? kHyperbola : kEllipse]++;
-                count_nonfinite(h, cnt);
-#pragma unroll
-                for (int c = 0; c < 6; c++) racc[c] += h[c];
-                add_column(wacc, j, h, bm, lane);
-            }
-        }
-    }
-    if (timed_out && threadIdx.x == 0) cnt.timeouts++;
-    // plain pairs: the universal-variable solver, per warp (mr is empty on rotation warps)
-    for (;;) {
-        const bool busy = (mr != 0u);
-        const unsigned bm = __ballot_sync(0xffffffffu, busy);
-        if (bm == 0u) break;
-        if (busy) {
-            const int k = __ffs(mr) - 1;
-            mr &= mr - 1u;
-            const int j = (lane + k) & 31;
-            double r[3], g[3], h[6];
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                r[c] = si[c] - ws[c * 32 + j];
-                g[c] = si[3 + c] - ws[(3 + c) * 32 + j];
-            }
-            const double eps_ij = hq ? A.eps_th * si[6] * ws[6 * 32 + j] : A.eps_th;
-            const int it = uv_halfdisp(eps_ij, dt, r, g, h);
-            cnt.it_uv += it;
-            if (it > kUvItMax) cnt.nonconverged++;
-            cnt.cls[alg_classify(eps_ij, r, g) == kClsDeg ? kDegenerate : kUniversal]++;
-            count_nonfinite(h, cnt);
-#pragma unroll
-            for (int c = 0; c < 6; c++) racc[c] += h[c];
-            add_column(wacc, j, h, bm, lane);
-        }
-    }
-    if (warp_learned) {
-        __syncwarp();
-#pragma unroll
-        for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
-    }
-    mlp_teardown(S, phase);
+    const bool timed_out = learned_block_solve(M, B, bi, bj, lane, live, racc, cacc, cnt);
     if (timed_out && threadIdx.x == 0 && !live) atomicAdd(&A.stats[kStatTimeouts], 1ull);
     if (!live) return;  // warp-uniform; no barrier follows
     flush_counters(cnt, A.stats, lane);
+    const int i = bi * 32 + lane;
     const int jown = bj * 32 + lane;
     const size_t plane = (size_t)A.npad;
     if (kDeterministic) {
         write_partials(A.part, plane, bi, bj, lane, racc, cacc);
-    } else if (diag) {
+    } else if (bi == bj) {
 #pragma unroll
         for (int c = 0; c < 6; c++)
             if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c] - cacc[c]);
@@ -621,7 +407,7 @@ int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
         U.nparts = nb;
         record_event(ctx);
         if (learned) st = launch_pair_learned<true>(A, ctx->stream);
-        else launch_pair_tiles<true>(A, grid, ctx->stream);
+        else launch_pair_tiles<true>(A, grid, ctx->stream, ctx->alg_tuned[1][ilog2_bucket(n)]);
         record_event(ctx);
     } else {
         A.part = (double *)ctx->acc.ptr;
@@ -630,7 +416,7 @@ int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
         cudaMemsetAsync(A.part, 0, 6 * (size_t)A.npad * sizeof(double), ctx->stream);
         record_event(ctx);
         if (learned) st = launch_pair_learned<false>(A, ctx->stream);
-        else launch_pair_tiles<false>(A, grid, ctx->stream);
+        else launch_pair_tiles<false>(A, grid, ctx->stream, ctx->alg_tuned[0][ilog2_bucket(n)]);
         record_event(ctx);
     }
     if (st != BIA_OK) return st;
@@ -721,6 +507,8 @@ int bia_context_create(bia_context **out, int device, void *stream)
     if (e != cudaSuccess) return cuda_status(e);
     bia_context *ctx = new bia_context();
     ctx->device = device;
+    for (int d = 0; d < 2; d++)
+        for (int b = 0; b < 32; b++) ctx->alg_tuned[d][b] = -1;
     ctx->stream = (cudaStream_t)stream;
     e = cudaMallocHost((void **)&ctx->h_stats, kNumStats * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_inv, 64 * sizeof(double));
@@ -753,6 +541,76 @@ int bia_context_set_heads(bia_context *ctx, const void *blob, size_t bytes)
     if (e != cudaSuccess) return cuda_status(e);
     ctx->heads_loaded = true;
     return BIA_OK;
+}
+
+int bia_context_autotune(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y, double *z,
+                         double *u, double *v, double *w, const double *q, int *variant, float *ms)
+{
+    int st = validate(cfg, n, x, y, z, u, v, w, ctx);
+    if (!ctx) return set_last_error(BIA_ERR_INVALID_ARGUMENT);
+    if (st != BIA_OK) return set_last_error(st);
+    if (variant) *variant = -1;
+    if (ms)
+        for (int k = 0; k < kVarCount; k++) ms[k] = -1.0f;
+    if (cfg->method != BIA_METHOD_ALG) return set_last_error(BIA_OK);  // one shape only
+    cudaError_t e = cudaSetDevice(ctx->device);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (e == cudaSuccess && ctx->stream) e = cudaStreamIsCapturing(ctx->stream, &cap);
+    if (e != cudaSuccess) return set_last_error(cuda_status(e));
+    if (cap != cudaStreamCaptureStatusNone) return set_last_error(BIA_ERR_INVALID_ARGUMENT);
+    st = ensure_step_buffers(ctx, cfg, n);
+    if (st != BIA_OK) return set_last_error(st);
+    const int nb = num_blocks32(n);
+    StepArgs A;
+    A.x = x; A.y = y; A.z = z; A.u = u; A.v = v; A.w = w; A.q = q;
+    A.stats = (unsigned long long *)ctx->stats.ptr;
+    A.n = n; A.nb = nb; A.npad = nb * 32;
+    A.nwb = (long long)nb * (nb + 1) / 2;
+    A.eps_th = cfg->eps_th;
+    A.P.dt = cfg->dt; A.P.err = cfg->err; A.P.relerr = cfg->rkf_relerr; A.P.abserr = cfg->rkf_abserr;
+    A.P.itr = cfg->itr; A.P.method = cfg->method;
+    A.heads = nullptr;
+    const int det = cfg->deterministic ? 1 : 0;
+    A.part = det ? (double *)ctx->part.ptr : (double *)ctx->acc.ptr;
+    const long long grid = (A.nwb + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    const int sms = phase_kernel_setup();
+    cudaEvent_t ev[2];
+    e = cudaEventCreate(&ev[0]);
+    if (e == cudaSuccess) e = cudaEventCreate(&ev[1]);
+    if (e != cudaSuccess) return set_last_error(cuda_status(e));
+    int best = -1;
+    float best_ms = 0.0f;
+    for (int var = 0; var < kVarCount && e == cudaSuccess; var++) {
+        if (var != kVarTiles8 && sms <= 0) continue;
+        float t_min = 0.0f;
+        for (int rep = 0; rep < 4 && e == cudaSuccess; rep++) {  // the first launch is a warm-up
+            if (!det) e = cudaMemsetAsync(A.part, 0, 6 * (size_t)A.npad * sizeof(double), ctx->stream);
+            if (e == cudaSuccess) e = cudaEventRecord(ev[0], ctx->stream);
+            if (det) launch_pair_tiles<true>(A, grid, ctx->stream, var);
+            else launch_pair_tiles<false>(A, grid, ctx->stream, var);
+            if (e == cudaSuccess) e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaEventRecord(ev[1], ctx->stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(ev[1]);
+            float t = 0.0f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&t, ev[0], ev[1]);
+            if (rep == 1 || (rep > 1 && t < t_min)) t_min = t;
+        }
+        if (e != cudaSuccess) break;
+        if (ms) ms[var] = t_min;
+        if (best < 0 || t_min < best_ms) {
+            best = var;
+            best_ms = t_min;
+        }
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    // the timing launches counted pairs: clear the counters
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->stats.ptr, 0, kNumStats * sizeof(unsigned long long), ctx->stream);
+    if (e == cudaSuccess) e = ctx->stream ? cudaStreamSynchronize(ctx->stream) : cudaDeviceSynchronize();
+    if (e != cudaSuccess) return set_last_error(cuda_status(e));
+    ctx->alg_tuned[det][ilog2_bucket(n)] = best;
+    if (variant) *variant = best;
+    return set_last_error(BIA_OK);
 }
 
 int bia_context_destroy(bia_context *ctx)
@@ -865,6 +723,9 @@ int bia_run(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y
     // a capturing stream needs a non-default stream; timing events are per launch, so
     // graph replay is only used with timing off
     if (use_graph && ctx->stream && !ctx->timing && nsteps > 0) {
+        // one-time kernel attribute set-up happens before the capture begins
+        if (cfg->method == BIA_METHOD_LEARNED && !learned_kernel_setup()) return BIA_ERR_CUDA;
+        if (cfg->method == BIA_METHOD_ALG) phase_kernel_setup();
         GraphKey key;
         key.n = n; key.nsteps = nsteps; key.method = cfg->method; key.itr = cfg->itr;
         key.deterministic = cfg->deterministic; key.eps = cfg->eps_th; key.dt = cfg->dt;

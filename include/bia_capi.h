@@ -95,6 +95,17 @@ typedef struct bia_context bia_context;
    the legacy default stream).  The context owns scratch buffers, grown on demand. */
 int bia_context_create(bia_context **ctx, int device, void *stream);
 int bia_context_destroy(bia_context *ctx);
+/* Autotuner: times the ALG pair-kernel shapes on this device state (the timed launches
+   write only scratch; the state is unchanged) and keeps the fastest for this reduction mode
+   and floor(log2 n) in the context, which later steps of that size then use.
+   Shapes: 0 = 8-warp CTAs, 1 = phase-locked 16-warp CTAs (2 per SM), 2 = phase-locked
+   32-warp CTAs (1 per SM).  variant (optional) receives the choice, ms (optional, 3 floats)
+   the best time of each shape (-1 when not run).  Other methods have one shape: variant = -1.
+   Synchronises the context's stream; not during stream capture.  No counterpart in the
+   reference. */
+int bia_context_autotune(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y,
+                         double *z, double *u, double *v, double *w, const double *q,
+                         int *variant, float *ms);
 /* Loads the two learned Kepler heads of BIA_METHOD_LEARNED from the bytes of
    learned_heads.bin (bia_3d_gpu_b200/train_heads.py writes it: "BIAHEAD1", version 1,
    2 heads of 19472 bytes).  No counterpart in the reference (the learned form is new). */

@@ -101,3 +101,29 @@ def test_large_ensemble_phase_locked_equals_single_steps(cuda):
             assert np.array_equal(got[:, off:off + n], t.cpu().numpy()), n
             off += n
         ens.close()
+
+
+def test_ensemble_learned_equals_single_system_steps(cuda):
+    """The learned form over the item table: each system equals its own learned step
+    (same per-block code and order, bitwise) and the oracle's plain step to 1e-12."""
+    from bia_3d_gpu_b200 import METHOD_LEARNED
+    states, eps = _systems(2)
+    whole = cuda.tensor(np.concatenate(states, axis=1), device="cuda")
+    with BIASolver() as solver:
+        solver.load_heads()
+        ens = solver.ensemble(SIZES, eps)
+        st = ens.run(whole, default_config(dt=1e-3, method=METHOD_LEARNED), 1, graph=True)
+        solver.stream.synchronize()
+        got = whole.cpu().numpy()
+        assert st["learned"] > 0 and st["nonfinite"] == 0 and st["timeouts"] == 0
+        off = 0
+        for s, e, n in zip(states, eps, SIZES):
+            t = cuda.tensor(s, device="cuda")
+            solver.step(t, default_config(eps_th=e, dt=1e-3, method=METHOD_LEARNED), stats=False)
+            solver.stream.synchronize()
+            assert np.array_equal(got[:, off:off + n], t.cpu().numpy()), n
+            r, _, _ = oracle.bia_step(s, e, 1e-3)
+            scale = max(np.abs(r[:3]).max(), 1e-300)
+            assert np.abs(got[:3, off:off + n] - r[:3]).max() <= 1e-12 * scale, n
+            off += n
+        ens.close()

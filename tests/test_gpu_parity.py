@@ -292,3 +292,24 @@ def test_phase_locked_kernel_modes_agree(cuda):
     got = da[:, sel].T
     assert np.abs(got[:, :3] - ref[:, :3]).max() <= 1e-12 * np.abs(s[:3]).max()
     assert np.abs(got[:, 3:] - ref[:, 3:]).max() <= 1e-12 * np.abs(s[3:]).max()
+
+
+def test_autotune_picks_a_shape_and_keeps_results(cuda):
+    """The autotuner times the ALG pair-kernel shapes on the state without changing it and
+    keeps the fastest; every shape computes the same per-block sums in the same order, so
+    the step is bitwise the same before and after tuning."""
+    s, eps, q = initial.coulomb_cube(8192, seed=28)
+    t = cuda.tensor(s, device="cuda")
+    qt = cuda.tensor(q, device="cuda")
+    cfg = default_config(eps_th=eps, dt=1e-5)
+    with BIASolver() as solver:
+        a = t.clone()
+        solver.step(a, cfg, q=qt)
+        var, ms = solver.autotune(t, cfg, q=qt)
+        assert cuda.equal(t, cuda.tensor(s, device="cuda"))   # state untouched
+        assert var in (0, 1, 2) and len(ms) == 3 and all(v > 0 for v in ms.values())
+        assert min(ms, key=ms.get) == ("tiles8", "phase16", "phase32")[var]
+        b = t.clone()
+        st = solver.step(b, cfg, q=qt)
+        assert st["hyperbola"] + st["ellipse"] + st["universal"] + st["parabola"] + st["degenerate"] == 8192 * 8191 // 2
+    assert cuda.equal(a, b)
