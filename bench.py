@@ -69,13 +69,15 @@ FLOPS = {
 LEARNED_TENSOR_FLOPS = 2 * (16 * 64 + 64 * 64 + 64 * 64)
 METHODS = {"rkf": 0, "alg": 1, "universal": 2, "learned": 3}
 
-# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the ALG pair
-# kernel at coulomb_cube_32768: one ncu capture of bia_pair_phase_kernel at n = 16384
-# (100.5 MB read + 3169.5 MB written, 1.342e8 pairs) scaled by the pairs per launch
-# (x 4.0001); both the partial sums and the local-memory traffic grow with the pairs.
-TRAFFIC_PAIRS_MEASURED = 16384 * 16383 // 2
-TRAFFIC_BYTES_MEASURED = 100.488e6 + 3169.538e6
-TRAFFIC_WORKLOAD = "coulomb_cube_32768"
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the dominant pair
+# kernel, from one ncu capture at n = 16384 of the same workload and method, scaled by the
+# pairs per launch (both the partial sums and any local-memory traffic grow with the pairs):
+#   (workload, method) -> (pairs in the capture, bytes in the capture)
+TRAFFIC = {
+    ("plummer_32768", 3): (16384 * 16383 // 2, 1.132e6 + 351.829e6),       # learned kernel
+    ("coulomb_cube_32768", 3): (16384 * 16383 // 2, 2.912e6 + 353.567e6),  # learned kernel
+    ("coulomb_cube_32768", 1): (16384 * 16383 // 2, 100.488e6 + 3169.538e6),  # phase-locked ALG
+}
 
 
 def pair_flops(stats, method):
@@ -518,11 +520,12 @@ def main():
     peak = measure_fp64_peak(local)
     achieved = per_launch_flops / per_launch_s / 1e12
     traffic = None
-    if args.workload == TRAFFIC_WORKLOAD and method == 1:
-        traffic = TRAFFIC_BYTES_MEASURED * pairs / TRAFFIC_PAIRS_MEASURED
+    if args.n is None and (args.workload, method) in TRAFFIC:
+        tp, tb = TRAFFIC[(args.workload, method)]
+        traffic = tb * pairs / tp
     roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak if peak else None, "traffic": traffic,
-                "traffic_note": "ncu capture of the ALG kernel at n = 16384 on coulomb_cube, "
+                "traffic_note": "ncu capture of the same kernel and workload at n = 16384, "
                                 "scaled by pairs per launch" if traffic else None,
                 "algorithmic_bytes_per_launch": nb_blocks * 6 * n * 8 + 6 * n * 8,
                 "peak_source": "measured live: bia_measure_fp64_peak DFMA loop on this GPU",
