@@ -109,6 +109,8 @@ def lib():
     L.bia_context_autotune.argtypes = ([_V, ctypes.POINTER(BiaConfig), _I] + [_V] * 7 +
                                        [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)])
     L.bia_context_autotune.restype = _I
+    L.bia_selftest_wait_timeout.argtypes = [_V]
+    L.bia_selftest_wait_timeout.restype = _I
     L.bia_context_set_heads.argtypes = [_V, ctypes.c_char_p, ctypes.c_size_t]
     L.bia_context_set_heads.restype = _I
     L.bia_learned_head_eval.argtypes = [_V, _I, _I, _V, _V]
@@ -160,4 +162,5 @@ EXPORTED_SYMBOLS = ("bia_config_default", "bia_context_create", "bia_context_des
                     "bia_ensemble_create", "bia_ensemble_destroy", "bia_ensemble_particles",
                     "bia_ensemble_run", "bia_ensemble_energy",
                     "bia_context_set_heads", "bia_learned_head_eval", "bia_context_autotune",
+                    "bia_selftest_wait_timeout",
                     "bia_last_error", "find_dxyuv_kernel_", "invariance_gpu_")

@@ -209,7 +209,7 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
                 const int it = uv_halfdisp(eps_ij, dt, r, g, h);
                 cnt.it_uv += it;
                 if (it > kUvItMax) cnt.nonconverged++;
-                cnt.cls[alg_classify(eps_ij, r, g) == kClsDeg ? kDegenerate : kUniversal]++;
+                cnt.cls[pair_degenerate(r, g) ? kDegenerate : kUniversal]++;
                 count_nonfinite(h, cnt);
             }
             const int back = (lane - k) & 31;
@@ -280,7 +280,7 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
             const int it = uv_halfdisp(eps_ij, dt, r, g, h);
             cnt.it_uv += it;
             if (it > kUvItMax) cnt.nonconverged++;
-            cnt.cls[alg_classify(eps_ij, r, g) == kClsDeg ? kDegenerate : kUniversal]++;
+            cnt.cls[pair_degenerate(r, g) ? kDegenerate : kUniversal]++;
             count_nonfinite(h, cnt);
 #pragma unroll
             for (int c = 0; c < 6; c++) racc[c] += h[c];

@@ -903,6 +903,17 @@ __device__ __forceinline__ int alg_classify(double eps_ij, const double r[3], co
     return alg_classify(eps_ij, r, g, E, Lsq);
 }
 
+// |g| == 0 or |L| == 0: the pair's frame is degenerate (counted apart from the other
+// universal-variable pairs)
+__device__ __forceinline__ bool pair_degenerate(const double r[3], const double g[3])
+{
+    const double gsq = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+    const double L0 = r[1] * g[2] - r[2] * g[1];
+    const double L1 = r[2] * g[0] - r[0] * g[2];
+    const double L2 = r[0] * g[1] - r[1] * g[0];
+    return gsq == 0.0 || (L0 * L0 + L1 * L1 + L2 * L2) == 0.0;
+}
+
 // M: the compiled method (kMethodRkf, kMethodAlg, kMethodUniversal); each kernel is
 // instantiated per method so it carries only that method's code and registers.
 constexpr int kMethodRkf = 0, kMethodAlg = 1, kMethodUniversal = 2, kMethodLearned = 3;

@@ -943,3 +943,48 @@ int bia_learned_head_eval(bia_context *ctx, int head, int n, const float *in, fl
     if (e != cudaSuccess) return set_last_error(cuda_status(e));
     return set_last_error(h ? BIA_ERR_DEVICE_TIMEOUT : BIA_OK);
 }
+
+// ---------------------------------------------------------------------------------------
+// Self-test of the bounded-wait path: one thread waits on an mbarrier that nothing
+// arrives at, with the same bounded try_wait loop the tensor-core pipeline uses (a short
+// limit here), and records that the wait gave up.  No fault, trap or endless loop.
+namespace bia {
+__global__ void bia_wait_selftest_kernel(int limit, int *gave_up)
+{
+    __shared__ alignas(8) uint64_t mbar;
+    if (threadIdx.x != 0) return;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&mbar)) : "memory");
+    const uint32_t a = smem_addr(&mbar);
+    int done = 0;
+    for (int it = 0; it < limit && !done; it++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(a), "r"(0u)
+            : "memory");
+        done = (int)ok;
+    }
+    *gave_up = done ? 0 : 1;
+}
+}  // namespace bia
+
+int bia_selftest_wait_timeout(bia_context *ctx)
+{
+    if (!ctx) return set_last_error(BIA_ERR_INVALID_ARGUMENT);
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e == cudaSuccess) e = ctx->stats.reserve(kNumStats * sizeof(unsigned long long));
+    int *flag = (int *)((unsigned long long *)ctx->stats.ptr + kStatTimeouts);
+    if (e == cudaSuccess) e = cudaMemsetAsync(flag, 0, sizeof(int), ctx->stream);
+    if (e != cudaSuccess) return set_last_error(cuda_status(e));
+    bia_wait_selftest_kernel<<<1, 32, 0, ctx->stream>>>(1 << 14, flag);
+    int h = 0;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = ctx->stream ? cudaStreamSynchronize(ctx->stream) : cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->stats.ptr, 0, kNumStats * sizeof(unsigned long long), ctx->stream);
+    if (e == cudaSuccess) e = ctx->stream ? cudaStreamSynchronize(ctx->stream) : cudaDeviceSynchronize();
+    if (e != cudaSuccess) return set_last_error(cuda_status(e));
+    return set_last_error(h ? BIA_ERR_DEVICE_TIMEOUT : BIA_OK);
+}

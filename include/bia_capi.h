@@ -106,6 +106,10 @@ int bia_context_destroy(bia_context *ctx);
 int bia_context_autotune(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y,
                          double *z, double *u, double *v, double *w, const double *q,
                          int *variant, float *ms);
+/* Self-test of the device-side bounded waits: a kernel waits on an mbarrier that nothing
+   completes, gives up after its limit and reports it; returns BIA_ERR_DEVICE_TIMEOUT (the
+   expected answer) and leaves the context usable.  No counterpart in the reference. */
+int bia_selftest_wait_timeout(bia_context *ctx);
 /* Loads the two learned Kepler heads of BIA_METHOD_LEARNED from the bytes of
    learned_heads.bin (bia_3d_gpu_b200/train_heads.py writes it: "BIAHEAD1", version 1,
    2 heads of 19472 bytes).  No counterpart in the reference (the learned form is new). */

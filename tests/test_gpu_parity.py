@@ -313,3 +313,19 @@ def test_autotune_picks_a_shape_and_keeps_results(cuda):
         st = solver.step(b, cfg, q=qt)
         assert st["hyperbola"] + st["ellipse"] + st["universal"] + st["parabola"] + st["degenerate"] == 8192 * 8191 // 2
     assert cuda.equal(a, b)
+
+
+def test_bounded_device_wait_reports_timeout(cuda):
+    """A device-side wait that nothing completes gives up after its limit and the step API
+    reports BIA_ERR_DEVICE_TIMEOUT; the context then runs a normal step."""
+    import ctypes
+    from bia_3d_gpu_b200 import capi
+    s, eps = initial.gravity_ball(64, seed=29)
+    with BIASolver() as solver:
+        st = capi.lib().bia_selftest_wait_timeout(solver._ctx)
+        assert st == capi.BIA_ERR_DEVICE_TIMEOUT
+        t = cuda.tensor(s, device="cuda")
+        stats = solver.step(t, default_config(eps_th=eps, dt=1e-4))
+        assert stats["nonfinite"] == 0 and stats["timeouts"] == 0
+    r, _, _ = oracle.bia_step(s, eps, 1e-4)
+    assert_parity(t.cpu().numpy(), r)
