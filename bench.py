@@ -472,6 +472,9 @@ def main():
         cfg_alg = default_config(eps_th=eps, dt=dt, method=1)
         var, tms = solver.autotune(d_state, cfg_alg, q=d_q)
         tuned = {"alg_shape": ("tiles8", "phase16", "phase32")[var], "ms": tms}
+    if method == 3:
+        lvar, lms = solver.autotune(d_state, cfg, q=d_q)
+        tuned = dict(tuned or {}, learned_layout=("one_kernel", "split")[lvar], learned_ms=lms)
     total_ms, clocks, stats, (kern_ms, kern_launches) = timed_steps(cfg, steps, sample_clocks=True)
     value = world * steps * pairs / (total_ms * 1e-3)
 

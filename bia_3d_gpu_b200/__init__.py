@@ -285,7 +285,8 @@ class BIASolver:
                                              self._qptr(q, n), ctypes.byref(var), ms)
         self._leave(cur)
         capi.check(st, "bia_context_autotune")
-        names = ("tiles8", "phase16", "phase32")
+        names = (("one_kernel", "split", "-") if cfg.method == capi.METHOD_LEARNED
+                 else ("tiles8", "phase16", "phase32"))
         return var.value, {names[k]: float(ms[k]) for k in range(3) if ms[k] >= 0}
 
     def load_heads(self, path=None):

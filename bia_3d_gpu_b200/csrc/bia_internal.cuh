@@ -74,9 +74,12 @@ struct bia_context {
     int ev_cap = 0, ev_used = 0;
     // autotuned ALG pair-kernel shape per reduction mode and floor(log2 n); -1: default rule
     int alg_tuned[2][32];
+    // autotuned learned-step layout (0 one kernel, 1 split), same indexing; -1: default rule
+    int learned_tuned[2][32];
     // learned heads (BIA_METHOD_LEARNED), 2 records of learned_heads.bin
     bia::DeviceBuffer heads;
     bool heads_loaded = false;
+    bia::DeviceBuffer lmask;    // learned-pair masks of a split learned step
     // graph cache
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;

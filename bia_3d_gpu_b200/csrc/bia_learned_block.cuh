@@ -91,9 +91,12 @@ __device__ __forceinline__ LearnedSmem learned_smem(uint8_t *raw)
 // Every thread of the CTA calls it (warps without a block pass live = false).  Returns the
 // row sums racc (particle 32 bi + lane), the column sums cacc (particle 32 bj + lane; the
 // caller writes -cacc) and the counters; true when the tensor-core pipeline timed out.
+// lmask (split mode, may be null): receives this lane's learned-pair mask (bit k: column
+// (lane + k) mod 32) and the plain pairs are left to bia_pair_rest_kernel; without it the
+// plain pairs are solved here too.
 __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const LearnedBlockIn &B, int bi, int bj,
                                                     int lane, bool live, double racc[6], double cacc[6],
-                                                    PairCounters &cnt)
+                                                    PairCounters &cnt, uint32_t *lmask = nullptr)
 {
     MlpSmem &S = *M.mlp;
     const int warp = threadIdx.x >> 5;
@@ -189,7 +192,11 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
 
     // 3. learned pairs from their guesses, per warp.  A warp without learned pairs walks the
     // rotation offsets instead (all its pairs plain; column sums by shuffle, no shared adds)
-    const bool warp_learned = __any_sync(0xffffffffu, (mh | me) != 0u);
+    if (lmask) {
+        if (live) *lmask = mh | me;
+        mr = 0u;  // the plain pairs go to the rest kernel
+    }
+    const bool warp_learned = lmask != nullptr || __any_sync(0xffffffffu, (mh | me) != 0u);
     if (!warp_learned) {
         const unsigned full = 0xffffffffu;
 #pragma unroll

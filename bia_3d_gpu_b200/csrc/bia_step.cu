@@ -50,6 +50,7 @@ struct StepArgs {
     double eps_th;
     PairParams P;
     const MlpHead *heads;  // BIA_METHOD_LEARNED
+    uint32_t *lmask;       // learned-pair masks (split learned step), nwb * 32 words
 };
 
 template <bool kDeterministic, int M>
@@ -210,6 +211,8 @@ static void launch_pair_tiles(const StepArgs &A, long long grid, cudaStream_t st
 }
 
 // Learned mixed-precision step kernel (BIA_METHOD_LEARNED): see bia_learned_block.cuh.
+// With A.lmask set (split mode) it solves only the learned pairs, records the learned-pair
+// mask of every lane, and bia_pair_rest_kernel adds the plain pairs afterwards.
 template <bool kDeterministic>
 __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const StepArgs A)
 {
@@ -224,7 +227,8 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const 
     const LearnedBlockIn B = {A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P.dt, A.heads};
     double racc[6], cacc[6];
     PairCounters cnt;
-    const bool timed_out = learned_block_solve(M, B, bi, bj, lane, live, racc, cacc, cnt);
+    uint32_t *lm = A.lmask ? A.lmask + (size_t)(live ? t : 0) * 32 + lane : nullptr;
+    const bool timed_out = learned_block_solve(M, B, bi, bj, lane, live, racc, cacc, cnt, lm);
     if (timed_out && threadIdx.x == 0 && !live) atomicAdd(&A.stats[kStatTimeouts], 1ull);
     if (!live) return;  // warp-uniform; no barrier follows
     flush_counters(cnt, A.stats, lane);
@@ -234,6 +238,86 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const 
     if (kDeterministic) {
         write_partials(A.part, plane, bi, bj, lane, racc, cacc);
     } else if (bi == bj) {
+#pragma unroll
+        for (int c = 0; c < 6; c++)
+            if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c] - cacc[c]);
+    } else {
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c]);
+            if (jown < A.n) atomicAdd(&A.part[c * plane + jown], -cacc[c]);
+        }
+    }
+}
+
+// The plain pairs of a split learned step: every pair whose bit is clear in the lane's
+// learned mask, by the universal-variable solver, lanes walking the rotation offsets, the
+// sums added onto the learned kernel's partials (each slot is written by one warp-block of
+// each kernel, in this fixed order: deterministic).
+template <bool kDeterministic>
+__global__ void __launch_bounds__(kThreads, TileOccupancy<kMethodUniversal>::kMinBlocks)
+    bia_pair_rest_kernel(const StepArgs A)
+{
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const long long t = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    if (t >= A.nwb) return;  // warp-uniform
+    int bi, bj;
+    warp_block_coords(t, bi, bj);
+    const int i = bi * 32 + lane;
+    const int jown = bj * 32 + lane;
+    const bool diag = (bi == bj);
+    const uint32_t learned = A.lmask[(size_t)t * 32 + lane];
+    double si[7], sj[7], racc[6], cacc[6];
+    load_particle(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, i, si);
+    load_particle(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, jown, sj);
+#pragma unroll
+    for (int c = 0; c < 6; c++) racc[c] = cacc[c] = 0.0;
+    PairCounters cnt;
+    counters_zero(cnt);
+    const int k0 = diag ? 1 : 0, k1 = diag ? 16 : 31;
+    for (int k = k0; k <= k1; k++) {
+        const int src = (lane + k) & 31;
+        double sc[7];
+#pragma unroll
+        for (int c = 0; c < 7; c++) sc[c] = __shfl_sync(full, sj[c], src);
+        const int j = bj * 32 + src;
+        const bool active = (!diag || k < 16 || lane < 16) && i < A.n && j < A.n && !((learned >> k) & 1u);
+        double h[6] = {0, 0, 0, 0, 0, 0};
+        if (active) {
+            const double r[3] = {si[0] - sc[0], si[1] - sc[1], si[2] - sc[2]};
+            const double g[3] = {si[3] - sc[3], si[4] - sc[4], si[5] - sc[5]};
+            const double eps_ij = A.q ? A.eps_th * si[6] * sc[6] : A.eps_th;
+            const int it = uv_halfdisp(eps_ij, A.P.dt, r, g, h);
+            cnt.it_uv += it;
+            if (it > kUvItMax) cnt.nonconverged++;
+            cnt.cls[pair_degenerate(r, g) ? kDegenerate : kUniversal]++;
+            count_nonfinite(h, cnt);
+        }
+        const int back = (lane - k) & 31;
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            racc[c] += h[c];
+            cacc[c] += __shfl_sync(full, h[c], back);
+        }
+    }
+    flush_counters(cnt, A.stats, lane);
+    const size_t plane = (size_t)A.npad;
+    if (kDeterministic) {
+        if (diag) {
+            double *dst = A.part + (size_t)bi * 6 * plane;
+#pragma unroll
+            for (int c = 0; c < 6; c++) dst[c * plane + i] += racc[c] - cacc[c];
+        } else {
+            double *drow = A.part + (size_t)bj * 6 * plane;
+            double *dcol = A.part + (size_t)bi * 6 * plane;
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                drow[c * plane + i] += racc[c];
+                dcol[c * plane + jown] -= cacc[c];
+            }
+        }
+    } else if (diag) {
 #pragma unroll
         for (int c = 0; c < 6; c++)
             if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c] - cacc[c]);
@@ -272,7 +356,20 @@ static int launch_pair_learned(const StepArgs &A, cudaStream_t st)
     if (!learned_kernel_setup()) return BIA_ERR_CUDA;
     const long long grid = (A.nwb + kLearnedWarps - 1) / kLearnedWarps;
     bia_pair_learned_kernel<kDeterministic><<<(unsigned)grid, kMlpThreads, kLearnedSmemBytes, st>>>(A);
+    if (A.lmask) {
+        const long long rgrid = (A.nwb + kWarpsPerBlock - 1) / kWarpsPerBlock;
+        bia_pair_rest_kernel<kDeterministic><<<(unsigned)rgrid, kThreads, 0, st>>>(A);
+    }
     return BIA_OK;
+}
+
+// Split learned steps (learned pairs in the learned kernel, plain pairs in the rest kernel
+// at the universal-variable kernel's occupancy) from two 32-warp CTAs per SM up, as the
+// phase-locked ALG kernel.
+static bool learned_split(long long nwb)
+{
+    const int sms = phase_kernel_setup();
+    return sms > 0 && (nwb + 31) / 32 >= 2LL * sms;
 }
 
 struct UpdateArgs {
@@ -333,6 +430,13 @@ int ensure_step_buffers(bia_context *ctx, const bia_config *cfg, int n)
     const int nb = num_blocks32(n);
     const size_t npad = (size_t)nb * 32;
     cudaError_t e;
+    if (cfg->method == BIA_METHOD_LEARNED) {
+        const long long nwb = (long long)nb * (nb + 1) / 2;
+        if (learned_split(nwb) || ctx->learned_tuned[cfg->deterministic ? 1 : 0][ilog2_bucket(n)] == 1) {
+            e = ctx->lmask.reserve((size_t)nwb * 32 * sizeof(uint32_t));
+            if (e != cudaSuccess) return cuda_status(e);
+        }
+    }
     if (cfg->deterministic) {
         e = ctx->part.reserve((size_t)nb * 6 * npad * sizeof(double));
     } else {
@@ -375,7 +479,7 @@ int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
                  double *u, double *v, double *w, const double *q, double *disp)
 {
     const int nb = num_blocks32(n);
-    StepArgs A;
+    StepArgs A{};
     A.x = x; A.y = y; A.z = z; A.u = u; A.v = v; A.w = w; A.q = q;
     A.stats = (unsigned long long *)ctx->stats.ptr;
     A.n = n;
@@ -399,6 +503,12 @@ int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
     U.dt = cfg->dt;
     A.heads = (const MlpHead *)ctx->heads.ptr;
     const bool learned = cfg->method == BIA_METHOD_LEARNED;
+    bool split = false;
+    if (learned) {
+        const int lt = ctx->learned_tuned[cfg->deterministic ? 1 : 0][ilog2_bucket(n)];
+        split = (lt >= 0) ? (lt == 1 && ctx->lmask.ptr) : learned_split(A.nwb);
+    }
+    A.lmask = split ? (uint32_t *)ctx->lmask.ptr : nullptr;
     if (learned && !ctx->heads_loaded) return BIA_ERR_INVALID_ARGUMENT;
     int st = BIA_OK;
     if (cfg->deterministic) {
@@ -508,7 +618,7 @@ int bia_context_create(bia_context **out, int device, void *stream)
     bia_context *ctx = new bia_context();
     ctx->device = device;
     for (int d = 0; d < 2; d++)
-        for (int b = 0; b < 32; b++) ctx->alg_tuned[d][b] = -1;
+        for (int b = 0; b < 32; b++) ctx->alg_tuned[d][b] = ctx->learned_tuned[d][b] = -1;
     ctx->stream = (cudaStream_t)stream;
     e = cudaMallocHost((void **)&ctx->h_stats, kNumStats * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_inv, 64 * sizeof(double));
@@ -552,7 +662,8 @@ int bia_context_autotune(bia_context *ctx, const bia_config *cfg, int n, double 
     if (variant) *variant = -1;
     if (ms)
         for (int k = 0; k < kVarCount; k++) ms[k] = -1.0f;
-    if (cfg->method != BIA_METHOD_ALG) return set_last_error(BIA_OK);  // one shape only
+    if (cfg->method != BIA_METHOD_ALG && cfg->method != BIA_METHOD_LEARNED)
+        return set_last_error(BIA_OK);  // one shape only
     cudaError_t e = cudaSetDevice(ctx->device);
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     if (e == cudaSuccess && ctx->stream) e = cudaStreamIsCapturing(ctx->stream, &cap);
@@ -561,7 +672,7 @@ int bia_context_autotune(bia_context *ctx, const bia_config *cfg, int n, double 
     st = ensure_step_buffers(ctx, cfg, n);
     if (st != BIA_OK) return set_last_error(st);
     const int nb = num_blocks32(n);
-    StepArgs A;
+    StepArgs A{};
     A.x = x; A.y = y; A.z = z; A.u = u; A.v = v; A.w = w; A.q = q;
     A.stats = (unsigned long long *)ctx->stats.ptr;
     A.n = n; A.nb = nb; A.npad = nb * 32;
@@ -569,9 +680,16 @@ int bia_context_autotune(bia_context *ctx, const bia_config *cfg, int n, double 
     A.eps_th = cfg->eps_th;
     A.P.dt = cfg->dt; A.P.err = cfg->err; A.P.relerr = cfg->rkf_relerr; A.P.abserr = cfg->rkf_abserr;
     A.P.itr = cfg->itr; A.P.method = cfg->method;
-    A.heads = nullptr;
+    A.heads = (const MlpHead *)ctx->heads.ptr;
+    A.lmask = nullptr;
     const int det = cfg->deterministic ? 1 : 0;
     A.part = det ? (double *)ctx->part.ptr : (double *)ctx->acc.ptr;
+    const bool learned = cfg->method == BIA_METHOD_LEARNED;
+    if (learned) {  // layouts: 0 one kernel, 1 split (learned pairs, then the rest kernel)
+        e = ctx->lmask.reserve((size_t)A.nwb * 32 * sizeof(uint32_t));
+        if (e != cudaSuccess) return set_last_error(cuda_status(e));
+    }
+    const int nvar = learned ? 2 : kVarCount;
     const long long grid = (A.nwb + kWarpsPerBlock - 1) / kWarpsPerBlock;
     const int sms = phase_kernel_setup();
     cudaEvent_t ev[2];
@@ -580,14 +698,22 @@ int bia_context_autotune(bia_context *ctx, const bia_config *cfg, int n, double 
     if (e != cudaSuccess) return set_last_error(cuda_status(e));
     int best = -1;
     float best_ms = 0.0f;
-    for (int var = 0; var < kVarCount && e == cudaSuccess; var++) {
-        if (var != kVarTiles8 && sms <= 0) continue;
+    for (int var = 0; var < nvar && e == cudaSuccess; var++) {
+        if (!learned && var != kVarTiles8 && sms <= 0) continue;
         float t_min = 0.0f;
         for (int rep = 0; rep < 4 && e == cudaSuccess; rep++) {  // the first launch is a warm-up
             if (!det) e = cudaMemsetAsync(A.part, 0, 6 * (size_t)A.npad * sizeof(double), ctx->stream);
             if (e == cudaSuccess) e = cudaEventRecord(ev[0], ctx->stream);
-            if (det) launch_pair_tiles<true>(A, grid, ctx->stream, var);
-            else launch_pair_tiles<false>(A, grid, ctx->stream, var);
+            int lst = BIA_OK;
+            if (learned) {
+                A.lmask = var == 1 ? (uint32_t *)ctx->lmask.ptr : nullptr;
+                lst = det ? launch_pair_learned<true>(A, ctx->stream) : launch_pair_learned<false>(A, ctx->stream);
+            } else if (det) {
+                launch_pair_tiles<true>(A, grid, ctx->stream, var);
+            } else {
+                launch_pair_tiles<false>(A, grid, ctx->stream, var);
+            }
+            if (lst != BIA_OK) e = cudaErrorUnknown;
             if (e == cudaSuccess) e = cudaGetLastError();
             if (e == cudaSuccess) e = cudaEventRecord(ev[1], ctx->stream);
             if (e == cudaSuccess) e = cudaEventSynchronize(ev[1]);
@@ -608,7 +734,8 @@ int bia_context_autotune(bia_context *ctx, const bia_config *cfg, int n, double 
     if (e == cudaSuccess) e = cudaMemsetAsync(ctx->stats.ptr, 0, kNumStats * sizeof(unsigned long long), ctx->stream);
     if (e == cudaSuccess) e = ctx->stream ? cudaStreamSynchronize(ctx->stream) : cudaDeviceSynchronize();
     if (e != cudaSuccess) return set_last_error(cuda_status(e));
-    ctx->alg_tuned[det][ilog2_bucket(n)] = best;
+    if (learned) ctx->learned_tuned[det][ilog2_bucket(n)] = best;
+    else ctx->alg_tuned[det][ilog2_bucket(n)] = best;
     if (variant) *variant = best;
     return set_last_error(BIA_OK);
 }
@@ -626,6 +753,7 @@ int bia_context_destroy(bia_context *ctx)
     ctx->part.release();
     ctx->acc.release();
     ctx->heads.release();
+    ctx->lmask.release();
     ctx->stats.release();
     ctx->state.release();
     ctx->inv.release();
@@ -861,7 +989,7 @@ extern "C" int bia_step_noalloc(const bia_config *cfg, int n, double *x, double 
     cudaError_t e = cudaMemsetAsync(counters, 0, kNumStats * sizeof(unsigned long long), s);
     if (e != cudaSuccess) return cuda_status(e);
     const int nb = (n + 31) / 32;
-    StepArgs A;
+    StepArgs A{};
     A.x = x; A.y = y; A.z = z; A.u = u; A.v = v; A.w = w; A.q = q;
     A.part = part;
     A.stats = counters;

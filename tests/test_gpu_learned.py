@@ -101,3 +101,48 @@ def test_learned_needs_heads(cuda):
     with BIASolver() as solver:
         with pytest.raises(BiaError):
             solver.step(t, default_config(eps_th=eps, dt=1e-4, method=METHOD_LEARNED))
+
+
+def test_learned_split_step_matches_oracle(cuda):
+    """At n = 6000 the learned step splits (learned pairs in the learned kernel, plain pairs
+    in the rest kernel, added onto the same partials): sampled particles against the
+    oracle's full pair sums, and momentum from the antisymmetry."""
+    s, eps, q = initial.coulomb_cube(6000, seed=36)
+    t = cuda.tensor(s, device="cuda")
+    qt = cuda.tensor(q, device="cuda")
+    d = cuda.zeros_like(t)
+    with BIASolver() as solver:
+        solver.load_heads()
+        st = solver.step(t, default_config(eps_th=eps, dt=1e-5, method=METHOD_LEARNED), q=qt, disp=d)
+    disp = d.cpu().numpy()
+    n = 6000
+    assert st["learned"] > 0.3 * n * (n - 1) // 2
+    assert sum(st[k] for k in ("hyperbola", "ellipse", "universal", "degenerate", "parabola")) == n * (n - 1) // 2
+    sel = np.random.default_rng(37).choice(n, 24, replace=False)
+    ref = oracle.particle_disp(s, eps, 1e-5, sel, q=q)
+    got = disp[:, sel].T
+    assert np.abs(got[:, :3] - ref[:, :3]).max() <= 1e-12 * np.abs(s[:3]).max()
+    assert np.abs(got[:, 3:] - ref[:, 3:]).max() <= 1e-12 * np.abs(s[3:]).max()
+    kick = disp[3:].sum(axis=1)
+    assert np.abs(kick).max() <= 1e-12 * np.abs(disp[3:]).sum(axis=1).max()
+
+
+def test_learned_autotune_layout(cuda):
+    """The autotuner times the learned step as one kernel and split, keeps the faster for
+    this size without changing the state, and the step then still matches the oracle."""
+    s, eps, q = initial.coulomb_cube(6000, seed=38)
+    t = cuda.tensor(s, device="cuda")
+    qt = cuda.tensor(q, device="cuda")
+    cfg = default_config(eps_th=eps, dt=1e-5, method=METHOD_LEARNED)
+    with BIASolver() as solver:
+        solver.load_heads()
+        var, ms = solver.autotune(t, cfg, q=qt)
+        assert var in (0, 1) and set(ms) == {"one_kernel", "split"}
+        assert cuda.equal(t, cuda.tensor(s, device="cuda"))
+        d = cuda.zeros_like(t)
+        solver.step(t, cfg, q=qt, disp=d)
+    sel = np.random.default_rng(39).choice(6000, 16, replace=False)
+    ref = oracle.particle_disp(s, eps, 1e-5, sel, q=q)
+    got = d.cpu().numpy()[:, sel].T
+    assert np.abs(got[:, :3] - ref[:, :3]).max() <= 1e-12 * np.abs(s[:3]).max()
+    assert np.abs(got[:, 3:] - ref[:, 3:]).max() <= 1e-12 * np.abs(s[3:]).max()
