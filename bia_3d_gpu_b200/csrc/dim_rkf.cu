@@ -17,6 +17,7 @@
 //  * errors set IER (10000 too many steps, 20000 zero tolerance, 30000 step underflow)
 //    and return instead of calling exit(0) (dim/rkf_kernel.cu:298-315,491-494).
 // Layout: SoA, component-major, 6 arrays of n (x, y, z, u, v, w).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -171,11 +172,12 @@ __global__ void __launch_bounds__(256) dim_esterr_kernel(int len, const double *
 }
 
 constexpr int kDimReduceBlocks = 148;
+constexpr int kDimCoopMaxBlocks = 1024;  // partials of the cooperative solver's reductions
 
 // Device buffers of one integration: 6n doubles each for yl0, yln, yh0, yhm, yhn, er, w
 // and 6 x 6n for k1..k6; plus reduction scratch and the step size.
 struct DimBuffers {
-    double *yl0, *yln, *yh0, *yhm, *yhn, *er, *w, *k, *red, *h, *scal;
+    double *yl0, *yln, *yh0, *yhm, *yhn, *er, *w, *wb, *k, *red, *h, *scal, *io;
 };
 
 struct DimRun {
@@ -316,7 +318,7 @@ static int dim_integrate(DimRun &R, double *y, double *x0, double xe, int init, 
 static size_t dim_buffer_doubles(int n)
 {
     const size_t len = (size_t)6 * n;
-    return 7 * len + 6 * len + kDimReduceBlocks + 8;
+    return 8 * len + 6 * len + kDimCoopMaxBlocks + 16;
 }
 
 static void dim_carve(double *base, int n, DimBuffers &B)
@@ -330,9 +332,327 @@ static void dim_carve(double *base, int n, DimBuffers &B)
     B.er = base + 5 * len;
     B.w = base + 6 * len;
     B.k = base + 7 * len;
-    B.red = base + 13 * len;
-    B.h = B.red + kDimReduceBlocks;
+    B.wb = base + 13 * len;
+    B.red = base + 14 * len;
+    B.h = B.red + kDimCoopMaxBlocks;
     B.scal = B.h + 1;
+    B.io = B.scal + 2;  // 6 doubles of the cooperative solver's inputs and outputs
+}
+
+
+
+// ---------------------------------------------------------------------------------------
+// The whole adaptive integration in one cooperative kernel: the same stages, arithmetic
+// and acceptance rule as dim_integrate below, with the step control on the device.  Every
+// block computes the decisions from the same grid-wide reductions (bitwise the same
+// values), so all blocks take the same path and meet at the same grid-wide barriers; the
+// loop is bounded by ITEMAX attempted steps.  Tracks are swapped, not copied.
+namespace cg = cooperative_groups;
+
+struct DimCoopArgs {
+    int n, len, init, itemax;
+    double eps, relerr, abserr, xe;
+    DimBuffers B;   // B.red holds >= gridDim.x doubles
+    double *y;      // state in (at io[0]) and out
+    double *ese;    // optional (yln - yhn) / 31 of the last step
+    double *io;     // in: [0] x0, [1] H; out: [0] x reached, [1] H, [2] nde, [3] accepted,
+                    // [4] rejected, [5] ier
+};
+
+// Fused stage of the cooperative solver: k_s = (v, a)(win) for the block's particles
+// (16 particles x 16 j-chunks per block, chunk sums added in order), and right away, by the
+// thread that owns particle i, the next stage's input for particle i: w = y0 + h sum_m
+// c_fehl[s][m] k_m (s < 5), or yn (row 5) and er (row 6) after the last stage.  The
+// combination is per particle, so only the next stage needs a grid-wide barrier.
+#ifndef BIA_DIM_COOP_PARTICLES
+#define BIA_DIM_COOP_PARTICLES 8
+#endif
+constexpr int kCoopParticles = BIA_DIM_COOP_PARTICLES, kCoopChunks = 256 / BIA_DIM_COOP_PARTICLES;
+
+__device__ void coop_stage(const DimCoopArgs &A, int s, double h, const double *__restrict__ y0,
+                           const double *__restrict__ win, double *__restrict__ wout, double *__restrict__ yn,
+                           bool want_er, double (*part)[3][kCoopParticles])
+{
+    const int n = A.n;
+    const size_t len = (size_t)A.len;
+    const int lane = threadIdx.x % kCoopParticles;
+    const int chunk = threadIdx.x / kCoopParticles;
+    const int ngroups = (n + kCoopParticles - 1) / kCoopParticles;
+    const double *X = win, *Y = win + n, *Z = win + 2 * (size_t)n;
+    double *k = A.B.k;
+    for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+        const int i = grp * kCoopParticles + lane;
+        double ax = 0.0, ay = 0.0, az = 0.0;
+        if (i < n) {
+            const double xi = X[i], yi = Y[i], zi = Z[i];
+            const int per = (n + kCoopChunks - 1) / kCoopChunks;
+            const int j0 = chunk * per;
+            const int j1 = min(n, j0 + per);
+            for (int j = j0; j < j1; j++) {
+                const double xij = xi - X[j], yij = yi - Y[j], zij = zi - Z[j];
+                const double rsq = xij * xij + yij * yij + zij * zij + 1e-99;
+                const double eee = A.eps / (rsq * sqrt(rsq));
+                ax += xij * eee;
+                ay += yij * eee;
+                az += zij * eee;
+            }
+        }
+        part[chunk][0][lane] = ax;
+        part[chunk][1][lane] = ay;
+        part[chunk][2][lane] = az;
+        __syncthreads();
+        if (chunk == 0 && i < n) {
+            double a3[3] = {0.0, 0.0, 0.0};
+            for (int c = 0; c < kCoopChunks; c++)
+                for (int d = 0; d < 3; d++) a3[d] += part[c][d][lane];
+            double *ks = k + (size_t)s * len;
+            for (int c = 0; c < 3; c++) {
+                ks[(size_t)c * n + i] = win[(size_t)(3 + c) * n + i];
+                ks[(size_t)(3 + c) * n + i] = a3[c];
+            }
+            for (int c = 0; c < 6; c++) {
+                const size_t e = (size_t)c * n + i;
+                if (s < 5) {
+                    double acc;
+                    if (s == 0) {
+                        acc = h * c_fehl[0][0] * k[e];
+                    } else {
+                        acc = 0.0;
+                        for (int m = 0; m <= s; m++) acc += c_fehl[s][m] * k[(size_t)m * len + e];
+                        acc = h * acc;
+                    }
+                    wout[e] = y0[e] + acc;
+                } else {
+                    double acc = 0.0;
+                    for (int m = 0; m < 6; m++) acc += c_fehl[5][m] * k[(size_t)m * len + e];
+                    yn[e] = y0[e] + h * acc;
+                    if (want_er) {
+                        double ae = 0.0;
+                        for (int m = 0; m < 6; m++) ae += c_fehl[6][m] * k[(size_t)m * len + e];
+                        A.B.er[e] = h * ae;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// One Fehlberg step of size h: six fused stages, one grid-wide barrier after each.
+__device__ void coop_fehl(const DimCoopArgs &A, cg::grid_group &grid, double h, const double *y0, double *yn,
+                          bool want_er, double (*part)[3][kCoopParticles])
+{
+    // stage inputs alternate between two scratch vectors so a stage never overwrites the
+    // input other blocks are still reading: w_a for even stages' output, w_b for odd
+    double *wa = A.B.w, *wb = A.B.wb;
+    const double *win = y0;
+    for (int st = 0; st < 6; st++) {
+        double *wout = (st % 2 == 0) ? wa : wb;
+        coop_stage(A, st, h, y0, win, wout, yn, want_er, part);
+        grid.sync();
+        win = wout;
+    }
+}
+
+// grid-wide max of |er| / et (negative when an et is zero), the same on every block
+__device__ double coop_errnorm(const DimCoopArgs &A, cg::grid_group &grid, const double *yl0, const double *yln,
+                               double *sh)
+{
+    double m = 0.0;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < A.len; e += gridDim.x * blockDim.x) {
+        const double et = A.relerr * (fabs(yl0[e]) + fabs(yln[e])) / 2 + A.abserr;
+        if (et == 0.0) m = -1.0e300;
+        else if (m >= 0.0) m = fmax(m, fabs(A.B.er[e]) / et);
+    }
+    sh[threadIdx.x] = m;
+    __syncthreads();
+    for (int s2 = 128; s2 > 0; s2 >>= 1) {
+        if (threadIdx.x < s2) {
+            const double a = sh[threadIdx.x], b = sh[threadIdx.x + s2];
+            sh[threadIdx.x] = (a < 0.0 || b < 0.0) ? -1.0e300 : fmax(a, b);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) A.B.red[blockIdx.x] = sh[0];
+    grid.sync();
+    __shared__ double total;
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int b = 0; b < (int)gridDim.x; b++) {
+            const double v = A.B.red[b];
+            t = (t < 0.0 || v < 0.0) ? -1.0e300 : fmax(t, v);
+        }
+        total = t;
+    }
+    __syncthreads();
+    const double r = total;
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(256) dim_coop_kernel(const DimCoopArgs A)
+{
+    cg::grid_group grid = cg::this_grid();
+    __shared__ double part[kCoopChunks][3][kCoopParticles];
+    __shared__ double sh[256];
+    __shared__ double total;
+    const double EPSMIN = 1e-15;
+    const int len = A.len;
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x, gsz = gridDim.x * blockDim.x;
+    double *yl0 = A.B.yl0, *yln = A.B.yln, *yh0 = A.B.yh0, *yhn = A.B.yhn;
+    for (int e = gid; e < len; e += gsz) {
+        yh0[e] = A.y[e];
+        yl0[e] = A.y[e];
+    }
+    double X = A.io[0], H = A.io[1];
+    int nde = 0;
+    grid.sync();
+    if (A.init == 1) {
+        coop_stage(A, 0, 0.0, yl0, yl0, A.B.wb, nullptr, false, part);  // k1 only (w unused)
+        grid.sync();
+        double m = INFINITY;
+        for (int e = gid; e < len; e += gsz)
+            if (fabs(A.B.k[e]) > 0.0) m = fmin(m, fabs((A.relerr * fabs(yl0[e]) + A.abserr) / A.B.k[e]));
+        sh[threadIdx.x] = m;
+        __syncthreads();
+        for (int s2 = 128; s2 > 0; s2 >>= 1) {
+            if (threadIdx.x < s2) sh[threadIdx.x] = fmin(sh[threadIdx.x], sh[threadIdx.x + s2]);
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) A.B.red[blockIdx.x] = sh[0];
+        grid.sync();
+        if (threadIdx.x == 0) {
+            double t = INFINITY;
+            for (int b = 0; b < (int)gridDim.x; b++) t = fmin(t, A.B.red[b]);
+            total = t;
+        }
+        __syncthreads();
+        const double toldy = total;
+        H = isinf(toldy) ? EPSMIN * (A.xe - X) : fmin((A.xe - X) / 100e0, pow(toldy, 0.2));
+        nde = 1;
+        grid.sync();  // the reduction scratch is reused below
+    }
+    long long acc = 0, rej = 0;
+    int ier = 10000;
+    for (int iter = 0; iter < A.itemax; iter++) {
+        coop_fehl(A, grid, H, yl0, yln, true, part);
+        nde += 6;
+        const double erret = coop_errnorm(A, grid, yl0, yln, sh);
+        if (erret < 0.0) {
+            ier = 20000;
+            break;
+        }
+        if (erret > 1) {
+            rej++;
+            if (erret >= 59049) H *= 0.1;
+            else H *= 0.9 / pow(erret, 0.2);
+            if (H <= EPSMIN) {
+                ier = 30000;
+                break;
+            }
+        } else if (X + H < A.xe) {
+            coop_fehl(A, grid, H / 2, yh0, A.B.yhm, false, part);
+            coop_fehl(A, grid, H / 2, A.B.yhm, yhn, false, part);
+            nde += 12;
+            X += H;
+            double *t1 = yl0; yl0 = yln; yln = t1;  // accepted: the new tracks become the old ones
+            double *t2 = yh0; yh0 = yhn; yhn = t2;
+            acc++;
+            if (erret <= 1.889568e-4) H *= 5.0;
+            else H *= 0.9 / pow(erret, 0.2);
+        } else {
+            H = A.xe - X;
+            coop_fehl(A, grid, H, yl0, yln, true, part);
+            coop_fehl(A, grid, H / 2, yh0, A.B.yhm, false, part);
+            coop_fehl(A, grid, H / 2, A.B.yhm, yhn, false, part);
+            nde += 18;
+            X = A.xe;
+            acc++;
+            ier = 0;
+            break;
+        }
+    }
+    // outputs: the state (the high track at xe, or the last accepted one), the low track
+    // in B.yl0, (yln - yhn) / 31
+    const double *yout = (ier == 0) ? yhn : yh0;
+    const double *lout = (ier == 0) ? yln : yl0;
+    for (int e = gid; e < len; e += gsz) {
+        if (A.ese && ier == 0) A.ese[e] = (yln[e] - yhn[e]) / 31;
+        A.y[e] = yout[e];
+    }
+    grid.sync();
+    if (lout != A.B.yl0)
+        for (int e = gid; e < len; e += gsz) A.B.yl0[e] = lout[e];
+    if (gid == 0) {
+        A.io[0] = X;
+        A.io[1] = H;
+        A.io[2] = nde;
+        A.io[3] = (double)acc;
+        A.io[4] = (double)rej;
+        A.io[5] = ier;
+    }
+}
+
+// The cooperative solver (dim_coop_kernel); *ran = false when the device cannot run it
+// (no cooperative launch), and the caller takes the host-controlled loop instead.
+static int dim_integrate_coop(DimRun &R, double *y, double *x0, double xe, int init, double *H, int *nde,
+                              long long *accepted, long long *rejected, double *ese, int *status, bool *ran)
+{
+    *ran = false;
+    *status = BIA_OK;
+    const char *force_host = getenv("BIA_DIM_HOST_CONTROL");
+    if (force_host && force_host[0] == '1') return 0;
+    int dev = 0, coop = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dim_coop_kernel, 256, 0) != cudaSuccess ||
+        per_sm < 1) {
+        cudaGetLastError();
+        return 0;
+    }
+    const int ngroups = (R.n + kCoopParticles - 1) / kCoopParticles;
+    int G = ngroups;
+    if (G > sms * per_sm) G = sms * per_sm;
+    if (G > kDimCoopMaxBlocks) G = kDimCoopMaxBlocks;  // B.red holds kDimCoopMaxBlocks partials
+    const char *gcap = getenv("BIA_DIM_COOP_BLOCKS");
+    if (gcap && atoi(gcap) > 0 && atoi(gcap) < G) G = atoi(gcap);
+    if (G < 1) G = 1;
+    DimCoopArgs A;
+    A.n = R.n;
+    A.len = R.len;
+    A.init = init;
+    A.itemax = 10000;
+    A.eps = R.eps;
+    A.relerr = R.relerr;
+    A.abserr = R.abserr;
+    A.xe = xe;
+    A.B = R.B;
+    A.y = y;
+    A.ese = ese;
+    A.io = R.B.io;
+    R.h_pinned[0] = *x0;
+    R.h_pinned[1] = *H;
+    cudaError_t e = cudaMemcpyAsync(R.B.io, R.h_pinned, 2 * sizeof(double), cudaMemcpyHostToDevice, R.st);
+    void *args[] = {(void *)&A};
+    if (e == cudaSuccess)
+        e = cudaLaunchCooperativeKernel((const void *)dim_coop_kernel, dim3(G), dim3(256), args, 0, R.st);
+    double out[6] = {0, 0, 0, 0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(R.h_pinned, R.B.io, 6 * sizeof(double), cudaMemcpyDeviceToHost, R.st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(R.st);
+    if (e != cudaSuccess) {
+        *status = cuda_status(e);
+        *ran = true;
+        return 0;
+    }
+    for (int k = 0; k < 6; k++) out[k] = R.h_pinned[k];
+    *x0 = out[0];
+    *H = out[1];
+    *nde = (int)out[2];
+    *accepted += (long long)out[3];
+    *rejected += (long long)out[4];
+    *ran = true;
+    return (int)out[5];
 }
 
 struct DimDropIn {
@@ -354,7 +674,7 @@ extern "C" int bia_dim_integrate(bia_context *ctx, int n, double eps_th, double 
     cudaError_t e = ctx->dim.reserve(dim_buffer_doubles(n) * sizeof(double));
     if (e != cudaSuccess) return cuda_status(e);
     if (!ctx->h_dim) {
-        e = cudaMallocHost((void **)&ctx->h_dim, 4 * sizeof(double));
+        e = cudaMallocHost((void **)&ctx->h_dim, 8 * sizeof(double));
         if (e != cudaSuccess) return cuda_status(e);
     }
     DimRun R;
@@ -369,7 +689,9 @@ extern "C" int bia_dim_integrate(bia_context *ctx, int n, double eps_th, double 
     double X = x0, H = 0.0;
     int nde = 0, status = BIA_OK;
     long long acc = 0, rej = 0;
-    const int ier = dim_integrate(R, y, &X, xe, 1, &H, &nde, &acc, &rej, nullptr, &status);
+    bool ran = false;
+    int ier = dim_integrate_coop(R, y, &X, xe, 1, &H, &nde, &acc, &rej, nullptr, &status, &ran);
+    if (!ran) ier = dim_integrate(R, y, &X, xe, 1, &H, &nde, &acc, &rej, nullptr, &status);
     if (stats) {
         stats->accepted = acc;
         stats->rejected = rej;
@@ -399,7 +721,7 @@ extern "C" void rkf_c_(const int neq, const double eps_th, double *X0, double *X
     DimDropIn &S = g_dim;
     cudaError_t e = cudaSuccess;
     if (!S.ready) {
-        e = cudaMallocHost((void **)&S.h_pinned, 4 * sizeof(double));
+        e = cudaMallocHost((void **)&S.h_pinned, 8 * sizeof(double));
         if (e != cudaSuccess) {
             set_last_error(cuda_status(e));
             return;
@@ -439,7 +761,9 @@ extern "C" void rkf_c_(const int neq, const double eps_th, double *X0, double *X
     int nde = 0, status = BIA_OK;
     long long acc = 0, rej = 0;
     const int init = *INIT;
-    const int ier = dim_integrate(R, dy, X0, *XE, init, H, &nde, &acc, &rej, dese, &status);
+    bool ran = false;
+    int ier = dim_integrate_coop(R, dy, X0, *XE, init, H, &nde, &acc, &rej, dese, &status, &ran);
+    if (!ran) ier = dim_integrate(R, dy, X0, *XE, init, H, &nde, &acc, &rej, dese, &status);
     if (init == 1) *INIT = 2;
     *NDE = nde;
     *IER = ier;
