@@ -508,8 +508,10 @@ def main():
     nb_blocks = (n + 31) // 32
     nwb = nb_blocks * (nb_blocks + 1) // 2
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    split = bool(tuned and tuned.get("learned_layout") == "split")
     if method == 3:
-        kernel_name = "bia_pair_learned_kernel<true>"
+        kernel_name = ("bia_pair_learned_kernel<true> + bia_pair_rest_kernel<true> (one timed interval)"
+                       if split else "bia_pair_learned_kernel<true>")
     elif method == 1 and tuned is not None:
         kernel_name = {"tiles8": "bia_pair_tiles_kernel<true, 1>", "phase16": "bia_pair_phase_kernel<true, 16, 2>",
                        "phase32": "bia_pair_phase_kernel<true, 32, 1>"}[tuned["alg_shape"]]
@@ -654,7 +656,7 @@ def main():
                                 "device copy; the e2e loop copies it into the host buffer)",
                        "parallelism": f"replicas x{world}", "autotuned": tuned},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-            "gpu_launches": 2 * steps, "plain_fp64": plain, "universal": universal,
+            "gpu_launches": (3 if split else 2) * steps, "plain_fp64": plain, "universal": universal,
             "reference_gpu_kernel": ref_gpu,
             "learned_pair_fraction": stats["learned"] / max(1, steps * pairs) if method == 3 else None,
             "stats": {k: v for k, v in stats.items()},

@@ -118,3 +118,24 @@ def test_context_without_device_reports_no_device():
     ctx = ctypes.c_void_p()
     st = capi.lib().bia_context_create(ctypes.byref(ctx), 0, None)
     assert st == capi.BIA_ERR_NO_DEVICE and not ctx.value
+
+
+def test_bench_reference_arm_prints_the_contract_line():
+    """`bench.py --impl reference` (the reference's CPU ALG path, restated in C, on the
+    host cores) prints one JSON line with the contract's keys, on the same metric and
+    workload as the default line; it needs no GPU."""
+    import json
+    import os
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference",
+                          "--steps", "1", "--warmup", "0"], capture_output=True, text=True,
+                         check=True, cwd=root, timeout=600).stdout
+    lines = [l for l in out.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "pair-updates/s" and d["value"] > 0
+    assert d["metric"].startswith("BIA pair-updates/s: learned-guess form vs plain FP64")
+    assert d["config"]["workload"] == "plummer_32768" and d["higher_is_better"] is True
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
