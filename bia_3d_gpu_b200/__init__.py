@@ -78,10 +78,11 @@ def invariance_gpu(N, eps_th, X, Y, Z, U, V, W):
     return tuple(o.value for o in outs)
 
 
-def rkf_c(neq, eps_th, X0, XE, YH0, INIT, RELERR, ABSERR):
+def rkf_c(neq, eps_th, X0, XE, YH0, INIT, RELERR, ABSERR, H=0.0):
     """Direct-integration run on the GPU, mirroring rkf_c_ (dim/rkf_kernel.cu:194-495) as
     called from dim/dim_3D.f90:30.  YH0: host AoS state (neq = 6n float64), updated to
-    the final state.  Returns a dict with YHN, ESE, NDE, IER, H, X0 (= XE), INIT."""
+    the final state; H: the step size to start from when INIT != 1 (the previous call's).
+    Returns a dict with YHN, ESE, NDE, IER, H, X0 (= XE), INIT."""
     L = capi.lib()
     n = int(neq)
     x0 = ctypes.c_double(X0)
@@ -91,7 +92,7 @@ def rkf_c(neq, eps_th, X0, XE, YH0, INIT, RELERR, ABSERR):
     abs_ = ctypes.c_double(ABSERR)
     nde = ctypes.c_int(0)
     ier = ctypes.c_int(0)
-    h = ctypes.c_double(0.0)
+    h = ctypes.c_double(H)
     yh0 = np.ascontiguousarray(YH0, dtype=np.float64)
     outs = {k: np.zeros(n) for k in ("YHN", "ESE", "YL0", "YLN", "ERR")}
     _host_f64(yh0, n, "YH0")

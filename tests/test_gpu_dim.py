@@ -63,3 +63,21 @@ def test_rkf_c_dropin(cuda):
     assert np.abs(out["YHN"] - yn).max() <= 1e-12 * np.abs(yn).max()
     assert np.array_equal(out["YH0"], out["YHN"])
     assert np.all(np.isfinite(out["ESE"])) and np.abs(out["ESE"]).max() < 1e-12
+
+
+def test_dim_driver_reproduces_reference_run(cuda, golden, golden_ic, tmp_path):
+    """dim/dim_3D.f90 through the driver on the reference's initial condition: the .DIM
+    record and particle 1's text line against the reference's own run."""
+    from bia_3d_gpu_b200 import driver, records
+    bbb = tmp_path / "0001332_10^0.bbb"
+    records.write_bbb(bbb, [golden_ic])
+    out = driver.run_dim(bbb, tmp_path / "0001332_10^0.DIM", tmp_path / "DIM_10^0.0001332",
+                         eps_th=golden["eps_dim"].item())
+    assert out[0][0] == 0
+    (t, g), = records.read_timed(tmp_path / "0001332_10^0.DIM")
+    ref = golden["dim_final_aos"].reshape(-1, 6).T
+    assert t == 1.0
+    assert rel_err(g[:3], ref[:3]) <= 1e-12 and rel_err(g[3:], ref[3:]) <= 1e-12
+    line = (tmp_path / "DIM_10^0.0001332").read_text().splitlines()[-1]
+    vals = [float(line[23 + 24 * k:23 + 24 * (k + 1)]) for k in range(6)]
+    assert np.abs(np.array(vals) - golden["dim_p1"][1:]).max() <= 1e-13

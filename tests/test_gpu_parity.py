@@ -329,3 +329,21 @@ def test_bounded_device_wait_reports_timeout(cuda):
         assert stats["nonfinite"] == 0 and stats["timeouts"] == 0
     r, _, _ = oracle.bia_step(s, eps, 1e-4)
     assert_parity(t.cpu().numpy(), r)
+
+
+def test_bia_driver_reproduces_reference_record(cuda, golden, golden_ic, tmp_path):
+    """bia/bia.f90 through the driver: the .bbb record in, the .BIA record (t, dX..dW) and
+    particle 1's text line out, against the reference's own run."""
+    from bia_3d_gpu_b200 import driver, records
+    bbb = tmp_path / "0001332_10^0.bbb"
+    records.write_bbb(bbb, [golden_ic])
+    stats, inv = driver.run_bia(bbb, tmp_path / "0001332_10^0.BIA", tmp_path / "BIA_10^0.0001332",
+                                eps_th=-6e-7, time_end=1.0)
+    assert stats[0]["nonfinite"] == 0 and inv["KE"] > 0
+    (t, d), = records.read_timed(tmp_path / "0001332_10^0.BIA")
+    ref_disp = golden["bia_disp_aos"].reshape(-1, 6).T
+    assert t == 1.0
+    assert_parity(golden_ic + d, golden_ic + ref_disp, tol_max=1e-11)
+    line = (tmp_path / "BIA_10^0.0001332").read_text().splitlines()[0]
+    vals = [float(line[23 + 24 * k:23 + 24 * (k + 1)]) for k in range(6)]
+    assert np.abs(np.array(vals) - golden["bia_p1"][1:]).max() <= 1e-13

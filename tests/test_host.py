@@ -139,3 +139,16 @@ def test_bench_reference_arm_prints_the_contract_line():
     assert d["config"]["workload"] == "plummer_32768" and d["higher_is_better"] is True
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
+
+
+def test_fortran_text_line_format():
+    """driver.fortran_line writes bia/bia.f90:207's '(es23.16,6es24.16)': widths 23 and 24,
+    16 digits after the point, a two-digit exponent; the values read back exactly."""
+    from bia_3d_gpu_b200.driver import fortran_line
+    vals = [-1.2345678901234567e-3, 2.0, 0.0, 3.141592653589793e7, -4.5e-10, 1e-5]
+    line = fortran_line(1.0, vals)
+    assert len(line) == 23 + 6 * 24
+    assert line[:23] == " 1.0000000000000000E+00"
+    back = [float(line[23 + 24 * k:23 + 24 * (k + 1)]) for k in range(6)]
+    assert back == vals
+    assert "-1.2345678901234567E-03" in line
