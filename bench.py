@@ -510,7 +510,7 @@ def main():
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     split = bool(tuned and tuned.get("learned_layout") == "split")
     if method == 3:
-        kernel_name = ("bia_pair_learned_kernel<true> + bia_pair_rest_kernel<true> (one timed interval)"
+        kernel_name = ("bia_pair_rest_kernel<true> + bia_pair_learned_list_kernel<true> (one timed interval)"
                        if split else "bia_pair_learned_kernel<true>")
     elif method == 1 and tuned is not None:
         kernel_name = {"tiles8": "bia_pair_tiles_kernel<true, 1>", "phase16": "bia_pair_phase_kernel<true, 16, 2>",

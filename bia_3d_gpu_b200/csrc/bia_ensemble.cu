@@ -154,7 +154,10 @@ __global__ void __launch_bounds__(kMlpThreads, 2) ens_pair_learned_kernel(const 
                               A.q ? A.q + base : nullptr, n, A.eps[s], A.P.dt, A.heads};
     double racc[6], cacc[6];
     PairCounters cnt;
-    const bool timed_out = learned_block_solve(M, B, bi, bj, lane, live, racc, cacc, cnt);
+    mlp_setup(*M.mlp);
+    uint32_t phase = 0;
+    const bool timed_out = learned_block_solve(M, B, bi, bj, lane, live, racc, cacc, cnt, phase);
+    mlp_teardown(*M.mlp, phase);
     if (timed_out && threadIdx.x == 0 && !live) atomicAdd(&A.stats[kStatTimeouts], 1ull);
     if (!live) return;  // warp-uniform; no barrier follows
     flush_counters(cnt, A.stats, lane);

@@ -13,6 +13,8 @@ namespace bia {
 //  1. Each lane classifies its pairs (hyperbolic head, elliptic head, plain) and writes the
 //     head inputs of its learned pairs into a CTA-wide row list in shared memory (packed
 //     BF16 pairs; hyperbolic rows first; offsets from a CTA scan of the per-lane counts).
+//     With a pair mask from the split step's rest kernel only the masked pairs are
+//     classified (and solved); the others are the rest kernel's.
 //  2. The CTA evaluates each head on its rows in full 256-row blocks on the tensor cores
 //     (mlp_tc.cuh) and writes each row's output over its input.
 //  3. Each warp finishes its learned pairs from the stored guesses (FP32 correction, FP64
@@ -88,23 +90,22 @@ __device__ __forceinline__ LearnedSmem learned_smem(uint8_t *raw)
     return L;
 }
 
-// Every thread of the CTA calls it (warps without a block pass live = false).  Returns the
-// row sums racc (particle 32 bi + lane), the column sums cacc (particle 32 bj + lane; the
-// caller writes -cacc) and the counters; true when the tensor-core pipeline timed out.
-// lmask (split mode, may be null): receives this lane's learned-pair mask (bit k: column
-// (lane + k) mod 32) and the plain pairs are left to bia_pair_rest_kernel; without it the
-// plain pairs are solved here too.
+// Every thread of the CTA calls it (warps without a block pass live = false), between the
+// CTA's mlp_setup and mlp_teardown; phase is the MMA barrier's phase, carried across
+// calls.  Returns the row sums racc (particle 32 bi + lane), the column sums cacc (particle
+// 32 bj + lane; the caller writes -cacc) and the counters; true when the tensor-core
+// pipeline timed out.  mask (split step, may be null): this lane's pairs to solve (bit k:
+// column (lane + k) mod 32); without it every pair of the block is solved here.
 __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const LearnedBlockIn &B, int bi, int bj,
                                                     int lane, bool live, double racc[6], double cacc[6],
-                                                    PairCounters &cnt, uint32_t *lmask = nullptr)
+                                                    PairCounters &cnt, uint32_t &phase,
+                                                    const uint32_t *mask = nullptr)
 {
     MlpSmem &S = *M.mlp;
     const int warp = threadIdx.x >> 5;
     double *ws = M.tiles + warp * kTileSmemDoubles;
     double *wacc = ws + 7 * 32;
     uint32_t *rows = M.rows;
-    mlp_setup(S);
-    uint32_t phase = 0;
     counters_zero(cnt);
     double si[7];
 #pragma unroll
@@ -127,7 +128,23 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
 
     // 1. classification and the head inputs
     unsigned mh = 0u, me = 0u, mr = 0u;
-    if (live) {
+    if (live && mask) {
+        unsigned m = *mask;
+        while (m) {
+            const int k = __ffs(m) - 1;
+            m &= m - 1u;
+            const int src = (lane + k) & 31;
+            const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
+            const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
+            const double eps_ij = hq ? B.eps_th * si[6] * ws[6 * 32 + src] : B.eps_th;
+            LearnedPair L;
+            learned_prepare(eps_ij, dt, r, g, L);
+            const unsigned bit = 1u << k;
+            if (L.kind == kLearnedHyp) mh |= bit;
+            else if (L.kind == kLearnedEll) me |= bit;
+            else mr |= bit;
+        }
+    } else if (live) {
         const int k0 = diag ? 1 : 0, k1 = diag ? 16 : 31;
         for (int k = k0; k <= k1; k++) {
             const int src = (lane + k) & 31;
@@ -170,14 +187,20 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
     }
     __syncthreads();
 
-    // 2. the heads on the tensor cores, 256 rows per evaluation
+    // 2. the heads on the tensor cores, 256 rows per evaluation; the head already in shared
+    // memory first (S.head is uniform here: written before the last barrier)
     bool timed_out = false;
+    const bool ell_first = S.head == kHeadEll;
     for (int pass = 0; pass < 2; pass++) {
-        const int head = pass == 0 ? kHeadHyp : kHeadEll;
-        const int r0 = pass == 0 ? 0 : rh;
-        const int nr = pass == 0 ? rh : re;
+        const bool hyp = (pass == 0) != ell_first;
+        const int head = hyp ? kHeadHyp : kHeadEll;
+        const int r0 = hyp ? 0 : rh;
+        const int nr = hyp ? rh : re;
         if (nr == 0) continue;  // uniform
-        mlp_load_head(S, B.heads, head);
+        if (S.head != head) {
+            __syncthreads();  // every thread has read S.head
+            mlp_load_head(S, B.heads, head);
+        }
         for (int b = 0; b < nr; b += kMlpThreads) {
             const int row = b + (int)threadIdx.x;
             const bool valid = row < nr;
@@ -191,12 +214,9 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
     __syncthreads();
 
     // 3. learned pairs from their guesses, per warp.  A warp without learned pairs walks the
-    // rotation offsets instead (all its pairs plain; column sums by shuffle, no shared adds)
-    if (lmask) {
-        if (live) *lmask = mh | me;
-        mr = 0u;  // the plain pairs go to the rest kernel
-    }
-    const bool warp_learned = lmask != nullptr || __any_sync(0xffffffffu, (mh | me) != 0u);
+    // rotation offsets instead (all its pairs plain; column sums by shuffle, no shared adds);
+    // with a mask the few plain pairs go through the per-lane loop below
+    const bool warp_learned = mask != nullptr || __any_sync(0xffffffffu, (mh | me) != 0u);
     if (!warp_learned) {
         const unsigned full = 0xffffffffu;
 #pragma unroll
@@ -299,7 +319,7 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
 #pragma unroll
         for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
     }
-    mlp_teardown(S, phase);
+    __syncthreads();  // the row list and the tiles are free for the CTA's next call
     return timed_out;
 }
 

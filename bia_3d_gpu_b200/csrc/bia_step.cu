@@ -50,7 +50,11 @@ struct StepArgs {
     double eps_th;
     PairParams P;
     const MlpHead *heads;  // BIA_METHOD_LEARNED
-    uint32_t *lmask;       // learned-pair masks (split learned step), nwb * 32 words
+    // split learned step: the rest kernel's pair masks (32 words per listed warp-block),
+    // the list of warp-blocks with masked pairs and its length
+    uint32_t *lmask;
+    unsigned int *wblist;
+    unsigned int *wbcount;
 };
 
 template <bool kDeterministic, int M>
@@ -210,9 +214,46 @@ static void launch_pair_tiles(const StepArgs &A, long long grid, cudaStream_t st
     }
 }
 
-// Learned mixed-precision step kernel (BIA_METHOD_LEARNED): see bia_learned_block.cuh.
-// With A.lmask set (split mode) it solves only the learned pairs, records the learned-pair
-// mask of every lane, and bia_pair_rest_kernel adds the plain pairs afterwards.
+// Adds a learned warp-block's sums onto the partials (deterministic: the rest kernel wrote
+// every slot first) or into the accumulators; assign: write the slots instead.
+template <bool kDeterministic>
+__device__ __forceinline__ void add_learned_sums(const StepArgs &A, int bi, int bj, int lane, const double racc[6],
+                                                 const double cacc[6], bool assign)
+{
+    const int i = bi * 32 + lane;
+    const int jown = bj * 32 + lane;
+    const size_t plane = (size_t)A.npad;
+    if (kDeterministic) {
+        if (assign) {
+            write_partials(A.part, plane, bi, bj, lane, racc, cacc);
+        } else if (bi == bj) {
+            double *dst = A.part + (size_t)bi * 6 * plane;
+#pragma unroll
+            for (int c = 0; c < 6; c++) dst[c * plane + i] += racc[c] - cacc[c];
+        } else {
+            double *drow = A.part + (size_t)bj * 6 * plane;
+            double *dcol = A.part + (size_t)bi * 6 * plane;
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                drow[c * plane + i] += racc[c];
+                dcol[c * plane + jown] -= cacc[c];
+            }
+        }
+    } else if (bi == bj) {
+#pragma unroll
+        for (int c = 0; c < 6; c++)
+            if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c] - cacc[c]);
+    } else {
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c]);
+            if (jown < A.n) atomicAdd(&A.part[c * plane + jown], -cacc[c]);
+        }
+    }
+}
+
+// Learned mixed-precision step kernel (BIA_METHOD_LEARNED) in one launch: every pair of
+// every warp-block, the learned ones from a head's guess (bia_learned_block.cuh).
 template <bool kDeterministic>
 __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const StepArgs A)
 {
@@ -227,33 +268,21 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const 
     const LearnedBlockIn B = {A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P.dt, A.heads};
     double racc[6], cacc[6];
     PairCounters cnt;
-    uint32_t *lm = A.lmask ? A.lmask + (size_t)(live ? t : 0) * 32 + lane : nullptr;
-    const bool timed_out = learned_block_solve(M, B, bi, bj, lane, live, racc, cacc, cnt, lm);
+    mlp_setup(*M.mlp);
+    uint32_t phase = 0;
+    const bool timed_out = learned_block_solve(M, B, bi, bj, lane, live, racc, cacc, cnt, phase);
+    mlp_teardown(*M.mlp, phase);
     if (timed_out && threadIdx.x == 0 && !live) atomicAdd(&A.stats[kStatTimeouts], 1ull);
     if (!live) return;  // warp-uniform; no barrier follows
     flush_counters(cnt, A.stats, lane);
-    const int i = bi * 32 + lane;
-    const int jown = bj * 32 + lane;
-    const size_t plane = (size_t)A.npad;
-    if (kDeterministic) {
-        write_partials(A.part, plane, bi, bj, lane, racc, cacc);
-    } else if (bi == bj) {
-#pragma unroll
-        for (int c = 0; c < 6; c++)
-            if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c] - cacc[c]);
-    } else {
-#pragma unroll
-        for (int c = 0; c < 6; c++) {
-            if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c]);
-            if (jown < A.n) atomicAdd(&A.part[c * plane + jown], -cacc[c]);
-        }
-    }
+    add_learned_sums<kDeterministic>(A, bi, bj, lane, racc, cacc, true);
 }
 
-// The plain pairs of a split learned step: every pair whose bit is clear in the lane's
-// learned mask, by the universal-variable solver, lanes walking the rotation offsets, the
-// sums added onto the learned kernel's partials (each slot is written by one warp-block of
-// each kernel, in this fixed order: deterministic).
+// Split learned step, first kernel: every pair outside the heads' FP32 domain filter
+// (learned_filter) by the universal-variable solver, lanes walking the rotation offsets;
+// the filtered pairs are left as a per-lane mask, and each warp-block with any is appended
+// to the list that bia_pair_learned_list_kernel works through afterwards.  Deterministic
+// mode writes every partial slot here; the learned kernel adds onto them.
 template <bool kDeterministic>
 __global__ void __launch_bounds__(kThreads, TileOccupancy<kMethodUniversal>::kMinBlocks)
     bia_pair_rest_kernel(const StepArgs A)
@@ -265,12 +294,11 @@ __global__ void __launch_bounds__(kThreads, TileOccupancy<kMethodUniversal>::kMi
     int bi, bj;
     warp_block_coords(t, bi, bj);
     const int i = bi * 32 + lane;
-    const int jown = bj * 32 + lane;
     const bool diag = (bi == bj);
-    const uint32_t learned = A.lmask[(size_t)t * 32 + lane];
+    uint32_t learned = 0u;
     double si[7], sj[7], racc[6], cacc[6];
     load_particle(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, i, si);
-    load_particle(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, jown, sj);
+    load_particle(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, bj * 32 + lane, sj);
 #pragma unroll
     for (int c = 0; c < 6; c++) racc[c] = cacc[c] = 0.0;
     PairCounters cnt;
@@ -282,12 +310,16 @@ __global__ void __launch_bounds__(kThreads, TileOccupancy<kMethodUniversal>::kMi
 #pragma unroll
         for (int c = 0; c < 7; c++) sc[c] = __shfl_sync(full, sj[c], src);
         const int j = bj * 32 + src;
-        const bool active = (!diag || k < 16 || lane < 16) && i < A.n && j < A.n && !((learned >> k) & 1u);
+        bool active = (!diag || k < 16 || lane < 16) && i < A.n && j < A.n;
         double h[6] = {0, 0, 0, 0, 0, 0};
+        const double r[3] = {si[0] - sc[0], si[1] - sc[1], si[2] - sc[2]};
+        const double g[3] = {si[3] - sc[3], si[4] - sc[4], si[5] - sc[5]};
+        const double eps_ij = A.q ? A.eps_th * si[6] * sc[6] : A.eps_th;
+        if (active && learned_filter(eps_ij, A.P.dt, r, g)) {
+            learned |= 1u << k;
+            active = false;
+        }
         if (active) {
-            const double r[3] = {si[0] - sc[0], si[1] - sc[1], si[2] - sc[2]};
-            const double g[3] = {si[3] - sc[3], si[4] - sc[4], si[5] - sc[5]};
-            const double eps_ij = A.q ? A.eps_th * si[6] * sc[6] : A.eps_th;
             const int it = uv_halfdisp(eps_ij, A.P.dt, r, g, h);
             cnt.it_uv += it;
             if (it > kUvItMax) cnt.nonconverged++;
@@ -302,69 +334,127 @@ __global__ void __launch_bounds__(kThreads, TileOccupancy<kMethodUniversal>::kMi
         }
     }
     flush_counters(cnt, A.stats, lane);
-    const size_t plane = (size_t)A.npad;
-    if (kDeterministic) {
-        if (diag) {
-            double *dst = A.part + (size_t)bi * 6 * plane;
-#pragma unroll
-            for (int c = 0; c < 6; c++) dst[c * plane + i] += racc[c] - cacc[c];
-        } else {
-            double *drow = A.part + (size_t)bj * 6 * plane;
-            double *dcol = A.part + (size_t)bi * 6 * plane;
-#pragma unroll
-            for (int c = 0; c < 6; c++) {
-                drow[c * plane + i] += racc[c];
-                dcol[c * plane + jown] -= cacc[c];
-            }
-        }
-    } else if (diag) {
-#pragma unroll
-        for (int c = 0; c < 6; c++)
-            if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c] - cacc[c]);
-    } else {
-#pragma unroll
-        for (int c = 0; c < 6; c++) {
-            if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c]);
-            if (jown < A.n) atomicAdd(&A.part[c * plane + jown], -cacc[c]);
-        }
+    add_learned_sums<kDeterministic>(A, bi, bj, lane, racc, cacc, true);
+    if (__any_sync(full, learned != 0u)) {
+        unsigned int slot = 0;
+        if (lane == 0) slot = atomicAdd(A.wbcount, 1u);
+        slot = __shfl_sync(full, slot, 0);
+        A.lmask[(size_t)slot * 32 + lane] = learned;
+        if (lane == 0) A.wblist[slot] = (unsigned int)t;
     }
 }
 
-// Once per device: dynamic shared memory opt-in of the learned kernels (false on failure).
-static bool learned_kernel_setup()
+// Split learned step, second kernel: persistent CTAs work through the listed warp-blocks,
+// eight at a time (one per warp), solving the masked pairs from the heads' guesses and
+// adding their sums onto the rest kernel's.  The tensor memory is allocated once per CTA.
+template <bool kDeterministic>
+__global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_list_kernel(const StepArgs A)
+{
+    extern __shared__ uint8_t learned_smem_raw[];
+    const LearnedSmem M = learned_smem(learned_smem_raw);
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const long long count = (long long)*A.wbcount;
+    const LearnedBlockIn B = {A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P.dt, A.heads};
+    mlp_setup(*M.mlp);
+    uint32_t phase = 0;
+    for (long long g0 = (long long)blockIdx.x * kLearnedWarps; g0 < count;
+         g0 += (long long)gridDim.x * kLearnedWarps) {
+        const long long e = g0 + warp;
+        const bool live = e < count;
+        int bi = 0, bj = 0;
+        uint32_t mask = 0u;
+        if (live) {
+            warp_block_coords((long long)A.wblist[e], bi, bj);
+            mask = A.lmask[(size_t)e * 32 + lane];
+        }
+        double racc[6], cacc[6];
+        PairCounters cnt;
+        const bool timed_out = learned_block_solve(M, B, bi, bj, lane, live, racc, cacc, cnt, phase, &mask);
+        if (timed_out && threadIdx.x == 0 && !live) atomicAdd(&A.stats[kStatTimeouts], 1ull);
+        if (live) {
+            flush_counters(cnt, A.stats, lane);
+            add_learned_sums<kDeterministic>(A, bi, bj, lane, racc, cacc, false);
+        }
+    }
+    mlp_teardown(*M.mlp, phase);
+}
+
+// Once per device: dynamic shared memory opt-in of the learned kernels; returns the grid
+// of the persistent list kernel (resident CTAs on the device), 0 on failure.
+static int learned_kernel_setup()
 {
     constexpr int kMaxDevices = 64;
     static std::mutex mu;
-    static int state_of[kMaxDevices] = {};  // 0 unknown, 1 ok, 2 failed
+    static int grid_of[kMaxDevices] = {};
+    static bool done_of[kMaxDevices] = {};
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return false;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 0;
     std::lock_guard<std::mutex> lk(mu);
-    if (state_of[dev] == 0) {
-        bool ok = cudaFuncSetAttribute(bia_pair_learned_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kLearnedSmemBytes) == cudaSuccess;
+    if (!done_of[dev]) {
+        const int bytes = (int)kLearnedSmemBytes;
+        int sms = 0, occ = 0;
+        bool ok = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(bia_pair_learned_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        bytes) == cudaSuccess;
         ok = ok && cudaFuncSetAttribute(bia_pair_learned_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kLearnedSmemBytes) == cudaSuccess;
+                                        bytes) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(bia_pair_learned_list_kernel<true>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(bia_pair_learned_list_kernel<false>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
+        // the largest shared-memory carveout, so that the occupancy query sees what the
+        // launch gets (without it the query assumes the default split: 1 CTA per SM)
+        for (const void *f : {(const void *)bia_pair_learned_list_kernel<true>,
+                              (const void *)bia_pair_learned_list_kernel<false>})
+            ok = ok && cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                            (int)cudaSharedmemCarveoutMaxShared) == cudaSuccess;
+        ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bia_pair_learned_list_kernel<true>, kMlpThreads,
+                                                                 (size_t)bytes) == cudaSuccess;
         if (!ok) cudaGetLastError();
-        state_of[dev] = ok ? 1 : 2;
+        // at least the launch bound's two CTAs per SM: CTAs beyond the resident ones wait
+        // for a slot, so a low answer costs nothing but a short queue
+        grid_of[dev] = ok ? sms * (occ > 2 ? occ : 2) : 0;
+        done_of[dev] = true;
     }
-    return state_of[dev] == 1;
+    return grid_of[dev];
 }
 
+// The learned step's pair launches: one kernel, or (A.lmask set) the rest kernel and the
+// persistent list kernel.
 template <bool kDeterministic>
 static int launch_pair_learned(const StepArgs &A, cudaStream_t st)
 {
-    if (!learned_kernel_setup()) return BIA_ERR_CUDA;
-    const long long grid = (A.nwb + kLearnedWarps - 1) / kLearnedWarps;
-    bia_pair_learned_kernel<kDeterministic><<<(unsigned)grid, kMlpThreads, kLearnedSmemBytes, st>>>(A);
-    if (A.lmask) {
-        const long long rgrid = (A.nwb + kWarpsPerBlock - 1) / kWarpsPerBlock;
-        bia_pair_rest_kernel<kDeterministic><<<(unsigned)rgrid, kThreads, 0, st>>>(A);
+    const int lgrid = learned_kernel_setup();
+    if (lgrid <= 0) return BIA_ERR_CUDA;
+    if (!A.lmask) {
+        const long long grid = (A.nwb + kLearnedWarps - 1) / kLearnedWarps;
+        bia_pair_learned_kernel<kDeterministic><<<(unsigned)grid, kMlpThreads, kLearnedSmemBytes, st>>>(A);
+        return BIA_OK;
     }
+    if (cudaMemsetAsync(A.wbcount, 0, sizeof(unsigned int), st) != cudaSuccess) return BIA_ERR_CUDA;
+    const long long rgrid = (A.nwb + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    bia_pair_rest_kernel<kDeterministic><<<(unsigned)rgrid, kThreads, 0, st>>>(A);
+    const long long need = (A.nwb + kLearnedWarps - 1) / kLearnedWarps;
+    const int grid = (int)(need < lgrid ? need : lgrid);
+    bia_pair_learned_list_kernel<kDeterministic><<<grid, kMlpThreads, kLearnedSmemBytes, st>>>(A);
     return BIA_OK;
 }
 
-// Split learned steps (learned pairs in the learned kernel, plain pairs in the rest kernel
-// at the universal-variable kernel's occupancy) from two 32-warp CTAs per SM up, as the
+// The split learned step's buffer: the list length (16 bytes), the list (nwb words) and the
+// masks (32 words per listed warp-block).
+static size_t split_buffer_bytes(long long nwb) { return 16 + (size_t)nwb * 33 * sizeof(uint32_t); }
+
+static void split_buffer_carve(void *base, long long nwb, StepArgs &A)
+{
+    uint8_t *b = (uint8_t *)base;
+    A.wbcount = (unsigned int *)b;
+    A.wblist = (unsigned int *)(b + 16);
+    A.lmask = (uint32_t *)(b + 16 + (size_t)nwb * sizeof(uint32_t));
+}
+
+// Split learned steps (plain pairs in the rest kernel at the universal-variable kernel's
+// occupancy, learned pairs in the list kernel) from two 32-warp CTAs per SM up, as the
 // phase-locked ALG kernel.
 static bool learned_split(long long nwb)
 {
@@ -433,7 +523,7 @@ int ensure_step_buffers(bia_context *ctx, const bia_config *cfg, int n)
     if (cfg->method == BIA_METHOD_LEARNED) {
         const long long nwb = (long long)nb * (nb + 1) / 2;
         if (learned_split(nwb) || ctx->learned_tuned[cfg->deterministic ? 1 : 0][ilog2_bucket(n)] == 1) {
-            e = ctx->lmask.reserve((size_t)nwb * 32 * sizeof(uint32_t));
+            e = ctx->lmask.reserve(split_buffer_bytes(nwb));
             if (e != cudaSuccess) return cuda_status(e);
         }
     }
@@ -508,7 +598,7 @@ int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
         const int lt = ctx->learned_tuned[cfg->deterministic ? 1 : 0][ilog2_bucket(n)];
         split = (lt >= 0) ? (lt == 1 && ctx->lmask.ptr) : learned_split(A.nwb);
     }
-    A.lmask = split ? (uint32_t *)ctx->lmask.ptr : nullptr;
+    if (split) split_buffer_carve(ctx->lmask.ptr, A.nwb, A);
     if (learned && !ctx->heads_loaded) return BIA_ERR_INVALID_ARGUMENT;
     int st = BIA_OK;
     if (cfg->deterministic) {
@@ -685,8 +775,8 @@ int bia_context_autotune(bia_context *ctx, const bia_config *cfg, int n, double 
     const int det = cfg->deterministic ? 1 : 0;
     A.part = det ? (double *)ctx->part.ptr : (double *)ctx->acc.ptr;
     const bool learned = cfg->method == BIA_METHOD_LEARNED;
-    if (learned) {  // layouts: 0 one kernel, 1 split (learned pairs, then the rest kernel)
-        e = ctx->lmask.reserve((size_t)A.nwb * 32 * sizeof(uint32_t));
+    if (learned) {  // layouts: 0 one kernel, 1 split (the rest kernel, then the list kernel)
+        e = ctx->lmask.reserve(split_buffer_bytes(A.nwb));
         if (e != cudaSuccess) return set_last_error(cuda_status(e));
     }
     const int nvar = learned ? 2 : kVarCount;
@@ -706,7 +796,8 @@ int bia_context_autotune(bia_context *ctx, const bia_config *cfg, int n, double 
             if (e == cudaSuccess) e = cudaEventRecord(ev[0], ctx->stream);
             int lst = BIA_OK;
             if (learned) {
-                A.lmask = var == 1 ? (uint32_t *)ctx->lmask.ptr : nullptr;
+                A.lmask = nullptr;
+                if (var == 1) split_buffer_carve(ctx->lmask.ptr, A.nwb, A);
                 lst = det ? launch_pair_learned<true>(A, ctx->stream) : launch_pair_learned<false>(A, ctx->stream);
             } else if (det) {
                 launch_pair_tiles<true>(A, grid, ctx->stream, var);
