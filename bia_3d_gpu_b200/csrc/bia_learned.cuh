@@ -100,34 +100,26 @@ __device__ __forceinline__ void learned_prepare(double eps_ij, double dt, const 
     }
 }
 
-// The heads' domain in FP32: the split step's filter that sends a pair to the learned
-// kernel.  The same quantities as learned_prepare (and the universal-variable band of
-// alg_classify, |e^2 - 1| < 0.1) in single precision: ellipses with e^2 < 0.9, attractive
-// hyperbolae with 1.1 < e^2 <= 2500 and |M1| <= 100.  An approximation is enough: the
-// learned kernel decides again in FP64 (learned_prepare) and solves a pair outside the
-// FP64 domain with the plain solver, so the filter only chooses the kernel.
-__device__ __forceinline__ bool learned_filter(double eps_ij, double dt, const double r[3], const double g[3])
+// The heads' domain as a cheap test on the universal-variable quantities of the pair (the
+// split step's filter that sends a pair to the learned kernel): with t = mu - r0 beta,
+// e^2 mu^2 = t^2 + sig^2 beta for ellipses and hyperbolae alike (no division, no root),
+// and the domain is that of learned_prepare and the universal-variable band of
+// alg_classify (|e^2 - 1| < 0.1): ellipses with e^2 < 0.9, attractive hyperbolae with
+// 1.1 < e^2 <= 2500 and |M1| <= 100 (that last test in FP32, on the few pairs in the band).
+// The learned kernel decides again with learned_prepare and solves a pair outside its
+// domain with the plain solver, so this test only chooses the kernel.
+__device__ __forceinline__ bool learned_filter(const UvPair &p, double dt)
 {
-    if (!(dt > 0.0) || !(eps_ij < 0.0)) return false;
-    const float rx = (float)r[0], ry = (float)r[1], rz = (float)r[2];
-    const float gx = (float)g[0], gy = (float)g[1], gz = (float)g[2];
-    const float mu = (float)(-eps_ij);
-    const float rsq = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-    const float v2 = fmaf(gx, gx, fmaf(gy, gy, gz * gz));
-    const float sig = fmaf(rx, gx, fmaf(ry, gy, rz * gz));
-    const float rinv = rsqrtf(rsq);
-    const float beta = 2.0f * mu * rinv - v2;
-    const float ab = fabsf(beta), sqb = sqrtf(ab);
-    const float c0m = rsq * rinv * ab / mu;
-    const float s0 = sig * sqb / mu;
-    if (beta > 0.0f) {
-        const float c0 = 1.0f - c0m;
-        return fmaf(c0, c0, s0 * s0) < 0.9f;
-    }
-    const float c0 = 1.0f + c0m;
-    const float e2 = (c0 - s0) * (c0 + s0);
-    if (!(e2 > 1.1f && e2 <= kHypEMax * kHypEMax)) return false;
-    const float M1 = s0 - asinhf(s0 * rsqrtf(e2)) + ab * sqb / mu * (float)dt;
+    if (!(dt > 0.0) || !(p.mu > 0.0)) return false;
+    const double t = fma(-p.r0, p.beta, p.mu);
+    const double e2m = fma(p.sig * p.sig, p.beta, t * t);
+    const double mu2 = p.mu * p.mu;
+    if (p.beta > 0.0) return e2m < 0.9 * mu2;
+    if (!(e2m > 1.1 * mu2 && e2m <= (double)(kHypEMax * kHypEMax) * mu2)) return false;
+    const float mu = (float)p.mu, ab = (float)(-p.beta), sqb = sqrtf(ab);
+    const float s0 = (float)p.sig * sqb / mu;
+    const float e = sqrtf((float)e2m) / mu;
+    const float M1 = s0 - asinhf(s0 / e) + ab * sqb / mu * (float)dt;
     return fabsf(M1) <= kHypMMax;
 }
 

@@ -287,7 +287,6 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
             }
         }
     }
-    if (timed_out && threadIdx.x == 0) cnt.timeouts++;
     // plain pairs: the universal-variable solver, per warp (mr is empty on rotation warps)
     for (;;) {
         const bool busy = (mr != 0u);
@@ -319,7 +318,10 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
 #pragma unroll
         for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
     }
-    __syncthreads();  // the row list and the tiles are free for the CTA's next call
+    // the row list and the tiles are free for the CTA's next call; a timeout of either
+    // warpgroup's tensor-core pipeline counts once
+    timed_out = __syncthreads_or(timed_out ? 1 : 0) != 0;
+    if (timed_out && threadIdx.x == 0) cnt.timeouts++;
     return timed_out;
 }
 

@@ -310,21 +310,27 @@ __global__ void __launch_bounds__(kThreads, TileOccupancy<kMethodUniversal>::kMi
 #pragma unroll
         for (int c = 0; c < 7; c++) sc[c] = __shfl_sync(full, sj[c], src);
         const int j = bj * 32 + src;
-        bool active = (!diag || k < 16 || lane < 16) && i < A.n && j < A.n;
+        const bool active = (!diag || k < 16 || lane < 16) && i < A.n && j < A.n;
         double h[6] = {0, 0, 0, 0, 0, 0};
-        const double r[3] = {si[0] - sc[0], si[1] - sc[1], si[2] - sc[2]};
-        const double g[3] = {si[3] - sc[3], si[4] - sc[4], si[5] - sc[5]};
-        const double eps_ij = A.q ? A.eps_th * si[6] * sc[6] : A.eps_th;
-        if (active && learned_filter(eps_ij, A.P.dt, r, g)) {
-            learned |= 1u << k;
-            active = false;
-        }
         if (active) {
-            const int it = uv_halfdisp(eps_ij, A.P.dt, r, g, h);
-            cnt.it_uv += it;
-            if (it > kUvItMax) cnt.nonconverged++;
-            cnt.cls[pair_degenerate(r, g) ? kDegenerate : kUniversal]++;
-            count_nonfinite(h, cnt);
+            const double r[3] = {si[0] - sc[0], si[1] - sc[1], si[2] - sc[2]};
+            const double g[3] = {si[3] - sc[3], si[4] - sc[4], si[5] - sc[5]};
+            const double eps_ij = A.q ? A.eps_th * si[6] * sc[6] : A.eps_th;
+            // uv_halfdisp in its pieces, the filter between them
+            const UvPair p = uv_prepare(eps_ij, r, g);
+            if (learned_filter(p, A.P.dt)) {
+                learned |= 1u << k;
+            } else if (A.P.dt != 0.0) {
+                double s = uv_start(p, A.P.dt);
+                const int it = uv_iterate(p, A.P.dt, s);
+                uv_compose(p, s, r, g, h);
+                cnt.it_uv += it;
+                if (it > kUvItMax) cnt.nonconverged++;
+                cnt.cls[pair_maybe_degenerate(p, g) && pair_degenerate(r, g) ? kDegenerate : kUniversal]++;
+                count_nonfinite(h, cnt);
+            } else {
+                cnt.cls[pair_degenerate(r, g) ? kDegenerate : kUniversal]++;
+            }
         }
         const int back = (lane - k) & 31;
 #pragma unroll
@@ -470,18 +476,39 @@ struct UpdateArgs {
     double dt;
 };
 
-// Sum of the partials in fixed order, drift and state update (bia/bia.f90:194-204).
-__global__ void __launch_bounds__(256) bia_reduce_update_kernel(const UpdateArgs A)
+// Sum of the partials in fixed order, drift and state update (bia/bia.f90:194-204).  A CTA
+// covers 32 particles with one warp per component: warp c sums component c of its 32
+// particles over the nparts planes in plane order (each load is 256 contiguous bytes, and
+// six warps per 32 particles keep enough loads in flight to stream the 1.5 n^2 bytes of
+// partials), then warp 0 applies the drift and the update.
+constexpr int kReduceThreads = 6 * 32;
+
+__global__ void __launch_bounds__(kReduceThreads) bia_reduce_update_kernel(const UpdateArgs A)
 {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= A.n) return;
+    __shared__ double s_sum[6][32];
+    const int lane = threadIdx.x & 31;
+    const int c = threadIdx.x >> 5;
+    const int p = blockIdx.x * 32 + lane;
     const size_t plane = (size_t)A.npad;
-    double s[6] = {0, 0, 0, 0, 0, 0};
-    for (int m = 0; m < A.nparts; m++) {
-        const double *src = A.part + (size_t)m * 6 * plane + p;
+    if (p < A.n) {
+        const double *src = A.part + (size_t)c * plane + p;
+        const size_t step = 6 * plane;
+        double sum = 0.0;
+        int m = 0;
+        for (; m + 8 <= A.nparts; m += 8) {
+            double t[8];
 #pragma unroll
-        for (int c = 0; c < 6; c++) s[c] += src[c * plane];
+            for (int k = 0; k < 8; k++) t[k] = src[(size_t)(m + k) * step];
+#pragma unroll
+            for (int k = 0; k < 8; k++) sum += t[k];
+        }
+        for (; m < A.nparts; m++) sum += src[(size_t)m * step];
+        s_sum[c][lane] = sum;
     }
+    __syncthreads();
+    if (c != 0 || p >= A.n) return;
+    const double s[6] = {s_sum[0][lane], s_sum[1][lane], s_sum[2][lane],
+                         s_sum[3][lane], s_sum[4][lane], s_sum[5][lane]};
     const double u = A.u[p], v = A.v[p], w = A.w[p];
     const double d[6] = {s[0] + u * A.dt, s[1] + v * A.dt, s[2] + w * A.dt, s[3], s[4], s[5]};
     A.x[p] = A.x[p] + d[0];
@@ -492,7 +519,7 @@ __global__ void __launch_bounds__(256) bia_reduce_update_kernel(const UpdateArgs
     A.w[p] = w + d[5];
     if (A.disp) {
 #pragma unroll
-        for (int c = 0; c < 6; c++) A.disp[(size_t)c * A.n + p] = d[c];
+        for (int k = 0; k < 6; k++) A.disp[(size_t)k * A.n + p] = d[k];
     }
 }
 
@@ -620,7 +647,7 @@ int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
         record_event(ctx);
     }
     if (st != BIA_OK) return st;
-    bia_reduce_update_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(U);
+    bia_reduce_update_kernel<<<(n + 31) / 32, kReduceThreads, 0, ctx->stream>>>(U);
     return cuda_status(cudaGetLastError());
 }
 
@@ -1106,7 +1133,7 @@ extern "C" int bia_step_noalloc(const bia_config *cfg, int n, double *x, double 
     U.npad = nb * 32;
     U.nparts = nb;
     U.dt = cfg->dt;
-    bia_reduce_update_kernel<<<(n + 255) / 256, 256, 0, s>>>(U);
+    bia_reduce_update_kernel<<<(n + 31) / 32, kReduceThreads, 0, s>>>(U);
     return cuda_status(cudaGetLastError());
 }
 
@@ -1124,7 +1151,8 @@ __global__ void __launch_bounds__(kMlpThreads, 1) bia_head_eval_kernel(const Mlp
     mlp_load_head(S, heads, head);
     uint32_t phase = 0;
     bool ok = true;
-    // the same number of rounds on every thread of the CTA (the MLP synchronises the CTA)
+    // the same number of rounds on every thread of a warpgroup (the MLP synchronises the
+    // warpgroup)
     for (long long row0 = (long long)blockIdx.x * kMlpThreads; row0 < n && ok;
          row0 += (long long)gridDim.x * kMlpThreads) {
         const long long row = row0 + threadIdx.x;
@@ -1134,7 +1162,7 @@ __global__ void __launch_bounds__(kMlpThreads, 1) bia_head_eval_kernel(const Mlp
         if (row < n) out[row] = ok ? y : __int_as_float(0x7fc00000);
     }
     mlp_teardown(S, phase);
-    if (!ok && threadIdx.x == 0) atomicAdd(timeouts, 1ull);
+    if (__syncthreads_or(ok ? 0 : 1) && threadIdx.x == 0) atomicAdd(timeouts, 1ull);
 }
 }  // namespace bia
 

@@ -9,6 +9,11 @@
 // 32 (w mod 4) .. + 31 of tile w / 4), adds the bias, applies ReLU, rounds to BF16 and
 // writes the row as the next layer's A operand.
 //
+// The two tiles are two independent pipelines: warpgroup g (warps 4g .. 4g + 3, rows
+// 128 g .. + 127) has its own A tile, TMEM columns, issuing thread and mbarrier and
+// synchronises on its own named barrier, so one warpgroup's epilogue runs while the other
+// waits for its MMAs.
+//
 // Operand layout: K-major, no swizzle, the canonical arrangement of 8-row x 16-byte core
 // matrices: element (row, k) of a [rows][K] BF16 matrix sits at byte
 //     ((row / 8) * (K / 8) + k / 8) * 128 + (row % 8) * 16 + (k % 8) * 2,
@@ -41,18 +46,19 @@ struct MlpHead {
 static_assert(sizeof(MlpHead) == 19472, "learned_heads.bin head record");
 constexpr int kMlpHeads = 2;  // 0 elliptic, 1 hyperbolic
 
-// Shared-memory image of one head and the activation tile (1024-aligned parts).  The
-// layer-1 rows (K = 16) live in the first 8 KB of the layer-2/3 tile: layer 1's MMA has
-// completed before the first epilogue overwrites them.
+// Shared-memory image of one head and the activation tile (1024-aligned parts).  Each
+// warpgroup's layer-1 rows (K = 16, 4 KB) live at the start of its own 16 KB half of the
+// layer-2/3 tile: its layer-1 MMA has completed before its first epilogue overwrites them.
+constexpr uint32_t kMlpTileBytes = 128u * kMlpHidden * 2;  // one warpgroup's A tile
 struct MlpSmem {
     alignas(1024) uint8_t w1[kMlpHidden * kMlpK1 * 2];        // 2 KB
     alignas(1024) uint8_t w2[kMlpHidden * kMlpHidden * 2];    // 8 KB
     alignas(1024) uint8_t w3[kMlpHidden * kMlpHidden * 2];    // 8 KB
     alignas(1024) uint8_t a2[kMlpThreads * kMlpHidden * 2];   // 32 KB; a1 = a2
     float b1[kMlpHidden], b2[kMlpHidden], b3[kMlpHidden], w4[kMlpHidden], b4;
-    alignas(8) uint64_t mbar;
+    alignas(8) uint64_t mbar[2];  // one per warpgroup
     uint32_t tmem_base;
-    int abort;
+    int abort[2];
     int turns;  // scratch for CTA-wide counts of the callers
     int head;   // the head whose weights are loaded (-1: none)
     int wsum[2][kMlpThreads / 32];  // per-warp totals of the callers' row scans
@@ -140,8 +146,9 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b)
     return *reinterpret_cast<const uint32_t *>(&v);
 }
 
-// One head's weights from global memory into the shared image (all threads; the caller
-// synchronises before the next MMA: mlp_layer does).
+// One head's weights from global memory into the shared image (all threads, with a CTA
+// barrier at the end: the two warpgroups' MMAs read every weight).  The caller makes sure
+// that no MMA on the old weights is in flight.
 __device__ __forceinline__ void mlp_load_head(MlpSmem &S, const MlpHead *heads, int h)
 {
     const int tid = threadIdx.x;
@@ -163,6 +170,8 @@ __device__ __forceinline__ void mlp_load_head(MlpSmem &S, const MlpHead *heads, 
         S.b4 = H.b4[0];
         S.head = h;
     }
+    fence_async_smem();
+    __syncthreads();
 }
 
 // Once per CTA (all threads): the mbarrier and the TMEM allocation (warp 0, 128 columns:
@@ -171,9 +180,10 @@ __device__ __forceinline__ void mlp_setup(MlpSmem &S)
 {
     const int tid = threadIdx.x;
     if (tid == 0) {
-        S.abort = 0;
+        S.abort[0] = S.abort[1] = 0;
         S.head = -1;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.mbar)) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.mbar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.mbar[1])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncwarp();  // the .sync.aligned TMEM instructions need the whole warp converged
@@ -189,47 +199,54 @@ __device__ __forceinline__ void mlp_setup(MlpSmem &S)
     tc_fence_after();
 }
 
-// Once per CTA at the end (all threads): free the TMEM columns.  After a timeout the MMA
-// group in flight is waited for once more (bounded) before the columns are released.
+// Once per CTA at the end (all threads): free the TMEM columns.  After a timeout the
+// warpgroup's MMA group in flight is waited for once more (bounded) before the columns are
+// released.
 __device__ __forceinline__ void mlp_teardown(MlpSmem &S, uint32_t phase)
 {
+    const int wg = threadIdx.x >> 7;
     tc_fence_before();
     __syncthreads();
+    if (S.abort[wg]) mbar_wait(&S.mbar[wg], phase);
+    __syncthreads();
     tc_fence_after();
-    if (S.abort) mbar_wait(&S.mbar, phase);
     __syncwarp();
     if ((threadIdx.x >> 5) == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(S.tmem_base) : "memory");
 }
 
-// Layer MMAs of both 128-row tiles for one layer, issued by thread 0, then the bounded
-// wait of every thread.  Returns false (and sets S.abort) on a timeout.
+// Barrier of this thread's warpgroup (named barriers 1 and 2; 0 is __syncthreads).
+__device__ __forceinline__ void wg_sync(int wg)
+{
+    asm volatile("bar.sync %0, 128;" ::"r"(1 + wg) : "memory");
+}
+
+// One layer of this warpgroup's 128-row tile: the MMAs issued by the warpgroup's first
+// thread (A rows at a + wg * kMlpTileBytes, K-major with K columns), then the bounded wait
+// of every thread of the warpgroup.  Returns false (and sets S.abort[wg]) on a timeout;
+// the answer is the same on every thread of the warpgroup.
 __device__ __forceinline__ bool mlp_layer(MlpSmem &S, const uint8_t *a, const uint8_t *w, int K, uint32_t &phase)
 {
+    const int wg = threadIdx.x >> 7;
     fence_async_smem();
     tc_fence_before();
-    __syncthreads();
+    wg_sync(wg);
     tc_fence_after();
-    if (S.abort) return false;  // uniform: read after the barrier
-    if (threadIdx.x == 0) {
+    if (S.abort[wg]) return false;  // uniform in the warpgroup: read after its barrier
+    if ((threadIdx.x & 127) == 0) {
         const uint32_t sbo = (uint32_t)K * 16;
-        const uint32_t tile_bytes = 128u * (uint32_t)K * 2;
-        for (int t = 0; t < 2; t++) {
-            for (int ks = 0; ks < K / 16; ks++) {
-                const uint64_t ad = mma_desc(smem_addr(a) + t * tile_bytes + ks * 256, 128, sbo);
-                const uint64_t bd = mma_desc(smem_addr(w) + ks * 256, 128, sbo);
-                tc_mma(S.tmem_base + (uint32_t)(t * 64), ad, bd, ks > 0 ? 1u : 0u);
-            }
+        for (int ks = 0; ks < K / 16; ks++) {
+            const uint64_t ad = mma_desc(smem_addr(a) + wg * kMlpTileBytes + ks * 256, 128, sbo);
+            const uint64_t bd = mma_desc(smem_addr(w) + ks * 256, 128, sbo);
+            tc_mma(S.tmem_base + (uint32_t)(wg * 64), ad, bd, ks > 0 ? 1u : 0u);
         }
-        tc_commit(&S.mbar);
+        tc_commit(&S.mbar[wg]);
     }
-    const bool ok = mbar_wait(&S.mbar, phase);
-    // every thread takes the same branch: a timeout anywhere aborts the CTA's MLP work
-    const int bad = __syncthreads_or(ok ? 0 : 1);
-    if (bad) {
-        if (threadIdx.x == 0) S.abort = 1;
-        return false;  // the phase stays: teardown waits for it once more
-    }
+    const bool ok = mbar_wait(&S.mbar[wg], phase);
+    // a timeout on any thread aborts the warpgroup's MLP work
+    if (!ok) S.abort[wg] = 1;
+    wg_sync(wg);
+    if (S.abort[wg]) return false;  // the phase stays: teardown waits for it once more
     phase ^= 1u;
     tc_fence_after();
     return true;
@@ -267,16 +284,18 @@ __device__ __forceinline__ float mlp_epilogue(MlpSmem &S, const float *bias, uin
 }
 
 // The loaded head's output for this thread's input row, given as packed BF16 (x0 in the
-// low half); every thread of the CTA calls it.  ok (the same on every thread) is false
-// when the tensor-core pipeline timed out; the CTA then issues no more MMAs.
+// low half); every thread of the CTA calls it.  ok (the same on every thread of a
+// warpgroup) is false when the warpgroup's tensor-core pipeline timed out; it then issues
+// no more MMAs.
 __device__ __forceinline__ float mlp_eval_cta(MlpSmem &S, uint32_t x01_bf16, uint32_t &phase, bool &ok)
 {
     const int tid = threadIdx.x;
-    uint8_t *a1 = S.a2;  // layer-1 rows alias the layer-2 tile
-    *(uint4 *)(a1 + kmajor_off(tid, 0, kMlpK1)) = make_uint4(x01_bf16, 0u, 0u, 0u);
-    *(uint4 *)(a1 + kmajor_off(tid, 8, kMlpK1)) = make_uint4(0u, 0u, 0u, 0u);
+    // layer-1 rows at the start of the warpgroup's own half of the layer-2 tile
+    uint8_t *a1 = S.a2 + (tid >> 7) * kMlpTileBytes;
+    *(uint4 *)(a1 + kmajor_off(tid & 127, 0, kMlpK1)) = make_uint4(x01_bf16, 0u, 0u, 0u);
+    *(uint4 *)(a1 + kmajor_off(tid & 127, 8, kMlpK1)) = make_uint4(0u, 0u, 0u, 0u);
     ok = false;
-    if (!mlp_layer(S, a1, S.w1, kMlpK1, phase)) return 0.0f;
+    if (!mlp_layer(S, S.a2, S.w1, kMlpK1, phase)) return 0.0f;
     mlp_epilogue(S, S.b1, S.a2);
     if (!mlp_layer(S, S.a2, S.w2, kMlpHidden, phase)) return 0.0f;
     mlp_epilogue(S, S.b2, S.a2);
