@@ -734,6 +734,16 @@ static __device__ __noinline__ int rkf_pair(double eps_th, double xe, double rel
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void stumpff(double x, double c[4])
 {
+    if (fabs(x) <= 1e-2) {
+        // the first five terms: the next ones, x^5/12! and x^5/13!, are below 2e-19
+        const double c2 = 0.5 - x * (1.0 / 24 - x * (1.0 / 720 - x * (1.0 / 40320 - x * (1.0 / 3628800))));
+        const double c3 = 1.0 / 6 - x * (1.0 / 120 - x * (1.0 / 5040 - x * (1.0 / 362880 - x * (1.0 / 39916800))));
+        c[0] = 1.0 - x * c2;
+        c[1] = 1.0 - x * c3;
+        c[2] = c2;
+        c[3] = c3;
+        return;
+    }
     int n = 0;
     while (fabs(x) > 0.1 && n < 200) { x *= 0.25; n++; }
     // c2 = sum (-x)^j / (2+2j)!, c3 = sum (-x)^j / (3+2j)!, j = 0..10 (|x| <= 0.1)
@@ -763,6 +773,7 @@ constexpr int kUvItMax = 200;
 // solvers can supply their own start; uv_halfdisp chains them.
 struct UvPair {
     double mu, r0, sig, beta;
+    double ir0;  // 1 / r0, so that start and composition need one division fewer each
 };
 
 __device__ __forceinline__ UvPair uv_prepare(double eps_th, const double r[3], const double g[3])
@@ -770,19 +781,19 @@ __device__ __forceinline__ UvPair uv_prepare(double eps_th, const double r[3], c
     UvPair p;
     p.mu = -eps_th;
     p.r0 = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    p.ir0 = 1.0 / p.r0;
     p.sig = r[0] * g[0] + r[1] * g[1] + r[2] * g[2];
     const double v2 = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
-    p.beta = 2.0 * p.mu / p.r0 - v2;
+    p.beta = 2.0 * p.mu * p.ir0 - v2;
     return p;
 }
 
 // second-order Taylor start s(dt) = dt/r0 - sig dt^2 / (2 r0^3)
 __device__ __forceinline__ double uv_start(const UvPair &p, double dt)
 {
-    double s = dt / p.r0;
-    s = s - p.sig * s * s / (2.0 * p.r0);
-    if (!(s > 0.0)) s = dt / p.r0;
-    return s;
+    const double s1 = dt * p.ir0;
+    const double s = s1 - p.sig * s1 * s1 * (0.5 * p.ir0);
+    return (s > 0.0) ? s : s1;
 }
 
 // Safeguarded Newton on F(s) = t(s) - dt, F' = r(s) > 0, with the bracket [lo, hi]
@@ -845,10 +856,11 @@ __device__ __forceinline__ void uv_compose(const UvPair &p, double s, const doub
     stumpff(p.beta * s * s, c);
     const double s2c2 = s * s * c[2], s3c3 = s * s * s * c[3];
     const double rr = p.r0 * c[0] + p.sig * s * c[1] + p.mu * s2c2;
-    const double fm1 = -p.mu * s2c2 / p.r0;
+    const double irr = 1.0 / rr;
+    const double fm1 = -p.mu * s2c2 * p.ir0;
     const double gmdt = -p.mu * s3c3;
-    const double fdot = -p.mu * s * c[1] / (rr * p.r0);
-    const double gdm1 = -p.mu * s2c2 / rr;
+    const double fdot = -p.mu * s * c[1] * (irr * p.ir0);
+    const double gdm1 = -p.mu * s2c2 * irr;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         h[k] = (fm1 * r[k] + gmdt * g[k]) * 0.5;
