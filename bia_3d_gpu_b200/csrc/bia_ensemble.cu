@@ -55,7 +55,7 @@ struct EnsArgs {
     double *part;
     unsigned long long *stats;
     PairParams P;
-    const MlpHead *heads;  // BIA_METHOD_LEARNED
+    const MlpImage *heads;  // BIA_METHOD_LEARNED
 };
 
 template <int M>
@@ -299,7 +299,7 @@ static int ens_enqueue_step(bia_context *ctx, bia_ensemble *E, const bia_config 
     A.P.abserr = cfg->rkf_abserr;
     A.P.itr = cfg->itr;
     A.P.method = cfg->method;
-    A.heads = (const MlpHead *)ctx->heads.ptr;
+    A.heads = (const MlpImage *)ctx->heads.ptr;
     const unsigned grid = (unsigned)((E->nitems + kEnsWarps - 1) / kEnsWarps);
     if (cfg->method == BIA_METHOD_LEARNED) {
         if (!ctx->heads_loaded || !ens_learned_setup()) return BIA_ERR_INVALID_ARGUMENT;

@@ -11,12 +11,14 @@ namespace bia {
 
 // A learned CTA: 8 warps, one warp-block each, two CTAs per SM, in three phases.
 //  1. Each lane classifies its pairs (hyperbolic head, elliptic head, plain) and writes the
-//     head inputs of its learned pairs into a CTA-wide row list in shared memory (packed
-//     BF16 pairs; hyperbolic rows first; offsets from a CTA scan of the per-lane counts).
-//     With a pair mask from the split step's rest kernel only the masked pairs are
-//     classified (and solved); the others are the rest kernel's.
-//  2. The CTA evaluates each head on its rows in full 256-row blocks on the tensor cores
-//     (mlp_tc.cuh) and writes each row's output over its input.
+//     head input of each learned pair (packed BF16) into the pair's own row slot
+//     (warp, lane, k) in shared memory.  With a pair mask from the split step's rest
+//     kernel only the masked pairs are classified (and solved); the others are the rest
+//     kernel's.
+//  2. A CTA scan of the per-lane counts numbers the learned pairs of each head in thread
+//     and bit order; the CTA evaluates each head on its pairs in full 256-row blocks on
+//     the tensor cores (mlp_tc.cuh), each thread finding its row's slot from the scan, and
+//     writes each row's output over its input.
 //  3. Each warp finishes its learned pairs from the stored guesses (FP32 correction, FP64
 //     Halley step, composition; the plain solver where the FP64 step does not settle),
 //     then its plain pairs with the universal-variable solver, with no CTA barrier.
@@ -70,11 +72,12 @@ struct LearnedBlockIn {
     const double *x, *y, *z, *u, *v, *w, *q;
     int n;
     double eps_th, dt;
-    const MlpHead *heads;
+    const MlpImage *heads;
 };
 
-// Dynamic shared memory of a learned CTA: the MLP image, the warps' column tiles, the row
-// list; base aligned to 1024 bytes.
+// Dynamic shared memory of a learned CTA: the MLP image, the warps' column tiles (the
+// column particles of all warps, then their column sums: the first 4 KB of the sums hold
+// the row numbering of phase 2), the row slots; base aligned to 1024 bytes.
 struct LearnedSmem {
     MlpSmem *mlp;
     double *tiles;
@@ -103,9 +106,11 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
 {
     MlpSmem &S = *M.mlp;
     const int warp = threadIdx.x >> 5;
-    double *ws = M.tiles + warp * kTileSmemDoubles;
-    double *wacc = ws + 7 * 32;
+    double *ws = M.tiles + warp * 7 * 32;
+    double *wacc = M.tiles + kLearnedWarps * 7 * 32 + warp * 6 * 32;
+    uint32_t *dec = reinterpret_cast<uint32_t *>(M.tiles + kLearnedWarps * 7 * 32);  // phase 2 only
     uint32_t *rows = M.rows;
+    uint32_t *myrows = rows + warp * 1024 + lane * 32;  // slot k: the pair with column (lane + k) mod 32
     counters_zero(cnt);
     double si[7];
 #pragma unroll
@@ -119,8 +124,6 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
         load_particle(B.x, B.y, B.z, B.u, B.v, B.w, B.q, n, bj * 32 + lane, sj);
 #pragma unroll
         for (int c = 0; c < 7; c++) ws[c * 32 + lane] = sj[c];
-#pragma unroll
-        for (int c = 0; c < 6; c++) wacc[c * 32 + lane] = 0.0;
         __syncwarp();
     }
     const int i = bi * 32 + lane;
@@ -140,6 +143,7 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
             LearnedPair L;
             learned_prepare(eps_ij, dt, r, g, L);
             const unsigned bit = 1u << k;
+            if (L.kind != kLearnedPlain) myrows[k] = pack_bf16(L.x0, L.x1);
             if (L.kind == kLearnedHyp) mh |= bit;
             else if (L.kind == kLearnedEll) me |= bit;
             else mr |= bit;
@@ -158,6 +162,7 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
                     LearnedPair L;
                     learned_prepare(eps_ij, dt, r, g, L);
                     kind = L.kind;
+                    if (kind != kLearnedPlain) myrows[k] = pack_bf16(L.x0, L.x1);
                 }
                 if (kind == kLearnedHyp) mh |= bit;
                 else if (kind == kLearnedEll) me |= bit;
@@ -165,26 +170,13 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
             }
         }
     }
+    // each thread's first row number per head (thread order, then bit order) and its masks
     int oh, oe, rh, re;
     cta_scan2(S, __popc(mh), __popc(me), oh, oe, rh, re);
-    oe += rh;  // elliptic rows follow the hyperbolic ones
-    {
-        int ih = oh, ie = oe;
-        unsigned m = mh | me;
-        while (m) {
-            const int k = __ffs(m) - 1;
-            m &= m - 1u;
-            const int src = (lane + k) & 31;
-            const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
-            const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
-            const double eps_ij = hq ? B.eps_th * si[6] * ws[6 * 32 + src] : B.eps_th;
-            LearnedPair L;
-            learned_prepare(eps_ij, dt, r, g, L);
-            const uint32_t x01 = pack_bf16(L.x0, L.x1);
-            if ((mh >> k) & 1u) rows[ih++] = x01;
-            else rows[ie++] = x01;
-        }
-    }
+    dec[threadIdx.x] = (uint32_t)oh;
+    dec[kMlpThreads + threadIdx.x] = (uint32_t)oe;
+    dec[2 * kMlpThreads + threadIdx.x] = mh;
+    dec[3 * kMlpThreads + threadIdx.x] = me;
     __syncthreads();
 
     // 2. the heads on the tensor cores, 256 rows per evaluation; the head already in shared
@@ -194,7 +186,8 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
     for (int pass = 0; pass < 2; pass++) {
         const bool hyp = (pass == 0) != ell_first;
         const int head = hyp ? kHeadHyp : kHeadEll;
-        const int r0 = hyp ? 0 : rh;
+        const uint32_t *first = dec + (hyp ? 0 : kMlpThreads);
+        const uint32_t *bits = dec + (hyp ? 2 : 3) * kMlpThreads;
         const int nr = hyp ? rh : re;
         if (nr == 0) continue;  // uniform
         if (S.head != head) {
@@ -204,14 +197,29 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
         for (int b = 0; b < nr; b += kMlpThreads) {
             const int row = b + (int)threadIdx.x;
             const bool valid = row < nr;
-            const uint32_t x01 = valid ? rows[r0 + row] : 0u;
+            int slot = 0;
+            if (valid) {
+                // the row's owner: the last thread whose first row is <= row (first[] does not
+                // decrease), then the (row - first)-th set bit of its mask
+                int o = 0;
+#pragma unroll
+                for (int step = kMlpThreads / 2; step > 0; step >>= 1)
+                    if (first[o + step] <= (uint32_t)row) o += step;
+                const int k = (int)__fns(bits[o], 0, row - (int)first[o] + 1);
+                slot = (o >> 5) * 1024 + (o & 31) * 32 + k;
+            }
+            const uint32_t x01 = valid ? rows[slot] : 0u;
             bool ok;
             const float y = mlp_eval_cta(S, x01, phase, ok);
             if (!ok) timed_out = true;
-            if (valid) rows[r0 + row] = __float_as_uint(ok ? y : __int_as_float(0x7fc00000));
+            if (valid) rows[slot] = __float_as_uint(ok ? y : __int_as_float(0x7fc00000));
         }
     }
     __syncthreads();
+    // the row numbering is read: the column sums start from zero
+#pragma unroll
+    for (int c = 0; c < 6; c++) wacc[c * 32 + lane] = 0.0;
+    __syncwarp();
 
     // 3. learned pairs from their guesses, per warp.  A warp without learned pairs walks the
     // rotation offsets instead (all its pairs plain; column sums by shuffle, no shared adds);
@@ -248,7 +256,6 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
         }
         mr = 0u;
     } else {
-        int ih = oh, ie = oe;
         unsigned m = mh | me;
         for (;;) {
             const bool busy = (m != 0u);
@@ -258,7 +265,7 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
                 const int k = __ffs(m) - 1;
                 m &= m - 1u;
                 const bool is_h = (mh >> k) & 1u;
-                const float y = __uint_as_float(rows[is_h ? ih++ : ie++]);
+                const float y = __uint_as_float(myrows[k]);
                 const int j = (lane + k) & 31;
                 double r[3], g[3], h[6];
 #pragma unroll

@@ -49,7 +49,7 @@ struct StepArgs {
     int n, nb, npad;
     double eps_th;
     PairParams P;
-    const MlpHead *heads;  // BIA_METHOD_LEARNED
+    const MlpImage *heads;  // BIA_METHOD_LEARNED
     // split learned step: the rest kernel's pair masks (32 words per listed warp-block),
     // the list of warp-blocks with masked pairs and its length
     uint32_t *lmask;
@@ -618,7 +618,7 @@ int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
     U.nb = nb;
     U.npad = nb * 32;
     U.dt = cfg->dt;
-    A.heads = (const MlpHead *)ctx->heads.ptr;
+    A.heads = (const MlpImage *)ctx->heads.ptr;
     const bool learned = cfg->method == BIA_METHOD_LEARNED;
     bool split = false;
     if (learned) {
@@ -760,10 +760,18 @@ int bia_context_set_heads(bia_context *ctx, const void *blob, size_t bytes)
     memcpy(&nheads, b + 12, 4);
     if (memcmp(b, "BIAHEAD1", 8) != 0 || version != 1 || nheads != (uint32_t)kMlpHeads)
         return BIA_ERR_INVALID_ARGUMENT;
+    // the kernels' image of each head (weights in the shared-memory operand layout)
+    MlpImage img[kMlpHeads];
+    for (int h = 0; h < kMlpHeads; h++) {
+        MlpHead H;
+        memcpy(&H, b + 16 + (size_t)h * sizeof(MlpHead), sizeof(MlpHead));
+        memset(&img[h], 0, sizeof(MlpImage));
+        mlp_image_from_head(H, img[h]);
+    }
     cudaError_t e = cudaSetDevice(ctx->device);
-    if (e == cudaSuccess) e = ctx->heads.reserve(kMlpHeads * sizeof(MlpHead));
+    if (e == cudaSuccess) e = ctx->heads.reserve(kMlpHeads * sizeof(MlpImage));
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(ctx->heads.ptr, b + 16, kMlpHeads * sizeof(MlpHead), cudaMemcpyHostToDevice, ctx->stream);
+        e = cudaMemcpyAsync(ctx->heads.ptr, img, kMlpHeads * sizeof(MlpImage), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = ctx->stream ? cudaStreamSynchronize(ctx->stream) : cudaDeviceSynchronize();
     if (e != cudaSuccess) return cuda_status(e);
     ctx->heads_loaded = true;
@@ -797,7 +805,7 @@ int bia_context_autotune(bia_context *ctx, const bia_config *cfg, int n, double 
     A.eps_th = cfg->eps_th;
     A.P.dt = cfg->dt; A.P.err = cfg->err; A.P.relerr = cfg->rkf_relerr; A.P.abserr = cfg->rkf_abserr;
     A.P.itr = cfg->itr; A.P.method = cfg->method;
-    A.heads = (const MlpHead *)ctx->heads.ptr;
+    A.heads = (const MlpImage *)ctx->heads.ptr;
     A.lmask = nullptr;
     const int det = cfg->deterministic ? 1 : 0;
     A.part = det ? (double *)ctx->part.ptr : (double *)ctx->acc.ptr;
@@ -1140,7 +1148,7 @@ extern "C" int bia_step_noalloc(const bia_config *cfg, int n, double *x, double 
 // ---------------------------------------------------------------------------------------
 // Head evaluation on its own (tests of the tensor-core network path).
 namespace bia {
-__global__ void __launch_bounds__(kMlpThreads, 1) bia_head_eval_kernel(const MlpHead *heads, int head, int n,
+__global__ void __launch_bounds__(kMlpThreads, 1) bia_head_eval_kernel(const MlpImage *heads, int head, int n,
                                                                       const float *in, float *out,
                                                                       unsigned long long *timeouts)
 {
@@ -1182,7 +1190,7 @@ int bia_learned_head_eval(bia_context *ctx, int head, int n, const float *in, fl
     int blocks = (n + kMlpThreads - 1) / kMlpThreads;
     if (blocks > 4096) blocks = 4096;
     bia_head_eval_kernel<<<blocks, kMlpThreads, 1024 + sizeof(MlpSmem), ctx->stream>>>(
-        (const MlpHead *)ctx->heads.ptr, head, n, in, out, timeouts);
+        (const MlpImage *)ctx->heads.ptr, head, n, in, out, timeouts);
     e = cudaGetLastError();
     unsigned long long h = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&h, timeouts, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);

@@ -27,7 +27,9 @@
 #pragma once
 #include <cuda_bf16.h>
 
+#include <cstddef>
 #include <cstdint>
+#include <cstring>
 
 namespace bia {
 
@@ -45,6 +47,16 @@ struct MlpHead {
 };
 static_assert(sizeof(MlpHead) == 19472, "learned_heads.bin head record");
 constexpr int kMlpHeads = 2;  // 0 elliptic, 1 hyperbolic
+
+// A head as the kernels keep it in device memory: the weights already in the shared-memory
+// operand layout (kmajor_off below; W1 at byte 0, W2 at 2048, W3 at 10240, as in MlpSmem),
+// then the FP32 vectors in MlpSmem's order, so that loading a head is a straight copy.
+constexpr int kMlpWeightBytes = (kMlpHidden * kMlpK1 + 2 * kMlpHidden * kMlpHidden) * 2;  // 18432
+struct MlpImage {
+    alignas(16) uint8_t w[kMlpWeightBytes];
+    float b1[kMlpHidden], b2[kMlpHidden], b3[kMlpHidden], w4[kMlpHidden], b4[4];
+};
+static_assert(sizeof(MlpImage) == 19472, "head image");
 
 // Shared-memory image of one head and the activation tile (1024-aligned parts).  Each
 // warpgroup's layer-1 rows (K = 16, 4 KB) live at the start of its own 16 KB half of the
@@ -69,7 +81,7 @@ __device__ __forceinline__ uint32_t smem_addr(const void *p)
     return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-__device__ __forceinline__ uint32_t kmajor_off(int row, int k, int K)
+__host__ __device__ __forceinline__ uint32_t kmajor_off(int row, int k, int K)
 {
     return (uint32_t)((((row >> 3) * (K >> 3)) + (k >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2);
 }
@@ -146,28 +158,41 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b)
     return *reinterpret_cast<const uint32_t *>(&v);
 }
 
-// One head's weights from global memory into the shared image (all threads, with a CTA
-// barrier at the end: the two warpgroups' MMAs read every weight).  The caller makes sure
-// that no MMA on the old weights is in flight.
-__device__ __forceinline__ void mlp_load_head(MlpSmem &S, const MlpHead *heads, int h)
+// The device image of a head from its file record (host side, once per set of heads).
+inline void mlp_image_from_head(const MlpHead &H, MlpImage &I)
 {
-    const int tid = threadIdx.x;
-    const MlpHead &H = heads[h];
-    for (int e = tid; e < kMlpHidden * kMlpK1; e += blockDim.x)
-        *(uint16_t *)(S.w1 + kmajor_off(e / kMlpK1, e % kMlpK1, kMlpK1)) = H.w1[e];
-    for (int e = tid; e < kMlpHidden * kMlpHidden; e += blockDim.x) {
+    for (int e = 0; e < kMlpHidden * kMlpK1; e++)
+        memcpy(I.w + kmajor_off(e / kMlpK1, e % kMlpK1, kMlpK1), &H.w1[e], 2);
+    for (int e = 0; e < kMlpHidden * kMlpHidden; e++) {
         const int n = e / kMlpHidden, k = e % kMlpHidden;
-        *(uint16_t *)(S.w2 + kmajor_off(n, k, kMlpHidden)) = H.w2[e];
-        *(uint16_t *)(S.w3 + kmajor_off(n, k, kMlpHidden)) = H.w3[e];
+        memcpy(I.w + 2048 + kmajor_off(n, k, kMlpHidden), &H.w2[e], 2);
+        memcpy(I.w + 10240 + kmajor_off(n, k, kMlpHidden), &H.w3[e], 2);
     }
-    for (int e = tid; e < kMlpHidden; e += blockDim.x) {
-        S.b1[e] = H.b1[e];
-        S.b2[e] = H.b2[e];
-        S.b3[e] = H.b3[e];
-        S.w4[e] = H.w4[e];
-    }
+    memcpy(I.b1, H.b1, sizeof(I.b1));
+    memcpy(I.b2, H.b2, sizeof(I.b2));
+    memcpy(I.b3, H.b3, sizeof(I.b3));
+    memcpy(I.w4, H.w4, sizeof(I.w4));
+    memcpy(I.b4, H.b4, sizeof(I.b4));
+}
+
+// One head from its device image into shared memory (all threads, 16-byte copies, with a
+// CTA barrier at the end: the two warpgroups' MMAs read every weight).  The caller makes
+// sure that no MMA on the old weights is in flight.
+__device__ __forceinline__ void mlp_load_head(MlpSmem &S, const MlpImage *heads, int h)
+{
+    static_assert(offsetof(MlpSmem, w2) == 2048 && offsetof(MlpSmem, w3) == 10240, "weight image layout");
+    static_assert(offsetof(MlpSmem, b2) == offsetof(MlpSmem, b1) + 256 && offsetof(MlpSmem, w4) == offsetof(MlpSmem, b1) + 768,
+                  "vector layout");
+    const int tid = threadIdx.x;
+    const MlpImage &I = heads[h];
+    const uint4 *src = reinterpret_cast<const uint4 *>(I.w);
+    uint4 *dst = reinterpret_cast<uint4 *>(S.w1);
+    for (int e = tid; e < kMlpWeightBytes / 16; e += blockDim.x) dst[e] = src[e];
+    const float4 *vs = reinterpret_cast<const float4 *>(I.b1);
+    float4 *vd = reinterpret_cast<float4 *>(S.b1);
+    for (int e = tid; e < 4 * kMlpHidden / 4; e += blockDim.x) vd[e] = vs[e];
     if (tid == 0) {
-        S.b4 = H.b4[0];
+        S.b4 = I.b4[0];
         S.head = h;
     }
     fence_async_smem();
