@@ -915,15 +915,6 @@ __device__ __forceinline__ int alg_classify(double eps_ij, const double r[3], co
     return alg_classify(eps_ij, r, g, E, Lsq);
 }
 
-// Necessary condition for pair_degenerate, from the universal-variable quantities: a pair
-// with g = 0 or with L = r x g rounding to zero has sig^2 within rounding of r0^2 |g|^2
-// (Lagrange: |L|^2 = r^2 g^2 - sig^2), so any pair below 1 - 1e-10 of it is not degenerate.
-__device__ __forceinline__ bool pair_maybe_degenerate(const UvPair &p, const double g[3])
-{
-    const double gsq = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
-    return gsq == 0.0 || p.sig * p.sig >= (1.0 - 1e-10) * (p.r0 * p.r0) * gsq;
-}
-
 // |g| == 0 or |L| == 0: the pair's frame is degenerate (counted apart from the other
 // universal-variable pairs)
 __device__ __forceinline__ bool pair_degenerate(const double r[3], const double g[3])

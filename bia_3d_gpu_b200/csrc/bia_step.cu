@@ -282,10 +282,13 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const 
 // (learned_filter) by the universal-variable solver, lanes walking the rotation offsets;
 // the filtered pairs are left as a per-lane mask, and each warp-block with any is appended
 // to the list that bia_pair_learned_list_kernel works through afterwards.  Deterministic
-// mode writes every partial slot here; the learned kernel adds onto them.
+// mode writes every partial slot here; the learned kernel adds onto them.  Its pairs are
+// counted as universal-variable pairs, degenerate ones included, as BIA_METHOD_UNIVERSAL
+// counts them (the exact degenerate test in this loop costs 7 % of the kernel).
 template <bool kDeterministic>
-__global__ void __launch_bounds__(kThreads, TileOccupancy<kMethodUniversal>::kMinBlocks)
-    bia_pair_rest_kernel(const StepArgs A)
+// Two CTAs per SM: at the universal-variable kernel's three the filter spills registers
+// inside the rotation loop (measured at n = 32768: 11.2 ms at three, 10.9 ms at two).
+__global__ void __launch_bounds__(kThreads, 2) bia_pair_rest_kernel(const StepArgs A)
 {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -326,10 +329,10 @@ __global__ void __launch_bounds__(kThreads, TileOccupancy<kMethodUniversal>::kMi
                 uv_compose(p, s, r, g, h);
                 cnt.it_uv += it;
                 if (it > kUvItMax) cnt.nonconverged++;
-                cnt.cls[pair_maybe_degenerate(p, g) && pair_degenerate(r, g) ? kDegenerate : kUniversal]++;
+                cnt.cls[kUniversal]++;
                 count_nonfinite(h, cnt);
             } else {
-                cnt.cls[pair_degenerate(r, g) ? kDegenerate : kUniversal]++;
+                cnt.cls[kUniversal]++;
             }
         }
         const int back = (lane - k) & 31;
