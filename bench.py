@@ -72,11 +72,13 @@ METHODS = {"rkf": 0, "alg": 1, "universal": 2, "learned": 3}
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the dominant pair
 # kernel, from one ncu capture at n = 16384 of the same workload and method, scaled by the
 # pairs per launch (both the partial sums and any local-memory traffic grow with the pairs):
-#   (workload, method) -> (pairs in the capture, bytes in the capture)
+#   (workload, method, learned layout) -> (pairs in the capture, bytes in the capture)
+# The split learned step is its two kernels (the rest kernel writes every partial slot, the
+# list kernel reads and writes back the slots of the warp-blocks it solves).
 TRAFFIC = {
-    ("plummer_32768", 3): (16384 * 16383 // 2, 1.132e6 + 351.829e6),       # learned kernel
-    ("coulomb_cube_32768", 3): (16384 * 16383 // 2, 2.912e6 + 353.567e6),  # learned kernel
-    ("coulomb_cube_32768", 1): (16384 * 16383 // 2, 100.488e6 + 3169.538e6),  # phase-locked ALG
+    ("plummer_32768", 3, "split"): (16384 * 16383 // 2, (0.830e6 + 354.303e6) + (256.362e6 + 201.966e6)),
+    ("coulomb_cube_32768", 3, "split"): (16384 * 16383 // 2, (1.054e6 + 361.449e6) + (422.594e6 + 362.519e6)),
+    ("coulomb_cube_32768", 1, None): (16384 * 16383 // 2, 100.488e6 + 3169.538e6),  # phase-locked ALG
 }
 
 
@@ -114,6 +116,9 @@ def parse():
     ap.add_argument("--no-universal", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="use the library's built-in kernel-shape rules instead of timing the shapes first "
+                         "(for profiler runs, whose serialised launches would mislead the autotuner)")
     return ap.parse_args()
 
 
@@ -468,11 +473,11 @@ def main():
 
     # the ALG pair-kernel shape for this size, chosen by the autotuner on this GPU
     tuned = None
-    if method == 1 or (method != 1 and not args.no_plain):
+    if (method == 1 or (method != 1 and not args.no_plain)) and not args.no_autotune:
         cfg_alg = default_config(eps_th=eps, dt=dt, method=1)
         var, tms = solver.autotune(d_state, cfg_alg, q=d_q)
         tuned = {"alg_shape": ("tiles8", "phase16", "phase32")[var], "ms": tms}
-    if method == 3:
+    if method == 3 and not args.no_autotune:
         lvar, lms = solver.autotune(d_state, cfg, q=d_q)
         tuned = dict(tuned or {}, learned_layout=("one_kernel", "split")[lvar], learned_ms=lms)
     total_ms, clocks, stats, (kern_ms, kern_launches) = timed_steps(cfg, steps, sample_clocks=True)
@@ -508,7 +513,10 @@ def main():
     nb_blocks = (n + 31) // 32
     nwb = nb_blocks * (nb_blocks + 1) // 2
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
-    split = bool(tuned and tuned.get("learned_layout") == "split")
+    if tuned and "learned_layout" in tuned:
+        split = tuned["learned_layout"] == "split"
+    else:  # the library's rule: split from two 32-warp CTAs per SM up
+        split = method == 3 and (nwb + 31) // 32 >= 2 * sms
     if method == 3:
         kernel_name = ("bia_pair_rest_kernel<true> + bia_pair_learned_list_kernel<true> (one timed interval)"
                        if split else "bia_pair_learned_kernel<true>")
@@ -525,8 +533,9 @@ def main():
     peak = measure_fp64_peak(local)
     achieved = per_launch_flops / per_launch_s / 1e12
     traffic = None
-    if args.n is None and (args.workload, method) in TRAFFIC:
-        tp, tb = TRAFFIC[(args.workload, method)]
+    tkey = (args.workload, method, ("split" if split else "one_kernel") if method == 3 else None)
+    if args.n is None and tkey in TRAFFIC:
+        tp, tb = TRAFFIC[tkey]
         traffic = tb * pairs / tp
     roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak if peak else None, "traffic": traffic,
