@@ -780,8 +780,10 @@ __device__ __forceinline__ UvPair uv_prepare(double eps_th, const double r[3], c
 {
     UvPair p;
     p.mu = -eps_th;
-    p.r0 = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-    p.ir0 = 1.0 / p.r0;
+    // one reciprocal square root for both r0 and 1/r0 (rsqrt: within 1 ulp)
+    const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    p.ir0 = rsqrt(r2);
+    p.r0 = (r2 > 0.0) ? r2 * p.ir0 : 0.0;
     p.sig = r[0] * g[0] + r[1] * g[1] + r[2] * g[2];
     const double v2 = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
     p.beta = 2.0 * p.mu * p.ir0 - v2;
@@ -807,18 +809,21 @@ __device__ __forceinline__ double uv_start(const UvPair &p, double dt)
 // bracket at least halves every two iterations: on hyperbolic branches Newton from far
 // above the root moves only ~1/sqrt(-beta) per step.  Returns the iterations
 // (kUvItMax + 1 when the cap was reached).
-__device__ __forceinline__ int uv_iterate(const UvPair &p, double dt, double &s_io)
+// ifp (optional): 1 / F' at the last evaluation, for uv_compose (F' = r(s)).
+__device__ __forceinline__ int uv_iterate(const UvPair &p, double dt, double &s_io, double *ifp = nullptr)
 {
     double c[4];
     double s = s_io;
     double lo = 0.0, hi = -1.0, dx = 1e300, dxold = 1e300;
+    double ifp_last = 0.0;
     int it;
     for (it = 1; it <= kUvItMax; it++) {
         stumpff(p.beta * s * s, c);
         const double F = p.r0 * s * c[1] + p.sig * s * s * c[2] + p.mu * s * s * s * c[3] - dt;
         const double Fp = p.r0 * c[0] + p.sig * s * c[1] + p.mu * s * s * c[2];
         if (F == 0.0) break;
-        const double step = F / Fp;
+        ifp_last = 1.0 / Fp;
+        const double step = F * ifp_last;
         if (Fp > 0.0 && fabs(step) <= 4.0 * 2.220446049250313e-16 * fabs(s)) {
             s = s - step;  // converged: the remaining correction is a few ulps
             break;
@@ -837,6 +842,7 @@ __device__ __forceinline__ int uv_iterate(const UvPair &p, double dt, double &s_
         if (newton && dx <= 1e-10 * fabs(s)) break;
     }
     s_io = s;
+    if (ifp) *ifp = ifp_last;
     return it;
 }
 
@@ -853,15 +859,18 @@ __device__ __forceinline__ double uv_halley_step(const UvPair &p, double dt, dou
 }
 
 // Half-displacement from the solved s: f - 1, g - dt, f', g' - 1 from the Stumpff
-// functions (no cancellation at small s).
+// functions (no cancellation at small s).  irr_hint (optional, 0: none): an approximation
+// of 1/r(s), such as uv_iterate's last 1/F'; within 1e-8 of it one Newton-Raphson step for
+// the reciprocal (x + x (1 - r x)) gives 1/r(s) to ~1e-16, else 1/r(s) is divided out.
 __device__ __forceinline__ void uv_compose(const UvPair &p, double s, const double r[3], const double g[3],
-                                           double h[6])
+                                           double h[6], double irr_hint = 0.0)
 {
     double c[4];
     stumpff(p.beta * s * s, c);
     const double s2c2 = s * s * c[2], s3c3 = s * s * s * c[3];
     const double rr = p.r0 * c[0] + p.sig * s * c[1] + p.mu * s2c2;
-    const double irr = 1.0 / rr;
+    const double e = fma(-rr, irr_hint, 1.0);
+    const double irr = (irr_hint != 0.0 && fabs(e) <= 1e-8) ? fma(irr_hint, e, irr_hint) : 1.0 / rr;
     const double fm1 = -p.mu * s2c2 * p.ir0;
     const double gmdt = -p.mu * s3c3;
     const double fdot = -p.mu * s * c[1] * (irr * p.ir0);
@@ -881,8 +890,9 @@ __device__ __forceinline__ int uv_halfdisp(double eps_th, double dt, const doubl
     if (dt == 0.0) return 0;
     const UvPair p = uv_prepare(eps_th, r, g);
     double s = uv_start(p, dt);
-    const int it = uv_iterate(p, dt, s);
-    uv_compose(p, s, r, g, h);
+    double ifp;
+    const int it = uv_iterate(p, dt, s, &ifp);
+    uv_compose(p, s, r, g, h, ifp);
     return it;
 }
 

@@ -325,8 +325,9 @@ __global__ void __launch_bounds__(kThreads, 2) bia_pair_rest_kernel(const StepAr
                 learned |= 1u << k;
             } else if (A.P.dt != 0.0) {
                 double s = uv_start(p, A.P.dt);
-                const int it = uv_iterate(p, A.P.dt, s);
-                uv_compose(p, s, r, g, h);
+                double ifp;
+                const int it = uv_iterate(p, A.P.dt, s, &ifp);
+                uv_compose(p, s, r, g, h, ifp);
                 cnt.it_uv += it;
                 if (it > kUvItMax) cnt.nonconverged++;
                 cnt.cls[kUniversal]++;

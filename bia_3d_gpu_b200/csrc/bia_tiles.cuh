@@ -23,7 +23,7 @@ namespace bia {
 #define BIA_ALG_MIN_BLOCKS 3
 #endif
 #ifndef BIA_UV_MIN_BLOCKS
-#define BIA_UV_MIN_BLOCKS 3
+#define BIA_UV_MIN_BLOCKS 2  // 3 spills in the rotation loop: 9.4 ms vs 8.6 ms at n = 32768
 #endif
 template <int M> struct TileOccupancy { static constexpr int kMinBlocks = 1; };
 template <> struct TileOccupancy<kMethodAlg> { static constexpr int kMinBlocks = BIA_ALG_MIN_BLOCKS; };
