@@ -518,8 +518,8 @@ def main():
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     if tuned and "learned_layout" in tuned:
         split = tuned["learned_layout"] == "split"
-    else:  # the library's rule: split from two 32-warp CTAs per SM up
-        split = method == 3 and (nwb + 31) // 32 >= 2 * sms
+    else:  # the library's rule: the learned step splits at every size
+        split = method == 3
     if method == 3:
         kernel_name = ("bia_pair_rest_kernel<true> + bia_pair_learned_list_kernel<true> (one timed interval)"
                        if split else "bia_pair_learned_kernel<true>")

@@ -34,6 +34,8 @@ struct bia_ensemble {
     double *d_part = nullptr;          // partial sums
     double *d_scratch = nullptr;       // [nitems + nparticles] energy scratch
     double *d_energy = nullptr;        // [2 nsys] KE, PE per system
+    // learned step: list length, list of items holding learned pairs, 32 masks per listed item
+    unsigned int *d_split = nullptr;   // [4 + nitems + 32 nitems]
     size_t part_doubles = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -56,6 +58,8 @@ struct EnsArgs {
     unsigned long long *stats;
     PairParams P;
     const MlpImage *heads;  // BIA_METHOD_LEARNED
+    unsigned int *wbcount, *wblist;  // learned step: the rest kernel's list of items
+    uint32_t *lmask;                 // and their pair masks
 };
 
 template <int M>
@@ -131,55 +135,105 @@ static int ens_phase_setup()
     return sms_of[dev];
 }
 
-// Learned mixed-precision form over the item table (bia_learned_block.cuh): CTAs of
-// kLearnedWarps warps, one item each.
-__global__ void __launch_bounds__(kMlpThreads, 2) ens_pair_learned_kernel(const EnsArgs A)
+// Learned step over the item table, first kernel: each item's plain pairs
+// (rest_block_solve, as bia_pair_rest_kernel); items holding pairs in the heads' domain are
+// listed with their masks for ens_pair_learned_list_kernel.
+__global__ void __launch_bounds__(kEnsThreads, 2) ens_pair_rest_kernel(const EnsArgs A)
 {
-    extern __shared__ uint8_t ens_learned_raw[];
-    const LearnedSmem M = learned_smem(ens_learned_raw);
+    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    const long long t = (long long)blockIdx.x * kLearnedWarps + warp;
-    const bool live = t < A.nitems;
-    int s = 0, bi = 0, bj = 0;
-    if (live) {
-        const uint2 it = A.items[t];
-        s = (int)it.x;
-        bi = (int)(it.y & 0xffffu);
-        bj = (int)(it.y >> 16);
-    }
+    const long long t = (long long)blockIdx.x * kEnsWarps + (threadIdx.x >> 5);
+    if (t >= A.nitems) return;  // warp-uniform
+    const uint2 it = A.items[t];
+    const int s = (int)it.x;
+    const int bi = (int)(it.y & 0xffffu), bj = (int)(it.y >> 16);
     const int base = A.off[s];
     const int n = A.off[s + 1] - base;
-    const LearnedBlockIn B = {A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base,
-                              A.q ? A.q + base : nullptr, n, A.eps[s], A.P.dt, A.heads};
     double racc[6], cacc[6];
     PairCounters cnt;
-    mlp_setup(*M.mlp);
-    uint32_t phase = 0;
-    const bool timed_out = learned_block_solve(M, B, bi, bj, lane, live, racc, cacc, cnt, phase);
-    mlp_teardown(*M.mlp, phase);
-    if (timed_out && threadIdx.x == 0 && !live) atomicAdd(&A.stats[kStatTimeouts], 1ull);
-    if (!live) return;  // warp-uniform; no barrier follows
+    const uint32_t learned = rest_block_solve(A.x + base, A.y + base, A.z + base, A.u + base, A.v + base,
+                                              A.w + base, A.q ? A.q + base : nullptr, n, A.eps[s], A.P.dt, bi,
+                                              bj, lane, racc, cacc, cnt);
     flush_counters(cnt, A.stats, lane);
     const int nb = (n + 31) / 32;
     write_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
+    if (__any_sync(full, learned != 0u)) {
+        unsigned int slot = 0;
+        if (lane == 0) slot = atomicAdd(A.wbcount, 1u);
+        slot = __shfl_sync(full, slot, 0);
+        A.lmask[(size_t)slot * 32 + lane] = learned;
+        if (lane == 0) A.wblist[slot] = (unsigned int)t;
+    }
 }
 
-static bool ens_learned_setup()
+// Learned step, second kernel: persistent CTAs work through the listed items eight at a
+// time (one per warp, of any systems), solve their masked pairs with the learned warp-block
+// and add the sums onto the rest kernel's partials.
+__global__ void __launch_bounds__(kMlpThreads, 2) ens_pair_learned_list_kernel(const EnsArgs A)
+{
+    extern __shared__ uint8_t ens_list_raw[];
+    const LearnedSmem M = learned_smem(ens_list_raw);
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const long long count = (long long)*A.wbcount;
+    mlp_setup(*M.mlp);
+    uint32_t phase = 0;
+    for (long long g0 = (long long)blockIdx.x * kLearnedWarps; g0 < count;
+         g0 += (long long)gridDim.x * kLearnedWarps) {
+        const long long e = g0 + warp;
+        const bool live = e < count;
+        int s = 0, bi = 0, bj = 0;
+        uint32_t mask = 0u;
+        if (live) {
+            const uint2 it = A.items[A.wblist[e]];
+            s = (int)it.x;
+            bi = (int)(it.y & 0xffffu);
+            bj = (int)(it.y >> 16);
+            mask = A.lmask[(size_t)e * 32 + lane];
+        }
+        const int base = A.off[s];
+        const int n = A.off[s + 1] - base;
+        const LearnedBlockIn B = {A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base,
+                                  A.q ? A.q + base : nullptr, n, A.eps[s], A.P.dt, A.heads};
+        double racc[6], cacc[6];
+        PairCounters cnt;
+        const bool timed_out = learned_block_solve(M, B, bi, bj, lane, live, racc, cacc, cnt, phase, &mask);
+        if (timed_out && threadIdx.x == 0 && !live) atomicAdd(&A.stats[kStatTimeouts], 1ull);
+        if (live) {
+            flush_counters(cnt, A.stats, lane);
+            const int nb = (n + 31) / 32;
+            add_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
+        }
+    }
+    mlp_teardown(*M.mlp, phase);
+}
+
+// Once per device: shared-memory opt-in of the learned ensemble kernels; returns the grid of
+// the persistent list kernel (resident CTAs, at least two per SM), 0 on failure.
+static int ens_learned_setup()
 {
     constexpr int kMaxDevices = 64;
     static std::mutex mu;
-    static int state_of[kMaxDevices] = {};
+    static int grid_of[kMaxDevices] = {};
+    static bool done_of[kMaxDevices] = {};
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return false;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 0;
     std::lock_guard<std::mutex> lk(mu);
-    if (state_of[dev] == 0) {
-        const bool ok = cudaFuncSetAttribute(ens_pair_learned_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)kLearnedSmemBytes) == cudaSuccess;
+    if (!done_of[dev]) {
+        const int bytes = (int)kLearnedSmemBytes;
+        int sms = 0, occ = 0;
+        bool ok = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(ens_pair_learned_list_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        bytes) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(ens_pair_learned_list_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        (int)cudaSharedmemCarveoutMaxShared) == cudaSuccess;
+        ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ens_pair_learned_list_kernel, kMlpThreads,
+                                                                 (size_t)bytes) == cudaSuccess;
         if (!ok) cudaGetLastError();
-        state_of[dev] = ok ? 1 : 2;
+        grid_of[dev] = ok ? sms * (occ > 2 ? occ : 2) : 0;
+        done_of[dev] = true;
     }
-    return state_of[dev] == 1;
+    return grid_of[dev];
 }
 
 struct EnsUpdateArgs {
@@ -284,7 +338,7 @@ __global__ void __launch_bounds__(256) ens_energy_kernel(const double *u, const 
 static int ens_enqueue_step(bia_context *ctx, bia_ensemble *E, const bia_config *cfg, double *x, double *y,
                             double *z, double *u, double *v, double *w, const double *q)
 {
-    EnsArgs A;
+    EnsArgs A{};
     A.x = x; A.y = y; A.z = z; A.u = u; A.v = v; A.w = w; A.q = q;
     A.off = E->d_off;
     A.part_off = E->d_part_off;
@@ -302,9 +356,20 @@ static int ens_enqueue_step(bia_context *ctx, bia_ensemble *E, const bia_config 
     A.heads = (const MlpImage *)ctx->heads.ptr;
     const unsigned grid = (unsigned)((E->nitems + kEnsWarps - 1) / kEnsWarps);
     if (cfg->method == BIA_METHOD_LEARNED) {
-        if (!ctx->heads_loaded || !ens_learned_setup()) return BIA_ERR_INVALID_ARGUMENT;
-        const unsigned lgrid = (unsigned)((E->nitems + kLearnedWarps - 1) / kLearnedWarps);
-        ens_pair_learned_kernel<<<lgrid, kMlpThreads, kLearnedSmemBytes, ctx->stream>>>(A);
+        // the split step of bia_step: the rest kernel, then the list kernel (the same
+        // per-warp-block arithmetic, so each system equals its own learned bia_step)
+        const int lsetup = ens_learned_setup();
+        if (!ctx->heads_loaded) return BIA_ERR_INVALID_ARGUMENT;
+        if (lsetup <= 0) return BIA_ERR_CUDA;
+        A.wbcount = E->d_split;
+        A.wblist = E->d_split + 4;
+        A.lmask = E->d_split + 4 + E->nitems;
+        cudaError_t e = cudaMemsetAsync(A.wbcount, 0, sizeof(unsigned int), ctx->stream);
+        if (e != cudaSuccess) return cuda_status(e);
+        ens_pair_rest_kernel<<<grid, kEnsThreads, 0, ctx->stream>>>(A);
+        const long long need = (E->nitems + kLearnedWarps - 1) / kLearnedWarps;
+        const unsigned lgrid = (unsigned)(need < lsetup ? need : lsetup);
+        ens_pair_learned_list_kernel<<<lgrid, kMlpThreads, kLearnedSmemBytes, ctx->stream>>>(A);
     } else {
         switch (cfg->method) {
     case BIA_METHOD_RKF: ens_pair_tiles_kernel<kMethodRkf><<<grid, kEnsThreads, 0, ctx->stream>>>(A); break;
@@ -348,6 +413,7 @@ static void ens_free(bia_ensemble *E)
     cudaFree(E->d_part);
     cudaFree(E->d_scratch);
     cudaFree(E->d_energy);
+    cudaFree(E->d_split);
     delete E;
 }
 
@@ -401,6 +467,7 @@ extern "C" int bia_ensemble_create(bia_context *ctx, int nsys, const int *sizes,
     ENS_ALLOC(E->d_part, part);
     ENS_ALLOC(E->d_scratch, nitems);
     ENS_ALLOC(E->d_energy, 2 * nsys);
+    ENS_ALLOC(E->d_split, 4 + 33 * nitems);
 #undef ENS_ALLOC
     if (e == cudaSuccess) e = cudaMemcpy(E->d_off, off.data(), sizeof(int) * (nsys + 1), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(E->d_psys, psys.data(), sizeof(int) * np, cudaMemcpyHostToDevice);

@@ -67,6 +67,69 @@ __device__ __forceinline__ void cta_scan2(MlpSmem &S, int a, int b, int &oa, int
 }
 
 
+// The split learned step's plain part of warp-block (bi, bj) of the system x..w[0, n)
+// (charges q, coupling eps_th): lanes walk the rotation offsets; every pair gets the
+// universal-variable prepare, then the heads' domain test on those quantities
+// (learned_filter); pairs outside it are solved here (uv_halfdisp in its pieces), the others
+// are left to the learned warp-block.  Returns the lane's mask of left pairs (bit k: column
+// (lane + k) mod 32) with the row sums racc and column sums cacc of the solved ones.  The
+// pairs are counted as universal-variable pairs, degenerate ones included, as
+// BIA_METHOD_UNIVERSAL counts them (the exact degenerate test costs 7 % here).
+__device__ __forceinline__ uint32_t rest_block_solve(const double *x, const double *y, const double *z,
+                                                     const double *u, const double *v, const double *w,
+                                                     const double *q, int n, double eps_th, double dt, int bi,
+                                                     int bj, int lane, double racc[6], double cacc[6],
+                                                     PairCounters &cnt)
+{
+    const unsigned full = 0xffffffffu;
+    const int i = bi * 32 + lane;
+    const bool diag = (bi == bj);
+    uint32_t learned = 0u;
+    double si[7], sj[7];
+    load_particle(x, y, z, u, v, w, q, n, i, si);
+    load_particle(x, y, z, u, v, w, q, n, bj * 32 + lane, sj);
+#pragma unroll
+    for (int c = 0; c < 6; c++) racc[c] = cacc[c] = 0.0;
+    counters_zero(cnt);
+    const int k0 = diag ? 1 : 0, k1 = diag ? 16 : 31;
+    for (int k = k0; k <= k1; k++) {
+        const int src = (lane + k) & 31;
+        double sc[7];
+#pragma unroll
+        for (int c = 0; c < 7; c++) sc[c] = __shfl_sync(full, sj[c], src);
+        const int j = bj * 32 + src;
+        const bool active = (!diag || k < 16 || lane < 16) && i < n && j < n;
+        double h[6] = {0, 0, 0, 0, 0, 0};
+        if (active) {
+            const double r[3] = {si[0] - sc[0], si[1] - sc[1], si[2] - sc[2]};
+            const double g[3] = {si[3] - sc[3], si[4] - sc[4], si[5] - sc[5]};
+            const double eps_ij = q ? eps_th * si[6] * sc[6] : eps_th;
+            const UvPair p = uv_prepare(eps_ij, r, g);
+            if (learned_filter(p, dt)) {
+                learned |= 1u << k;
+            } else if (dt != 0.0) {
+                double s = uv_start(p, dt);
+                double ifp;
+                const int it = uv_iterate(p, dt, s, &ifp);
+                uv_compose(p, s, r, g, h, ifp);
+                cnt.it_uv += it;
+                if (it > kUvItMax) cnt.nonconverged++;
+                cnt.cls[kUniversal]++;
+                count_nonfinite(h, cnt);
+            } else {
+                cnt.cls[kUniversal]++;
+            }
+        }
+        const int back = (lane - k) & 31;
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            racc[c] += h[c];
+            cacc[c] += __shfl_sync(full, h[c], back);
+        }
+    }
+    return learned;
+}
+
 // The system a warp-block belongs to: particles x..w[0, n) (and charges q), coupling eps_th.
 struct LearnedBlockIn {
     const double *x, *y, *z, *u, *v, *w, *q;

@@ -224,21 +224,8 @@ __device__ __forceinline__ void add_learned_sums(const StepArgs &A, int bi, int 
     const int jown = bj * 32 + lane;
     const size_t plane = (size_t)A.npad;
     if (kDeterministic) {
-        if (assign) {
-            write_partials(A.part, plane, bi, bj, lane, racc, cacc);
-        } else if (bi == bj) {
-            double *dst = A.part + (size_t)bi * 6 * plane;
-#pragma unroll
-            for (int c = 0; c < 6; c++) dst[c * plane + i] += racc[c] - cacc[c];
-        } else {
-            double *drow = A.part + (size_t)bj * 6 * plane;
-            double *dcol = A.part + (size_t)bi * 6 * plane;
-#pragma unroll
-            for (int c = 0; c < 6; c++) {
-                drow[c * plane + i] += racc[c];
-                dcol[c * plane + jown] -= cacc[c];
-            }
-        }
+        if (assign) write_partials(A.part, plane, bi, bj, lane, racc, cacc);
+        else add_partials(A.part, plane, bi, bj, lane, racc, cacc);
     } else if (bi == bj) {
 #pragma unroll
         for (int c = 0; c < 6; c++)
@@ -278,13 +265,10 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const 
     add_learned_sums<kDeterministic>(A, bi, bj, lane, racc, cacc, true);
 }
 
-// Split learned step, first kernel: every pair outside the heads' FP32 domain filter
-// (learned_filter) by the universal-variable solver, lanes walking the rotation offsets;
-// the filtered pairs are left as a per-lane mask, and each warp-block with any is appended
-// to the list that bia_pair_learned_list_kernel works through afterwards.  Deterministic
-// mode writes every partial slot here; the learned kernel adds onto them.  Its pairs are
-// counted as universal-variable pairs, degenerate ones included, as BIA_METHOD_UNIVERSAL
-// counts them (the exact degenerate test in this loop costs 7 % of the kernel).
+// Split learned step, first kernel: every warp-block's plain pairs (rest_block_solve); the
+// pairs in the heads' domain are left as a per-lane mask, and each warp-block with any is
+// appended to the list that bia_pair_learned_list_kernel works through afterwards.
+// Deterministic mode writes every partial slot here; the learned kernel adds onto them.
 template <bool kDeterministic>
 // Two CTAs per SM: at the universal-variable kernel's three the filter spills registers
 // inside the rotation loop (measured at n = 32768: 11.2 ms at three, 10.9 ms at two).
@@ -296,53 +280,10 @@ __global__ void __launch_bounds__(kThreads, 2) bia_pair_rest_kernel(const StepAr
     if (t >= A.nwb) return;  // warp-uniform
     int bi, bj;
     warp_block_coords(t, bi, bj);
-    const int i = bi * 32 + lane;
-    const bool diag = (bi == bj);
-    uint32_t learned = 0u;
-    double si[7], sj[7], racc[6], cacc[6];
-    load_particle(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, i, si);
-    load_particle(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, bj * 32 + lane, sj);
-#pragma unroll
-    for (int c = 0; c < 6; c++) racc[c] = cacc[c] = 0.0;
+    double racc[6], cacc[6];
     PairCounters cnt;
-    counters_zero(cnt);
-    const int k0 = diag ? 1 : 0, k1 = diag ? 16 : 31;
-    for (int k = k0; k <= k1; k++) {
-        const int src = (lane + k) & 31;
-        double sc[7];
-#pragma unroll
-        for (int c = 0; c < 7; c++) sc[c] = __shfl_sync(full, sj[c], src);
-        const int j = bj * 32 + src;
-        const bool active = (!diag || k < 16 || lane < 16) && i < A.n && j < A.n;
-        double h[6] = {0, 0, 0, 0, 0, 0};
-        if (active) {
-            const double r[3] = {si[0] - sc[0], si[1] - sc[1], si[2] - sc[2]};
-            const double g[3] = {si[3] - sc[3], si[4] - sc[4], si[5] - sc[5]};
-            const double eps_ij = A.q ? A.eps_th * si[6] * sc[6] : A.eps_th;
-            // uv_halfdisp in its pieces, the filter between them
-            const UvPair p = uv_prepare(eps_ij, r, g);
-            if (learned_filter(p, A.P.dt)) {
-                learned |= 1u << k;
-            } else if (A.P.dt != 0.0) {
-                double s = uv_start(p, A.P.dt);
-                double ifp;
-                const int it = uv_iterate(p, A.P.dt, s, &ifp);
-                uv_compose(p, s, r, g, h, ifp);
-                cnt.it_uv += it;
-                if (it > kUvItMax) cnt.nonconverged++;
-                cnt.cls[kUniversal]++;
-                count_nonfinite(h, cnt);
-            } else {
-                cnt.cls[kUniversal]++;
-            }
-        }
-        const int back = (lane - k) & 31;
-#pragma unroll
-        for (int c = 0; c < 6; c++) {
-            racc[c] += h[c];
-            cacc[c] += __shfl_sync(full, h[c], back);
-        }
-    }
+    const uint32_t learned = rest_block_solve(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P.dt, bi, bj,
+                                              lane, racc, cacc, cnt);
     flush_counters(cnt, A.stats, lane);
     add_learned_sums<kDeterministic>(A, bi, bj, lane, racc, cacc, true);
     if (__any_sync(full, learned != 0u)) {
@@ -463,14 +404,10 @@ static void split_buffer_carve(void *base, long long nwb, StepArgs &A)
     A.lmask = (uint32_t *)(b + 16 + (size_t)nwb * sizeof(uint32_t));
 }
 
-// Split learned steps (plain pairs in the rest kernel at the universal-variable kernel's
-// occupancy, learned pairs in the list kernel) from two 32-warp CTAs per SM up, as the
-// phase-locked ALG kernel.
-static bool learned_split(long long nwb)
-{
-    const int sms = phase_kernel_setup();
-    return sms > 0 && (nwb + 31) / 32 >= 2LL * sms;
-}
+// The learned step splits (plain pairs in the rest kernel, learned pairs in the list
+// kernel) at every size unless the autotuner chose the one-kernel layout: the ensemble takes
+// the same split, so each of its systems equals its own bia_step bit for bit.
+static bool learned_split(long long nwb) { return nwb > 0; }
 
 struct UpdateArgs {
     double *x, *y, *z, *u, *v, *w;
