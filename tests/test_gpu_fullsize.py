@@ -109,3 +109,39 @@ def test_plummer_full_step_matches_oracle(cuda):
     assert np.linalg.norm(new[3:] - ref[3:]) / np.linalg.norm(ref[3:]) <= 1e-12
     assert np.abs(new[:3] - ref[:3]).max() <= 1e-10
     assert np.abs(new[3:] - ref[3:]).max() <= 1e-12 * np.abs(ref[3:]).max()
+
+
+def test_cold_collapse_learned_next_to_plain_on_quad_subset(cuda):
+    """The cold collapse (uniform ball, zero velocities, dt = 5e-5) with the learned
+    mixed-precision form next to the plain FP64 form, on a seeded 4096-particle subset of
+    cold_ball_131072 evolved as its own system: one step of each against the oracle's step
+    (relative position and velocity error <= 1e-12), then the workload's 50 steps of each,
+    with the energy drift taken from the quad-precision invariants (bia/Invariance_QPU.f90):
+    the two forms' drifts agree to 1e-12 of |E0|."""
+    from bia_3d_gpu_b200 import METHOD_ALG, METHOD_LEARNED
+    from conftest import rel_err
+    s, eps, _, dt, steps = initial.make("cold_ball_131072")
+    sel = np.sort(np.random.default_rng(11).choice(s.shape[1], 4096, replace=False))
+    sub = np.ascontiguousarray(s[:, sel])
+    ref, _, _ = oracle.bia_step(sub, eps, dt)
+    e0 = oracle.invariance(sub, eps, quad=True)
+    drift = {}
+    for method in (METHOD_ALG, METHOD_LEARNED):
+        cfg = default_config(eps_th=eps, dt=dt, method=method)
+        with BIASolver() as solver:
+            if method == METHOD_LEARNED:
+                solver.load_heads()
+            t = cuda.tensor(sub, device="cuda")
+            st = solver.step(t, cfg)
+            solver.stream.synchronize()
+            g = t.cpu().numpy()
+            assert st["nonfinite"] == 0
+            assert rel_err(g[:3], ref[:3]) <= 1e-12 and rel_err(g[3:], ref[3:]) <= 1e-12
+            t = cuda.tensor(sub, device="cuda")
+            st = solver.run(t, cfg, steps)
+            assert st["nonfinite"] == 0 and st["timeouts"] == 0
+            e1 = oracle.invariance(t.cpu().numpy(), eps, quad=True)
+        drift[method] = ((e1["KE"] + e1["PE"]) - (e0["KE"] + e0["PE"])) / abs(e0["KE"] + e0["PE"])
+    print(f"cold collapse subset n=4096, {steps} steps: energy drift plain {drift[METHOD_ALG]:.3e}, "
+          f"learned {drift[METHOD_LEARNED]:.3e}")
+    assert abs(drift[METHOD_LEARNED] - drift[METHOD_ALG]) <= 1e-12
