@@ -54,14 +54,22 @@ __device__ __forceinline__ bool learned_candidate(double eps_ij, double dt, cons
     return c == kClsHyp && E * Lsq <= (double)(kHypEMax * kHypEMax - 1.0f) * (eps_ij * eps_ij);
 }
 
+// known_kind (kLearnedEll or kLearnedHyp): the pair was accepted before with that kind, so
+// the classification, the domain tests and the head inputs are skipped; every field the
+// finishing step reads comes out as in the full call.
 __device__ __forceinline__ void learned_prepare(double eps_ij, double dt, const double r[3], const double g[3],
-                                                LearnedPair &L)
+                                                LearnedPair &L, int known_kind = kLearnedPlain)
 {
     L.p = uv_prepare(eps_ij, r, g);
     L.kind = kLearnedPlain;
     L.x0 = L.x1 = 0.0f;
-    const int c = alg_classify(eps_ij, r, g);
-    if (!(dt > 0.0) || !(L.p.mu > 0.0) || (c != kClsHyp && c != kClsEll)) return;
+    int c;
+    if (known_kind == kLearnedPlain) {
+        c = alg_classify(eps_ij, r, g);
+        if (!(dt > 0.0) || !(L.p.mu > 0.0) || (c != kClsHyp && c != kClsEll)) return;
+    } else {
+        c = (known_kind == kLearnedEll) ? kClsEll : kClsHyp;
+    }
     const double ab = fabs(L.p.beta);
     L.sqb = sqrt(ab);
     const double c0m = L.p.r0 * ab / L.p.mu;
@@ -72,8 +80,6 @@ __device__ __forceinline__ void learned_prepare(double eps_ij, double dt, const 
     L.dM = (float)n_dt;
     if (c == kClsEll) {
         const double c0 = 1.0 - c0m;
-        const float e = (float)sqrt(c0 * c0 + s0 * s0);
-        if (!(e <= kEllEMax)) return;
         L.C0 = (float)c0;
         L.A0 = atan2f(L.S0, L.C0);
         const float M1 = L.A0 - L.S0 + L.dM;
@@ -81,21 +87,27 @@ __device__ __forceinline__ void learned_prepare(double eps_ij, double dt, const 
         const float Mr = M1 - kTwoPiF * k;
         L.unfold_sign = (Mr < 0.0f) ? -1.0f : 1.0f;
         L.unfold_shift = kTwoPiF * k;
-        L.x0 = 2.0f * e / kEllEMax - 1.0f;
-        L.x1 = 2.0f * fabsf(Mr) / kPiF - 1.0f;
+        if (known_kind == kLearnedPlain) {
+            const float e = (float)sqrt(c0 * c0 + s0 * s0);
+            if (!(e <= kEllEMax)) return;
+            L.x0 = 2.0f * e / kEllEMax - 1.0f;
+            L.x1 = 2.0f * fabsf(Mr) / kPiF - 1.0f;
+        }
         L.kind = kLearnedEll;
     } else {
         const double c0 = 1.0 + c0m;
         const float e = (float)sqrt((c0 - s0) * (c0 + s0));
-        if (!(e >= kHypEMin && e <= kHypEMax)) return;
+        if (known_kind == kLearnedPlain && !(e >= kHypEMin && e <= kHypEMax)) return;
         L.C0 = (float)c0;
         L.A0 = asinhf(L.S0 / e);
         const float M1 = L.S0 - L.A0 + L.dM;
-        if (!(fabsf(M1) <= kHypMMax)) return;
+        if (known_kind == kLearnedPlain) {
+            if (!(fabsf(M1) <= kHypMMax)) return;
+            L.x0 = 2.0f * logf(e) / logf(kHypEMax) - 1.0f;
+            L.x1 = 2.0f * log1pf(fabsf(M1)) / log1pf(kHypMMax) - 1.0f;
+        }
         L.unfold_sign = (M1 < 0.0f) ? -1.0f : 1.0f;
         L.unfold_shift = 0.0f;
-        L.x0 = 2.0f * logf(e) / logf(kHypEMax) - 1.0f;
-        L.x1 = 2.0f * log1pf(fabsf(M1)) / log1pf(kHypMMax) - 1.0f;
         L.kind = kLearnedHyp;
     }
 }

@@ -338,7 +338,7 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
                 }
                 const double eps_ij = hq ? B.eps_th * si[6] * ws[6 * 32 + j] : B.eps_th;
                 LearnedPair L;
-                learned_prepare(eps_ij, dt, r, g, L);
+                learned_prepare(eps_ij, dt, r, g, L, is_h ? kLearnedHyp : kLearnedEll);
                 bool coarse = true;
                 const bool done = learned_finish(L, dt, y, r, g, h, coarse);
                 cnt.learned++;

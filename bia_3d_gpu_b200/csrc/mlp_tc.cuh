@@ -151,6 +151,16 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float v[16])
     for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
 }
 
+// max(a, 0), max(b, 0) rounded to BF16 (nearest even), a in the low half: one paired
+// conversion with the ReLU built in (rounding is monotone and keeps 0, so this equals
+// rounding the ReLU's FP32 output)
+__device__ __forceinline__ uint32_t pack_bf16_relu(float a, float b)
+{
+    uint32_t d;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(b), "f"(a));
+    return d;
+}
+
 // (a, b) rounded to BF16 (nearest even), a in the low half: one paired conversion
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b)
 {
@@ -291,18 +301,18 @@ __device__ __forceinline__ float mlp_epilogue(MlpSmem &S, const float *bias, uin
         float v[16];
         tc_ld16(taddr + (uint32_t)c, v);
 #pragma unroll
-        for (int j = 0; j < 16; j++) v[j] = fmaxf(v[j] + bias[c + j], 0.0f);
+        for (int j = 0; j < 16; j++) v[j] += bias[c + j];
         if (dst) {
             uint4 lo, hi;
-            lo.x = pack_bf16(v[0], v[1]); lo.y = pack_bf16(v[2], v[3]);
-            lo.z = pack_bf16(v[4], v[5]); lo.w = pack_bf16(v[6], v[7]);
-            hi.x = pack_bf16(v[8], v[9]); hi.y = pack_bf16(v[10], v[11]);
-            hi.z = pack_bf16(v[12], v[13]); hi.w = pack_bf16(v[14], v[15]);
+            lo.x = pack_bf16_relu(v[0], v[1]); lo.y = pack_bf16_relu(v[2], v[3]);
+            lo.z = pack_bf16_relu(v[4], v[5]); lo.w = pack_bf16_relu(v[6], v[7]);
+            hi.x = pack_bf16_relu(v[8], v[9]); hi.y = pack_bf16_relu(v[10], v[11]);
+            hi.z = pack_bf16_relu(v[12], v[13]); hi.w = pack_bf16_relu(v[14], v[15]);
             *(uint4 *)(dst + kmajor_off(tid, c, kMlpHidden)) = lo;
             *(uint4 *)(dst + kmajor_off(tid, c + 8, kMlpHidden)) = hi;
         } else {
 #pragma unroll
-            for (int j = 0; j < 16; j++) dot = fmaf(v[j], S.w4[c + j], dot);
+            for (int j = 0; j < 16; j++) dot = fmaf(fmaxf(v[j], 0.0f), S.w4[c + j], dot);
         }
     }
     return dot + S.b4;
