@@ -54,6 +54,24 @@ __device__ __forceinline__ bool learned_candidate(double eps_ij, double dt, cons
     return c == kClsHyp && E * Lsq <= (double)(kHypEMax * kHypEMax - 1.0f) * (eps_ij * eps_ij);
 }
 
+// The heads' eccentricity bands on the universal-variable quantities of the pair: with
+// t = mu - r0 beta, e^2 mu^2 = t^2 + sig^2 beta for ellipses and hyperbolae alike (no
+// division, no root).  Ellipses with e^2 < 0.9 and attractive hyperbolae with
+// 1.1 < e^2 <= 2500 (the universal-variable band of alg_classify, |e^2 - 1| < 0.1, and the
+// hyperbolic head's e <= 50); radial (L = 0), zero-velocity and parabolic pairs have e = 1.
+// Returns kLearnedEll, kLearnedHyp or kLearnedPlain; e2m = e^2 mu^2.
+__device__ __forceinline__ int learned_band(const UvPair &p, double dt, double &e2m)
+{
+    e2m = 0.0;
+    if (!(dt > 0.0) || !(p.mu > 0.0)) return kLearnedPlain;
+    const double t = fma(-p.r0, p.beta, p.mu);
+    e2m = fma(p.sig * p.sig, p.beta, t * t);
+    const double mu2 = p.mu * p.mu;
+    if (p.beta > 0.0) return e2m < 0.9 * mu2 ? kLearnedEll : kLearnedPlain;
+    if (p.beta < 0.0 && e2m > 1.1 * mu2 && e2m <= (double)(kHypEMax * kHypEMax) * mu2) return kLearnedHyp;
+    return kLearnedPlain;
+}
+
 // known_kind (kLearnedEll or kLearnedHyp): the pair was accepted before with that kind, so
 // the classification, the domain tests and the head inputs are skipped; every field the
 // finishing step reads comes out as in the full call.
@@ -65,8 +83,10 @@ __device__ __forceinline__ void learned_prepare(double eps_ij, double dt, const 
     L.x0 = L.x1 = 0.0f;
     int c;
     if (known_kind == kLearnedPlain) {
-        c = alg_classify(eps_ij, r, g);
-        if (!(dt > 0.0) || !(L.p.mu > 0.0) || (c != kClsHyp && c != kClsEll)) return;
+        double e2m;
+        const int band = learned_band(L.p, dt, e2m);
+        if (band == kLearnedPlain) return;
+        c = (band == kLearnedEll) ? kClsEll : kClsHyp;
     } else {
         c = (known_kind == kLearnedEll) ? kClsEll : kClsHyp;
     }
@@ -113,21 +133,15 @@ __device__ __forceinline__ void learned_prepare(double eps_ij, double dt, const 
 }
 
 // The heads' domain as a cheap test on the universal-variable quantities of the pair (the
-// split step's filter that sends a pair to the learned kernel): with t = mu - r0 beta,
-// e^2 mu^2 = t^2 + sig^2 beta for ellipses and hyperbolae alike (no division, no root),
-// and the domain is that of learned_prepare and the universal-variable band of
-// alg_classify (|e^2 - 1| < 0.1): ellipses with e^2 < 0.9, attractive hyperbolae with
-// 1.1 < e^2 <= 2500 and |M1| <= 100 (that last test in FP32, on the few pairs in the band).
-// The learned kernel decides again with learned_prepare and solves a pair outside its
-// domain with the plain solver, so this test only chooses the kernel.
+// split step's filter that sends a pair to the learned kernel): learned_band, then for the
+// hyperbolae in the band |M1| <= 100 in FP32.  The learned kernel decides again with
+// learned_prepare (the same band, |M1| from its own elements) and solves a pair outside
+// its domain with the plain solver, so this test only chooses the kernel.
 __device__ __forceinline__ bool learned_filter(const UvPair &p, double dt)
 {
-    if (!(dt > 0.0) || !(p.mu > 0.0)) return false;
-    const double t = fma(-p.r0, p.beta, p.mu);
-    const double e2m = fma(p.sig * p.sig, p.beta, t * t);
-    const double mu2 = p.mu * p.mu;
-    if (p.beta > 0.0) return e2m < 0.9 * mu2;
-    if (!(e2m > 1.1 * mu2 && e2m <= (double)(kHypEMax * kHypEMax) * mu2)) return false;
+    double e2m;
+    const int band = learned_band(p, dt, e2m);
+    if (band != kLearnedHyp) return band == kLearnedEll;
     const float mu = (float)p.mu, ab = (float)(-p.beta), sqb = sqrtf(ab);
     const float s0 = (float)p.sig * sqb / mu;
     const float e = sqrtf((float)e2m) / mu;
