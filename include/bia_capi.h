@@ -99,8 +99,9 @@ int bia_context_destroy(bia_context *ctx);
    write only scratch; the state is unchanged) and keeps the fastest for this reduction mode
    and floor(log2 n) in the context, which later steps of that size then use.
    Shapes: 0 = 8-warp CTAs, 1 = phase-locked 16-warp CTAs (2 per SM), 2 = phase-locked
-   32-warp CTAs (1 per SM).  BIA_METHOD_LEARNED: 0 = one kernel, 1 = split (learned pairs,
-   then the plain pairs in a universal-variable kernel).  variant (optional) receives the
+   32-warp CTAs (1 per SM).  BIA_METHOD_LEARNED: 0 = one kernel, 1 = split (the plain pairs
+   in a universal-variable kernel that lists the warp-blocks holding learned pairs, then a
+   persistent kernel over that list; the untuned default at every size).  variant (optional) receives the
    choice, ms (optional, 3 floats) the best time of each candidate (-1 when not run).  RKF
    and universal variables have one shape: variant = -1.
    Synchronises the context's stream; not during stream capture.  No counterpart in the
