@@ -34,7 +34,7 @@ constexpr float kPiF = 3.141592653589793f;
 // The pair in elements, FP64 parts and the FP32 inputs of its head.
 struct LearnedPair {
     UvPair p;
-    double sqb;            // sqrt(|beta|)
+    double sqb, isqb;      // sqrt(|beta|) and its reciprocal
     float C0m, S0, C0;     // C0m = |1 - C0| = r0 |beta| / mu (no cancellation)
     float dM, A0;          // n dt, initial anomaly
     float x0, x1;          // head inputs
@@ -90,11 +90,14 @@ __device__ __forceinline__ void learned_prepare(double eps_ij, double dt, const 
     } else {
         c = (known_kind == kLearnedEll) ? kClsEll : kClsHyp;
     }
+    // one rsqrt and one reciprocal for the elements (|beta| > 0 inside the bands)
     const double ab = fabs(L.p.beta);
-    L.sqb = sqrt(ab);
-    const double c0m = L.p.r0 * ab / L.p.mu;
-    const double s0 = L.p.sig * L.sqb / L.p.mu;
-    const double n_dt = ab * L.sqb / L.p.mu * dt;
+    L.isqb = rsqrt(ab);
+    L.sqb = ab * L.isqb;
+    const double imu = 1.0 / L.p.mu;
+    const double c0m = L.p.r0 * ab * imu;
+    const double s0 = L.p.sig * L.sqb * imu;
+    const double n_dt = ab * L.sqb * imu * dt;
     L.C0m = (float)c0m;
     L.S0 = (float)s0;
     L.dM = (float)n_dt;
@@ -108,7 +111,7 @@ __device__ __forceinline__ void learned_prepare(double eps_ij, double dt, const 
         L.unfold_sign = (Mr < 0.0f) ? -1.0f : 1.0f;
         L.unfold_shift = kTwoPiF * k;
         if (known_kind == kLearnedPlain) {
-            const float e = (float)sqrt(c0 * c0 + s0 * s0);
+            const float e = sqrtf((float)fma(c0, c0, s0 * s0));  // a head input only
             if (!(e <= kEllEMax)) return;
             L.x0 = 2.0f * e / kEllEMax - 1.0f;
             L.x1 = 2.0f * fabsf(Mr) / kPiF - 1.0f;
@@ -116,7 +119,7 @@ __device__ __forceinline__ void learned_prepare(double eps_ij, double dt, const 
         L.kind = kLearnedEll;
     } else {
         const double c0 = 1.0 + c0m;
-        const float e = (float)sqrt((c0 - s0) * (c0 + s0));
+        const float e = sqrtf((float)((c0 - s0) * (c0 + s0)));  // head input and A0 only
         if (known_kind == kLearnedPlain && !(e >= kHypEMin && e <= kHypEMax)) return;
         L.C0 = (float)c0;
         L.A0 = asinhf(L.S0 / e);
@@ -216,7 +219,7 @@ __device__ __forceinline__ float learned_first_correction(const LearnedPair &L, 
             F = L.C0m * sh + L.S0 * chm1 + sinhmx_f(D) - L.dM;
             Fp = L.C0m * (chm1 + 1.0f) + L.S0 * sh + chm1;
         }
-        const float step = F / Fp;
+        const float step = __fdividef(F, Fp);  // a guess for the FP64 step: 2 ulp suffice
         D = D - step;
         if (!(fabsf(step) > 1e-6f * fabsf(D))) break;
     }
@@ -233,7 +236,7 @@ __device__ __forceinline__ bool learned_finish(const LearnedPair &L, double dt, 
     const float D = learned_first_correction(L, y, fp32_steps);
     const float Aguess = (L.kind == kLearnedEll) ? L.unfold_sign * (y * kPiF) + L.unfold_shift
                                                  : L.unfold_sign * (y * kHypOut);
-    double s = (double)D / L.sqb;
+    double s = (double)D * L.isqb;
     if (!(s > 0.0) || !isfinite(s)) {
         coarse = true;
         return false;
