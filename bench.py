@@ -80,7 +80,7 @@ METHODS = {"rkf": 0, "alg": 1, "universal": 2, "learned": 3}
 # list kernel reads and writes back the slots of the warp-blocks it solves).
 TRAFFIC = {
     ("plummer_32768", 3, "split"): (16384 * 16383 // 2, (0.886e6 + 353.564e6) + (256.364e6 + 197.810e6)),
-    ("coulomb_cube_32768", 3, "split"): (16384 * 16383 // 2, (1.054e6 + 361.449e6) + (422.594e6 + 362.519e6)),
+    ("coulomb_cube_32768", 3, "split"): (16384 * 16383 // 2, (1.048e6 + 360.475e6) + (421.979e6 + 353.333e6)),
     ("coulomb_cube_32768", 1, None): (16384 * 16383 // 2, 100.488e6 + 3169.538e6),  # phase-locked ALG
 }
 

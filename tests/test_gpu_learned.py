@@ -146,3 +146,14 @@ def test_learned_autotune_layout(cuda):
     got = d.cpu().numpy()[:, sel].T
     assert np.abs(got[:, :3] - ref[:, :3]).max() <= 1e-12 * np.abs(s[:3]).max()
     assert np.abs(got[:, 3:] - ref[:, 3:]).max() <= 1e-12 * np.abs(s[3:]).max()
+
+
+@pytest.mark.parametrize("n", [2, 31, 33, 97, 1025])
+def test_learned_split_step_ragged_sizes(cuda, n):
+    """The split learned step (the untuned layout at every size) at particle counts that
+    leave partial warp-blocks, down to one pair: against the oracle's ALG step."""
+    s, eps, q = initial.coulomb_cube(n, seed=40 + n, dmin=1e-2)
+    g, r, st = _learned_vs_oracle(cuda, s, eps, 1e-5, q=q, steps=1)
+    assert rel_err(g[:3], r[:3]) <= 1e-12 and rel_err(g[3:], r[3:]) <= 1e-12
+    assert sum(st[k] for k in ("hyperbola", "ellipse", "universal", "degenerate", "parabola")) == n * (n - 1) // 2
+    assert st["nonfinite"] == 0 and st["timeouts"] == 0
