@@ -672,8 +672,16 @@ def main():
             "reference_gpu_kernel": ref_gpu,
             "learned_pair_fraction": stats["learned"] / max(1, steps * pairs) if method == 3 else None,
             "stats": {k: v for k, v in stats.items()},
-            "iterations_per_classical_pair": stats["iterations"] / max(
-                1, stats["hyperbola"] + stats["ellipse"] + stats["parabola"]),
+            # Newton iterations per pair of each solver the measured form ran
+            "newton_iterations": {
+                "classical_per_pair": (stats["iterations"] / max(1, stats["hyperbola"] + stats["ellipse"]
+                                                                 + stats["parabola"])) if method == 1 else None,
+                "universal_per_pair": stats["iter_universal"] / max(
+                    1, stats["universal"] + stats["degenerate"] + stats["learned_fallbacks"]),
+                "learned_fp32_per_learned_pair": (stats["learned_fp32_steps"] / max(1, stats["learned"])
+                                                  if method == 3 else None),
+                "learned_fp64_per_learned_pair": (1.0 if method == 3 else None),  # one Halley step each
+            },
         }
         print(json.dumps(line), flush=True)
     solver.close()

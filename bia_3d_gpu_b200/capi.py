@@ -34,7 +34,7 @@ class BiaConfig(ctypes.Structure):
 STAT_FIELDS = ("hyperbola", "parabola", "ellipse", "degenerate", "rkf", "universal",
                "iterations", "iter_hyperbola", "iter_ellipse", "iter_parabola", "iter_universal",
                "rkf_steps", "nonconverged", "bracket_exits", "fallbacks", "nonfinite",
-               "learned", "learned_fallbacks", "learned_coarse", "timeouts")
+               "learned", "learned_fallbacks", "learned_coarse", "timeouts", "learned_fp32_steps")
 
 
 class BiaStats(ctypes.Structure):

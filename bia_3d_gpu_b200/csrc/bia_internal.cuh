@@ -11,7 +11,7 @@ namespace bia {
 // device counters in the stats buffer: hyperbola, parabola, ellipse, degenerate, rkf,
 // universal, iter_hyperbola, iter_ellipse, iter_parabola, iter_universal, rkf_steps,
 // nonconverged, bracket_exits, fallbacks, nonfinite
-constexpr int kNumStats = 19;
+constexpr int kNumStats = 20;
 constexpr int kStatNonfinite = 14;
 constexpr int kStatTimeouts = 18;  // tensor-core waits that gave up
 

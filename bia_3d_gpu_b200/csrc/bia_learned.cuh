@@ -223,6 +223,7 @@ __device__ __forceinline__ float learned_first_correction(const LearnedPair &L, 
         D = D - step;
         if (!(fabsf(step) > 1e-6f * fabsf(D))) break;
     }
+    if (steps > kLearnedFp32Steps) steps = kLearnedFp32Steps;  // the loop ran out: that many steps
     return D;
 }
 
@@ -230,9 +231,8 @@ __device__ __forceinline__ float learned_first_correction(const LearnedPair &L, 
 // Returns false (nothing written to h) when the FP64 step did not settle: the caller then
 // runs the plain solver.  coarse: the head's guess was more than 1e-2 off in anomaly.
 __device__ __forceinline__ bool learned_finish(const LearnedPair &L, double dt, float y, const double r[3],
-                                               const double g[3], double h[6], bool &coarse)
+                                               const double g[3], double h[6], bool &coarse, int &fp32_steps)
 {
-    int fp32_steps;
     const float D = learned_first_correction(L, y, fp32_steps);
     const float Aguess = (L.kind == kLearnedEll) ? L.unfold_sign * (y * kPiF) + L.unfold_shift
                                                  : L.unfold_sign * (y * kHypOut);

@@ -340,8 +340,10 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
                 LearnedPair L;
                 learned_prepare(eps_ij, dt, r, g, L, is_h ? kLearnedHyp : kLearnedEll);
                 bool coarse = true;
-                const bool done = learned_finish(L, dt, y, r, g, h, coarse);
+                int fp32_steps = 0;
+                const bool done = learned_finish(L, dt, y, r, g, h, coarse, fp32_steps);
                 cnt.learned++;
+                cnt.learned_fp32 += fp32_steps;
                 if (coarse) cnt.learned_coarse++;
                 if (!done) {
                     cnt.learned_fallbacks++;

@@ -77,6 +77,7 @@ struct PairCounters {
     int nonfinite;
     int learned, learned_fallbacks, learned_coarse;  // BIA_METHOD_LEARNED
     int timeouts;
+    int learned_fp32;  // FP32 Newton steps of the learned pairs' first correction
 };
 
 __device__ __forceinline__ void counters_zero(PairCounters &c)
@@ -85,7 +86,7 @@ __device__ __forceinline__ void counters_zero(PairCounters &c)
     for (int k = 0; k < 6; k++) c.cls[k] = 0;
     c.it_hyp = c.it_ell = c.it_par = c.it_uv = 0;
     c.rkf_steps = c.nonconverged = c.bracket_exits = c.fallbacks = c.nonfinite = 0;
-    c.learned = c.learned_fallbacks = c.learned_coarse = c.timeouts = 0;
+    c.learned = c.learned_fallbacks = c.learned_coarse = c.timeouts = c.learned_fp32 = 0;
 }
 
 #ifndef BIA_DIRECT_HALF_SINES

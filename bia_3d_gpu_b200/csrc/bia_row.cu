@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(128) bia_row_kernel(const RowArgs A)
     int vals[kNumStats] = {cnt.cls[0], cnt.cls[1], cnt.cls[2], cnt.cls[3], cnt.cls[4], cnt.cls[5],
                            cnt.it_hyp, cnt.it_ell, cnt.it_par, cnt.it_uv, cnt.rkf_steps,
                            cnt.nonconverged, cnt.bracket_exits, cnt.fallbacks, cnt.nonfinite,
-                           cnt.learned, cnt.learned_fallbacks, cnt.learned_coarse, cnt.timeouts};
+                           cnt.learned, cnt.learned_fallbacks, cnt.learned_coarse, cnt.timeouts, cnt.learned_fp32};
 #pragma unroll
     for (int k = 0; k < kNumStats; k++) {
         int s = __reduce_add_sync(full, vals[k]);

@@ -614,6 +614,7 @@ static void copy_stats(const unsigned long long *h, bia_stats *s)
     s->learned_fallbacks = (long long)h[16];
     s->learned_coarse = (long long)h[17];
     s->timeouts = (long long)h[18];
+    s->learned_fp32_steps = (long long)h[19];
 }
 
 static int fetch_stats(bia_context *ctx, bia_stats *stats)

@@ -59,7 +59,7 @@ __device__ __forceinline__ void flush_counters(const PairCounters &c, unsigned l
     int vals[kNumStats] = {c.cls[0], c.cls[1], c.cls[2], c.cls[3], c.cls[4], c.cls[5],
                            c.it_hyp, c.it_ell, c.it_par, c.it_uv, c.rkf_steps,
                            c.nonconverged, c.bracket_exits, c.fallbacks, c.nonfinite,
-                           c.learned, c.learned_fallbacks, c.learned_coarse, c.timeouts};
+                           c.learned, c.learned_fallbacks, c.learned_coarse, c.timeouts, c.learned_fp32};
 #pragma unroll
     for (int k = 0; k < kNumStats; k++) {
         int s = __reduce_add_sync(full, vals[k]);

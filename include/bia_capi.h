@@ -87,6 +87,8 @@ typedef struct bia_stats {
     long long learned_coarse;    /* ... whose head guess was > 1e-2 off in anomaly */
     long long timeouts;      /* bounded tensor-core waits that gave up (the step returns
                                 BIA_ERR_DEVICE_TIMEOUT) */
+    long long learned_fp32_steps; /* FP32 Newton steps of the learned pairs' first correction
+                                     (each learned pair then takes one FP64 Halley step) */
 } bia_stats;
 
 typedef struct bia_context bia_context;

@@ -59,6 +59,8 @@ def test_learned_coulomb_matches_oracle(cuda):
     assert st["learned"] > 0.3 * 1500 * 1499 // 2
     assert st["learned_fallbacks"] <= 0.01 * st["learned"]
     assert st["nonfinite"] == 0 and st["timeouts"] == 0
+    # one to four FP32 Newton steps per learned pair before its FP64 step
+    assert st["learned"] <= st["learned_fp32_steps"] <= 4 * st["learned"]
 
 
 def test_learned_gravity_ball_matches_oracle(cuda):
