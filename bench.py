@@ -62,10 +62,11 @@ FLOPS = {
     "ellipse": (447, 47),      # per pair, per Kepler Newton step
     "parabola": (429, 76),     # per pair, per Barker Newton step
     "rkf": (147, 758),         # per pair, per accepted RKF45 step (3 Fehlberg stages sets)
-    # universal variables (this library's solver, not the reference's): prepare 20, third-order
-    # start 17, composition 66 per pair, 43 per Newton iteration, with the five-term Stumpff
-    # series that every pair of the benchmark workloads takes (|beta s^2| <= 1e-2)
-    "universal": (103, 43),
+    # universal variables (this library's solver, not the reference's): prepare 20, fifth-order
+    # start with its exactness test 76, composition 66 per pair, 43 per Newton iteration (almost
+    # none at the benchmark steps), with the five-term Stumpff series that every pair of the
+    # benchmark workloads takes (|beta s^2| <= 1e-2)
+    "universal": (162, 43),
     "learned": (330, 0),       # per learned pair: elements, FP64 Halley step, composition
 }
 # BF16 tensor-core flops per learned pair: 2 x (16 x 64 + 64 x 64 + 64 x 64) multiply-adds

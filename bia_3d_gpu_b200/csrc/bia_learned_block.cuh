@@ -108,9 +108,10 @@ __device__ __forceinline__ uint32_t rest_block_solve(const double *x, const doub
             if (learned_filter(p, dt)) {
                 learned |= 1u << k;
             } else if (dt != 0.0) {
-                double s = uv_start(p, dt);
-                double ifp;
-                const int it = uv_iterate(p, dt, s, &ifp);
+                bool exact;
+                double s = uv_start_fast(p, dt, exact);
+                double ifp = 0.0;
+                const int it = exact ? 0 : uv_iterate(p, dt, s, &ifp);
                 uv_compose(p, s, r, g, h, ifp);
                 cnt.it_uv += it;
                 if (it > kUvItMax) cnt.nonconverged++;

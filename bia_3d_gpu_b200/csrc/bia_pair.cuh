@@ -804,6 +804,72 @@ __device__ __forceinline__ double uv_start(const UvPair &p, double dt)
     return (s > 0.0) ? s : x;
 }
 
+// Fifth-order start (uv_start_fast, the universal-variable method and the split learned
+// step's plain pairs): the series reversion of the universal Kepler equation
+//   t = b1 s + b2 s^2 + b3 s^3 + b4 s^4 + b5 s^5 + O(s^6),
+//   b1 = r0, b2 = sig/2, b3 = (mu - beta r0)/6, b4 = -sig beta/24, b5 = beta (beta r0 - mu)/120
+// (the Stumpff series of r0 s c1 + sig s^2 c2 + mu s^3 c3), inverted with the Lagrange
+// reversion coefficients (Abramowitz and Stegun 3.6.25):
+//   a1 = 1/b1, a2 = -b2/b1^3, a3 = (2 b2^2 - b1 b3)/b1^5, a4 = (5 b1 b2 b3 - b1^2 b4 - 5 b2^3)/b1^7,
+//   a5 = (6 b1^2 b2 b4 + 3 b1^2 b3^2 + 14 b2^4 - b1^3 b5 - 21 b1 b2^2 b3)/b1^9,
+//   s = a1 t + a2 t^2 + a3 t^3 + a4 t^4 + a5 t^5 + O(t^6).
+// When every |a_k t^(k-1)| <= Q^(k-1) a1 with Q = 2e-4 (the step is that small against the
+// pair's time scales), the fifth-order sum is returned with exact_out = true: its truncation is
+// below 2e-18 relative (checked in extended precision against the solved equation on
+// 20000 pairs drawn around that boundary), so no Newton correction is needed.  Otherwise the
+// third-order sum (error O((dt/T)^3), one Newton correction below the 1e-10 acceptance at
+// small steps) is returned with exact_out = false.  The ALG kernels keep uv_start: changing
+// the code they inline changes how the compiler contracts their own FP64 expressions.
+// Every product and sum is written out (fma, __dmul_rn, __dsub_rn) so that each kernel
+// that inlines this computes the same bits and takes the same branch: the ensemble's
+// systems equal their own steps bit for bit.
+__device__ __forceinline__ double uv_start_fast(const UvPair &p, double dt, bool &exact_out)
+{
+    const double r0 = p.r0, ir0 = p.ir0;
+    const double ir2 = __dmul_rn(ir0, ir0);
+    const double h = 0.5 * p.sig;  // exact
+    const double br = __dmul_rn(p.beta, r0);
+    const double b3 = __dmul_rn(__dsub_rn(p.mu, br), 1.0 / 6.0);
+    const double a1 = ir0;
+    const double a2 = __dmul_rn(-h, __dmul_rn(ir0, ir2));
+    const double hh = __dmul_rn(h, h);
+    const double a3 = __dmul_rn(fma(2.0, hh, -__dmul_rn(r0, b3)), __dmul_rn(__dmul_rn(ir2, ir2), ir0));
+    const double t = dt;
+    const double s3 = __dmul_rn(t, fma(t, fma(t, a3, a2), a1));
+    bool *exact = &exact_out;
+    {
+        const double b4 = __dmul_rn(__dmul_rn(-h, p.beta), 1.0 / 12.0);
+        const double b5 = __dmul_rn(__dmul_rn(p.beta, __dsub_rn(br, p.mu)), 1.0 / 120.0);
+        const double r02 = __dmul_rn(r0, r0);
+        const double ir7 = __dmul_rn(__dmul_rn(__dmul_rn(ir2, ir2), ir2), ir0);
+        // a4 = (5 r0 h b3 - r0^2 b4 - 5 h^3) / r0^7
+        const double n4 = fma(5.0 * r0, __dmul_rn(h, b3), -fma(r02, b4, __dmul_rn(5.0 * hh, h)));
+        const double a4 = __dmul_rn(n4, ir7);
+        // a5 = (6 r0^2 h b4 + 3 r0^2 b3^2 + 14 h^4 - r0^3 b5 - 21 r0 h^2 b3) / r0^9
+        double n5 = __dmul_rn(__dmul_rn(6.0 * r02, h), b4);
+        n5 = fma(3.0 * r02, __dmul_rn(b3, b3), n5);
+        n5 = fma(14.0 * hh, hh, n5);
+        n5 = fma(-__dmul_rn(r02, r0), b5, n5);
+        n5 = fma(-21.0 * r0, __dmul_rn(hh, b3), n5);
+        const double a5 = __dmul_rn(n5, __dmul_rn(ir7, ir2));
+        constexpr double Q = 2e-4;
+        const double t2 = __dmul_rn(t, t);
+        const bool small = fabs(__dmul_rn(a2, t)) <= Q * a1 && fabs(__dmul_rn(a3, t2)) <= (Q * Q) * a1 &&
+                           fabs(__dmul_rn(a4, __dmul_rn(t2, t))) <= (Q * Q * Q) * a1 &&
+                           fabs(__dmul_rn(a5, __dmul_rn(t2, t2))) <= (Q * Q * Q * Q) * a1;
+        *exact = false;
+        if (small) {
+            const double s5 = __dmul_rn(t, fma(t, fma(t, fma(t, fma(t, a5, a4), a3), a2), a1));
+            if (s5 > 0.0) {
+                *exact = true;
+                return s5;
+            }
+        }
+    }
+    const double x = __dmul_rn(dt, ir0);
+    return (s3 > 0.0) ? s3 : x;
+}
+
 // Safeguarded Newton on F(s) = t(s) - dt, F' = r(s) > 0, with the bracket [lo, hi]
 // (F(0) = -dt < 0; hi < 0 until an upper bound is seen).  A Newton step that leaves the
 // bracket, or is not below half the step before last, is replaced by bisection, so the
@@ -893,6 +959,23 @@ __device__ __forceinline__ int uv_halfdisp(double eps_th, double dt, const doubl
     double s = uv_start(p, dt);
     double ifp;
     const int it = uv_iterate(p, dt, s, &ifp);
+    uv_compose(p, s, r, g, h, ifp);
+    return it;
+}
+
+// uv_halfdisp from the fifth-order start: no Newton correction where the series alone is
+// exact (returns 0 iterations for those pairs).  The ALG kernels keep uv_halfdisp.
+__device__ __forceinline__ int uv_halfdisp_fast(double eps_th, double dt, const double r[3], const double g[3],
+                                                double h[6])
+{
+#pragma unroll
+    for (int k = 0; k < 6; k++) h[k] = 0.0;
+    if (dt == 0.0) return 0;
+    const UvPair p = uv_prepare(eps_th, r, g);
+    bool exact;
+    double s = uv_start_fast(p, dt, exact);
+    double ifp = 0.0;
+    const int it = exact ? 0 : uv_iterate(p, dt, s, &ifp);
     uv_compose(p, s, r, g, h, ifp);
     return it;
 }
@@ -1019,7 +1102,7 @@ __device__ __forceinline__ void pair_halfdisp(const PairParams &P, double eps_ij
                                               const double g[3], double h[6], PairCounters &cnt)
 {
     if (M == kMethodUniversal) {
-        const int it = uv_halfdisp(eps_ij, P.dt, r, g, h);
+        const int it = uv_halfdisp_fast(eps_ij, P.dt, r, g, h);
         cnt.it_uv += it;
         if (it > kUvItMax) cnt.nonconverged++;
         cnt.cls[kUniversal]++;
