@@ -813,10 +813,11 @@ __device__ __forceinline__ double uv_start(const UvPair &p, double dt)
 //   a1 = 1/b1, a2 = -b2/b1^3, a3 = (2 b2^2 - b1 b3)/b1^5, a4 = (5 b1 b2 b3 - b1^2 b4 - 5 b2^3)/b1^7,
 //   a5 = (6 b1^2 b2 b4 + 3 b1^2 b3^2 + 14 b2^4 - b1^3 b5 - 21 b1 b2^2 b3)/b1^9,
 //   s = a1 t + a2 t^2 + a3 t^3 + a4 t^4 + a5 t^5 + O(t^6).
-// When every |a_k t^(k-1)| <= Q^(k-1) a1 with Q = 2e-4 (the step is that small against the
+// When every |a_k t^(k-1)| <= Q^(k-1) a1 with Q = 3e-4 (the step is that small against the
 // pair's time scales), the fifth-order sum is returned with exact_out = true: its truncation is
-// below 2e-18 relative (checked in extended precision against the solved equation on
-// 20000 pairs drawn around that boundary), so no Newton correction is needed.  Otherwise the
+// below 1.1e-17 relative, a tenth of an FP64 ulp (checked in extended precision against the
+// solved equation on 12000 attractive and repulsive pairs drawn around that boundary), so no
+// Newton correction is needed.  Otherwise the
 // third-order sum (error O((dt/T)^3), one Newton correction below the 1e-10 acceptance at
 // small steps) is returned with exact_out = false.  The ALG kernels keep uv_start: changing
 // the code they inline changes how the compiler contracts their own FP64 expressions.
@@ -852,7 +853,7 @@ __device__ __forceinline__ double uv_start_fast(const UvPair &p, double dt, bool
         n5 = fma(-__dmul_rn(r02, r0), b5, n5);
         n5 = fma(-21.0 * r0, __dmul_rn(hh, b3), n5);
         const double a5 = __dmul_rn(n5, __dmul_rn(ir7, ir2));
-        constexpr double Q = 2e-4;
+        constexpr double Q = 3e-4;
         const double t2 = __dmul_rn(t, t);
         const bool small = fabs(__dmul_rn(a2, t)) <= Q * a1 && fabs(__dmul_rn(a3, t2)) <= (Q * Q) * a1 &&
                            fabs(__dmul_rn(a4, __dmul_rn(t2, t))) <= (Q * Q * Q) * a1 &&
