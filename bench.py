@@ -80,7 +80,7 @@ METHODS = {"rkf": 0, "alg": 1, "universal": 2, "learned": 3}
 # The split learned step is its two kernels (the rest kernel writes every partial slot, the
 # list kernel reads and writes back the slots of the warp-blocks it solves).
 TRAFFIC = {
-    ("plummer_32768", 3, "split"): (16384 * 16383 // 2, (0.886e6 + 353.564e6) + (256.364e6 + 197.810e6)),
+    ("plummer_32768", 3, "split"): (16384 * 16383 // 2, (1.255e6 + 354.301e6) + (256.467e6 + 196.120e6)),
     ("coulomb_cube_32768", 3, "split"): (16384 * 16383 // 2, (1.048e6 + 360.475e6) + (421.979e6 + 353.333e6)),
     ("coulomb_cube_32768", 1, None): (16384 * 16383 // 2, 100.488e6 + 3169.538e6),  # phase-locked ALG
 }
