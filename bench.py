@@ -263,7 +263,7 @@ def _max_over_ranks(dist, value, dev):
 
 
 def run_ensemble(args, rank, world, local):
-    """4096 independent Plummer systems of uneven size, 200 steps in
+    """The batched ensemble: 4096 independent Plummer systems of uneven size, 200 steps in
     one CUDA graph (one pair-kernel launch per step over all systems)."""
     import torch
 

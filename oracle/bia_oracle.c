@@ -10,7 +10,7 @@
  * follows the Fortran source (left-to-right evaluation, ** as repeated
  * multiplication) and the library is built with -ffp-contract=off so no FMA
  * contraction changes the rounding.  Deliberate deviations from the reference
- * are marked "DEVIATION" and listed in DESIGN.md:
+ * are marked "DEVIATION" in the code; they are:
  *   - find_hyperbola leaves theta_stock uninitialised when the Newton loop never
  *     improves on the starting residual (bia/find_hyperbola.f90:93-119); here it
  *     starts as the starting iterate.

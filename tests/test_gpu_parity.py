@@ -1,6 +1,6 @@
 """GPU parity: the CUDA pair step against the CPU oracle, through the C-ABI.
 
-Tolerances: global relative error ||X_gpu - X_oracle|| / ||X_oracle||
+Tolerances (the parity bar of the plain form): global relative error ||X_gpu - X_oracle|| / ||X_oracle||
 <= 1e-12 for positions and velocities, and the per-particle maximum
 max|X_gpu - X_oracle| / max|X_oracle| <= 1e-12 at the workloads' step lengths, against
 both the FP64 oracle (the reference's CPU path) and its quad-precision evaluation (the

@@ -34,8 +34,8 @@ def test_fixture_is_all_hyperbolic(fixture_step):
 def test_oracle_matches_reference_bia_record(golden, golden_ic, fixture_step):
     """Oracle step vs the reference's .BIA record (its GPU ALG run).
 
-    Tolerance: global relative error <= 1e-12 in positions and velocities (the
-    north-star bar).  The per-particle maximum is looser, 1e-11 of max|X|: a pair
+    Tolerance: global relative error <= 1e-12 in positions and velocities (the parity
+    bar of the plain form).  The per-particle maximum is looser, 1e-11 of max|X|: a pair
     that starts at pericentre gets its start angle from acos(1 - delta)
     (bia/find_hyperbola.f90:38), whose conditioning ~1/sqrt(delta) turns one ulp into
     ~1e-11 of displacement at dt = 1; the reference's CPU and GPU paths differ there
