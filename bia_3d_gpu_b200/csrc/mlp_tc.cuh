@@ -137,20 +137,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t phase)
     return false;
 }
 
-// 16 consecutive FP32 accumulator columns of this thread's TMEM lane
-__device__ __forceinline__ void tc_ld16(uint32_t taddr, float v[16])
-{
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
-}
-
 // max(a, 0), max(b, 0) rounded to BF16 (nearest even), a in the low half: one paired
 // conversion with the ReLU built in (rounding is monotone and keeps 0, so this equals
 // rounding the ReLU's FP32 output)
@@ -159,6 +145,23 @@ __device__ __forceinline__ uint32_t pack_bf16_relu(float a, float b)
     uint32_t d;
     asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(b), "f"(a));
     return d;
+}
+
+// 32 consecutive FP32 accumulator columns of this thread's TMEM lane (one load, one wait)
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float v[32])
+{
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = __uint_as_float(r[j]);
 }
 
 // (a, b) rounded to BF16 (nearest even), a in the low half: one paired conversion
@@ -297,22 +300,22 @@ __device__ __forceinline__ float mlp_epilogue(MlpSmem &S, const float *bias, uin
     float dot = 0.0f;
     __syncwarp();
 #pragma unroll
-    for (int c = 0; c < kMlpHidden; c += 16) {
-        float v[16];
-        tc_ld16(taddr + (uint32_t)c, v);
+    for (int c = 0; c < kMlpHidden; c += 32) {
+        float v[32];
+        tc_ld32(taddr + (uint32_t)c, v);
 #pragma unroll
-        for (int j = 0; j < 16; j++) v[j] += bias[c + j];
+        for (int j = 0; j < 32; j++) v[j] += bias[c + j];
         if (dst) {
-            uint4 lo, hi;
-            lo.x = pack_bf16_relu(v[0], v[1]); lo.y = pack_bf16_relu(v[2], v[3]);
-            lo.z = pack_bf16_relu(v[4], v[5]); lo.w = pack_bf16_relu(v[6], v[7]);
-            hi.x = pack_bf16_relu(v[8], v[9]); hi.y = pack_bf16_relu(v[10], v[11]);
-            hi.z = pack_bf16_relu(v[12], v[13]); hi.w = pack_bf16_relu(v[14], v[15]);
-            *(uint4 *)(dst + kmajor_off(tid, c, kMlpHidden)) = lo;
-            *(uint4 *)(dst + kmajor_off(tid, c + 8, kMlpHidden)) = hi;
+#pragma unroll
+            for (int q = 0; q < 32; q += 8) {
+                uint4 o;
+                o.x = pack_bf16_relu(v[q + 0], v[q + 1]); o.y = pack_bf16_relu(v[q + 2], v[q + 3]);
+                o.z = pack_bf16_relu(v[q + 4], v[q + 5]); o.w = pack_bf16_relu(v[q + 6], v[q + 7]);
+                *(uint4 *)(dst + kmajor_off(tid, c + q, kMlpHidden)) = o;
+            }
         } else {
 #pragma unroll
-            for (int j = 0; j < 16; j++) dot = fmaf(fmaxf(v[j], 0.0f), S.w4[c + j], dot);
+            for (int j = 0; j < 32; j++) dot = fmaf(fmaxf(v[j], 0.0f), S.w4[c + j], dot);
         }
     }
     return dot + S.b4;
