@@ -112,7 +112,7 @@ __device__ __forceinline__ uint32_t rest_block_solve(const double *x, const doub
                 double s = uv_start_fast(p, dt, exact);
                 double ifp = 0.0;
                 const int it = exact ? 0 : uv_iterate(p, dt, s, &ifp);
-                uv_compose(p, s, r, g, h, ifp);
+                uv_compose<true>(p, s, r, g, h, exact ? p.ir0 : ifp);
                 cnt.it_uv += it;
                 if (it > kUvItMax) cnt.nonconverged++;
                 cnt.cls[kUniversal]++;

@@ -930,6 +930,10 @@ __device__ __forceinline__ double uv_halley_step(const UvPair &p, double dt, dou
 // functions (no cancellation at small s).  irr_hint (optional, 0: none): an approximation
 // of 1/r(s), such as uv_iterate's last 1/F'; within 1e-8 of it one Newton-Raphson step for
 // the reciprocal (x + x (1 - r x)) gives 1/r(s) to ~1e-16, else 1/r(s) is divided out.
+// kTwoSteps (the universal-variable method and the split step's plain pairs, which pass
+// 1/r0 when no Newton iteration ran): two Newton-Raphson steps from a hint within 1e-4
+// (error e^4 <= 1e-16); the ALG kernels keep the one-step form.
+template <bool kTwoSteps = false>
 __device__ __forceinline__ void uv_compose(const UvPair &p, double s, const double r[3], const double g[3],
                                            double h[6], double irr_hint = 0.0)
 {
@@ -938,7 +942,17 @@ __device__ __forceinline__ void uv_compose(const UvPair &p, double s, const doub
     const double s2c2 = s * s * c[2], s3c3 = s * s * s * c[3];
     const double rr = p.r0 * c[0] + p.sig * s * c[1] + p.mu * s2c2;
     const double e = fma(-rr, irr_hint, 1.0);
-    const double irr = (irr_hint != 0.0 && fabs(e) <= 1e-8) ? fma(irr_hint, e, irr_hint) : 1.0 / rr;
+    double irr;
+    if (kTwoSteps) {
+        if (irr_hint != 0.0 && fabs(e) <= 1e-4) {
+            const double x1 = fma(irr_hint, e, irr_hint);
+            irr = fma(x1, fma(-rr, x1, 1.0), x1);
+        } else {
+            irr = 1.0 / rr;
+        }
+    } else {
+        irr = (irr_hint != 0.0 && fabs(e) <= 1e-8) ? fma(irr_hint, e, irr_hint) : 1.0 / rr;
+    }
     const double fm1 = -p.mu * s2c2 * p.ir0;
     const double gmdt = -p.mu * s3c3;
     const double fdot = -p.mu * s * c[1] * (irr * p.ir0);
@@ -977,7 +991,7 @@ __device__ __forceinline__ int uv_halfdisp_fast(double eps_th, double dt, const 
     double s = uv_start_fast(p, dt, exact);
     double ifp = 0.0;
     const int it = exact ? 0 : uv_iterate(p, dt, s, &ifp);
-    uv_compose(p, s, r, g, h, ifp);
+    uv_compose<true>(p, s, r, g, h, exact ? p.ir0 : ifp);
     return it;
 }
 
