@@ -106,9 +106,10 @@ def test_learned_needs_heads(cuda):
 
 
 def test_learned_split_step_matches_oracle(cuda):
-    """At n = 6000 the learned step splits (learned pairs in the learned kernel, plain pairs
-    in the rest kernel, added onto the same partials): sampled particles against the
-    oracle's full pair sums, and momentum from the antisymmetry."""
+    """The split learned step at n = 6000 (the plain pairs in the rest kernel, which lists
+    the warp-blocks holding learned pairs; those in the list kernel, added onto the same
+    partials): sampled particles against the oracle's full pair sums, and momentum from the
+    antisymmetry."""
     s, eps, q = initial.coulomb_cube(6000, seed=36)
     t = cuda.tensor(s, device="cuda")
     qt = cuda.tensor(q, device="cuda")
