@@ -244,12 +244,16 @@ def metric_name(method):
 
 
 def _init_dist(world):
+    """The replicas' process group (NCCL on GPUs; gloo where there is none, for the host-only
+    checks of the replica timing); None for one process."""
     if world <= 1:
         return None
     import datetime
 
+    import torch
     import torch.distributed as dist
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    backend = "nccl" if torch.cuda.is_available() else "gloo"
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return dist
 
 
@@ -408,12 +412,7 @@ def main():
     if args.workload == "dim_lattice_1332":
         run_dim(args, rank, world, local)
         return
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dist = _init_dist(world)
 
     state, eps, q, dt, steps_cfg = initial.make(args.workload, n=args.n)
     n = state.shape[1]
@@ -437,11 +436,7 @@ def main():
             torch.cuda.synchronize()
 
     def max_over_ranks(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return _max_over_ranks(dist, v, dev)
 
     def timed_steps(c, k_steps, sample_clocks=False):
         """k_steps steps of config c, each from the seeded state (untimed device copy) after
