@@ -34,8 +34,9 @@ struct bia_ensemble {
     double *d_part = nullptr;          // partial sums
     double *d_scratch = nullptr;       // [nitems + nparticles] energy scratch
     double *d_energy = nullptr;        // [2 nsys] KE, PE per system
-    // learned step: list length, list of items holding learned pairs, 32 masks per listed item
-    unsigned int *d_split = nullptr;   // [4 + nitems + 32 nitems]
+    // learned step: per-bin list lengths, the bins' lists of items holding learned pairs, 32
+    // pair masks per item
+    unsigned int *d_split = nullptr;   // [16 + kEnsBins nitems + 32 nitems]
     size_t part_doubles = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -46,6 +47,9 @@ namespace bia {
 
 constexpr int kEnsWarps = 8;
 constexpr int kEnsThreads = kEnsWarps * 32;
+// the learned step lists its items in bins of floor(log2(learned pairs of the item)), so
+// that the eight items a CTA of the list kernel takes at a time carry similar work
+constexpr int kEnsBins = 11;
 
 struct EnsArgs {
     const double *x, *y, *z, *u, *v, *w, *q;
@@ -58,8 +62,8 @@ struct EnsArgs {
     unsigned long long *stats;
     PairParams P;
     const MlpImage *heads;  // BIA_METHOD_LEARNED
-    unsigned int *wbcount, *wblist;  // learned step: the rest kernel's list of items
-    uint32_t *lmask;                 // and their pair masks
+    unsigned int *wbcount, *wblist;  // learned step: kEnsBins list lengths, lists (nitems each)
+    uint32_t *lmask;                 // and the pair masks of every item
 };
 
 template <int M>
@@ -157,52 +161,58 @@ __global__ void __launch_bounds__(kEnsThreads, 2) ens_pair_rest_kernel(const Ens
     flush_counters(cnt, A.stats, lane);
     const int nb = (n + 31) / 32;
     write_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
-    if (__any_sync(full, learned != 0u)) {
-        unsigned int slot = 0;
-        if (lane == 0) slot = atomicAdd(A.wbcount, 1u);
-        slot = __shfl_sync(full, slot, 0);
-        A.lmask[(size_t)slot * 32 + lane] = learned;
-        if (lane == 0) A.wblist[slot] = (unsigned int)t;
+    const unsigned total = __reduce_add_sync(full, (unsigned)__popc(learned));
+    if (total != 0u) {
+        const int bin = min(kEnsBins - 1, 31 - __clz((int)total));
+        A.lmask[(size_t)t * 32 + lane] = learned;
+        if (lane == 0) {
+            const unsigned int slot = atomicAdd(&A.wbcount[bin], 1u);
+            A.wblist[(size_t)bin * A.nitems + slot] = (unsigned int)t;
+        }
     }
 }
 
 // Learned step, second kernel: persistent CTAs work through the listed items eight at a
-// time (one per warp, of any systems), solve their masked pairs with the learned warp-block
-// and add the sums onto the rest kernel's partials.
+// time (one per warp, of any systems), the heaviest bin first, solve their masked pairs with
+// the learned warp-block and add the sums onto the rest kernel's partials.
 __global__ void __launch_bounds__(kMlpThreads, 2) ens_pair_learned_list_kernel(const EnsArgs A)
 {
     extern __shared__ uint8_t ens_list_raw[];
     const LearnedSmem M = learned_smem(ens_list_raw);
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const long long count = (long long)*A.wbcount;
     mlp_setup(*M.mlp);
     uint32_t phase = 0;
-    for (long long g0 = (long long)blockIdx.x * kLearnedWarps; g0 < count;
-         g0 += (long long)gridDim.x * kLearnedWarps) {
-        const long long e = g0 + warp;
-        const bool live = e < count;
-        int s = 0, bi = 0, bj = 0;
-        uint32_t mask = 0u;
-        if (live) {
-            const uint2 it = A.items[A.wblist[e]];
-            s = (int)it.x;
-            bi = (int)(it.y & 0xffffu);
-            bj = (int)(it.y >> 16);
-            mask = A.lmask[(size_t)e * 32 + lane];
-        }
-        const int base = A.off[s];
-        const int n = A.off[s + 1] - base;
-        const LearnedBlockIn B = {A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base,
-                                  A.q ? A.q + base : nullptr, n, A.eps[s], A.P.dt, A.heads};
-        double racc[6], cacc[6];
-        PairCounters cnt;
-        const bool timed_out = learned_block_solve(M, B, bi, bj, lane, live, racc, cacc, cnt, phase, &mask);
-        if (timed_out && threadIdx.x == 0 && !live) atomicAdd(&A.stats[kStatTimeouts], 1ull);
-        if (live) {
-            flush_counters(cnt, A.stats, lane);
-            const int nb = (n + 31) / 32;
-            add_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
+    for (int bin = kEnsBins - 1; bin >= 0; bin--) {
+        const long long count = (long long)A.wbcount[bin];
+        const unsigned int *list = A.wblist + (size_t)bin * A.nitems;
+        for (long long g0 = (long long)blockIdx.x * kLearnedWarps; g0 < count;
+             g0 += (long long)gridDim.x * kLearnedWarps) {
+            const long long e = g0 + warp;
+            const bool live = e < count;
+            int s = 0, bi = 0, bj = 0;
+            uint32_t mask = 0u;
+            if (live) {
+                const unsigned int item = list[e];
+                const uint2 it = A.items[item];
+                s = (int)it.x;
+                bi = (int)(it.y & 0xffffu);
+                bj = (int)(it.y >> 16);
+                mask = A.lmask[(size_t)item * 32 + lane];
+            }
+            const int base = A.off[s];
+            const int n = A.off[s + 1] - base;
+            const LearnedBlockIn B = {A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base,
+                                      A.q ? A.q + base : nullptr, n, A.eps[s], A.P.dt, A.heads};
+            double racc[6], cacc[6];
+            PairCounters cnt;
+            const bool timed_out = learned_block_solve(M, B, bi, bj, lane, live, racc, cacc, cnt, phase, &mask);
+            if (timed_out && threadIdx.x == 0 && !live) atomicAdd(&A.stats[kStatTimeouts], 1ull);
+            if (live) {
+                flush_counters(cnt, A.stats, lane);
+                const int nb = (n + 31) / 32;
+                add_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
+            }
         }
     }
     mlp_teardown(*M.mlp, phase);
@@ -362,9 +372,9 @@ static int ens_enqueue_step(bia_context *ctx, bia_ensemble *E, const bia_config 
         if (!ctx->heads_loaded) return BIA_ERR_INVALID_ARGUMENT;
         if (lsetup <= 0) return BIA_ERR_CUDA;
         A.wbcount = E->d_split;
-        A.wblist = E->d_split + 4;
-        A.lmask = E->d_split + 4 + E->nitems;
-        cudaError_t e = cudaMemsetAsync(A.wbcount, 0, sizeof(unsigned int), ctx->stream);
+        A.wblist = E->d_split + 16;
+        A.lmask = E->d_split + 16 + (size_t)kEnsBins * E->nitems;
+        cudaError_t e = cudaMemsetAsync(A.wbcount, 0, kEnsBins * sizeof(unsigned int), ctx->stream);
         if (e != cudaSuccess) return cuda_status(e);
         ens_pair_rest_kernel<<<grid, kEnsThreads, 0, ctx->stream>>>(A);
         const long long need = (E->nitems + kLearnedWarps - 1) / kLearnedWarps;
@@ -467,7 +477,7 @@ extern "C" int bia_ensemble_create(bia_context *ctx, int nsys, const int *sizes,
     ENS_ALLOC(E->d_part, part);
     ENS_ALLOC(E->d_scratch, nitems);
     ENS_ALLOC(E->d_energy, 2 * nsys);
-    ENS_ALLOC(E->d_split, 4 + 33 * nitems);
+    ENS_ALLOC(E->d_split, 16 + (kEnsBins + 32) * nitems);
 #undef ENS_ALLOC
     if (e == cudaSuccess) e = cudaMemcpy(E->d_off, off.data(), sizeof(int) * (nsys + 1), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(E->d_psys, psys.data(), sizeof(int) * np, cudaMemcpyHostToDevice);
