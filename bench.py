@@ -120,6 +120,9 @@ def parse():
     ap.add_argument("--no-universal", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--no-oracle-check", action="store_true", help="skip error_vs_oracle")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the other configurations timed beside the main line")
     ap.add_argument("--no-autotune", action="store_true",
                     help="use the library's built-in kernel-shape rules instead of timing the shapes first "
                          "(for profiler runs, whose serialised launches would mislead the autotuner)")
@@ -183,12 +186,13 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def cpu_sample(state, eps, q, dt, method, seconds, seed=0):
-    """Time the oracle on a seeded row sample sized to about `seconds` of host work."""
+def cpu_sample(state, eps, q, dt, method, seconds, seed=0, threads=None):
+    """Time the oracle on a seeded row sample sized to about `seconds` of host work, on
+    `threads` host threads (default: all cores)."""
     import oracle
     n = state.shape[1]
     rng = np.random.default_rng(seed)
-    threads = os.cpu_count() or 1
+    threads = threads or os.cpu_count() or 1
     rows = rng.choice(n - 1, size=min(n - 1, max(threads, 8)), replace=False)
     t0 = time.perf_counter()
     _, pairs, _ = oracle.bia_rows(state, eps, dt, rows, method=method, q=q, nthreads=threads)
@@ -208,8 +212,9 @@ def run_reference(args, rank, world):
         return
     from bia_3d_gpu_b200 import initial
     state, eps, q, dt, steps_cfg = initial.make(args.workload, n=args.n)
-    # the reference has no learned form: its CPU ALG path is the reference arm for it too
-    method = {"rkf": 0, "alg": 1, "universal": 2, "learned": 1}[args.method]
+    # the reference has no learned form or universal-variable solver: its CPU ALG path is
+    # the reference arm for every method but RKF
+    method = {"rkf": 0, "alg": 1, "universal": 1, "learned": 1}[args.method]
     steps = args.steps if args.steps is not None else steps_cfg
     per_step = max(0.5, min(3.0, 120.0 / max(1, steps + args.warmup)))
     for w in range(args.warmup):
@@ -226,8 +231,10 @@ def run_reference(args, rank, world):
         "value": value, "unit": "pair-updates/s", "n_gpus": world, "steps": steps,
         "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": args.workload, "n": n, "pairs_per_step": n * (n - 1) // 2,
-                   "dt": dt, "method": args.method},
+        "config": config_keys(args.workload, n, dt, "rkf" if method == 0 else "alg", world,
+                              reduction="host loop in pair order (bia/bia.f90:141-196)",
+                              precision="FP64", l2="host CPU (no GPU)",
+                              state="the seeded state for every sampled row"),
         "cpu_baseline": {"value": value, "unit": "pair-updates/s", "cores": cores, "kind": "port",
                          "sample": f"per step: {info}; the reference's Fortran CPU path "
                                    "cannot be compiled here, its C restatement runs instead"},
@@ -235,6 +242,13 @@ def run_reference(args, rank, world):
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def config_keys(workload, n, dt, method, world, reduction, precision, l2, state, autotuned=None):
+    """The config object of a bench line; both arms print the same keys."""
+    return {"workload": workload, "n": n, "pairs_per_step": n * (n - 1) // 2, "dt": dt,
+            "method": method, "reduction": reduction, "precision": precision, "l2": l2,
+            "state": state, "parallelism": f"replicas x{world}", "autotuned": autotuned}
 
 
 def metric_name(method):
@@ -392,6 +406,130 @@ def run_dim(args, rank, world, local):
         dist.destroy_process_group()
 
 
+class StepTimer:
+    """Times BIA steps of one configuration on the solver's stream: every step starts from
+    the seeded state (untimed device copy) after an untimed write of a 256 MB buffer (L2
+    flush), and is bracketed by CUDA events on the solver's stream; max over ranks."""
+
+    def __init__(self, solver, dist, dev, local):
+        import torch
+        self.torch = torch
+        self.solver = solver
+        self.dist = dist
+        self.dev = dev
+        self.local = local
+        self.flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def barrier(self):
+        self.torch.cuda.synchronize()
+        if self.dist is not None:
+            self.dist.barrier()
+            self.torch.cuda.synchronize()
+
+    def time(self, d_init, cfg, d_q, k_steps, warmup, sample_clocks=False):
+        """Returns (total ms over k_steps, clocks, counters, (kernel ms, kernel launches))."""
+        torch, solver = self.torch, self.solver
+        stream = solver.stream
+        d_state = d_init.clone()
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                d_state.copy_(d_init)
+                solver.step(d_state, cfg, q=d_q, stats=False)
+        solver.counters(reset=True)
+        solver.set_timing(True)
+        solver.kernel_ms()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(k_steps)]
+        sampler = ClockSampler(self.local) if sample_clocks else None
+        self.barrier()
+        if sampler:
+            sampler.start()
+        with torch.cuda.stream(stream):
+            for k in range(k_steps):
+                d_state.copy_(d_init)              # untimed: every step starts from the seeded state
+                self.flush.zero_()                 # untimed L2 flush (256 MB > 126 MB L2)
+                ev[k][0].record(stream)
+                solver.step(d_state, cfg, q=d_q, stats=False)
+                ev[k][1].record(stream)
+        self.barrier()
+        clk = sampler.stop() if sampler else None
+        total = float(sum(a.elapsed_time(b) for a, b in ev))
+        kern = solver.kernel_ms()
+        solver.set_timing(False)
+        counters = solver.counters(reset=True)
+        return _max_over_ranks(self.dist, total, self.dev), clk, counters, kern
+
+    def graph_run(self, d_init, cfg, d_q, steps):
+        """`steps` consecutive steps (a trajectory) replayed from one CUDA graph; returns
+        (ms, counters)."""
+        torch, solver = self.torch, self.solver
+        stream = solver.stream
+        t = d_init.clone()
+        with torch.cuda.stream(stream):
+            solver.run(t, cfg, steps, q=d_q, graph=True, stats=False)   # capture and warm
+            t.copy_(d_init)
+        solver.counters(reset=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        self.barrier()
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            solver.run(t, cfg, steps, q=d_q, graph=True, stats=False)
+            e1.record(stream)
+        self.barrier()
+        return _max_over_ranks(self.dist, e0.elapsed_time(e1), self.dev), solver.counters(reset=True)
+
+
+def newton_per_pair(st, method):
+    """Newton iterations per pair of each solver a step of `method` ran (from its counters)."""
+    classical = st["hyperbola"] + st["ellipse"] + st["parabola"]
+    uv_pairs = st["universal"] + st["degenerate"] + st["learned_fallbacks"]
+    return {
+        "classical_per_pair": st["iterations"] / classical if classical else None,
+        "universal_per_pair": st["iter_universal"] / uv_pairs if uv_pairs else None,
+        "learned_fp32_per_learned_pair": (st["learned_fp32_steps"] / st["learned"]
+                                          if method == 3 and st["learned"] else None),
+        "learned_fp64_per_learned_pair": (1.0 if method == 3 and st["learned"] else None),
+        "learned_pairs": st["learned"] if method == 3 else None,
+    }
+
+
+def error_vs_oracle(solver, cfg, d_init, d_q, state, eps, q, dt, nsel=16, nquad=6, seed=17):
+    """One step of `cfg` from the seeded state, outside any timed region.  The displacement
+    of `nsel` seeded particles against the oracle (the reference's FP64 CPU ALG path; max
+    error over max|x| and max|v|), and `nquad` of them against the quad-precision oracle (the
+    same algorithm without rounding: the exact step), as relative errors of the interaction
+    displacement dX - U dt and of the kick dV, each against its own norm.  The FP64 oracle's
+    own interaction errors are given beside them."""
+    import torch
+
+    import oracle
+    t = d_init.clone()
+    d = torch.zeros_like(t)
+    with torch.cuda.stream(solver.stream):
+        solver.step(t, cfg, q=d_q, disp=d, stats=False)
+    torch.cuda.synchronize()
+    disp = d.cpu().numpy()
+    n = state.shape[1]
+    sel = np.random.default_rng(seed).choice(n, nsel, replace=False)
+    got = disp[:, sel].T
+    ref = oracle.particle_disp(state, eps, dt, sel, q=q)
+    refq = oracle.particle_disp(state, eps, dt, sel[:nquad], q=q, quad=True)
+    drift = state[3:, sel[:nquad]].T * dt
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    return {
+        "sample": f"{nsel} seeded particles against the FP64 oracle, {nquad} of them against the quad oracle",
+        "pos_max_err_over_max_x": float(np.abs(got[:, :3] - ref[:, :3]).max() / np.abs(state[:3]).max()),
+        "vel_max_err_over_max_v": float(np.abs(got[:, 3:] - ref[:, 3:]).max() / np.abs(state[3:]).max()),
+        "interaction_dx_rel_err_vs_exact": rel(got[:nquad, :3] - drift, refq[:, :3] - drift),
+        "dv_rel_err_vs_exact": rel(got[:nquad, 3:], refq[:, 3:]),
+        "fp64_oracle_interaction_dx_rel_err_vs_exact": rel(ref[:nquad, :3] - drift, refq[:, :3] - drift),
+        "fp64_oracle_dv_rel_err_vs_exact": rel(ref[:nquad, 3:], refq[:, 3:]),
+    }
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -427,48 +565,7 @@ def main():
     d_init = torch.tensor(state, device=dev)
     d_state = d_init.clone()
     d_q = torch.tensor(q, device=dev) if q is not None else None
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-
-    def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-            torch.cuda.synchronize()
-
-    def max_over_ranks(v):
-        return _max_over_ranks(dist, v, dev)
-
-    def timed_steps(c, k_steps, sample_clocks=False):
-        """k_steps steps of config c, each from the seeded state (untimed device copy) after
-        an untimed L2 flush, each bracketed by CUDA events on the solver's stream.  Returns
-        (total ms, clocks, counters, (kernel ms, kernel launches))."""
-        with torch.cuda.stream(stream):
-            for _ in range(args.warmup):
-                d_state.copy_(d_init)
-                solver.step(d_state, c, q=d_q, stats=False)
-        solver.counters(reset=True)
-        solver.set_timing(True)
-        solver.kernel_ms()
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(k_steps)]
-        sampler = ClockSampler(local) if sample_clocks else None
-        barrier()
-        if sampler:
-            sampler.start()
-        with torch.cuda.stream(stream):
-            for k in range(k_steps):
-                d_state.copy_(d_init)              # untimed: every step starts from the seeded state
-                flush.zero_()                      # untimed L2 flush (256 MB > 126 MB L2)
-                ev[k][0].record(stream)
-                solver.step(d_state, c, q=d_q, stats=False)
-                ev[k][1].record(stream)
-        barrier()
-        clk = sampler.stop() if sampler else None
-        total = float(sum(a.elapsed_time(b) for a, b in ev))
-        kern = solver.kernel_ms()
-        solver.set_timing(False)
-        counters = solver.counters(reset=True)
-        return max_over_ranks(total), clk, counters, kern
+    timer = StepTimer(solver, dist, dev, local)
 
     # the ALG pair-kernel shape for this size, chosen by the autotuner on this GPU
     tuned = None
@@ -479,7 +576,8 @@ def main():
     if method == 3 and not args.no_autotune:
         lvar, lms = solver.autotune(d_state, cfg, q=d_q)
         tuned = dict(tuned or {}, learned_layout=("one_kernel", "split")[lvar], learned_ms=lms)
-    total_ms, clocks, stats, (kern_ms, kern_launches) = timed_steps(cfg, steps, sample_clocks=True)
+    total_ms, clocks, stats, (kern_ms, kern_launches) = timer.time(d_init, cfg, d_q, steps, args.warmup,
+                                                                   sample_clocks=True)
     value = world * steps * pairs / (total_ms * 1e-3)
 
     # end-to-end through the host-buffer call with pinned host memory
@@ -491,16 +589,16 @@ def main():
         hq = h_q.numpy() if h_q is not None else None
         solver.run_host(hs, cfg, 1, q=hq)      # warm: host-path graph built
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        barrier()
+        timer.barrier()
         t0 = time.perf_counter()
         e0.record(stream)
         for _ in range(steps):
             np.copyto(hs, state)               # each step's input: the seeded state (timed)
             solver.run_host(hs, cfg, 1, q=hq)
         e1.record(stream)
-        barrier()
+        timer.barrier()
         wall = time.perf_counter() - t0
-        e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+        e2e_ms = _max_over_ranks(dist, e0.elapsed_time(e1), dev)
         h2d = 6 * n * 8 + (n * 8 if q is not None else 0)
         e2e = {"value": world * steps * pairs / (e2e_ms * 1e-3), "unit": "pair-updates/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 6 * n * 8,
@@ -525,7 +623,7 @@ def main():
     elif method == 1 and (nwb + 31) // 32 >= 2 * sms:
         kernel_name = "bia_pair_phase_kernel<true, 32, 1>"
     else:
-        kernel_name = "bia_pair_tiles_kernel<true>"
+        kernel_name = "bia_pair_tiles_kernel<true, %d>" % method
     flops_total = pair_flops(stats, method)
     per_launch_flops = flops_total / max(kern_launches, 1)
     per_launch_s = kern_ms * 1e-3 / max(kern_launches, 1)
@@ -552,13 +650,13 @@ def main():
     plain = None
     if method != 1 and not args.no_plain:
         cfg_p = default_config(eps_th=eps, dt=dt, method=1)
-        p_ms, _, p_stats, _ = timed_steps(cfg_p, steps)
+        p_ms, _, p_stats, _ = timer.time(d_init, cfg_p, d_q, steps, args.warmup)
         a_state = d_init.clone()
         b_state = d_init.clone()
         with torch.cuda.stream(stream):
             solver.step(a_state, cfg_p, q=d_q, stats=False)
             solver.step(b_state, cfg, q=d_q, stats=False)
-        barrier()
+        timer.barrier()
         aa, bb = a_state.cpu().numpy(), b_state.cpu().numpy()
         solver.counters(reset=True)
         plain = {"method": "alg", "value": world * steps * pairs / (p_ms * 1e-3),
@@ -567,28 +665,31 @@ def main():
                                                         np.linalg.norm(aa[:3])),
                  "one_step_rel_vel_err_vs_plain": float(np.linalg.norm(bb[3:] - aa[3:]) /
                                                         np.linalg.norm(aa[3:])),
-                 "newton_iterations_per_classical_pair": p_stats["iterations"] / max(
-                     1, p_stats["hyperbola"] + p_stats["ellipse"] + p_stats["parabola"])}
+                 "newton_iterations": newton_per_pair(p_stats, 1)}
 
-    # the same workload advanced by the universal-variable method (every pair on the
-    # Stumpff-function solver): K steps timed as one graph launch
+    # the universal-variable method (every pair on the Stumpff-function solver, this
+    # library's fastest plain FP64 form), timed exactly as the measured form
     universal = None
     if method != 2 and not args.no_universal:
         cfg_u = default_config(eps_th=eps, dt=dt, method=2)
-        u_state = d_init.clone()
-        with torch.cuda.stream(stream):
-            solver.run(u_state, cfg_u, 1, q=d_q, graph=True, stats=False)  # warm graph
-            u_state.copy_(d_init)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            barrier()
-            e0.record(stream)
-            solver.run(u_state, cfg_u, steps, q=d_q, graph=True, stats=False)
-            e1.record(stream)
-            barrier()
-        u_ms = max_over_ranks(e0.elapsed_time(e1))
-        ust = solver.counters(reset=True)
-        universal = {"value": world * steps * pairs / (u_ms * 1e-3), "unit": "pair-updates/s",
-                     "ms_per_step": u_ms / steps, "graph": True, "nonconverged": ust["nonconverged"]}
+        u_ms, _, u_stats, _ = timer.time(d_init, cfg_u, d_q, steps, args.warmup)
+        universal = {"method": "universal", "value": world * steps * pairs / (u_ms * 1e-3),
+                     "unit": "pair-updates/s", "ms_per_step": u_ms / steps,
+                     "nonconverged": u_stats["nonconverged"],
+                     "newton_iterations": newton_per_pair(u_stats, 2)}
+    # the learned form against the fastest plain FP64 form measured in this run
+    learned_vs_best_plain = None
+    if method == 3:
+        plain_ms = [x["ms_per_step"] for x in (plain, universal) if x is not None]
+        if plain_ms:
+            learned_vs_best_plain = {"ratio": min(plain_ms) / (total_ms / steps),
+                                     "best_plain": "universal" if universal and universal["ms_per_step"] == min(plain_ms)
+                                     else "alg", "best_plain_ms_per_step": min(plain_ms),
+                                     "learned_ms_per_step": total_ms / steps}
+
+    errors = None
+    if rank == 0 and world == 1 and not args.no_oracle_check:
+        errors = error_vs_oracle(solver, cfg, d_init, d_q, state, eps, q, dt)
 
     # the reference's own GPU pair kernel (bia/find_dXYUV_kernel.cu built for sm_100a by
     # oracle/build_ref.sh) on a seeded row sample of a global-coupling workload
@@ -596,55 +697,22 @@ def main():
     # through its per-particle entry with its own per-call allocation and copies
     ref_gpu = None
     if rank == 0 and world == 1 and not args.no_reference_gpu:
-        import oracle
-        if oracle.ref_gpu_available():
-            ps, peps, _, pdt, _ = initial.make("plummer_32768")
-            pn = ps.shape[1]
-            rows = np.random.default_rng(5).choice(np.arange(2, pn + 1), 256, replace=False)
-            oracle.ref_gpu_rows(ps, peps, pdt, rows[:4])
-            t0 = time.perf_counter()
-            oracle.ref_gpu_rows(ps, peps, pdt, rows)
-            el = time.perf_counter() - t0
-            rpairs = int(sum(pn - r for r in rows))
-            # ours through the same per-row drop-in entry (host buffers, one row per call)
-            from bia_3d_gpu_b200 import find_dxyuv_kernel
-            acc = [np.zeros(pn) for _ in range(6)]
-            rel, out = np.zeros(6 * pn), np.zeros(6 * pn)
-
-            def _our_rows(rr):
-                for r_ in rr:
-                    for k_ in range(6):
-                        rel[k_::6] = ps[k_, r_ - 1] - ps[k_]
-                    find_dxyuv_kernel(1, pn, int(r_), peps, pdt, 18, *acc, rel, out)
-
-            _our_rows(rows[:4])
-            t0 = time.perf_counter()
-            _our_rows(rows)
-            el_ours = time.perf_counter() - t0
-            pt = torch.tensor(ps, device=dev)
-            pcfg = default_config(eps_th=peps, dt=pdt)
-            with torch.cuda.stream(stream):
-                solver.step(pt, pcfg, stats=False)
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                for _ in range(3):
-                    solver.step(pt, pcfg, stats=False)
-                e1.record(stream)
-            torch.cuda.synchronize()
-            ref_gpu = {"workload": "plummer_32768", "unit": "pair-updates/s",
-                       "reference_kernel": rpairs / el,
-                       "ours_dropin_rows": rpairs / el_ours,
-                       "ours_alg": 3 * (pn * (pn - 1) // 2) / (e0.elapsed_time(e1) * 1e-3),
-                       "sample": f"{len(rows)} seeded rows I through find_dxyuv_kernel_ (reference, "
-                                 f"and ours as reference_kernel / ours_dropin_rows; ours_alg "
-                                 f"is the whole-step kernel path), "
-                                 f"{rpairs} pairs, {el:.2f} s wall"}
+        ref_gpu = reference_gpu_kernel(solver, dev, stream)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, cores, sample = cpu_sample(state, eps, q, dt, 1 if method == 3 else method, args.cpu_seconds)
+        cmethod = {0: 0, 1: 1, 2: 1, 3: 1}[method]
+        v, cores, sample = cpu_sample(state, eps, q, dt, cmethod, args.cpu_seconds)
+        v1, _, sample1 = cpu_sample(state, eps, q, dt, cmethod, args.cpu_seconds / 2, seed=1, threads=1)
         cpu = {"value": v, "unit": "pair-updates/s", "cores": cores, "kind": "port",
-               "sample": sample}
+               "sample": sample,
+               "single_thread": {"value": v1, "unit": "pair-updates/s", "cores": 1, "sample": sample1,
+                                 "note": "the reference's own single-threaded CPU figure is for "
+                                         "its Fortran build (README.md:43)"}}
+
+    extras = None
+    if rank == 0 and world == 1 and not args.no_extras and args.n is None:
+        extras = run_extras(solver, timer, args)
 
     if dist is not None:
         dist.barrier()
@@ -654,35 +722,130 @@ def main():
             "unit": "pair-updates/s", "n_gpus": world, "steps": steps, "warmup": args.warmup,
             "ms_per_step": total_ms / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": args.workload, "n": n, "pairs_per_step": pairs, "dt": dt,
-                       "method": args.method, "reduction": "deterministic",
-                       "precision": ("heads: BF16 operands, FP32 accumulation; first correction "
-                                     "FP32; final step, composition and sums FP64"
-                                     if method == 3 else "FP64"),
-                       "l2": "256 MB buffer written between timed steps (untimed)",
-                       "state": "reset to the seeded state before every timed step (untimed "
-                                "device copy; the e2e loop copies it into the host buffer)",
-                       "parallelism": f"replicas x{world}", "autotuned": tuned},
+            "config": config_keys(args.workload, n, dt, args.method, world, reduction="deterministic",
+                                  precision=("heads: BF16 operands, FP32 accumulation; first correction "
+                                             "FP32; final step, composition and sums FP64"
+                                             if method == 3 else "FP64"),
+                                  l2="256 MB buffer written between timed steps (untimed)",
+                                  state="reset to the seeded state before every timed step (untimed "
+                                        "device copy; the e2e loop copies it into the host buffer)",
+                                  autotuned=tuned),
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-            "gpu_launches": (3 if split else 2) * steps, "plain_fp64": plain, "universal": universal,
+            "gpu_launches": (3 if split else 2) * steps,
+            "learned_vs_best_plain": learned_vs_best_plain,
+            "error_vs_oracle": errors,
+            "plain_fp64": plain, "universal": universal,
             "reference_gpu_kernel": ref_gpu,
             "learned_pair_fraction": stats["learned"] / max(1, steps * pairs) if method == 3 else None,
             "stats": {k: v for k, v in stats.items()},
             # Newton iterations per pair of each solver the measured form ran
-            "newton_iterations": {
-                "classical_per_pair": (stats["iterations"] / max(1, stats["hyperbola"] + stats["ellipse"]
-                                                                 + stats["parabola"])) if method == 1 else None,
-                "universal_per_pair": stats["iter_universal"] / max(
-                    1, stats["universal"] + stats["degenerate"] + stats["learned_fallbacks"]),
-                "learned_fp32_per_learned_pair": (stats["learned_fp32_steps"] / max(1, stats["learned"])
-                                                  if method == 3 else None),
-                "learned_fp64_per_learned_pair": (1.0 if method == 3 else None),  # one Halley step each
-            },
+            "newton_iterations": newton_per_pair(stats, method),
+            "extra_workloads": extras,
         }
         print(json.dumps(line), flush=True)
     solver.close()
     if dist is not None:
         dist.destroy_process_group()
+
+
+def reference_gpu_kernel(solver, dev, stream):
+    """The reference's GPU kernel through its per-row entry against ours (see main)."""
+    import torch
+
+    import oracle
+    from bia_3d_gpu_b200 import default_config, find_dxyuv_kernel, initial
+    if not oracle.ref_gpu_available():
+        return None
+    ps, peps, _, pdt, _ = initial.make("plummer_32768")
+    pn = ps.shape[1]
+    rows = np.random.default_rng(5).choice(np.arange(2, pn + 1), 256, replace=False)
+    oracle.ref_gpu_rows(ps, peps, pdt, rows[:4])
+    t0 = time.perf_counter()
+    oracle.ref_gpu_rows(ps, peps, pdt, rows)
+    el = time.perf_counter() - t0
+    rpairs = int(sum(pn - r for r in rows))
+    # ours through the same per-row drop-in entry (host buffers, one row per call)
+    acc = [np.zeros(pn) for _ in range(6)]
+    rel, out = np.zeros(6 * pn), np.zeros(6 * pn)
+
+    def _our_rows(rr):
+        for r_ in rr:
+            for k_ in range(6):
+                rel[k_::6] = ps[k_, r_ - 1] - ps[k_]
+            find_dxyuv_kernel(1, pn, int(r_), peps, pdt, 18, *acc, rel, out)
+
+    _our_rows(rows[:4])
+    t0 = time.perf_counter()
+    _our_rows(rows)
+    el_ours = time.perf_counter() - t0
+    pt = torch.tensor(ps, device=dev)
+    pcfg = default_config(eps_th=peps, dt=pdt)
+    with torch.cuda.stream(stream):
+        solver.step(pt, pcfg, stats=False)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            solver.step(pt, pcfg, stats=False)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    return {"workload": "plummer_32768", "unit": "pair-updates/s",
+            "reference_kernel": rpairs / el,
+            "ours_dropin_rows": rpairs / el_ours,
+            "ours_alg": 3 * (pn * (pn - 1) // 2) / (e0.elapsed_time(e1) * 1e-3),
+            "sample": f"{len(rows)} seeded rows I through find_dxyuv_kernel_ (reference, "
+                      f"and ours as reference_kernel / ours_dropin_rows; ours_alg "
+                      f"is the whole-step kernel path), "
+                      f"{rpairs} pairs, {el:.2f} s wall"}
+
+
+def run_extras(solver, timer, args):
+    """The other configurations, each timed as the main line (steps from the seeded state,
+    L2 flushed between them, CUDA events), with fewer steps: {workload: {form: result}}."""
+    import torch
+
+    from bia_3d_gpu_b200 import default_config, initial
+    out = {}
+    dev = timer.dev
+
+    def forms(name, entries, steps, warmup):
+        s, eps, q, dt, _ = initial.make(name)
+        n = s.shape[1]
+        pairs = n * (n - 1) // 2
+        d_init = torch.tensor(s, device=dev)
+        d_q = torch.tensor(q, device=dev) if q is not None else None
+        res = {"n": n, "dt": dt, "steps": steps, "warmup": warmup}
+        for label, m, kw in entries:
+            fdt = kw.pop("dt", dt)
+            c = default_config(eps_th=eps, dt=fdt, method=m, **kw)
+            ms, _, st, _ = timer.time(d_init, c, d_q, steps, warmup)
+            res[label] = {"ms_per_step": ms / steps, "pair_updates_per_s": steps * pairs / (ms * 1e-3),
+                          "newton_iterations": newton_per_pair(st, m), "nonfinite": st["nonfinite"]}
+            if fdt != dt:
+                res[label]["dt"] = fdt
+            if m == 0:
+                res[label]["rkf_steps_per_pair"] = st["rkf_steps"] / max(1, st["rkf"] + st["degenerate"])
+        return res
+
+    out["coulomb_cube_32768"] = forms("coulomb_cube_32768", [
+        ("alg", 1, {}), ("universal", 2, {}), ("learned", 3, {}),
+        ("rkf_rel_1e-12", 0, {"rkf_relerr": 1e-12, "rkf_abserr": 1e-16}),
+        ("rkf_reference_tol_0_1e-16", 0, {})], steps=3, warmup=3)
+    out["coulomb_cube_32768"]["learned_long_step_dt_1e-3"] = forms(
+        "coulomb_cube_32768", [("learned", 3, {"dt": 1e-3}), ("universal", 2, {"dt": 1e-3})],
+        steps=3, warmup=3)
+    out["cold_ball_131072"] = forms("cold_ball_131072", [("alg", 1, {}), ("universal", 2, {}),
+                                                         ("learned", 3, {})], steps=3, warmup=3)
+    out["gravity_ball_1332"] = forms("gravity_ball_1332", [("alg", 1, {}), ("universal", 2, {}),
+                                                           ("learned", 3, {})], steps=20, warmup=3)
+    # a trajectory: the learned configuration's 100 consecutive steps in one CUDA graph
+    s, eps, q, dt, steps_cfg = initial.make("plummer_32768")
+    d_init = torch.tensor(s, device=dev)
+    traj = {"steps": steps_cfg, "graph": True}
+    for label, m in (("learned", 3), ("universal", 2)):
+        ms, st = timer.graph_run(d_init, default_config(eps_th=eps, dt=dt, method=m), None, steps_cfg)
+        traj[label] = {"ms_per_step": ms / steps_cfg, "newton_iterations": newton_per_pair(st, m)}
+    out["plummer_32768_trajectory"] = traj
+    return out
 
 
 if __name__ == "__main__":

@@ -162,5 +162,5 @@ EXPORTED_SYMBOLS = ("bia_config_default", "bia_context_create", "bia_context_des
                     "bia_ensemble_create", "bia_ensemble_destroy", "bia_ensemble_particles",
                     "bia_ensemble_run", "bia_ensemble_energy",
                     "bia_context_set_heads", "bia_learned_head_eval", "bia_context_autotune",
-                    "bia_selftest_wait_timeout",
+                    "bia_selftest_wait_timeout", "bia_step_noalloc",
                     "bia_last_error", "find_dxyuv_kernel_", "invariance_gpu_")

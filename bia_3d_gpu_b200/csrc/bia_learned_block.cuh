@@ -69,12 +69,14 @@ __device__ __forceinline__ void cta_scan2(MlpSmem &S, int a, int b, int &oa, int
 
 // The split learned step's plain part of warp-block (bi, bj) of the system x..w[0, n)
 // (charges q, coupling eps_th): lanes walk the rotation offsets; every pair gets the
-// universal-variable prepare, then the heads' domain test on those quantities
-// (learned_filter); pairs outside it are solved here (uv_halfdisp in its pieces), the others
-// are left to the learned warp-block.  Returns the lane's mask of left pairs (bit k: column
-// (lane + k) mod 32) with the row sums racc and column sums cacc of the solved ones.  The
-// pairs are counted as universal-variable pairs, degenerate ones included, as
-// BIA_METHOD_UNIVERSAL counts them (the exact degenerate test costs 7 % here).
+// universal-variable prepare and the fifth-order start (uv_start_fast).  A pair whose start
+// is already exact needs no iteration and is composed here.  Of the others, those inside a
+// head's domain (learned_filter) are left to the learned warp-block, where the head's guess
+// replaces the Newton iterations; the rest run the plain Newton iteration here.  Returns the
+// lane's mask of left pairs (bit k: column (lane + k) mod 32) with the row sums racc and
+// column sums cacc of the solved ones.  The pairs are counted as universal-variable pairs,
+// degenerate ones included, as BIA_METHOD_UNIVERSAL counts them (the exact degenerate test
+// costs 7 % here).
 __device__ __forceinline__ uint32_t rest_block_solve(const double *x, const double *y, const double *z,
                                                      const double *u, const double *v, const double *w,
                                                      const double *q, int n, double eps_th, double dt, int bi,
@@ -105,18 +107,20 @@ __device__ __forceinline__ uint32_t rest_block_solve(const double *x, const doub
             const double g[3] = {si[3] - sc[3], si[4] - sc[4], si[5] - sc[5]};
             const double eps_ij = q ? eps_th * si[6] * sc[6] : eps_th;
             const UvPair p = uv_prepare(eps_ij, r, g);
-            if (learned_filter(p, dt)) {
-                learned |= 1u << k;
-            } else if (dt != 0.0) {
+            if (dt != 0.0) {
                 bool exact;
                 double s = uv_start_fast(p, dt, exact);
-                double ifp = 0.0;
-                const int it = exact ? 0 : uv_iterate(p, dt, s, &ifp);
-                uv_compose<true>(p, s, r, g, h, exact ? p.ir0 : ifp);
-                cnt.it_uv += it;
-                if (it > kUvItMax) cnt.nonconverged++;
-                cnt.cls[kUniversal]++;
-                count_nonfinite(h, cnt);
+                if (!exact && learned_filter(p, dt)) {
+                    learned |= 1u << k;
+                } else {
+                    double ifp = 0.0;
+                    const int it = exact ? 0 : uv_iterate(p, dt, s, &ifp);
+                    uv_compose<true>(p, s, r, g, h, exact ? p.ir0 : ifp);
+                    cnt.it_uv += it;
+                    if (it > kUvItMax) cnt.nonconverged++;
+                    cnt.cls[kUniversal]++;
+                    count_nonfinite(h, cnt);
+                }
             } else {
                 cnt.cls[kUniversal]++;
             }
@@ -223,10 +227,15 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
                 const unsigned bit = 1u << k;
                 int kind = kLearnedPlain;
                 if (learned_candidate(eps_ij, dt, r, g)) {
-                    LearnedPair L;
-                    learned_prepare(eps_ij, dt, r, g, L);
-                    kind = L.kind;
-                    if (kind != kLearnedPlain) myrows[k] = pack_bf16(L.x0, L.x1);
+                    // the split step's routing: a pair whose fifth-order start is exact stays plain
+                    bool exact;
+                    uv_start_fast(uv_prepare(eps_ij, r, g), dt, exact);
+                    if (!exact) {
+                        LearnedPair L;
+                        learned_prepare(eps_ij, dt, r, g, L);
+                        kind = L.kind;
+                        if (kind != kLearnedPlain) myrows[k] = pack_bf16(L.x0, L.x1);
+                    }
                 }
                 if (kind == kLearnedHyp) mh |= bit;
                 else if (kind == kLearnedEll) me |= bit;
@@ -305,7 +314,7 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
                     g[c] = si[3 + c] - ws[(3 + c) * 32 + src];
                 }
                 const double eps_ij = hq ? B.eps_th * si[6] * ws[6 * 32 + src] : B.eps_th;
-                const int it = uv_halfdisp(eps_ij, dt, r, g, h);
+                const int it = uv_halfdisp_fast(eps_ij, dt, r, g, h);
                 cnt.it_uv += it;
                 if (it > kUvItMax) cnt.nonconverged++;
                 cnt.cls[pair_degenerate(r, g) ? kDegenerate : kUniversal]++;

@@ -326,11 +326,18 @@ __device__ __forceinline__ int hyperbola(double eps_th, double dt, int ITR, cons
         theta_end = th_gss_end;
         error_ = error_gss_;
     }
-    // minimum-residual Newton loop with cycle detection (bia/find_hyperbola.f90:93-120)
+    // minimum-residual Newton loop with cycle detection (bia/find_hyperbola.f90:93-120).
+    // The reference compares each residual with every earlier one (error_restore_); here
+    // the last four are kept in registers (h0 newest): an indexed history array lives in
+    // local memory, whose write-back was most of the ALG kernel's DRAM traffic.  A cycle
+    // only arises once the iteration sits at the rounding floor, where the iterates that
+    // repeat are a few ulps apart; cycles of period 1-4 stop at the same iteration as in
+    // the reference, a longer one runs on to the ITR cap with the same stock update rule.
     double err_stock = error_;
     double theta_stock = theta_end;
     double best_res = fabs(error_);
-    double hist[64];
+    const double kNoResidual = __longlong_as_double(0x7ff8000000000000LL);  // compares unequal
+    double h0 = kNoResidual, h1 = kNoResidual, h2 = kNoResidual, h3 = kNoResidual;
     int IR = 0;
     *bracket_exit = 0;
     while (IR < ITR) {
@@ -344,11 +351,11 @@ __device__ __forceinline__ int hyperbola(double eps_th, double dt, int ITR, cons
         error_ = e;
         theta_end = (e == 0.0) ? theta_now : theta_now - e / d;
         IR++;
-        bool cycle = false;
-        for (int num = IR - 1; num >= 1; num--)
-            if (hist[num] == error_) { cycle = true; break; }
-        if (cycle) break;
-        hist[IR] = error_;
+        if (error_ == h0 || error_ == h1 || error_ == h2 || error_ == h3) break;
+        h3 = h2;
+        h2 = h1;
+        h1 = h0;
+        h0 = error_;
         best_res = fmin(best_res, fabs(error_));
         if (fabs(error_) < fabs(err_stock)) {
             err_stock = error_ * b_0 / g_0;

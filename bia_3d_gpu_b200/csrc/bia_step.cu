@@ -1019,18 +1019,24 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocPartDoubles + 
 
 // Device address of g_noalloc_scratch per device ordinal.  The host-side name of the
 // array is only a stand-in: it must be resolved with cudaGetSymbolAddress while the
-// device is current.
+// device is current.  It is resolved again on every call made outside stream capture (a
+// cheap query that allocates nothing), so a device reset or a recreated primary context,
+// which loads the module again at a new address, is picked up; during a capture the
+// address of the last call outside capture is used.
 static double *g_noalloc_addr[kNoAllocMaxDevices] = {};
 static std::mutex g_noalloc_mutex;
 
-static int noalloc_scratch(double **out)
+static int noalloc_scratch(cudaStream_t s, double **out)
 {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_status(e);
     if (dev < 0 || dev >= kNoAllocMaxDevices) return BIA_ERR_INVALID_ARGUMENT;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(s, &cap);
+    if (e != cudaSuccess) return cuda_status(e);
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_addr[dev]) {
+    if (cap == cudaStreamCaptureStatusNone || !g_noalloc_addr[dev]) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return cuda_status(e);
@@ -1046,16 +1052,16 @@ extern "C" int bia_step_noalloc(const bia_config *cfg, int n, double *x, double 
                                 double *v, double *w, const double *q, double *disp, void *stream)
 {
     int st = validate(cfg, n, x, y, z, u, v, w);
-    if (st != BIA_OK) return st;
-    if (n > kNoAllocMaxN) return BIA_ERR_INVALID_ARGUMENT;  // beyond the fixed scratch
-    double *part = nullptr;
-    st = noalloc_scratch(&part);
-    if (st != BIA_OK) return st;
-    unsigned long long *counters = (unsigned long long *)(part + kNoAllocPartDoubles);
+    if (st != BIA_OK) return set_last_error(st);
+    if (n > kNoAllocMaxN) return set_last_error(BIA_ERR_INVALID_ARGUMENT);  // beyond the fixed scratch
     cudaStream_t s = (cudaStream_t)stream;
+    double *part = nullptr;
+    st = noalloc_scratch(s, &part);
+    if (st != BIA_OK) return set_last_error(st);
+    unsigned long long *counters = (unsigned long long *)(part + kNoAllocPartDoubles);
     // the partials are fully rewritten by every step; only the counters start at zero
     cudaError_t e = cudaMemsetAsync(counters, 0, kNumStats * sizeof(unsigned long long), s);
-    if (e != cudaSuccess) return cuda_status(e);
+    if (e != cudaSuccess) return set_last_error(cuda_status(e));
     const int nb = (n + 31) / 32;
     StepArgs A{};
     A.x = x; A.y = y; A.z = z; A.u = u; A.v = v; A.w = w; A.q = q;
@@ -1084,7 +1090,7 @@ extern "C" int bia_step_noalloc(const bia_config *cfg, int n, double *x, double 
     U.nparts = nb;
     U.dt = cfg->dt;
     bia_reduce_update_kernel<<<(n + 31) / 32, kReduceThreads, 0, s>>>(U);
-    return cuda_status(cudaGetLastError());
+    return set_last_error(cuda_status(cudaGetLastError()));
 }
 
 // ---------------------------------------------------------------------------------------

@@ -164,9 +164,12 @@ int bia_run_host(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
    disp [6][n]; kernels and one memset are enqueued on `stream` (a cudaStream_t, NULL =
    legacy default stream) and the call returns without synchronising.  The reduction is
    always the deterministic one (cfg->deterministic is ignored); no counters are returned.
-   The first call on a device resolves the array's device address (cudaGetSymbolAddress),
-   so make that first call before any stream capture.  All calls share the one array:
-   calls whose work overlaps on the GPU (different streams, or host threads) race. */
+   Every call made outside stream capture resolves the array's device address
+   (cudaGetSymbolAddress, no allocation); a call during a capture uses the address of the
+   last call outside it, so make the first call on a device before any stream capture.  All
+   calls share the one array: calls whose work overlaps on the GPU (different streams, or
+   host threads) race.  The status (also kept for bia_last_error) comes from the launch
+   checks, so an asynchronous error left on the device by earlier work can surface here. */
 int bia_step_noalloc(const bia_config *cfg, int n, double *x, double *y, double *z, double *u,
                      double *v, double *w, const double *q, double *disp, void *stream);
 

@@ -5,8 +5,14 @@
 # invariance_gpu_ (bia/find_dXYUV_kernel.cu:526-561, bia/invariance.cu:50-110).
 # Only METHOD = 1 (ALG) of the kernel is ever called: its RKF mode reaches a
 # __syncthreads() inside divergent code (bia/bia-rkf.cu:102).
+#
+#   bash oracle/build_ref.sh <reference checkout>      (or BIA_REFERENCE_DIR=<checkout>)
 set -e
-REF=${1:-/root/reference}
+REF=${1:-${BIA_REFERENCE_DIR:-}}
+if [ -z "$REF" ]; then
+  echo "usage: build_ref.sh <reference checkout> (or set BIA_REFERENCE_DIR); skipping"
+  exit 0
+fi
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 mkdir -p "$OUT"

@@ -56,4 +56,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("BIA_REFERENCE_DIR")
+    if not root:
+        sys.exit("usage: make_golden.py <reference checkout> (or set BIA_REFERENCE_DIR)")
+    main(root)

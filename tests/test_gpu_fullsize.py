@@ -6,18 +6,33 @@ import numpy as np
 import pytest
 
 import oracle
-from bia_3d_gpu_b200 import BIASolver, default_config, initial
+from bia_3d_gpu_b200 import (METHOD_ALG, METHOD_LEARNED, METHOD_UNIVERSAL, BIASolver, default_config,
+                             initial)
 
 pytestmark = pytest.mark.gpu
 
 
-def one_step(cuda, s, eps, dt, q=None):
+def one_step(cuda, s, eps, dt, q=None, method=METHOD_ALG):
     t = cuda.tensor(s, device="cuda")
     qt = cuda.tensor(q, device="cuda") if q is not None else None
     d = cuda.zeros_like(t)
     with BIASolver() as solver:
-        st = solver.step(t, default_config(eps_th=eps, dt=dt), q=qt, disp=d)
+        if method == METHOD_LEARNED:
+            solver.load_heads()
+        st = solver.step(t, default_config(eps_th=eps, dt=dt, method=method), q=qt, disp=d)
     return t.cpu().numpy(), d.cpu().numpy(), st
+
+
+def interaction_errors(got, ref, s, sel, dt):
+    """Relative errors of the interaction displacement dX - U dt and of the velocity kick dV
+    of the sampled particles, each against its own norm: the parts of the step that the pair
+    forces make, which a bar scaled by the state's size does not see (at dt = 1e-4 the
+    interaction part of dX is ~1e-9 while |x| ~ 1)."""
+    drift = s[3:, sel].T * dt
+    xi_got, xi_ref = got[:, :3] - drift, ref[:, :3] - drift
+    ex = float(np.linalg.norm(xi_got - xi_ref) / np.linalg.norm(xi_ref))
+    ev = float(np.linalg.norm(got[:, 3:] - ref[:, 3:]) / np.linalg.norm(ref[:, 3:]))
+    return ex, ev
 
 
 @pytest.mark.parametrize("name", ["coulomb_cube_32768", "plummer_32768"])
@@ -145,3 +160,61 @@ def test_cold_collapse_learned_next_to_plain_on_quad_subset(cuda):
     print(f"cold collapse subset n=4096, {steps} steps: energy drift plain {drift[METHOD_ALG]:.3e}, "
           f"learned {drift[METHOD_LEARNED]:.3e}")
     assert abs(drift[METHOD_LEARNED] - drift[METHOD_ALG]) <= 1e-12
+
+
+@pytest.mark.parametrize("method", [METHOD_UNIVERSAL, METHOD_LEARNED])
+@pytest.mark.parametrize("name", ["plummer_32768", "coulomb_cube_32768"])
+def test_fast_forms_full_size_match_oracle(cuda, name, method):
+    """The universal-variable and learned forms at the benchmark sizes (the learned form on
+    plummer_32768 is the headline configuration).  48 sampled particles against the oracle's
+    full pair sums of the reference's CPU ALG path (bia/bia.f90:141-196), to 1e-12 of the
+    state; 6 of them against the quad-precision oracle (the same algorithm without rounding,
+    the exact step): the interaction displacement dX - U dt and the kick dV each to 1e-10 of
+    their own norm.  The reference's FP64 ALG path itself is off the exact interaction
+    displacement by ~1e-4 (Plummer) and ~2e-7 (Coulomb) here: its conic solvers difference
+    absolute positions on the orbit, of magnitude r, so its rounding is 1e-16 r per pair
+    while the interaction part is ~1e-13 per pair; the universal-variable composition has
+    no such cancellation."""
+    s, eps, q, dt, _ = initial.make(name)
+    new, disp, st = one_step(cuda, s, eps, dt, q, method=method)
+    n = s.shape[1]
+    assert st["nonfinite"] == 0 and st["timeouts"] == 0 and st["nonconverged"] == 0
+    assert sum(st[k] for k in ("hyperbola", "ellipse", "parabola", "degenerate", "universal")) == n * (n - 1) // 2
+    sel = np.random.default_rng(17).choice(n, 48, replace=False)
+    ref = oracle.particle_disp(s, eps, dt, sel, q=q)
+    got = disp[:, sel].T
+    xscale = np.abs(s[:3]).max()
+    vscale = np.abs(s[3:]).max()
+    assert np.abs(got[:, :3] - ref[:, :3]).max() <= 1e-12 * xscale
+    assert np.abs(got[:, 3:] - ref[:, 3:]).max() <= 1e-12 * vscale
+    refq = oracle.particle_disp(s, eps, dt, sel[:6], q=q, quad=True)
+    ex, ev = interaction_errors(got[:6], refq, s, sel[:6], dt)
+    ex_ref, ev_ref = interaction_errors(ref[:6], refq, s, sel[:6], dt)
+    print(f"{name} method {method}: interaction dX rel err {ex:.2e} (FP64 ALG oracle {ex_ref:.2e}), "
+          f"dV rel err {ev:.2e} (oracle {ev_ref:.2e}); learned pairs {st['learned']}")
+    assert ex <= 1e-10 and ev <= 1e-12
+    kick = disp[3:].sum(axis=1)
+    assert np.abs(kick).max() <= 1e-12 * np.abs(disp[3:]).sum(axis=1).max()
+
+
+def test_learned_long_step_full_size(cuda):
+    """coulomb_cube_32768 at dt = 1e-3, a step long enough that the fifth-order start is
+    exact for almost no pair and ~45 % of the pairs start from a head's guess: sampled
+    particles against the FP64 oracle (1e-12 of the state) and the exact step (interaction
+    displacement and kick to 1e-10 of their norms)."""
+    s, eps, q, _, _ = initial.make("coulomb_cube_32768")
+    dt = 1e-3
+    n = s.shape[1]
+    new, disp, st = one_step(cuda, s, eps, dt, q, method=METHOD_LEARNED)
+    assert st["learned"] > 0.3 * n * (n - 1) // 2
+    assert st["learned_fallbacks"] <= 1e-3 * st["learned"]
+    assert st["nonfinite"] == 0 and st["timeouts"] == 0
+    sel = np.random.default_rng(18).choice(n, 24, replace=False)
+    ref = oracle.particle_disp(s, eps, dt, sel, q=q)
+    got = disp[:, sel].T
+    assert np.abs(got[:, :3] - ref[:, :3]).max() <= 1e-12 * np.abs(s[:3]).max()
+    assert np.abs(got[:, 3:] - ref[:, 3:]).max() <= 1e-12 * np.abs(s[3:]).max()
+    refq = oracle.particle_disp(s, eps, dt, sel[:6], q=q, quad=True)
+    ex, ev = interaction_errors(got[:6], refq, s, sel[:6], dt)
+    print(f"coulomb dt=1e-3 learned: {st['learned']} learned pairs, interaction dX rel err {ex:.2e}, dV {ev:.2e}")
+    assert ex <= 1e-10 and ev <= 1e-10

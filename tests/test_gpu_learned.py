@@ -3,8 +3,12 @@
 * The heads evaluated on the tensor cores (tcgen05, BF16 operands, FP32 accumulators in
   tensor memory) agree with the numpy evaluation of the same BF16 network.
 * Learned steps match the FP64 oracle's ALG step to the plain form's bar (<= 1e-12
-  relative, positions and velocities) on mixed-class systems; pairs inside a head's domain
-  take the learned path, few of them fall back to the plain solver.
+  relative, positions and velocities) on mixed-class systems.  A pair goes to a head when
+  its fifth-order universal-variable start is not exact and it lies inside a head's
+  domain; at the benchmark steps (dt = 1e-5 on the Coulomb cube) that is under 0.1 % of
+  the pairs, so these tests take steps of dt = 1e-3, where ~45 % of the Coulomb pairs and
+  a few percent of the gravitational ones start from a head's guess; few of them fall back
+  to the plain solver.
 * Deterministic mode is bitwise reproducible; the method is refused without heads.
 """
 import numpy as np
@@ -36,7 +40,7 @@ def test_tensor_core_heads_match_numpy(cuda, head):
     assert np.median(diff) <= 1e-5 and diff.max() <= 2e-3, (np.median(diff), diff.max())
 
 
-def _learned_vs_oracle(cuda, s, eps, dt, q=None, steps=1):
+def _learned_vs_oracle(cuda, s, eps, dt, q=None, steps=1, method=1):
     t = cuda.tensor(s, device="cuda")
     qt = cuda.tensor(q, device="cuda") if q is not None else None
     with BIASolver() as solver:
@@ -47,13 +51,21 @@ def _learned_vs_oracle(cuda, s, eps, dt, q=None, steps=1):
     g = t.cpu().numpy()
     r = s
     for _ in range(steps):
-        r, _, _ = oracle.bia_step(r, eps, dt, q=q)
+        r, _, _ = oracle.bia_step(r, eps, dt, q=q, method=method)
     return g, r, st
 
 
 def test_learned_coulomb_matches_oracle(cuda):
+    """Coulomb cube n = 1500 at dt = 1e-3: one learned step against the oracle's step of the
+    reference's ALG path; two steps against the oracle's FP64 universal-variable path.  (Two
+    steps of the FP64 ALG path are already ~3e-13 off the exact, quad-precision steps in
+    velocity at this step length, from its close pairs; the universal-variable path stays
+    within 3e-16 of them.)"""
     s, eps, q = initial.coulomb_cube(1500, seed=31, dmin=1e-2)
-    g, r, st = _learned_vs_oracle(cuda, s, eps, 1e-5, q=q, steps=2)
+    g, r, st = _learned_vs_oracle(cuda, s, eps, 1e-3, q=q, steps=1)
+    assert rel_err(g[:3], r[:3]) <= 1e-12 and rel_err(g[3:], r[3:]) <= 1e-12
+    assert max_rel_err(g[:3], r[:3]) <= 1e-12 and max_rel_err(g[3:], r[3:]) <= 1e-12
+    g, r, st = _learned_vs_oracle(cuda, s, eps, 1e-3, q=q, steps=2, method=2)
     assert rel_err(g[:3], r[:3]) <= 1e-12 and rel_err(g[3:], r[3:]) <= 1e-12
     assert max_rel_err(g[:3], r[:3]) <= 1e-12 and max_rel_err(g[3:], r[3:]) <= 1e-12
     assert st["learned"] > 0.3 * 1500 * 1499 // 2
@@ -65,7 +77,7 @@ def test_learned_coulomb_matches_oracle(cuda):
 
 def test_learned_gravity_ball_matches_oracle(cuda):
     s, eps = initial.gravity_ball(400, seed=32)
-    g, r, st = _learned_vs_oracle(cuda, s, eps, 1e-4, steps=3)
+    g, r, st = _learned_vs_oracle(cuda, s, eps, 1e-3, steps=3)
     assert rel_err(g[:3], r[:3]) <= 1e-12 and rel_err(g[3:], r[3:]) <= 1e-12
     assert max_rel_err(g[:3], r[:3]) <= 1e-12 and max_rel_err(g[3:], r[3:]) <= 1e-12
     assert st["learned"] > 0 and st["nonfinite"] == 0 and st["timeouts"] == 0
@@ -77,9 +89,10 @@ def test_learned_against_quad(cuda):
     qt = cuda.tensor(q, device="cuda")
     with BIASolver() as solver:
         solver.load_heads()
-        solver.step(t, default_config(eps_th=eps, dt=1e-5, method=METHOD_LEARNED), q=qt)
+        st = solver.step(t, default_config(eps_th=eps, dt=1e-3, method=METHOD_LEARNED), q=qt)
     g = t.cpu().numpy()
-    rq, _, _ = oracle.bia_step(s, eps, 1e-5, q=q, quad=True)
+    assert st["learned"] > 0.3 * 600 * 599 // 2
+    rq, _, _ = oracle.bia_step(s, eps, 1e-3, q=q, quad=True)
     assert max_rel_err(g[:3], rq[:3]) <= 1e-13 and max_rel_err(g[3:], rq[3:]) <= 1e-13
 
 
@@ -91,7 +104,7 @@ def test_learned_deterministic_and_atomic(cuda):
         qt = cuda.tensor(q, device="cuda")
         with BIASolver() as solver:
             solver.load_heads()
-            solver.step(t, default_config(eps_th=eps, dt=1e-5, method=METHOD_LEARNED, deterministic=det), q=qt)
+            solver.step(t, default_config(eps_th=eps, dt=1e-3, method=METHOD_LEARNED, deterministic=det), q=qt)
         outs.append(t.cpu().numpy())
     assert np.array_equal(outs[0], outs[1])
     assert rel_err(outs[2], outs[0]) <= 1e-15
@@ -105,24 +118,26 @@ def test_learned_needs_heads(cuda):
             solver.step(t, default_config(eps_th=eps, dt=1e-4, method=METHOD_LEARNED))
 
 
-def test_learned_split_step_matches_oracle(cuda):
+@pytest.mark.parametrize("dt", [1e-5, 1e-3])
+def test_learned_split_step_matches_oracle(cuda, dt):
     """The split learned step at n = 6000 (the plain pairs in the rest kernel, which lists
     the warp-blocks holding learned pairs; those in the list kernel, added onto the same
     partials): sampled particles against the oracle's full pair sums, and momentum from the
-    antisymmetry."""
+    antisymmetry.  At dt = 1e-5 almost every start is exact and the list is short; at
+    dt = 1e-3 ~45 % of the pairs are listed."""
     s, eps, q = initial.coulomb_cube(6000, seed=36)
     t = cuda.tensor(s, device="cuda")
     qt = cuda.tensor(q, device="cuda")
     d = cuda.zeros_like(t)
     with BIASolver() as solver:
         solver.load_heads()
-        st = solver.step(t, default_config(eps_th=eps, dt=1e-5, method=METHOD_LEARNED), q=qt, disp=d)
+        st = solver.step(t, default_config(eps_th=eps, dt=dt, method=METHOD_LEARNED), q=qt, disp=d)
     disp = d.cpu().numpy()
     n = 6000
-    assert st["learned"] > 0.3 * n * (n - 1) // 2
+    assert st["learned"] > (0.3 if dt > 1e-4 else 1e-4) * n * (n - 1) // 2
     assert sum(st[k] for k in ("hyperbola", "ellipse", "universal", "degenerate", "parabola")) == n * (n - 1) // 2
     sel = np.random.default_rng(37).choice(n, 24, replace=False)
-    ref = oracle.particle_disp(s, eps, 1e-5, sel, q=q)
+    ref = oracle.particle_disp(s, eps, dt, sel, q=q)
     got = disp[:, sel].T
     assert np.abs(got[:, :3] - ref[:, :3]).max() <= 1e-12 * np.abs(s[:3]).max()
     assert np.abs(got[:, 3:] - ref[:, 3:]).max() <= 1e-12 * np.abs(s[3:]).max()
@@ -154,9 +169,10 @@ def test_learned_autotune_layout(cuda):
 @pytest.mark.parametrize("n", [2, 31, 33, 97, 1025])
 def test_learned_split_step_ragged_sizes(cuda, n):
     """The split learned step (the untuned layout at every size) at particle counts that
-    leave partial warp-blocks, down to one pair: against the oracle's ALG step."""
+    leave partial warp-blocks, down to one pair: against the oracle's ALG step (dt = 1e-3,
+    so that heads are used)."""
     s, eps, q = initial.coulomb_cube(n, seed=40 + n, dmin=1e-2)
-    g, r, st = _learned_vs_oracle(cuda, s, eps, 1e-5, q=q, steps=1)
+    g, r, st = _learned_vs_oracle(cuda, s, eps, 1e-3, q=q, steps=1)
     assert rel_err(g[:3], r[:3]) <= 1e-12 and rel_err(g[3:], r[3:]) <= 1e-12
     assert sum(st[k] for k in ("hyperbola", "ellipse", "universal", "degenerate", "parabola")) == n * (n - 1) // 2
     assert st["nonfinite"] == 0 and st["timeouts"] == 0

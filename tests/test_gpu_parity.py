@@ -20,10 +20,10 @@ pytestmark = pytest.mark.gpu
 
 
 def gpu_run(cuda, state, eps, dt, nsteps, q=None, method=METHOD_ALG, deterministic=1,
-            graph=False, disp=False):
+            graph=False, disp=False, **cfg_fields):
     t = cuda.tensor(state, dtype=cuda.float64, device="cuda").contiguous()
     qt = cuda.tensor(q, dtype=cuda.float64, device="cuda") if q is not None else None
-    cfg = default_config(eps_th=eps, dt=dt, method=method, deterministic=deterministic)
+    cfg = default_config(eps_th=eps, dt=dt, method=method, deterministic=deterministic, **cfg_fields)
     d = cuda.zeros_like(t) if disp else None
     with BIASolver() as s:
         if graph:
@@ -37,11 +37,11 @@ def gpu_run(cuda, state, eps, dt, nsteps, q=None, method=METHOD_ALG, determinist
     return (out, stats, d.cpu().numpy()) if disp else (out, stats)
 
 
-def oracle_run(state, eps, dt, nsteps, q=None, method=1, quad=False):
+def oracle_run(state, eps, dt, nsteps, q=None, method=1, quad=False, relerr=0.0, abserr=1e-16):
     s = state
     st = None
     for _ in range(nsteps):
-        s, _, st = oracle.bia_step(s, eps, dt, method=method, q=q, quad=quad)
+        s, _, st = oracle.bia_step(s, eps, dt, method=method, q=q, quad=quad, relerr=relerr, abserr=abserr)
     return s, st
 
 
@@ -114,10 +114,14 @@ def test_plummer_matches_oracle(cuda):
     assert_parity(g, r)
 
 
-def test_rkf_mode_matches_oracle(cuda):
+@pytest.mark.parametrize("relerr", [0.0, 1e-12])
+def test_rkf_mode_matches_oracle(cuda, relerr):
+    """Per-pair RKF45 with the reference's tolerances (relerr 0, abserr 1e-16,
+    bia/find_dXYUV_RKF.f90:4) and with the scale configuration's relative tolerance 1e-12
+    (abserr kept at 1e-16): the same accepted step counts as the oracle, and its step."""
     s, eps, q = initial.coulomb_cube(96, seed=24, dmin=1e-2)
-    g, st = gpu_run(cuda, s, eps, 1e-5, 2, q=q, method=METHOD_RKF)
-    r, rst = oracle_run(s, eps, 1e-5, 2, q=q, method=0)
+    g, st = gpu_run(cuda, s, eps, 1e-5, 2, q=q, method=METHOD_RKF, rkf_relerr=relerr, rkf_abserr=1e-16)
+    r, rst = oracle_run(s, eps, 1e-5, 2, q=q, method=0, relerr=relerr, abserr=1e-16)
     assert st["rkf"] == 96 * 95 // 2 and st["rkf_steps"] == rst["rkf_steps"]
     assert_parity(g, r)
 

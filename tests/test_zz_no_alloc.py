@@ -5,7 +5,9 @@ pool belongs to another framework, or a real-time loop must not call into the CU
 allocator): its scratch is a fixed array inside libbia_b200.so, for n <= 2048.  The
 test compares two consecutive steps with the context-based bia_step on the same input
 (same tolerance as the parity tests; the kernels and the reduction order are the same,
-so the results are in fact identical), and checks that n above the limit is refused.
+so the results are in fact identical), for the ALG and universal-variable methods and at
+the size limit itself (n = 2048 fills the whole partial array); the first step is also
+checked against the CPU oracle directly.  n above the limit is refused.
 This file is collected last so that a failure here comes after every other test.
 """
 import ctypes
@@ -13,7 +15,8 @@ import ctypes
 import numpy as np
 import pytest
 
-from bia_3d_gpu_b200 import BIASolver, capi, default_config, initial
+import oracle
+from bia_3d_gpu_b200 import METHOD_ALG, METHOD_UNIVERSAL, BIASolver, capi, default_config, initial
 from conftest import max_rel_err, rel_err
 
 pytestmark = pytest.mark.gpu
@@ -24,9 +27,11 @@ def _ptrs(t):
     return [ctypes.c_void_p(t.data_ptr() + k * n * 8) for k in range(6)]
 
 
-def test_noalloc_step_matches_context_step(cuda):
-    s, eps, q = initial.coulomb_cube(1500, seed=61)
-    cfg = default_config(eps_th=eps, dt=1e-5)
+@pytest.mark.parametrize("method", [METHOD_ALG, METHOD_UNIVERSAL])
+@pytest.mark.parametrize("n", [1500, 2048])
+def test_noalloc_step_matches_context_step(cuda, n, method):
+    s, eps, q = initial.coulomb_cube(n, seed=61)
+    cfg = default_config(eps_th=eps, dt=1e-5, method=method)
     a = cuda.tensor(s, device="cuda")
     b = cuda.tensor(s, device="cuda")
     qt = cuda.tensor(q, device="cuda")
@@ -35,7 +40,7 @@ def test_noalloc_step_matches_context_step(cuda):
     stream = cuda.cuda.Stream()
     stream.wait_stream(cuda.cuda.current_stream())
     with BIASolver(stream=stream) as solver:
-        for _ in range(2):
+        for call in range(2):
             solver.step(a, cfg, q=qt, disp=da, stats=False)
             st = capi.lib().bia_step_noalloc(ctypes.byref(cfg), s.shape[1], *_ptrs(b),
                                              ctypes.c_void_p(qt.data_ptr()),
@@ -47,6 +52,10 @@ def test_noalloc_step_matches_context_step(cuda):
             assert rel_err(gb[:3], ga[:3]) <= 1e-12 and max_rel_err(gb[:3], ga[:3]) <= 1e-12
             assert rel_err(gb[3:], ga[3:]) <= 1e-12 and max_rel_err(gb[3:], ga[3:]) <= 1e-12
             assert np.array_equal(db.cpu().numpy(), da.cpu().numpy())
+            if call == 0:
+                ref, _, _ = oracle.bia_step(s, eps, 1e-5, method=method, q=q)
+                assert rel_err(gb[:3], ref[:3]) <= 1e-12 and max_rel_err(gb[:3], ref[:3]) <= 1e-12
+                assert rel_err(gb[3:], ref[3:]) <= 1e-12 and max_rel_err(gb[3:], ref[3:]) <= 1e-12
 
 
 def test_noalloc_step_rejects_n_above_limit(cuda):
