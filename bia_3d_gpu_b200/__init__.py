@@ -23,7 +23,7 @@ from .capi import (BIA_ERR_NONFINITE, BIA_OK, METHOD_ALG, METHOD_LEARNED, METHOD
 
 __all__ = ["find_dxyuv_kernel", "invariance_gpu", "BIASolver", "default_config", "BiaConfig",
            "BiaError", "METHOD_ALG", "METHOD_RKF", "METHOD_UNIVERSAL", "METHOD_LEARNED",
-           "INVARIANT_NAMES", "measure_fp64_peak", "HEADS_PATH"]
+           "INVARIANT_NAMES", "measure_fp64_peak", "HEADS_PATH", "HeadTrainer"]
 
 # the trained heads of BIA_METHOD_LEARNED (bia_3d_gpu_b200/train_heads.py writes them)
 HEADS_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "learned_heads.bin")
@@ -310,6 +310,11 @@ class BIASolver:
         self._leave(cur)
         capi.check(st, "bia_learned_head_eval")
 
+    def trainer(self, head, nsamples=1 << 22, seed=0):
+        """A device trainer of learned head `head` (0 elliptic, 1 hyperbolic) on this
+        solver's device and stream (bia_trainer_*)."""
+        return HeadTrainer(self, head, nsamples, seed)
+
     def ensemble(self, sizes, eps):
         """An ensemble of independent systems (sizes[s] particles, pair coupling eps[s])
         stored back to back; returns an Ensemble bound to this solver."""
@@ -381,3 +386,83 @@ class Ensemble:
         s._leave(cur)
         capi.check(st, "bia_ensemble_energy")
         return out[0::2].copy(), out[1::2].copy()
+
+
+class HeadTrainer:
+    """Training of one learned head on the GPU (bia_trainer_*): samples from the FP64 Kepler
+    solver on the device, forward and backward passes on the tensor cores (BF16 operands,
+    FP32 accumulation), Adam on FP32 master parameters."""
+
+    def __init__(self, solver, head, nsamples, seed):
+        self._solver = solver
+        self._t = ctypes.c_void_p()
+        cur = solver._enter()
+        st = capi.lib().bia_trainer_create(solver._ctx, int(head), int(nsamples), int(seed), ctypes.byref(self._t))
+        solver._leave(cur)
+        capi.check(st, "bia_trainer_create")
+        self.head = head
+        self.nparams = capi.lib().bia_trainer_param_count()
+
+    def close(self):
+        if self._t:
+            capi.lib().bia_trainer_destroy(self._t)
+            self._t = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _fp(self, a):
+        return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+    def params(self):
+        out = np.zeros(self.nparams, np.float32)
+        capi.check(capi.lib().bia_trainer_get_params(self._t, self._fp(out)), "bia_trainer_get_params")
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        capi.check(capi.lib().bia_trainer_set_params(self._t, self._fp(p)), "bia_trainer_set_params")
+
+    def samples(self):
+        """(x, y, n): device pointers of the samples' inputs [n][2] and targets [n]."""
+        x, y, n = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_longlong()
+        capi.check(capi.lib().bia_trainer_samples(self._t, ctypes.byref(x), ctypes.byref(y), ctypes.byref(n)))
+        return x.value, y.value, n.value
+
+    def copy_samples(self, first, count):
+        """Host copies (x float32[count][2], y float32[count]) of samples first .. + count."""
+        x = np.zeros((count, 2), np.float32)
+        y = np.zeros(count, np.float32)
+        capi.check(capi.lib().bia_trainer_copy_samples(self._t, int(first), int(count), self._fp(x), self._fp(y)),
+                   "bia_trainer_copy_samples")
+        return x, y
+
+    def gradient(self, x_ptr, y_ptr, rows):
+        """Gradient of the mean squared error on device rows (pointers) at the current
+        parameters: (grad float32[nparams], loss)."""
+        g = np.zeros(self.nparams, np.float32)
+        loss = ctypes.c_float(0.0)
+        cur = self._solver._enter()
+        st = capi.lib().bia_trainer_gradient(self._t, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr), int(rows),
+                                             self._fp(g), ctypes.byref(loss))
+        self._solver._leave(cur)
+        capi.check(st, "bia_trainer_gradient")
+        return g, loss.value
+
+    def train(self, epochs, batch=4096, lr=2e-3):
+        """Adam over the samples; returns the mean squared error of each epoch."""
+        losses = np.zeros(epochs, np.float32)
+        cur = self._solver._enter()
+        st = capi.lib().bia_trainer_train(self._t, int(epochs), int(batch), float(lr), self._fp(losses))
+        self._solver._leave(cur)
+        capi.check(st, "bia_trainer_train")
+        return losses
+
+    def export(self):
+        """The head as a learned_heads.bin record (bytes)."""
+        buf = ctypes.create_string_buffer(19472)
+        capi.check(capi.lib().bia_trainer_export(self._t, buf), "bia_trainer_export")
+        return buf.raw

@@ -125,6 +125,23 @@ def lib():
     L.find_dxyuv_kernel_.restype = None
     L.invariance_gpu_.argtypes = [_I, _D] + [_PD] * 6 + [_PD] * 11
     L.invariance_gpu_.restype = None
+    _PF = ctypes.POINTER(ctypes.c_float)
+    L.bia_trainer_create.argtypes = [_V, _I, ctypes.c_longlong, ctypes.c_ulonglong, ctypes.POINTER(_V)]
+    L.bia_trainer_destroy.argtypes = [_V]
+    L.bia_trainer_param_count.argtypes = []
+    L.bia_trainer_get_params.argtypes = [_V, _PF]
+    L.bia_trainer_set_params.argtypes = [_V, _PF]
+    L.bia_trainer_gradient.argtypes = [_V, _V, _V, _I, _PF, _PF]
+    L.bia_trainer_train.argtypes = [_V, _I, _I, ctypes.c_float, _PF]
+    L.bia_trainer_export.argtypes = [_V, ctypes.c_char_p]
+    L.bia_trainer_samples.argtypes = [_V, ctypes.POINTER(_V), ctypes.POINTER(_V),
+                                      ctypes.POINTER(ctypes.c_longlong)]
+    L.bia_trainer_copy_samples.argtypes = [_V, ctypes.c_longlong, ctypes.c_longlong, _PF, _PF]
+    for name in ("bia_trainer_create", "bia_trainer_destroy", "bia_trainer_param_count",
+                 "bia_trainer_get_params", "bia_trainer_set_params", "bia_trainer_gradient",
+                 "bia_trainer_train", "bia_trainer_export", "bia_trainer_samples",
+                 "bia_trainer_copy_samples"):
+        getattr(L, name).restype = _I
     for name in ("bia_context_create", "bia_context_destroy", "bia_context_set_stream",
                  "bia_context_set_timing", "bia_context_kernel_ms", "bia_step", "bia_run",
                  "bia_run_host", "bia_invariance", "bia_measure_fp64_peak", "bia_context_stats"):
@@ -163,4 +180,8 @@ EXPORTED_SYMBOLS = ("bia_config_default", "bia_context_create", "bia_context_des
                     "bia_ensemble_run", "bia_ensemble_energy",
                     "bia_context_set_heads", "bia_learned_head_eval", "bia_context_autotune",
                     "bia_selftest_wait_timeout", "bia_step_noalloc",
+                    "bia_trainer_create", "bia_trainer_destroy", "bia_trainer_param_count",
+                    "bia_trainer_get_params", "bia_trainer_set_params", "bia_trainer_gradient",
+                    "bia_trainer_train", "bia_trainer_export", "bia_trainer_samples",
+                    "bia_trainer_copy_samples",
                     "bia_last_error", "find_dxyuv_kernel_", "invariance_gpu_")

@@ -845,6 +845,18 @@ int bia_trainer_samples(bia_trainer *t, const float **x, const float **y, long l
     return BIA_OK;
 }
 
+int bia_trainer_copy_samples(bia_trainer *t, long long first, long long count, float *x, float *y)
+{
+    if (!t || !x || !y || first < 0 || count < 0 || first + count > t->n) return BIA_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(t->device);
+    cudaError_t e = cudaMemcpyAsync(x, t->x + 2 * first, (size_t)count * 2 * sizeof(float), cudaMemcpyDeviceToHost,
+                                    t->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(y, t->y + first, (size_t)count * sizeof(float), cudaMemcpyDeviceToHost, t->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
+    return cuda_status(e);
+}
+
 int bia_trainer_param_count(void) { return kParams; }
 
 }  // extern "C"

@@ -1,6 +1,13 @@
 """Train the two learned Kepler heads and write bia_3d_gpu_b200/learned_heads.bin.
 
-    python -m bia_3d_gpu_b200.train_heads [--samples 4194304] [--epochs 24] [--seed 0]
+    python -m bia_3d_gpu_b200.train_heads [--samples 4194304] [--epochs 24] [--seed 0] [--torch]
+
+By default the heads are trained on the GPU by libbia_b200.so (bia_trainer_*): the samples
+come from the FP64 Kepler solver on the device, the forward and backward passes run on the
+tensor cores (BF16 operands, FP32 accumulation in tensor memory) and Adam updates FP32
+master parameters on the device.  --torch trains the same network in FP32 with torch on
+the CPU instead (the numpy solver below makes its samples); the tests use it as the
+reference of the device gradients.
 
 Each head is an MLP 2 -> 64 -> 64 -> 64 -> 1 (ReLU) that maps an orbit's eccentricity and
 mean anomaly to a starting guess of its anomaly:
@@ -191,14 +198,66 @@ def read_heads(path=OUT):
     return heads
 
 
+def write_records(path, records):
+    """learned_heads.bin from head records (bytes of 19472 each, as bia_trainer_export
+    returns them)."""
+    with open(path, "wb") as f:
+        f.write(b"BIAHEAD1")
+        f.write(struct.pack("<II", 1, len(records)))
+        for r in records:
+            f.write(r)
+
+
+def guess_error(head, x, y, scale):
+    """|head guess - solved anomaly| (radians) on samples (x, y) of one head."""
+    guess = head_forward(head, x.astype(np.float32)) * scale
+    return np.abs(guess - y * scale)
+
+
+def train_device(samples=1 << 22, epochs=24, seed=0, batch=4096, lr=2e-3, device=0, log=print):
+    """Both heads trained on the GPU (bia_trainer_*).  Returns (records, info): the head
+    records in file order and per head the epoch losses and the training time."""
+    import time as _time
+
+    from . import BIASolver
+    records, info = [], []
+    with BIASolver(device=device) as solver:
+        for head in (0, 1):
+            t0 = _time.perf_counter()
+            tr = solver.trainer(head, samples, seed + head)
+            t1 = _time.perf_counter()
+            losses = tr.train(epochs, batch, lr)
+            t2 = _time.perf_counter()
+            records.append(tr.export())
+            tr.close()
+            info.append({"samples_s": t1 - t0, "train_s": t2 - t1, "losses": losses.tolist()})
+            log(f"  head {head}: samples {t1 - t0:.2f} s, {epochs} epochs {t2 - t1:.2f} s, "
+                f"final mse {losses[-1]:.3e}")
+    return records, info
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--samples", type=int, default=1 << 22)
     ap.add_argument("--epochs", type=int, default=24)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=OUT)
+    ap.add_argument("--torch", action="store_true", help="train with torch on the CPU instead of the GPU")
     args = ap.parse_args()
     log = lambda s: print(s, flush=True)
+    if not args.torch:
+        t0 = time.time()
+        records, _ = train_device(args.samples, args.epochs, args.seed, log=log)
+        write_records(args.out, records)
+        rng = np.random.default_rng(args.seed + 100)
+        ell, hyp = make_samples(200000, rng)
+        for (name, (x, y, e, M), scale), head in zip((("elliptic", ell, np.pi), ("hyperbolic", hyp, HYP_OUT)),
+                                                     read_heads(args.out)):
+            err = guess_error(head, x, y, scale)
+            log(f"  {name} head (BF16) guess error on new samples: median {np.median(err):.2e}, "
+                f"p99 {np.quantile(err, 0.99):.2e}, max {err.max():.2e}")
+        log(f"wrote {args.out} ({os.path.getsize(args.out)} bytes, {time.time() - t0:.0f} s)")
+        return
     rng = np.random.default_rng(args.seed)
     t0 = time.time()
     ell, hyp = make_samples(args.samples, rng)

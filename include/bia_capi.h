@@ -207,6 +207,40 @@ int bia_ensemble_energy(bia_context *ctx, bia_ensemble *ens, const double *x, co
                         const double *z, const double *u, const double *v, const double *w,
                         const double *q, double *energy);
 
+/* Device trainer of one learned head (0 elliptic, 1 hyperbolic), the training of
+   BIA_METHOD_LEARNED's heads on the GPU.  No counterpart in the reference (the learned form
+   is new).  Create draws nsamples (eccentricity, mean anomaly) pairs uniformly over the
+   head's domain from `seed` (counter-based), solves Kepler's equation for each in FP64 on
+   the device, and initialises the FP32 master parameters from `seed` (uniform in
+   +-1/sqrt(fan_in)).  Training steps run forward and backward on the tensor cores (BF16
+   operands, FP32 accumulation in tensor memory) and Adam on the device; results are the
+   same for the same seed.  Parameters (FP32, bia_trainer_param_count() of them) are ordered
+   W1[64][2], b1[64], W2[64][64], b2[64], W3[64][64], b3[64], w4[64], b4 (weights
+   output-major). */
+typedef struct bia_trainer bia_trainer;
+int bia_trainer_create(bia_context *ctx, int head, long long nsamples, unsigned long long seed,
+                       bia_trainer **trainer);
+int bia_trainer_destroy(bia_trainer *trainer);
+int bia_trainer_param_count(void);
+int bia_trainer_get_params(bia_trainer *trainer, float *params);
+/* replaces the parameters (host array) and clears the Adam state */
+int bia_trainer_set_params(bia_trainer *trainer, const float *params);
+/* gradient of the mean squared error over `rows` device rows x[rows][2] -> y[rows] at the
+   current parameters, no update: grad (host, param_count floats), loss (host, optional) */
+int bia_trainer_gradient(bia_trainer *trainer, const float *x, const float *y, int rows,
+                         float *grad, float *loss);
+/* `epochs` passes of Adam (beta 0.9 / 0.999, eps 1e-8) over the samples in batches of
+   `batch` rows (a multiple of 128 dividing nsamples, which must be a power of two; each
+   epoch visits the samples in its own permuted order), learning rate lr annealed by a
+   cosine over the epochs; loss_per_epoch (host, optional): the epoch's mean squared error */
+int bia_trainer_train(bia_trainer *trainer, int epochs, int batch, float lr, float *loss_per_epoch);
+/* the head as a learned_heads.bin record (19472 bytes: BF16 weights, FP32 vectors) */
+int bia_trainer_export(bia_trainer *trainer, void *record);
+/* the device arrays of the samples: x[n][2] (the head's inputs), y[n] (target / scale) */
+int bia_trainer_samples(bia_trainer *trainer, const float **x, const float **y, long long *n);
+/* host copies of samples first .. first + count - 1: x[count][2], y[count] */
+int bia_trainer_copy_samples(bia_trainer *trainer, long long first, long long count, float *x, float *y);
+
 /* Direct-integration (DIM) reference solver: rebuilds rkf_c_ (dim/rkf_kernel.cu:194-495).
    y: device state, 6 arrays of n (x, y, z, u, v, w), advanced in place from x0 to xe with
    a_i = eps_th * sum_j (r_i - r_j) / (|r_ij|^2 + 1e-99)^{3/2} (per-particle coupling as in
