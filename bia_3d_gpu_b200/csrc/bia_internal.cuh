@@ -93,4 +93,7 @@ int cuda_status(cudaError_t e);
 int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y, double *z,
                  double *u, double *v, double *w, const double *q, double *disp);
 int ensure_step_buffers(bia_context *ctx, const bia_config *cfg, int n);
+// SM count of the current device (cached); the grid of a persistent warp-block kernel
+int device_sm_count();
+long long persistent_grid(long long blocks_needed);
 }  // namespace bia

@@ -83,29 +83,37 @@ __device__ __forceinline__ uint32_t rest_block_solve(const double *x, const doub
                                                      int bj, int lane, double racc[6], double cacc[6],
                                                      PairCounters &cnt)
 {
-    const unsigned full = 0xffffffffu;
+    // column states and sums in the warp's shared slice (as warp_block_solve_uv: slot
+    // (lane + k) mod 32 takes its pairs in ascending k)
+    __shared__ double s_rest[kTileWarps][kTileSmemDoubles];
+    double *ws = s_rest[(threadIdx.x >> 5) % kTileWarps];
+    double *wacc = ws + 7 * 32;
     const int i = bi * 32 + lane;
     const bool diag = (bi == bj);
     uint32_t learned = 0u;
-    double si[7], sj[7];
-    load_particle(x, y, z, u, v, w, q, n, i, si);
-    load_particle(x, y, z, u, v, w, q, n, bj * 32 + lane, sj);
+    double si[7];
+    {
+        double sj[7];
+        load_particle(x, y, z, u, v, w, q, n, i, si);
+        load_particle(x, y, z, u, v, w, q, n, bj * 32 + lane, sj);
 #pragma unroll
-    for (int c = 0; c < 6; c++) racc[c] = cacc[c] = 0.0;
+        for (int c = 0; c < 7; c++) ws[c * 32 + lane] = sj[c];
+#pragma unroll
+        for (int c = 0; c < 6; c++) wacc[c * 32 + lane] = 0.0;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < 6; c++) racc[c] = 0.0;
     counters_zero(cnt);
     const int k0 = diag ? 1 : 0, k1 = diag ? 16 : 31;
     for (int k = k0; k <= k1; k++) {
         const int src = (lane + k) & 31;
-        double sc[7];
-#pragma unroll
-        for (int c = 0; c < 7; c++) sc[c] = __shfl_sync(full, sj[c], src);
-        const int j = bj * 32 + src;
-        const bool active = (!diag || k < 16 || lane < 16) && i < n && j < n;
+        const bool active = (!diag || k < 16 || lane < 16) && i < n && bj * 32 + src < n;
         double h[6] = {0, 0, 0, 0, 0, 0};
         if (active) {
-            const double r[3] = {si[0] - sc[0], si[1] - sc[1], si[2] - sc[2]};
-            const double g[3] = {si[3] - sc[3], si[4] - sc[4], si[5] - sc[5]};
-            const double eps_ij = q ? eps_th * si[6] * sc[6] : eps_th;
+            const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
+            const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
+            const double eps_ij = q ? eps_th * si[6] * ws[6 * 32 + src] : eps_th;
             const UvPair p = uv_prepare(eps_ij, r, g);
             if (dt != 0.0) {
                 bool exact;
@@ -125,13 +133,16 @@ __device__ __forceinline__ uint32_t rest_block_solve(const double *x, const doub
                 cnt.cls[kUniversal]++;
             }
         }
-        const int back = (lane - k) & 31;
 #pragma unroll
         for (int c = 0; c < 6; c++) {
             racc[c] += h[c];
-            cacc[c] += __shfl_sync(full, h[c], back);
+            wacc[c * 32 + src] += h[c];
         }
+        __syncwarp();  // slot src is the next offset's slot of lane - 1
     }
+#pragma unroll
+    for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
+    __syncwarp();  // the slice is reused by this warp's next block
     return learned;
 }
 

@@ -57,38 +57,52 @@ struct StepArgs {
     unsigned int *wbcount;
 };
 
+// Each warp solves warp-blocks t = (its global warp index) + k * (warps in the grid): one
+// block per warp when the grid covers every block, several in a persistent grid (the
+// universal-variable and split-step rest kernels launch one resident grid, kPersistentCtas
+// CTAs per SM).  The counters are summed per warp in registers and flushed every
+// kFlushBlocks blocks: one set of atomics per warp instead of one per block.
 template <bool kDeterministic, int M>
 __global__ void __launch_bounds__(kThreads, TileOccupancy<M>::kMinBlocks) bia_pair_tiles_kernel(const StepArgs A)
 {
     const int lane = threadIdx.x & 31;
-    const long long t = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
-    if (t >= A.nwb) return;  // warp-uniform
-    int bi, bj;
-    warp_block_coords(t, bi, bj);
-    const int i = bi * 32 + lane;
-    const int jown = bj * 32 + lane;
-    const bool diag = (bi == bj);
-    double racc[6], cacc[6];
-    PairCounters cnt;
-    warp_block_solve<M>(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P, bi, bj, lane, racc, cacc, cnt);
-    flush_counters(cnt, A.stats, lane);
-
-    const size_t plane = (size_t)A.npad;
-    if (kDeterministic) {
-        write_partials(A.part, plane, bi, bj, lane, racc, cacc);
-    } else {
-        if (diag) {
-#pragma unroll
-            for (int c = 0; c < 6; c++)
-                if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c] - cacc[c]);
+    PairCounters tot;
+    counters_zero(tot);
+    int nblk = 0;
+    for (long long t = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); t < A.nwb;
+         t += (long long)gridDim.x * kWarpsPerBlock) {  // warp-uniform
+        int bi, bj;
+        warp_block_coords(t, bi, bj);
+        const int i = bi * 32 + lane;
+        const int jown = bj * 32 + lane;
+        const bool diag = (bi == bj);
+        double racc[6], cacc[6];
+        PairCounters cnt;
+        warp_block_solve<M>(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P, bi, bj, lane, racc, cacc, cnt);
+        counters_add(tot, cnt);
+        if (++nblk == kFlushBlocks) {
+            flush_counters(tot, A.stats, lane);
+            counters_zero(tot);
+            nblk = 0;
+        }
+        const size_t plane = (size_t)A.npad;
+        if (kDeterministic) {
+            write_partials(A.part, plane, bi, bj, lane, racc, cacc);
         } else {
+            if (diag) {
 #pragma unroll
-            for (int c = 0; c < 6; c++) {
-                if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c]);
-                if (jown < A.n) atomicAdd(&A.part[c * plane + jown], -cacc[c]);
+                for (int c = 0; c < 6; c++)
+                    if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c] - cacc[c]);
+            } else {
+#pragma unroll
+                for (int c = 0; c < 6; c++) {
+                    if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c]);
+                    if (jown < A.n) atomicAdd(&A.part[c * plane + jown], -cacc[c]);
+                }
             }
         }
     }
+    if (nblk > 0) flush_counters(tot, A.stats, lane);
 }
 
 // Phase-locked ALG step kernel (see phase_block_solve): CTAs of kW warps, kMinB of them
@@ -178,6 +192,36 @@ static int alg_variant_for(long long nwb, int tuned)
     return ((nwb + 31) / 32 >= 2LL * sms) ? kVarPhase32 : kVarTiles8;
 }
 
+// CTAs per SM of the persistent universal-variable and rest kernels (their launch bound)
+constexpr int kPersistentCtas = 2;
+
+// SM count of the current device (cached per device); 0 when the query fails
+int device_sm_count()
+{
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static int sms_of[kMaxDevices] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 0;
+    std::lock_guard<std::mutex> lk(mu);
+    if (sms_of[dev] == 0) {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        sms_of[dev] = sms;
+    }
+    return sms_of[dev];
+}
+
+// the grid of a persistent warp-block kernel: every block covered, at most one resident wave
+long long persistent_grid(long long blocks_needed)
+{
+    const long long cap = (long long)device_sm_count() * kPersistentCtas;
+    return (cap > 0 && blocks_needed > cap) ? cap : blocks_needed;
+}
+
 static int ilog2_bucket(int n)
 {
     int b = 0;
@@ -206,7 +250,8 @@ static void launch_pair_tiles(const StepArgs &A, long long grid, cudaStream_t st
         bia_pair_tiles_kernel<kDeterministic, kMethodRkf><<<(unsigned)grid, kThreads, 0, st>>>(A);
         break;
     case kMethodUniversal:
-        bia_pair_tiles_kernel<kDeterministic, kMethodUniversal><<<(unsigned)grid, kThreads, 0, st>>>(A);
+        bia_pair_tiles_kernel<kDeterministic, kMethodUniversal>
+            <<<(unsigned)persistent_grid(grid), kThreads, 0, st>>>(A);
         break;
     default:
         bia_pair_tiles_kernel<kDeterministic, kMethodAlg><<<(unsigned)grid, kThreads, 0, st>>>(A);
@@ -270,29 +315,40 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const 
 // appended to the list that bia_pair_learned_list_kernel works through afterwards.
 // Deterministic mode writes every partial slot here; the learned kernel adds onto them.
 template <bool kDeterministic>
-// Two CTAs per SM: at the universal-variable kernel's three the filter spills registers
-// inside the rotation loop (measured at n = 32768: 11.2 ms at three, 10.9 ms at two).
-__global__ void __launch_bounds__(kThreads, 2) bia_pair_rest_kernel(const StepArgs A)
+// Two CTAs per SM (kPersistentCtas): at three the filter spills registers inside the
+// rotation loop (measured at n = 32768: 11.2 ms at three, 10.9 ms at two).  A persistent grid
+// with the counters flushed per warp, as bia_pair_tiles_kernel.
+__global__ void __launch_bounds__(kThreads, kPersistentCtas) bia_pair_rest_kernel(const StepArgs A)
 {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const long long t = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
-    if (t >= A.nwb) return;  // warp-uniform
-    int bi, bj;
-    warp_block_coords(t, bi, bj);
-    double racc[6], cacc[6];
-    PairCounters cnt;
-    const uint32_t learned = rest_block_solve(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P.dt, bi, bj,
-                                              lane, racc, cacc, cnt);
-    flush_counters(cnt, A.stats, lane);
-    add_learned_sums<kDeterministic>(A, bi, bj, lane, racc, cacc, true);
-    if (__any_sync(full, learned != 0u)) {
-        unsigned int slot = 0;
-        if (lane == 0) slot = atomicAdd(A.wbcount, 1u);
-        slot = __shfl_sync(full, slot, 0);
-        A.lmask[(size_t)slot * 32 + lane] = learned;
-        if (lane == 0) A.wblist[slot] = (unsigned int)t;
+    PairCounters tot;
+    counters_zero(tot);
+    int nblk = 0;
+    for (long long t = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); t < A.nwb;
+         t += (long long)gridDim.x * kWarpsPerBlock) {  // warp-uniform
+        int bi, bj;
+        warp_block_coords(t, bi, bj);
+        double racc[6], cacc[6];
+        PairCounters cnt;
+        const uint32_t learned = rest_block_solve(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P.dt, bi,
+                                                  bj, lane, racc, cacc, cnt);
+        counters_add(tot, cnt);
+        if (++nblk == kFlushBlocks) {
+            flush_counters(tot, A.stats, lane);
+            counters_zero(tot);
+            nblk = 0;
+        }
+        add_learned_sums<kDeterministic>(A, bi, bj, lane, racc, cacc, true);
+        if (__any_sync(full, learned != 0u)) {
+            unsigned int slot = 0;
+            if (lane == 0) slot = atomicAdd(A.wbcount, 1u);
+            slot = __shfl_sync(full, slot, 0);
+            A.lmask[(size_t)slot * 32 + lane] = learned;
+            if (lane == 0) A.wblist[slot] = (unsigned int)t;
+        }
     }
+    if (nblk > 0) flush_counters(tot, A.stats, lane);
 }
 
 // Split learned step, second kernel: persistent CTAs work through the listed warp-blocks,
@@ -384,7 +440,7 @@ static int launch_pair_learned(const StepArgs &A, cudaStream_t st)
         return BIA_OK;
     }
     if (cudaMemsetAsync(A.wbcount, 0, sizeof(unsigned int), st) != cudaSuccess) return BIA_ERR_CUDA;
-    const long long rgrid = (A.nwb + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    const long long rgrid = persistent_grid((A.nwb + kWarpsPerBlock - 1) / kWarpsPerBlock);
     bia_pair_rest_kernel<kDeterministic><<<(unsigned)rgrid, kThreads, 0, st>>>(A);
     const long long need = (A.nwb + kLearnedWarps - 1) / kLearnedWarps;
     const int grid = (int)(need < lgrid ? need : lgrid);

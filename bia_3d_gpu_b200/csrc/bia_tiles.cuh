@@ -234,6 +234,75 @@ __device__ __forceinline__ void phase_block_solve(const double *x, const double 
     for (int c = 0; c < 6; c++) cacc[c] = ws[(7 + c) * 32 + lane];
 }
 
+// Universal-variable warp-block: lanes walk the rotation offsets as in warp_block_solve,
+// with the column states and the column sums in the warp's shared slice instead of
+// registers and shuffles.  Lane l adds its pair at offset k into column slot (l + k) mod 32,
+// a different slot on every lane, so the slots take their pairs in ascending k, the order
+// of the shuffle walk: the sums are bitwise the same.  Measured at n = 32768: 6.48 ms
+// against 6.79 ms for the shuffle walk (100 instead of 118 registers, no shuffles).
+__device__ __forceinline__ void warp_block_solve_uv(const double *x, const double *y, const double *z,
+                                                    const double *u, const double *v, const double *w,
+                                                    const double *q, int n, double eps_th, const PairParams &P,
+                                                    int bi, int bj, int lane, double racc[6], double cacc[6],
+                                                    PairCounters &cnt)
+{
+    __shared__ double s_uv[kTileWarps][kTileSmemDoubles];
+    double *ws = s_uv[(threadIdx.x >> 5) % kTileWarps];
+    double *wacc = ws + 7 * 32;
+    const int i = bi * 32 + lane;
+    double si[7];
+    {
+        double sj[7];
+        load_particle(x, y, z, u, v, w, q, n, i, si);
+        load_particle(x, y, z, u, v, w, q, n, bj * 32 + lane, sj);
+#pragma unroll
+        for (int c = 0; c < 7; c++) ws[c * 32 + lane] = sj[c];
+#pragma unroll
+        for (int c = 0; c < 6; c++) wacc[c * 32 + lane] = 0.0;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < 6; c++) racc[c] = 0.0;
+    counters_zero(cnt);
+    const bool diag = (bi == bj);
+    const int k0 = diag ? 1 : 0;
+    const int k1 = diag ? 16 : 31;
+    for (int k = k0; k <= k1; k++) {
+        const int src = (lane + k) & 31;
+        const bool active = (!diag || k < 16 || lane < 16) && i < n && bj * 32 + src < n;
+        double h[6] = {0, 0, 0, 0, 0, 0};
+        if (active) {
+            const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
+            const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
+            const double eps_ij = q ? eps_th * si[6] * ws[6 * 32 + src] : eps_th;
+            pair_halfdisp<kMethodUniversal>(P, eps_ij, r, g, h, cnt);
+        }
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            racc[c] += h[c];
+            wacc[c * 32 + src] += h[c];
+        }
+        __syncwarp();  // slot src is the next offset's slot of lane - 1
+    }
+#pragma unroll
+    for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
+    __syncwarp();  // the slice is reused by this warp's next block
+}
+
+// Running sums of a warp's counters over the blocks it solves (persistent kernels flush
+// them every kFlushBlocks blocks instead of once per block: one set of atomics per warp).
+constexpr int kFlushBlocks = 64;
+__device__ __forceinline__ void counters_add(PairCounters &a, const PairCounters &b)
+{
+#pragma unroll
+    for (int k = 0; k < 6; k++) a.cls[k] += b.cls[k];
+    a.it_hyp += b.it_hyp; a.it_ell += b.it_ell; a.it_par += b.it_par; a.it_uv += b.it_uv;
+    a.rkf_steps += b.rkf_steps; a.nonconverged += b.nonconverged; a.bracket_exits += b.bracket_exits;
+    a.fallbacks += b.fallbacks; a.nonfinite += b.nonfinite; a.learned += b.learned;
+    a.learned_fallbacks += b.learned_fallbacks; a.learned_coarse += b.learned_coarse;
+    a.timeouts += b.timeouts; a.learned_fp32 += b.learned_fp32;
+}
+
 // Pairs of warp-block (bi, bj) of the system whose particles are x[0..n) etc.: row sums
 // racc (particle 32 bi + lane) and column sums cacc (particle 32 bj + lane) of the pair
 // half-displacements h (row receives +h, column -h: the caller writes -cacc).
@@ -246,6 +315,10 @@ __device__ __forceinline__ void warp_block_solve(const double *x, const double *
 {
     if (M == kMethodAlg && BIA_ALG_COMPACT) {
         warp_block_solve_compact(x, y, z, u, v, w, q, n, eps_th, P, bi, bj, lane, racc, cacc, cnt);
+        return;
+    }
+    if (M == kMethodUniversal) {
+        warp_block_solve_uv(x, y, z, u, v, w, q, n, eps_th, P, bi, bj, lane, racc, cacc, cnt);
         return;
     }
     const unsigned full = 0xffffffffu;

@@ -182,6 +182,7 @@ struct DimBuffers {
 
 struct DimRun {
     int n, len;
+    bool fast_inv = false;  // the cooperative solver's rsqrt-based inverse cube
     double eps, relerr, abserr;
     cudaStream_t st;
     DimBuffers B;
@@ -359,52 +360,82 @@ struct DimCoopArgs {
                     // [4] rejected, [5] ier
 };
 
-// Fused stage of the cooperative solver: k_s = (v, a)(win) for the block's particles
-// (16 particles x 16 j-chunks per block, chunk sums added in order), and right away, by the
-// thread that owns particle i, the next stage's input for particle i: w = y0 + h sum_m
-// c_fehl[s][m] k_m (s < 5), or yn (row 5) and er (row 6) after the last stage.  The
-// combination is per particle, so only the next stage needs a grid-wide barrier.
-#ifndef BIA_DIM_COOP_PARTICLES
-#define BIA_DIM_COOP_PARTICLES 8
-#endif
-constexpr int kCoopParticles = BIA_DIM_COOP_PARTICLES, kCoopChunks = 256 / BIA_DIM_COOP_PARTICLES;
+// Fused stage of the cooperative solver: k_s = (v, a)(win) for a group of P particles, and
+// right away, by the thread that owns particle i, the next stage's input for particle i:
+// w = y0 + h sum_m c_fehl[s][m] k_m (s < 5), or yn (row 5) and er (row 6) after the last
+// stage.  The combination is per particle, so only the next stage needs a grid-wide
+// barrier.
+//
+// j-tiles: the block's 256 threads load the positions of 256 particles j at a time into
+// shared memory (coalesced structure-of-arrays loads, one element per thread and
+// component); thread (particle lane, chunk c) of the block's P x C threads (C = 256 / P)
+// adds the tile's entries c, c + C, ..., and the C chunk sums of a particle are added in
+// chunk order at the end (deterministic).  P = 8 below n = 4096 (more groups than SMs at
+// small n), 32 above (each tile then serves 32 particles, 32 entries per thread).
+//
+// Inverse cube: kFastInv (bia_dim_integrate) eps r^-3 from one rsqrt (r^-1, then its cube;
+// rsqrt is within 1 ulp, the product within ~4 ulp of eps / r^3); otherwise the
+// reference's eps / (rsq sqrt(rsq)) (dim/rkf_kernel.cu:44-46), the form rkf_c_ keeps.
+constexpr int kCoopTile = 256;
+template <int P>
+struct CoopShared {
+    double part[256 / P][3][P];
+    double tile[3][kCoopTile];
+};
 
+template <int P, bool kFastInv>
 __device__ void coop_stage(const DimCoopArgs &A, int s, double h, const double *__restrict__ y0,
                            const double *__restrict__ win, double *__restrict__ wout, double *__restrict__ yn,
-                           bool want_er, double (*part)[3][kCoopParticles])
+                           bool want_er, CoopShared<P> &sh)
 {
+    constexpr int C = 256 / P;
     const int n = A.n;
     const size_t len = (size_t)A.len;
-    const int lane = threadIdx.x % kCoopParticles;
-    const int chunk = threadIdx.x / kCoopParticles;
-    const int ngroups = (n + kCoopParticles - 1) / kCoopParticles;
+    const int lane = threadIdx.x % P;
+    const int chunk = threadIdx.x / P;
+    const int ngroups = (n + P - 1) / P;
     const double *X = win, *Y = win + n, *Z = win + 2 * (size_t)n;
     double *k = A.B.k;
     for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
-        const int i = grp * kCoopParticles + lane;
+        const int i = grp * P + lane;
+        const bool live = i < n;
+        const double xi = live ? X[i] : 0.0, yi = live ? Y[i] : 0.0, zi = live ? Z[i] : 0.0;
         double ax = 0.0, ay = 0.0, az = 0.0;
-        if (i < n) {
-            const double xi = X[i], yi = Y[i], zi = Z[i];
-            const int per = (n + kCoopChunks - 1) / kCoopChunks;
-            const int j0 = chunk * per;
-            const int j1 = min(n, j0 + per);
-            for (int j = j0; j < j1; j++) {
-                const double xij = xi - X[j], yij = yi - Y[j], zij = zi - Z[j];
-                const double rsq = xij * xij + yij * yij + zij * zij + 1e-99;
-                const double eee = A.eps / (rsq * sqrt(rsq));
-                ax += xij * eee;
-                ay += yij * eee;
-                az += zij * eee;
+        for (int jt = 0; jt < n; jt += kCoopTile) {
+            __syncthreads();  // the previous tile (or group) is consumed
+            const int jl = jt + (int)threadIdx.x;
+            if (jl < n) {
+                sh.tile[0][threadIdx.x] = X[jl];
+                sh.tile[1][threadIdx.x] = Y[jl];
+                sh.tile[2][threadIdx.x] = Z[jl];
+            }
+            __syncthreads();
+            const int cnt = min(kCoopTile, n - jt);
+            if (live) {
+                for (int q = chunk; q < cnt; q += C) {
+                    const double xij = xi - sh.tile[0][q], yij = yi - sh.tile[1][q], zij = zi - sh.tile[2][q];
+                    const double rsq = xij * xij + yij * yij + zij * zij + 1e-99;
+                    double eee;
+                    if (kFastInv) {
+                        const double ir = rsqrt(rsq);
+                        eee = A.eps * (ir * ir * ir);
+                    } else {
+                        eee = A.eps / (rsq * sqrt(rsq));
+                    }
+                    ax += xij * eee;
+                    ay += yij * eee;
+                    az += zij * eee;
+                }
             }
         }
-        part[chunk][0][lane] = ax;
-        part[chunk][1][lane] = ay;
-        part[chunk][2][lane] = az;
+        sh.part[chunk][0][lane] = ax;
+        sh.part[chunk][1][lane] = ay;
+        sh.part[chunk][2][lane] = az;
         __syncthreads();
-        if (chunk == 0 && i < n) {
+        if (chunk == 0 && live) {
             double a3[3] = {0.0, 0.0, 0.0};
-            for (int c = 0; c < kCoopChunks; c++)
-                for (int d = 0; d < 3; d++) a3[d] += part[c][d][lane];
+            for (int c = 0; c < C; c++)
+                for (int d = 0; d < 3; d++) a3[d] += sh.part[c][d][lane];
             double *ks = k + (size_t)s * len;
             for (int c = 0; c < 3; c++) {
                 ks[(size_t)c * n + i] = win[(size_t)(3 + c) * n + i];
@@ -434,13 +465,14 @@ __device__ void coop_stage(const DimCoopArgs &A, int s, double h, const double *
                 }
             }
         }
-        __syncthreads();
     }
+    __syncthreads();
 }
 
 // One Fehlberg step of size h: six fused stages, one grid-wide barrier after each.
+template <int P, bool kFastInv>
 __device__ void coop_fehl(const DimCoopArgs &A, cg::grid_group &grid, double h, const double *y0, double *yn,
-                          bool want_er, double (*part)[3][kCoopParticles])
+                          bool want_er, CoopShared<P> &part)
 {
     // stage inputs alternate between two scratch vectors so a stage never overwrites the
     // input other blocks are still reading: w_a for even stages' output, w_b for odd
@@ -448,7 +480,7 @@ __device__ void coop_fehl(const DimCoopArgs &A, cg::grid_group &grid, double h, 
     const double *win = y0;
     for (int st = 0; st < 6; st++) {
         double *wout = (st % 2 == 0) ? wa : wb;
-        coop_stage(A, st, h, y0, win, wout, yn, want_er, part);
+        coop_stage<P, kFastInv>(A, st, h, y0, win, wout, yn, want_er, part);
         grid.sync();
         win = wout;
     }
@@ -490,10 +522,11 @@ __device__ double coop_errnorm(const DimCoopArgs &A, cg::grid_group &grid, const
     return r;
 }
 
+template <int P, bool kFastInv>
 __global__ void __launch_bounds__(256) dim_coop_kernel(const DimCoopArgs A)
 {
     cg::grid_group grid = cg::this_grid();
-    __shared__ double part[kCoopChunks][3][kCoopParticles];
+    __shared__ CoopShared<P> part;
     __shared__ double sh[256];
     __shared__ double total;
     const double EPSMIN = 1e-15;
@@ -508,7 +541,7 @@ __global__ void __launch_bounds__(256) dim_coop_kernel(const DimCoopArgs A)
     int nde = 0;
     grid.sync();
     if (A.init == 1) {
-        coop_stage(A, 0, 0.0, yl0, yl0, A.B.wb, nullptr, false, part);  // k1 only (w unused)
+        coop_stage<P, kFastInv>(A, 0, 0.0, yl0, yl0, A.B.wb, nullptr, false, part);  // k1 only (w unused)
         grid.sync();
         double m = INFINITY;
         for (int e = gid; e < len; e += gsz)
@@ -535,7 +568,7 @@ __global__ void __launch_bounds__(256) dim_coop_kernel(const DimCoopArgs A)
     long long acc = 0, rej = 0;
     int ier = 10000;
     for (int iter = 0; iter < A.itemax; iter++) {
-        coop_fehl(A, grid, H, yl0, yln, true, part);
+        coop_fehl<P, kFastInv>(A, grid, H, yl0, yln, true, part);
         nde += 6;
         const double erret = coop_errnorm(A, grid, yl0, yln, sh);
         if (erret < 0.0) {
@@ -551,8 +584,8 @@ __global__ void __launch_bounds__(256) dim_coop_kernel(const DimCoopArgs A)
                 break;
             }
         } else if (X + H < A.xe) {
-            coop_fehl(A, grid, H / 2, yh0, A.B.yhm, false, part);
-            coop_fehl(A, grid, H / 2, A.B.yhm, yhn, false, part);
+            coop_fehl<P, kFastInv>(A, grid, H / 2, yh0, A.B.yhm, false, part);
+            coop_fehl<P, kFastInv>(A, grid, H / 2, A.B.yhm, yhn, false, part);
             nde += 12;
             X += H;
             double *t1 = yl0; yl0 = yln; yln = t1;  // accepted: the new tracks become the old ones
@@ -562,9 +595,9 @@ __global__ void __launch_bounds__(256) dim_coop_kernel(const DimCoopArgs A)
             else H *= 0.9 / pow(erret, 0.2);
         } else {
             H = A.xe - X;
-            coop_fehl(A, grid, H, yl0, yln, true, part);
-            coop_fehl(A, grid, H / 2, yh0, A.B.yhm, false, part);
-            coop_fehl(A, grid, H / 2, A.B.yhm, yhn, false, part);
+            coop_fehl<P, kFastInv>(A, grid, H, yl0, yln, true, part);
+            coop_fehl<P, kFastInv>(A, grid, H / 2, yh0, A.B.yhm, false, part);
+            coop_fehl<P, kFastInv>(A, grid, H / 2, A.B.yhm, yhn, false, part);
             nde += 18;
             X = A.xe;
             acc++;
@@ -606,12 +639,16 @@ static int dim_integrate_coop(DimRun &R, double *y, double *x0, double xe, int i
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
     if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dim_coop_kernel, 256, 0) != cudaSuccess ||
-        per_sm < 1) {
+    // groups of 8 particles below n = 4096, of 32 above; the inverse-cube form of the run
+    const bool wide = R.n >= 4096;
+    const void *kern = wide ? (R.fast_inv ? (const void *)dim_coop_kernel<32, true> : (const void *)dim_coop_kernel<32, false>)
+                            : (R.fast_inv ? (const void *)dim_coop_kernel<8, true> : (const void *)dim_coop_kernel<8, false>);
+    const int P = wide ? 32 : 8;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0) != cudaSuccess || per_sm < 1) {
         cudaGetLastError();
         return 0;
     }
-    const int ngroups = (R.n + kCoopParticles - 1) / kCoopParticles;
+    const int ngroups = (R.n + P - 1) / P;
     int G = ngroups;
     if (G > sms * per_sm) G = sms * per_sm;
     if (G > kDimCoopMaxBlocks) G = kDimCoopMaxBlocks;  // B.red holds kDimCoopMaxBlocks partials
@@ -636,7 +673,7 @@ static int dim_integrate_coop(DimRun &R, double *y, double *x0, double xe, int i
     cudaError_t e = cudaMemcpyAsync(R.B.io, R.h_pinned, 2 * sizeof(double), cudaMemcpyHostToDevice, R.st);
     void *args[] = {(void *)&A};
     if (e == cudaSuccess)
-        e = cudaLaunchCooperativeKernel((const void *)dim_coop_kernel, dim3(G), dim3(256), args, 0, R.st);
+        e = cudaLaunchCooperativeKernel(kern, dim3(G), dim3(256), args, 0, R.st);
     double out[6] = {0, 0, 0, 0, 0, 0};
     if (e == cudaSuccess) e = cudaMemcpyAsync(R.h_pinned, R.B.io, 6 * sizeof(double), cudaMemcpyDeviceToHost, R.st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(R.st);
@@ -685,6 +722,7 @@ extern "C" int bia_dim_integrate(bia_context *ctx, int n, double eps_th, double 
     R.abserr = abserr;
     R.st = ctx->stream;
     R.h_pinned = ctx->h_dim;
+    R.fast_inv = true;
     dim_carve((double *)ctx->dim.ptr, n, R.B);
     double X = x0, H = 0.0;
     int nde = 0, status = BIA_OK;
