@@ -121,6 +121,9 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--no-oracle-check", action="store_true", help="skip error_vs_oracle")
+    ap.add_argument("--shard", action="store_true",
+                    help="split the one system over the ranks (its pairs in shards, the per-particle sums "
+                         "all-reduced over NCCL) instead of one replica per rank")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the other configurations timed beside the main line")
     ap.add_argument("--no-autotune", action="store_true",
@@ -244,11 +247,13 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def config_keys(workload, n, dt, method, world, reduction, precision, l2, state, autotuned=None):
+def config_keys(workload, n, dt, method, world, reduction, precision, l2, state, autotuned=None, shard=False):
     """The config object of a bench line; both arms print the same keys."""
     return {"workload": workload, "n": n, "pairs_per_step": n * (n - 1) // 2, "dt": dt,
             "method": method, "reduction": reduction, "precision": precision, "l2": l2,
-            "state": state, "parallelism": f"replicas x{world}", "autotuned": autotuned}
+            "state": state, "parallelism": (f"pair shards x{world}, NCCL all-reduce of 6n FP64 per step"
+                                            if shard else f"replicas x{world}"),
+            "autotuned": autotuned}
 
 
 def metric_name(method):
@@ -280,41 +285,38 @@ def _max_over_ranks(dist, value, dev):
     return float(t.item())
 
 
-def run_ensemble(args, rank, world, local):
-    """The batched ensemble: 4096 independent Plummer systems of uneven size, 200 steps in
-    one CUDA graph (one pair-kernel launch per step over all systems)."""
+def ensemble_forms(solver, nsys, steps, warmup, forms, dist=None, dev=None, sample_clocks=False, autotune=True):
+    """The batched ensemble (Plummer systems, N_s uniform in [32, 1024], seeded), each form
+    in `forms` ((label, method) pairs) autotuned on these systems, then `steps` steps from
+    the seeded state replayed from one CUDA graph.  Returns ({label: result}, clocks of the
+    first form, system sizes, pairs per step)."""
     import torch
 
-    from bia_3d_gpu_b200 import BIASolver, default_config, initial
-    dist = _init_dist(world)
-    dev = torch.device("cuda", local)
-    nsys = args.systems
+    from bia_3d_gpu_b200 import default_config, initial
     sizes = initial.ensemble_sizes(nsys, 32, 1024, seed=4)
     states = [initial.plummer(int(n), seed=10000 + k)[0] for k, n in enumerate(sizes)]
     eps = -2.0 / sizes.astype(np.float64)
     host = np.ascontiguousarray(np.concatenate(states, axis=1))
-    steps = args.steps if args.steps is not None else 200
     dt = 1e-4
-    method = METHODS[args.method] if args.method != "learned" else 1
-    cfg = default_config(dt=dt, method=method)
     pairs = int(sum(int(n) * (int(n) - 1) // 2 for n in sizes))
-    solver = BIASolver(device=local)
-    solver.load_heads()
     ens = solver.ensemble(sizes, eps)
     d = torch.tensor(host, device=dev)
     ke0, pe0 = ens.energy(d)
-
-    def timed(c, sample_clocks):
-        """warm-up, graph capture, then the timed graph replay of `steps` steps from the
-        seeded state; returns (ms, clocks, counters, per-system energy drift)."""
+    out, clocks = {}, None
+    for k, (label, method) in enumerate(forms):
+        c = default_config(dt=dt, method=method)
+        tuned = None
+        if autotune:
+            shape, tms = ens.autotune(d, c)
+            tuned = {"shape": shape, "ms": tms}
         with torch.cuda.stream(solver.stream):
-            ens.run(d, c, args.warmup, graph=False, stats=False)     # warm-up (untimed)
+            ens.run(d, c, warmup, graph=False, stats=False)     # warm-up (untimed)
         d.copy_(torch.tensor(host, device=dev))
         ens.run(d, c, steps, graph=True, stats=False)              # capture the graph
         d.copy_(torch.tensor(host, device=dev))
         torch.cuda.synchronize()
         solver.counters(reset=True)
-        sampler = ClockSampler(local) if sample_clocks else None
+        sampler = ClockSampler(dev.index if dev is not None else 0) if (sample_clocks and k == 0) else None
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         if dist is not None:
             dist.barrier()
@@ -325,27 +327,47 @@ def run_ensemble(args, rank, world, local):
         ens.run(d, c, steps, graph=True, stats=False)
         e1.record(solver.stream)
         torch.cuda.synchronize()
-        clk = sampler.stop() if sampler else None
+        if sampler:
+            clocks = sampler.stop()
         t_ms = _max_over_ranks(dist, e0.elapsed_time(e1), dev)
         counters = solver.counters(reset=True)
         ke1, pe1 = ens.energy(d)
         dr = np.abs((ke1 + pe1) / (ke0 + pe0) - 1)
-        return t_ms, clk, counters, dr
+        d.copy_(torch.tensor(host, device=dev))
+        out[label] = {"ms_per_step": t_ms / steps, "systems_steps_per_s": nsys * steps / (t_ms * 1e-3),
+                      "pair_updates_per_s": pairs * steps / (t_ms * 1e-3), "autotuned": tuned,
+                      "newton_iterations": newton_per_pair(counters, method),
+                      "energy_drift": {"max": float(dr.max()), "median": float(np.median(dr)),
+                                       "p99": float(np.quantile(dr, 0.99))},
+                      "stats": counters}
+    ens.close()
+    return out, clocks, sizes, pairs
 
-    ms, clocks, stats, drift = timed(cfg, True)
-    learned = None
-    if not args.no_plain and method == 1:
-        l_ms, _, l_stats, l_drift = timed(default_config(dt=dt, method=3), False)
-        learned = {"value": world * nsys * steps / (l_ms * 1e-3), "unit": "systems-steps/s",
-                   "pair_updates_per_s": world * pairs * steps / (l_ms * 1e-3),
-                   "ms_per_step": l_ms / steps, "speedup_vs_plain": ms / l_ms,
-                   "learned_pair_fraction": l_stats["learned"] / max(1, steps * pairs),
-                   "learned_fallbacks": l_stats["learned_fallbacks"],
-                   "energy_drift": {"max": float(l_drift.max()), "median": float(np.median(l_drift)),
-                                    "p99": float(np.quantile(l_drift, 0.99))}}
+
+def run_ensemble(args, rank, world, local):
+    """The batched ensemble: 4096 independent Plummer systems of uneven size, 200 steps in
+    one CUDA graph (one pair-kernel launch per step over all systems, two for the learned
+    form), each form's launch shape chosen by the ensemble autotuner first."""
+    import torch
+
+    from bia_3d_gpu_b200 import BIASolver
+    dist = _init_dist(world)
+    dev = torch.device("cuda", local)
+    nsys = args.systems
+    steps = args.steps if args.steps is not None else 200
+    method = METHODS[args.method]
+    solver = BIASolver(device=local)
+    solver.load_heads()
+    forms = [(args.method, method)]
+    if not args.no_plain:
+        forms += [(lbl, m) for lbl, m in (("alg", 1), ("universal", 2), ("learned", 3)) if m != method]
+    res, clocks, sizes, pairs = ensemble_forms(solver, nsys, steps, args.warmup, forms, dist, dev,
+                                               sample_clocks=True, autotune=not args.no_autotune)
+    main_r = res[args.method]
+    ms = main_r["ms_per_step"] * steps
     if rank == 0:
-        print(json.dumps({
-            "metric": "BIA ensemble systems-steps/s (plain FP64 step)",
+        line = {
+            "metric": "BIA ensemble systems-steps/s (%s step)" % args.method,
             "value": world * nsys * steps / (ms * 1e-3), "unit": "systems-steps/s",
             "pair_updates_per_s": world * pairs * steps / (ms * 1e-3), "n_gpus": world,
             "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps,
@@ -353,17 +375,19 @@ def run_ensemble(args, rank, world, local):
             "data": "synthetic (seeded)",
             "config": {"workload": "plummer_ensemble_4096", "systems": nsys,
                        "n_min": int(sizes.min()), "n_max": int(sizes.max()),
-                       "particles": int(sizes.sum()), "pairs_per_step": pairs, "dt": dt,
+                       "particles": int(sizes.sum()), "pairs_per_step": pairs, "dt": 1e-4,
                        "method": args.method, "graph": True,
                        "l2": "per-step working set (partials %.1f GB) exceeds the 126 MB L2"
                              % (sum(6 * 32 * ((int(n) + 31) // 32) ** 2 for n in sizes) * 8e-9),
-                       "parallelism": f"replicas x{world}"},
-            "learned": learned,
-            "energy_drift": {"max": float(drift.max()), "median": float(np.median(drift)),
-                             "p99": float(np.quantile(drift, 0.99))},
-            "clocks": clocks, "gpu_launches": 2 * steps,
-            "stats": stats}), flush=True)
-    ens.close()
+                       "parallelism": f"replicas x{world}", "autotuned": main_r["autotuned"]},
+            "forms": {k: {kk: vv for kk, vv in v.items() if kk != "stats"} for k, v in res.items()},
+            "energy_drift": main_r["energy_drift"],
+            "clocks": clocks, "gpu_launches": (3 if method == 3 else 2) * steps,
+            "stats": main_r["stats"]}
+        if "learned" in res:
+            best = min(v["ms_per_step"] for k, v in res.items() if k in ("alg", "universal"))
+            line["learned_vs_best_plain"] = best / res["learned"]["ms_per_step"]
+        print(json.dumps(line), flush=True)
     solver.close()
     if dist is not None:
         dist.destroy_process_group()
@@ -426,15 +450,19 @@ class StepTimer:
             self.dist.barrier()
             self.torch.cuda.synchronize()
 
-    def time(self, d_init, cfg, d_q, k_steps, warmup, sample_clocks=False):
-        """Returns (total ms over k_steps, clocks, counters, (kernel ms, kernel launches))."""
+    def time(self, d_init, cfg, d_q, k_steps, warmup, sample_clocks=False, step=None):
+        """Returns (total ms over k_steps, clocks, counters, (kernel ms, kernel launches)).
+        step (optional): the step call, step(state, cfg, q); default BIASolver.step."""
         torch, solver = self.torch, self.solver
         stream = solver.stream
+        if step is None:
+            def step(st, c, q):
+                solver.step(st, c, q=q, stats=False)
         d_state = d_init.clone()
         with torch.cuda.stream(stream):
             for _ in range(warmup):
                 d_state.copy_(d_init)
-                solver.step(d_state, cfg, q=d_q, stats=False)
+                step(d_state, cfg, d_q)
         solver.counters(reset=True)
         solver.set_timing(True)
         solver.kernel_ms()
@@ -449,7 +477,7 @@ class StepTimer:
                 d_state.copy_(d_init)              # untimed: every step starts from the seeded state
                 self.flush.zero_()                 # untimed L2 flush (256 MB > 126 MB L2)
                 ev[k][0].record(stream)
-                solver.step(d_state, cfg, q=d_q, stats=False)
+                step(d_state, cfg, d_q)
                 ev[k][1].record(stream)
         self.barrier()
         clk = sampler.stop() if sampler else None
@@ -576,13 +604,19 @@ def main():
     if method == 3 and not args.no_autotune:
         lvar, lms = solver.autotune(d_state, cfg, q=d_q)
         tuned = dict(tuned or {}, learned_layout=("one_kernel", "split")[lvar], learned_ms=lms)
+    shard = args.shard and world > 1
+    step_fn = None
+    if shard:
+        def step_fn(st, c, q):
+            solver.step_distributed(st, c, q=q)
     total_ms, clocks, stats, (kern_ms, kern_launches) = timer.time(d_init, cfg, d_q, steps, args.warmup,
-                                                                   sample_clocks=True)
-    value = world * steps * pairs / (total_ms * 1e-3)
+                                                                   sample_clocks=True, step=step_fn)
+    # replicas: every rank advances its own copy of the system; shards: the ranks split one
+    value = (1 if shard else world) * steps * pairs / (total_ms * 1e-3)
 
     # end-to-end through the host-buffer call with pinned host memory
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and not shard:
         h_state = torch.tensor(state).pin_memory()
         h_q = torch.tensor(q).pin_memory() if q is not None else None
         hs = h_state.numpy()
@@ -720,7 +754,8 @@ def main():
         line = {
             "metric": metric_name(args.method), "value": value,
             "unit": "pair-updates/s", "n_gpus": world, "steps": steps, "warmup": args.warmup,
-            "ms_per_step": total_ms / steps, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": total_ms / steps, "higher_is_better": True,
+            "scaling": "strong" if shard else "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "config": config_keys(args.workload, n, dt, args.method, world, reduction="deterministic",
                                   precision=("heads: BF16 operands, FP32 accumulation; first correction "
@@ -729,9 +764,11 @@ def main():
                                   l2="256 MB buffer written between timed steps (untimed)",
                                   state="reset to the seeded state before every timed step (untimed "
                                         "device copy; the e2e loop copies it into the host buffer)",
-                                  autotuned=tuned),
+                                  autotuned=tuned, shard=shard),
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-            "gpu_launches": (3 if split else 2) * steps,
+            # pair kernel(s) and the reduction per step; a shard's reduction is two launches
+            # (the shard's sums, then the update after the all-reduce)
+            "gpu_launches": ((3 if split else 2) + (1 if shard else 0)) * steps,
             "learned_vs_best_plain": learned_vs_best_plain,
             "error_vs_oracle": errors,
             "plain_fp64": plain, "universal": universal,
@@ -845,6 +882,11 @@ def run_extras(solver, timer, args):
         ms, st = timer.graph_run(d_init, default_config(eps_th=eps, dt=dt, method=m), None, steps_cfg)
         traj[label] = {"ms_per_step": ms / steps_cfg, "newton_iterations": newton_per_pair(st, m)}
     out["plummer_32768_trajectory"] = traj
+    ens, _, sizes, epairs = ensemble_forms(solver, 4096, 20, 3, [("alg", 1), ("universal", 2), ("learned", 3)],
+                                           dev=dev)
+    out["plummer_ensemble_4096"] = {"systems": 4096, "pairs_per_step": epairs, "steps": 20, "graph": True,
+                                    "forms": {k: {kk: vv for kk, vv in v.items() if kk != "stats"}
+                                              for k, v in ens.items()}}
     # the DIM direct-sum RKF45 solver as the physics check of the learned step on the same
     # sphere: DIM from 0 to dt (per-particle coupling eps/2) against one BIA step
     t = d_init.clone()

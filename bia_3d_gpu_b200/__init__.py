@@ -211,6 +211,44 @@ class BIASolver:
             return None
         return self._finish(st, s, "bia_step")
 
+    def step_shard(self, state, cfg, shard, nshards, sums, q=None, stats=False):
+        """Shard `shard` of `nshards` of one step (bia_step_shard): its pairs' sums into
+        sums ((6, n) float64 CUDA tensor); the state is unchanged."""
+        n = self._check_state(state)
+        if sums.shape != (6, n) or not sums.is_contiguous():
+            raise ValueError("sums must be a contiguous (6, n) float64 tensor")
+        st_ = BiaStats()
+        cur = self._enter()
+        st = capi.lib().bia_step_shard(self._ctx, ctypes.byref(cfg), n, *self._ptrs(state), self._qptr(q, n),
+                                       int(shard), int(nshards), ctypes.c_void_p(sums.data_ptr()),
+                                       ctypes.byref(st_) if stats else None)
+        self._leave(cur)
+        if not stats:
+            capi.check(st, "bia_step_shard")
+            return None
+        return self._finish(st, st_, "bia_step_shard")
+
+    def apply_update(self, state, dt, sums):
+        """Drift and update from the summed shard sums (bia_apply_update)."""
+        n = self._check_state(state)
+        cur = self._enter()
+        st = capi.lib().bia_apply_update(self._ctx, n, float(dt), *self._ptrs(state),
+                                         ctypes.c_void_p(sums.data_ptr()))
+        self._leave(cur)
+        capi.check(st, "bia_apply_update")
+
+    def step_distributed(self, state, cfg, q=None, group=None):
+        """One step of a system split over the ranks of a torch.distributed process group
+        (NCCL over NVLink on GPUs): every rank holds the whole state, solves its shard of the
+        pairs, the shard sums are all-reduced (6n FP64) and every rank applies the same
+        update."""
+        import torch.distributed as dist
+        rank, world = dist.get_rank(group), dist.get_world_size(group)
+        sums = self._torch.empty_like(state)
+        self.step_shard(state, cfg, rank, world, sums, q=q)
+        dist.all_reduce(sums, group=group)
+        self.apply_update(state, cfg.dt, sums)
+
     def run(self, state, cfg, nsteps, q=None, graph=True, stats=True):
         """nsteps steps; the step sequence is captured once in a CUDA graph and replayed."""
         n = self._check_state(state)
@@ -359,6 +397,44 @@ class Ensemble:
         except Exception:
             pass
 
+    def step_shard(self, state, cfg, shard, nshards, sums, q=None, stats=False):
+        """Shard `shard` of `nshards` of one step (bia_step_shard): its pairs' sums into
+        sums ((6, n) float64 CUDA tensor); the state is unchanged."""
+        n = self._check_state(state)
+        if sums.shape != (6, n) or not sums.is_contiguous():
+            raise ValueError("sums must be a contiguous (6, n) float64 tensor")
+        st_ = BiaStats()
+        cur = self._enter()
+        st = capi.lib().bia_step_shard(self._ctx, ctypes.byref(cfg), n, *self._ptrs(state), self._qptr(q, n),
+                                       int(shard), int(nshards), ctypes.c_void_p(sums.data_ptr()),
+                                       ctypes.byref(st_) if stats else None)
+        self._leave(cur)
+        if not stats:
+            capi.check(st, "bia_step_shard")
+            return None
+        return self._finish(st, st_, "bia_step_shard")
+
+    def apply_update(self, state, dt, sums):
+        """Drift and update from the summed shard sums (bia_apply_update)."""
+        n = self._check_state(state)
+        cur = self._enter()
+        st = capi.lib().bia_apply_update(self._ctx, n, float(dt), *self._ptrs(state),
+                                         ctypes.c_void_p(sums.data_ptr()))
+        self._leave(cur)
+        capi.check(st, "bia_apply_update")
+
+    def step_distributed(self, state, cfg, q=None, group=None):
+        """One step of a system split over the ranks of a torch.distributed process group
+        (NCCL over NVLink on GPUs): every rank holds the whole state, solves its shard of the
+        pairs, the shard sums are all-reduced (6n FP64) and every rank applies the same
+        update."""
+        import torch.distributed as dist
+        rank, world = dist.get_rank(group), dist.get_world_size(group)
+        sums = self._torch.empty_like(state)
+        self.step_shard(state, cfg, rank, world, sums, q=q)
+        dist.all_reduce(sums, group=group)
+        self.apply_update(state, cfg.dt, sums)
+
     def run(self, state, cfg, nsteps, q=None, graph=True, stats=True):
         s = self.solver
         n = s._check_state(state)
@@ -374,6 +450,26 @@ class Ensemble:
             capi.check(st, "bia_ensemble_run")
             return None
         return s._finish(st, st_, "bia_ensemble_run")
+
+    SHAPES = {1: ("tiles8", "phase16", "phase32"), 2: ("item_per_warp", "persistent"),
+              3: ("list_1_cta_per_sm", "list_2_ctas_per_sm")}
+
+    def autotune(self, state, cfg, q=None):
+        """Time the launch shapes of cfg.method's pair kernels on these systems and keep the
+        fastest (bia_ensemble_autotune); returns (shape name or None, {shape: ms})."""
+        s = self.solver
+        n = s._check_state(state)
+        var = ctypes.c_int(-1)
+        ms = (ctypes.c_float * 3)()
+        cur = s._enter()
+        st = capi.lib().bia_ensemble_autotune(s._ctx, self._ens, ctypes.byref(cfg), *s._ptrs(state),
+                                              s._qptr(q, n), ctypes.byref(var), ms)
+        s._leave(cur)
+        capi.check(st, "bia_ensemble_autotune")
+        names = self.SHAPES.get(cfg.method)
+        if names is None:
+            return None, {}
+        return names[var.value], {names[k]: float(ms[k]) for k in range(len(names)) if ms[k] >= 0}
 
     def energy(self, state, q=None):
         """(KE, PE) arrays per system: KE = sum |v|^2, PE = eps_s sum_{i<j} (q_i q_j)/r_ij."""

@@ -94,6 +94,13 @@ def lib():
     L.bia_invariance.argtypes = [_V, _I, _D] + [_V] * 7 + [_PD]
     L.bia_measure_fp64_peak.argtypes = [_I, _PD]
     L.bia_context_stats.argtypes = [_V, ctypes.POINTER(BiaStats), _I]
+    L.bia_shard_columns.argtypes = [_I, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)]
+    L.bia_shard_columns.restype = _I
+    L.bia_step_shard.argtypes = ([_V, ctypes.POINTER(BiaConfig), _I] + [_V] * 7 + [_I, _I, _V,
+                                 ctypes.POINTER(BiaStats)])
+    L.bia_step_shard.restype = _I
+    L.bia_apply_update.argtypes = [_V, _I, _D] + [_V] * 7
+    L.bia_apply_update.restype = _I
     L.bia_step_noalloc.argtypes = [ctypes.POINTER(BiaConfig), _I] + [_V] * 9
     L.bia_step_noalloc.restype = _I
     L.bia_ensemble_create.argtypes = [_V, _I, ctypes.POINTER(ctypes.c_int), _PD, ctypes.POINTER(_V)]
@@ -103,6 +110,9 @@ def lib():
     L.bia_ensemble_run.argtypes = ([_V, _V, ctypes.POINTER(BiaConfig)] + [_V] * 7 +
                                    [_I, _I, ctypes.POINTER(BiaStats)])
     L.bia_ensemble_energy.argtypes = [_V, _V] + [_V] * 7 + [_PD]
+    L.bia_ensemble_autotune.argtypes = ([_V, _V, ctypes.POINTER(BiaConfig)] + [_V] * 7 +
+                                        [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)])
+    L.bia_ensemble_autotune.restype = _I
     for name in ("bia_ensemble_create", "bia_ensemble_destroy", "bia_ensemble_run",
                  "bia_ensemble_energy"):
         getattr(L, name).restype = _I
@@ -177,11 +187,21 @@ EXPORTED_SYMBOLS = ("bia_config_default", "bia_context_create", "bia_context_des
                     "bia_step", "bia_run", "bia_run_host", "bia_invariance", "bia_status_string",
                     "bia_measure_fp64_peak", "bia_context_stats", "bia_dim_integrate", "rkf_c_",
                     "bia_ensemble_create", "bia_ensemble_destroy", "bia_ensemble_particles",
-                    "bia_ensemble_run", "bia_ensemble_energy",
+                    "bia_ensemble_run", "bia_ensemble_energy", "bia_ensemble_autotune",
                     "bia_context_set_heads", "bia_learned_head_eval", "bia_context_autotune",
                     "bia_selftest_wait_timeout", "bia_step_noalloc",
+                    "bia_shard_columns", "bia_step_shard", "bia_apply_update",
                     "bia_trainer_create", "bia_trainer_destroy", "bia_trainer_param_count",
                     "bia_trainer_get_params", "bia_trainer_set_params", "bia_trainer_gradient",
                     "bia_trainer_train", "bia_trainer_export", "bia_trainer_samples",
                     "bia_trainer_copy_samples",
                     "bia_last_error", "find_dxyuv_kernel_", "invariance_gpu_")
+
+
+def shard_columns(n, shard, nshards):
+    """(c0, c1): the 32-particle column blocks whose pairs shard `shard` of `nshards` owns
+    (host-only, no GPU needed)."""
+    c0, c1 = ctypes.c_int(0), ctypes.c_int(0)
+    check(lib().bia_shard_columns(int(n), int(shard), int(nshards), ctypes.byref(c0), ctypes.byref(c1)),
+          "bia_shard_columns")
+    return c0.value, c1.value

@@ -38,6 +38,9 @@ struct bia_ensemble {
     // pair masks per item
     unsigned int *d_split = nullptr;   // [16 + kEnsBins nitems + 32 nitems]
     size_t part_doubles = 0;
+    // launch shape chosen by bia_ensemble_autotune per method (index BIA_METHOD_*), -1: the
+    // built-in rule
+    int tuned[4] = {-1, -1, -1, -1};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     bia::GraphKey graph_key;
@@ -66,35 +69,49 @@ struct EnsArgs {
     uint32_t *lmask;                 // and the pair masks of every item
 };
 
+// Each warp takes items t = (its global warp index) + k * (warps in the grid), as
+// bia_pair_tiles_kernel (a persistent grid for the universal-variable method, the counters
+// flushed per warp every kFlushBlocks items).
 template <int M>
 __global__ void __launch_bounds__(kEnsThreads, TileOccupancy<M>::kMinBlocks) ens_pair_tiles_kernel(const EnsArgs A)
 {
     const int lane = threadIdx.x & 31;
-    const long long t = (long long)blockIdx.x * kEnsWarps + (threadIdx.x >> 5);
-    if (t >= A.nitems) return;  // warp-uniform
-    const uint2 it = A.items[t];
-    const int s = (int)it.x;
-    const int bi = (int)(it.y & 0xffffu), bj = (int)(it.y >> 16);
-    const int base = A.off[s];
-    const int n = A.off[s + 1] - base;
-    const double *q = A.q ? A.q + base : nullptr;
-    double racc[6], cacc[6];
-    PairCounters cnt;
-    warp_block_solve<M>(A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base, q, n,
+    PairCounters tot;
+    counters_zero(tot);
+    int nblk = 0;
+    for (long long t = (long long)blockIdx.x * kEnsWarps + (threadIdx.x >> 5); t < A.nitems;
+         t += (long long)gridDim.x * kEnsWarps) {  // warp-uniform
+        const uint2 it = A.items[t];
+        const int s = (int)it.x;
+        const int bi = (int)(it.y & 0xffffu), bj = (int)(it.y >> 16);
+        const int base = A.off[s];
+        const int n = A.off[s + 1] - base;
+        const double *q = A.q ? A.q + base : nullptr;
+        double racc[6], cacc[6];
+        PairCounters cnt;
+        warp_block_solve<M>(A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base, q, n,
                             A.eps[s], A.P, bi, bj, lane, racc, cacc, cnt);
-    flush_counters(cnt, A.stats, lane);
-    const int nb = (n + 31) / 32;
-    write_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
+        counters_add(tot, cnt);
+        if (++nblk == kFlushBlocks) {
+            flush_counters(tot, A.stats, lane);
+            counters_zero(tot);
+            nblk = 0;
+        }
+        const int nb = (n + 31) / 32;
+        write_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
+    }
+    if (nblk > 0) flush_counters(tot, A.stats, lane);
 }
 
-// Phase-locked ALG variant of ens_pair_tiles_kernel (see phase_block_solve): one CTA of
-// kPhaseWarps warps per SM, each warp on one item; bitwise the same results.
-__global__ void __launch_bounds__(kPhaseWarps * 32, kPhaseMinBlocks) ens_pair_phase_kernel(const EnsArgs A)
+// Phase-locked ALG variant of ens_pair_tiles_kernel (see phase_block_solve): CTAs of kW
+// warps, kMinB of them per SM, each warp on one item; bitwise the same results.
+template <int kW, int kMinB>
+__global__ void __launch_bounds__(kW * 32, kMinB) ens_pair_phase_kernel(const EnsArgs A)
 {
     extern __shared__ double phase_smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const long long t = (long long)blockIdx.x * kPhaseWarps + warp;
+    const long long t = (long long)blockIdx.x * kW + warp;
     const bool live = t < A.nitems;
     int s = 0, bi = 0, bj = 0;
     if (live) {
@@ -130,8 +147,10 @@ static int ens_phase_setup()
     if (!done_of[dev]) {
         int sms = 0;
         bool ok = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess;
-        ok = ok && cudaFuncSetAttribute(ens_pair_phase_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        kPhaseSmemBytes) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(ens_pair_phase_kernel<32, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        32 * kTileSmemDoubles * (int)sizeof(double)) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(ens_pair_phase_kernel<16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        16 * kTileSmemDoubles * (int)sizeof(double)) == cudaSuccess;
         if (!ok) cudaGetLastError();
         sms_of[dev] = ok ? sms : 0;
         done_of[dev] = true;
@@ -146,30 +165,40 @@ __global__ void __launch_bounds__(kEnsThreads, 2) ens_pair_rest_kernel(const Ens
 {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const long long t = (long long)blockIdx.x * kEnsWarps + (threadIdx.x >> 5);
-    if (t >= A.nitems) return;  // warp-uniform
-    const uint2 it = A.items[t];
-    const int s = (int)it.x;
-    const int bi = (int)(it.y & 0xffffu), bj = (int)(it.y >> 16);
-    const int base = A.off[s];
-    const int n = A.off[s + 1] - base;
-    double racc[6], cacc[6];
-    PairCounters cnt;
-    const uint32_t learned = rest_block_solve(A.x + base, A.y + base, A.z + base, A.u + base, A.v + base,
-                                              A.w + base, A.q ? A.q + base : nullptr, n, A.eps[s], A.P.dt, bi,
-                                              bj, lane, racc, cacc, cnt);
-    flush_counters(cnt, A.stats, lane);
-    const int nb = (n + 31) / 32;
-    write_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
-    const unsigned total = __reduce_add_sync(full, (unsigned)__popc(learned));
-    if (total != 0u) {
-        const int bin = min(kEnsBins - 1, 31 - __clz((int)total));
-        A.lmask[(size_t)t * 32 + lane] = learned;
-        if (lane == 0) {
-            const unsigned int slot = atomicAdd(&A.wbcount[bin], 1u);
-            A.wblist[(size_t)bin * A.nitems + slot] = (unsigned int)t;
+    PairCounters tot;
+    counters_zero(tot);
+    int nblk = 0;
+    for (long long t = (long long)blockIdx.x * kEnsWarps + (threadIdx.x >> 5); t < A.nitems;
+         t += (long long)gridDim.x * kEnsWarps) {  // warp-uniform
+        const uint2 it = A.items[t];
+        const int s = (int)it.x;
+        const int bi = (int)(it.y & 0xffffu), bj = (int)(it.y >> 16);
+        const int base = A.off[s];
+        const int n = A.off[s + 1] - base;
+        double racc[6], cacc[6];
+        PairCounters cnt;
+        const uint32_t learned = rest_block_solve(A.x + base, A.y + base, A.z + base, A.u + base, A.v + base,
+                                                  A.w + base, A.q ? A.q + base : nullptr, n, A.eps[s], A.P.dt,
+                                                  bi, bj, lane, racc, cacc, cnt);
+        counters_add(tot, cnt);
+        if (++nblk == kFlushBlocks) {
+            flush_counters(tot, A.stats, lane);
+            counters_zero(tot);
+            nblk = 0;
+        }
+        const int nb = (n + 31) / 32;
+        write_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
+        const unsigned total = __reduce_add_sync(full, (unsigned)__popc(learned));
+        if (total != 0u) {
+            const int bin = min(kEnsBins - 1, 31 - __clz((int)total));
+            A.lmask[(size_t)t * 32 + lane] = learned;
+            if (lane == 0) {
+                const unsigned int slot = atomicAdd(&A.wbcount[bin], 1u);
+                A.wblist[(size_t)bin * A.nitems + slot] = (unsigned int)t;
+            }
         }
     }
+    if (nblk > 0) flush_counters(tot, A.stats, lane);
 }
 
 // Learned step, second kernel: persistent CTAs work through the listed items eight at a
@@ -345,6 +374,65 @@ __global__ void __launch_bounds__(256) ens_energy_kernel(const double *u, const 
     }
 }
 
+// Launch shapes of the ensemble's pair kernels (bia_ensemble_autotune chooses among them):
+//   ALG          0: 8-warp CTAs (ens_pair_tiles_kernel), 1: phase-locked 16-warp CTAs (2 per SM),
+//                2: phase-locked 32-warp CTAs (1 per SM); built-in rule: 2 from two of its CTAs
+//                per SM up, else 0
+//   universal    0: one item per warp, 1: a persistent grid of 2 CTAs per SM (built-in)
+//   learned      the persistent list kernel with 0: 1 CTA per SM, 1: 2 CTAs per SM (built-in)
+// Every shape runs the same per-item arithmetic in the same order: the results are bitwise
+// the same.
+constexpr int kEnsShapes = 3;
+
+static int ens_pair_launch(bia_context *ctx, bia_ensemble *E, EnsArgs &A, int method, int shape)
+{
+    const unsigned grid = (unsigned)((E->nitems + kEnsWarps - 1) / kEnsWarps);
+    cudaStream_t st = ctx->stream;
+    if (method == BIA_METHOD_LEARNED) {
+        // the split step of bia_step: the rest kernel, then the list kernel (the same
+        // per-warp-block arithmetic, so each system equals its own learned bia_step)
+        const int lsetup = ens_learned_setup();
+        if (!ctx->heads_loaded) return BIA_ERR_INVALID_ARGUMENT;
+        if (lsetup <= 0) return BIA_ERR_CUDA;
+        A.wbcount = E->d_split;
+        A.wblist = E->d_split + 16;
+        A.lmask = E->d_split + 16 + (size_t)kEnsBins * E->nitems;
+        cudaError_t e = cudaMemsetAsync(A.wbcount, 0, kEnsBins * sizeof(unsigned int), st);
+        if (e != cudaSuccess) return cuda_status(e);
+        ens_pair_rest_kernel<<<(unsigned)persistent_grid(grid), kEnsThreads, 0, st>>>(A);
+        const long long need = (E->nitems + kLearnedWarps - 1) / kLearnedWarps;
+        long long cap = lsetup;
+        if (shape == 0 || shape == 1) cap = (long long)device_sm_count() * (shape + 1);
+        const unsigned lgrid = (unsigned)(need < cap ? need : cap);
+        ens_pair_learned_list_kernel<<<lgrid, kMlpThreads, kLearnedSmemBytes, st>>>(A);
+        return cuda_status(cudaGetLastError());
+    }
+    switch (method) {
+    case BIA_METHOD_RKF: ens_pair_tiles_kernel<kMethodRkf><<<grid, kEnsThreads, 0, st>>>(A); break;
+    case BIA_METHOD_UNIVERSAL:
+        ens_pair_tiles_kernel<kMethodUniversal>
+            <<<shape == 0 ? grid : (unsigned)persistent_grid(grid), kEnsThreads, 0, st>>>(A);
+        break;
+    default: {
+        const int sms = BIA_PHASE_WARPS > 0 ? ens_phase_setup() : 0;
+        int var = shape;
+        if (var < 0 || var >= kEnsShapes) var = (sms > 0 && (E->nitems + 31) / 32 >= 2LL * sms) ? 2 : 0;
+        if (sms <= 0) var = 0;
+        if (var == 2) {
+            ens_pair_phase_kernel<32, 1><<<(unsigned)((E->nitems + 31) / 32), 32 * 32,
+                                            32 * kTileSmemDoubles * sizeof(double), st>>>(A);
+        } else if (var == 1) {
+            ens_pair_phase_kernel<16, 2><<<(unsigned)((E->nitems + 15) / 16), 16 * 32,
+                                            16 * kTileSmemDoubles * sizeof(double), st>>>(A);
+        } else {
+            ens_pair_tiles_kernel<kMethodAlg><<<grid, kEnsThreads, 0, st>>>(A);
+        }
+        break;
+    }
+    }
+    return cuda_status(cudaGetLastError());
+}
+
 static int ens_enqueue_step(bia_context *ctx, bia_ensemble *E, const bia_config *cfg, double *x, double *y,
                             double *z, double *u, double *v, double *w, const double *q)
 {
@@ -364,39 +452,8 @@ static int ens_enqueue_step(bia_context *ctx, bia_ensemble *E, const bia_config 
     A.P.itr = cfg->itr;
     A.P.method = cfg->method;
     A.heads = (const MlpImage *)ctx->heads.ptr;
-    const unsigned grid = (unsigned)((E->nitems + kEnsWarps - 1) / kEnsWarps);
-    if (cfg->method == BIA_METHOD_LEARNED) {
-        // the split step of bia_step: the rest kernel, then the list kernel (the same
-        // per-warp-block arithmetic, so each system equals its own learned bia_step)
-        const int lsetup = ens_learned_setup();
-        if (!ctx->heads_loaded) return BIA_ERR_INVALID_ARGUMENT;
-        if (lsetup <= 0) return BIA_ERR_CUDA;
-        A.wbcount = E->d_split;
-        A.wblist = E->d_split + 16;
-        A.lmask = E->d_split + 16 + (size_t)kEnsBins * E->nitems;
-        cudaError_t e = cudaMemsetAsync(A.wbcount, 0, kEnsBins * sizeof(unsigned int), ctx->stream);
-        if (e != cudaSuccess) return cuda_status(e);
-        ens_pair_rest_kernel<<<grid, kEnsThreads, 0, ctx->stream>>>(A);
-        const long long need = (E->nitems + kLearnedWarps - 1) / kLearnedWarps;
-        const unsigned lgrid = (unsigned)(need < lsetup ? need : lsetup);
-        ens_pair_learned_list_kernel<<<lgrid, kMlpThreads, kLearnedSmemBytes, ctx->stream>>>(A);
-    } else {
-        switch (cfg->method) {
-    case BIA_METHOD_RKF: ens_pair_tiles_kernel<kMethodRkf><<<grid, kEnsThreads, 0, ctx->stream>>>(A); break;
-    case BIA_METHOD_UNIVERSAL:
-        ens_pair_tiles_kernel<kMethodUniversal><<<grid, kEnsThreads, 0, ctx->stream>>>(A);
-        break;
-    default: {
-        const long long pgrid = (E->nitems + kPhaseWarps - 1) / kPhaseWarps;
-        const int sms = BIA_PHASE_WARPS > 0 ? ens_phase_setup() : 0;
-        if (sms > 0 && pgrid >= 2LL * sms)
-            ens_pair_phase_kernel<<<(unsigned)pgrid, kPhaseWarps * 32, kPhaseSmemBytes, ctx->stream>>>(A);
-        else
-            ens_pair_tiles_kernel<kMethodAlg><<<grid, kEnsThreads, 0, ctx->stream>>>(A);
-        break;
-    }
-        }
-    }
+    const int st = ens_pair_launch(ctx, E, A, cfg->method, E->tuned[cfg->method & 3]);
+    if (st != BIA_OK) return st;
     EnsUpdateArgs U;
     U.x = x; U.y = y; U.z = z; U.u = u; U.v = v; U.w = w;
     U.off = E->d_off;
@@ -571,4 +628,77 @@ extern "C" int bia_ensemble_energy(bia_context *ctx, bia_ensemble *E, const doub
                                     ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     return cuda_status(e);
+}
+
+extern "C" int bia_ensemble_autotune(bia_context *ctx, bia_ensemble *E, const bia_config *cfg, double *x, double *y,
+                                     double *z, double *u, double *v, double *w, const double *q, int *variant,
+                                     float *ms)
+{
+    if (!ctx || !E || !cfg || !x || !y || !z || !u || !v || !w) return BIA_ERR_INVALID_ARGUMENT;
+    if (variant) *variant = -1;
+    if (ms)
+        for (int k = 0; k < kEnsShapes; k++) ms[k] = -1.0f;
+    const int method = cfg->method;
+    if (method == BIA_METHOD_LEARNED && !ctx->heads_loaded) return BIA_ERR_INVALID_ARGUMENT;
+    const int nshapes = method == BIA_METHOD_ALG ? 3 : (method == BIA_METHOD_UNIVERSAL || method == BIA_METHOD_LEARNED) ? 2 : 0;
+    if (nshapes == 0) return BIA_OK;  // one shape only
+    cudaError_t e = cudaSetDevice(ctx->device);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (e == cudaSuccess && ctx->stream) e = cudaStreamIsCapturing(ctx->stream, &cap);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (cap != cudaStreamCaptureStatusNone) return BIA_ERR_INVALID_ARGUMENT;
+    if (method == BIA_METHOD_LEARNED && !ens_learned_setup()) return BIA_ERR_CUDA;
+    EnsArgs A{};
+    A.x = x; A.y = y; A.z = z; A.u = u; A.v = v; A.w = w; A.q = q;
+    A.off = E->d_off;
+    A.part_off = E->d_part_off;
+    A.eps = E->d_eps;
+    A.items = E->d_items;
+    A.nitems = E->nitems;
+    A.part = E->d_part;
+    A.stats = (unsigned long long *)ctx->stats.ptr;
+    A.P.dt = cfg->dt; A.P.err = cfg->err; A.P.relerr = cfg->rkf_relerr; A.P.abserr = cfg->rkf_abserr;
+    A.P.itr = cfg->itr; A.P.method = method;
+    A.heads = (const MlpImage *)ctx->heads.ptr;
+    cudaEvent_t ev[2];
+    e = cudaEventCreate(&ev[0]);
+    if (e == cudaSuccess) e = cudaEventCreate(&ev[1]);
+    if (e != cudaSuccess) return cuda_status(e);
+    int best = -1;
+    float best_ms = 0.0f;
+    int st = BIA_OK;
+    for (int var = 0; var < nshapes && st == BIA_OK && e == cudaSuccess; var++) {
+        float t_min = 0.0f;
+        for (int rep = 0; rep < 4 && st == BIA_OK && e == cudaSuccess; rep++) {  // the first is a warm-up
+            e = cudaEventRecord(ev[0], ctx->stream);
+            if (e == cudaSuccess) st = ens_pair_launch(ctx, E, A, method, var);
+            if (e == cudaSuccess && st == BIA_OK) e = cudaEventRecord(ev[1], ctx->stream);
+            if (e == cudaSuccess && st == BIA_OK) e = cudaEventSynchronize(ev[1]);
+            float t = 0.0f;
+            if (e == cudaSuccess && st == BIA_OK) e = cudaEventElapsedTime(&t, ev[0], ev[1]);
+            if (rep == 1 || (rep > 1 && t < t_min)) t_min = t;
+        }
+        if (e != cudaSuccess || st != BIA_OK) break;
+        if (ms) ms[var] = t_min;
+        if (best < 0 || t_min < best_ms) {
+            best = var;
+            best_ms = t_min;
+        }
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    if (st != BIA_OK) return st;
+    // the timing launches counted pairs: clear the counters
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->stats.ptr, 0, kNumStats * sizeof(unsigned long long), ctx->stream);
+    if (e == cudaSuccess) e = ctx->stream ? cudaStreamSynchronize(ctx->stream) : cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_status(e);
+    if (E->tuned[method] != best && E->graph_exec) {  // a captured step sequence has the old shape
+        cudaGraphExecDestroy(E->graph_exec);
+        cudaGraphDestroy(E->graph);
+        E->graph_exec = nullptr;
+        E->graph = nullptr;
+    }
+    E->tuned[method] = best;
+    if (variant) *variant = best;
+    return BIA_OK;
 }

@@ -45,7 +45,8 @@ struct StepArgs {
     const double *x, *y, *z, *u, *v, *w, *q;
     double *part;   // deterministic partials, or atomic accumulators
     unsigned long long *stats;
-    long long nwb;  // number of warp-blocks = nb*(nb+1)/2
+    long long nwb;  // warp-blocks of the launch: t0 .. t0 + nwb - 1 (all: nb*(nb+1)/2)
+    long long t0;   // first warp-block (a shard of a multi-GPU step; 0 otherwise)
     int n, nb, npad;
     double eps_th;
     PairParams P;
@@ -69,10 +70,10 @@ __global__ void __launch_bounds__(kThreads, TileOccupancy<M>::kMinBlocks) bia_pa
     PairCounters tot;
     counters_zero(tot);
     int nblk = 0;
-    for (long long t = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); t < A.nwb;
-         t += (long long)gridDim.x * kWarpsPerBlock) {  // warp-uniform
+    for (long long tl = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); tl < A.nwb;
+         tl += (long long)gridDim.x * kWarpsPerBlock) {  // warp-uniform
         int bi, bj;
-        warp_block_coords(t, bi, bj);
+        warp_block_coords(A.t0 + tl, bi, bj);
         const int i = bi * 32 + lane;
         const int jown = bj * 32 + lane;
         const bool diag = (bi == bj);
@@ -113,10 +114,10 @@ __global__ void __launch_bounds__(kW * 32, kMinB) bia_pair_phase_kernel(const St
     extern __shared__ double phase_smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const long long t = (long long)blockIdx.x * kW + warp;
-    const bool live = t < A.nwb;
+    const long long tl = (long long)blockIdx.x * kW + warp;
+    const bool live = tl < A.nwb;
     int bi = 0, bj = 0;
-    if (live) warp_block_coords(t, bi, bj);
+    if (live) warp_block_coords(A.t0 + tl, bi, bj);
     double racc[6], cacc[6];
     PairCounters cnt;
     phase_block_solve(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P, bi, bj, lane, live,
@@ -293,10 +294,10 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const 
     const LearnedSmem M = learned_smem(learned_smem_raw);
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const long long t = (long long)blockIdx.x * kLearnedWarps + warp;
-    const bool live = t < A.nwb;
+    const long long tl = (long long)blockIdx.x * kLearnedWarps + warp;
+    const bool live = tl < A.nwb;
     int bi = 0, bj = 0;
-    if (live) warp_block_coords(t, bi, bj);
+    if (live) warp_block_coords(A.t0 + tl, bi, bj);
     const LearnedBlockIn B = {A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P.dt, A.heads};
     double racc[6], cacc[6];
     PairCounters cnt;
@@ -325,8 +326,9 @@ __global__ void __launch_bounds__(kThreads, kPersistentCtas) bia_pair_rest_kerne
     PairCounters tot;
     counters_zero(tot);
     int nblk = 0;
-    for (long long t = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); t < A.nwb;
-         t += (long long)gridDim.x * kWarpsPerBlock) {  // warp-uniform
+    for (long long tl = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); tl < A.nwb;
+         tl += (long long)gridDim.x * kWarpsPerBlock) {  // warp-uniform
+        const long long t = A.t0 + tl;
         int bi, bj;
         warp_block_coords(t, bi, bj);
         double racc[6], cacc[6];
@@ -589,8 +591,10 @@ static void record_event(bia_context *ctx)
     cudaEventRecord(ctx->ev[ctx->ev_used++], ctx->stream);
 }
 
-int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y, double *z,
-                 double *u, double *v, double *w, const double *q, double *disp)
+// The pair launches of a step over warp-blocks t0 .. t0 + nwb - 1 (all of them: t0 = 0,
+// nwb = -1), into the deterministic partials or the atomic accumulators of the context.
+static int enqueue_pairs(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y, double *z,
+                         double *u, double *v, double *w, const double *q, long long t0, long long nwb)
 {
     const int nb = num_blocks32(n);
     StepArgs A{};
@@ -599,7 +603,9 @@ int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
     A.n = n;
     A.nb = nb;
     A.npad = nb * 32;
-    A.nwb = (long long)nb * (nb + 1) / 2;
+    const long long all = (long long)nb * (nb + 1) / 2;
+    A.t0 = t0;
+    A.nwb = nwb < 0 ? all : nwb;
     A.eps_th = cfg->eps_th;
     A.P.dt = cfg->dt;
     A.P.err = cfg->err;
@@ -608,6 +614,44 @@ int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
     A.P.itr = cfg->itr;
     A.P.method = cfg->method;
     const long long grid = (A.nwb + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    A.heads = (const MlpImage *)ctx->heads.ptr;
+    const bool learned = cfg->method == BIA_METHOD_LEARNED;
+    bool split = false;
+    if (learned) {
+        const int lt = ctx->learned_tuned[cfg->deterministic ? 1 : 0][ilog2_bucket(n)];
+        split = (lt >= 0) ? (lt == 1 && ctx->lmask.ptr) : learned_split(all);
+    }
+    if (split) split_buffer_carve(ctx->lmask.ptr, all, A);
+    if (learned && !ctx->heads_loaded) return BIA_ERR_INVALID_ARGUMENT;
+    if (A.nwb == 0) {  // an empty shard: nothing to launch (the accumulators are cleared)
+        if (!cfg->deterministic)
+            return cuda_status(cudaMemsetAsync(ctx->acc.ptr, 0, 6 * (size_t)A.npad * sizeof(double), ctx->stream));
+        return BIA_OK;
+    }
+    int st = BIA_OK;
+    if (cfg->deterministic) {
+        A.part = (double *)ctx->part.ptr;
+        record_event(ctx);
+        if (learned) st = launch_pair_learned<true>(A, ctx->stream);
+        else launch_pair_tiles<true>(A, grid, ctx->stream, ctx->alg_tuned[1][ilog2_bucket(n)]);
+        record_event(ctx);
+    } else {
+        A.part = (double *)ctx->acc.ptr;
+        cudaMemsetAsync(A.part, 0, 6 * (size_t)A.npad * sizeof(double), ctx->stream);
+        record_event(ctx);
+        if (learned) st = launch_pair_learned<false>(A, ctx->stream);
+        else launch_pair_tiles<false>(A, grid, ctx->stream, ctx->alg_tuned[0][ilog2_bucket(n)]);
+        record_event(ctx);
+    }
+    return st;
+}
+
+int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y, double *z,
+                 double *u, double *v, double *w, const double *q, double *disp)
+{
+    const int st = enqueue_pairs(ctx, cfg, n, x, y, z, u, v, w, q, 0, -1);
+    if (st != BIA_OK) return st;
+    const int nb = num_blocks32(n);
     UpdateArgs U;
     U.x = x; U.y = y; U.z = z; U.u = u; U.v = v; U.w = w;
     U.disp = disp;
@@ -615,37 +659,79 @@ int enqueue_step(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
     U.nb = nb;
     U.npad = nb * 32;
     U.dt = cfg->dt;
-    A.heads = (const MlpImage *)ctx->heads.ptr;
-    const bool learned = cfg->method == BIA_METHOD_LEARNED;
-    bool split = false;
-    if (learned) {
-        const int lt = ctx->learned_tuned[cfg->deterministic ? 1 : 0][ilog2_bucket(n)];
-        split = (lt >= 0) ? (lt == 1 && ctx->lmask.ptr) : learned_split(A.nwb);
-    }
-    if (split) split_buffer_carve(ctx->lmask.ptr, A.nwb, A);
-    if (learned && !ctx->heads_loaded) return BIA_ERR_INVALID_ARGUMENT;
-    int st = BIA_OK;
-    if (cfg->deterministic) {
-        A.part = (double *)ctx->part.ptr;
-        U.part = A.part;
-        U.nparts = nb;
-        record_event(ctx);
-        if (learned) st = launch_pair_learned<true>(A, ctx->stream);
-        else launch_pair_tiles<true>(A, grid, ctx->stream, ctx->alg_tuned[1][ilog2_bucket(n)]);
-        record_event(ctx);
-    } else {
-        A.part = (double *)ctx->acc.ptr;
-        U.part = A.part;
-        U.nparts = 1;
-        cudaMemsetAsync(A.part, 0, 6 * (size_t)A.npad * sizeof(double), ctx->stream);
-        record_event(ctx);
-        if (learned) st = launch_pair_learned<false>(A, ctx->stream);
-        else launch_pair_tiles<false>(A, grid, ctx->stream, ctx->alg_tuned[0][ilog2_bucket(n)]);
-        record_event(ctx);
-    }
-    if (st != BIA_OK) return st;
+    U.part = cfg->deterministic ? (double *)ctx->part.ptr : (double *)ctx->acc.ptr;
+    U.nparts = cfg->deterministic ? nb : 1;
     bia_reduce_update_kernel<<<(n + 31) / 32, kReduceThreads, 0, ctx->stream>>>(U);
     return cuda_status(cudaGetLastError());
+}
+
+// ----------------------------------------------------------------------------------
+// Multi-GPU shards.  Shard s of S owns the warp-blocks of the triangle's columns
+// [c0, c1) (column bj holds bj + 1 blocks; the boundaries split the blocks, so the pairs, as
+// evenly as whole columns allow).  Those blocks are one contiguous range of the linear order
+// t = bj (bj + 1) / 2 + bi, and they write these partial planes of particle p (block b):
+// rows, m = bj for bj in [max(c0, b + 1), c1), and, when b is one of the shard's columns,
+// columns and diagonal, m = 0 .. b.  The shard's reduction sums exactly those planes in
+// ascending m, the order of the whole step's reduction.
+void shard_columns(int nb, int shard, int nshards, int *c0, int *c1)
+{
+    const long long all = (long long)nb * (nb + 1) / 2;
+    auto boundary = [&](int r) {
+        if (r <= 0) return 0;
+        if (r >= nshards) return nb;
+        const long long target = (all * r + nshards - 1) / nshards;  // ceil(all r / S) blocks
+        long long c = (long long)((sqrt(8.0 * (double)target + 1.0) - 1.0) * 0.5);
+        while (c > 0 && c * (c + 1) / 2 >= target) c--;
+        while (c * (c + 1) / 2 < target) c++;
+        return (int)(c < nb ? c : nb);
+    };
+    *c0 = boundary(shard);
+    *c1 = boundary(shard + 1);
+}
+
+struct ShardReduceArgs {
+    const double *part;
+    double *out;  // [6][n]
+    int n, npad, nparts, c0, c1;
+};
+
+// out[c][p] = the shard's partial planes of particle p summed in ascending plane order
+// (deterministic), or the atomic accumulator (nparts = 1): one warp per component per 32
+// particles, as bia_reduce_update_kernel.
+__global__ void __launch_bounds__(kReduceThreads) bia_shard_reduce_kernel(const ShardReduceArgs A)
+{
+    const int lane = threadIdx.x & 31;
+    const int c = threadIdx.x >> 5;
+    const int p = blockIdx.x * 32 + lane;
+    if (p >= A.n) return;
+    const size_t plane = (size_t)A.npad;
+    const double *src = A.part + (size_t)c * plane + p;
+    const size_t step = 6 * plane;
+    double sum = 0.0;
+    if (A.nparts == 1) {
+        sum = src[0];
+    } else {
+        const int b = p / 32;
+        if (b >= A.c0 && b < A.c1)
+            for (int m = 0; m <= b; m++) sum += src[(size_t)m * step];
+        for (int m = max(A.c0, b + 1); m < A.c1; m++) sum += src[(size_t)m * step];
+    }
+    A.out[(size_t)c * A.n + p] = sum;
+}
+
+// x += sums[0..2] + u dt, u += sums[3..5] (bia/bia.f90:194-204)
+__global__ void __launch_bounds__(256) bia_apply_update_kernel(int n, double dt, double *x, double *y, double *z,
+                                                                 double *u, double *v, double *w, const double *sums)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const double uu = u[p], vv = v[p], ww = w[p];
+    x[p] = x[p] + (sums[p] + uu * dt);
+    y[p] = y[p] + (sums[(size_t)n + p] + vv * dt);
+    z[p] = z[p] + (sums[2 * (size_t)n + p] + ww * dt);
+    u[p] = uu + sums[3 * (size_t)n + p];
+    v[p] = vv + sums[4 * (size_t)n + p];
+    w[p] = ww + sums[5 * (size_t)n + p];
 }
 
 static void copy_stats(const unsigned long long *h, bia_stats *s)
@@ -1045,6 +1131,56 @@ int bia_run_host(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
     e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return cuda_status(e);
     return st2;
+}
+
+int bia_shard_columns(int n, int shard, int nshards, int *c0, int *c1)
+{
+    if (n < 1 || nshards < 1 || shard < 0 || shard >= nshards || !c0 || !c1) return BIA_ERR_INVALID_ARGUMENT;
+    shard_columns(num_blocks32(n), shard, nshards, c0, c1);
+    return BIA_OK;
+}
+
+int bia_step_shard(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y, double *z, double *u,
+                   double *v, double *w, const double *q, int shard, int nshards, double *sums, bia_stats *stats)
+{
+    if (!ctx || !sums || nshards < 1 || shard < 0 || shard >= nshards) return BIA_ERR_INVALID_ARGUMENT;
+    int st = validate(cfg, n, x, y, z, u, v, w, ctx);
+    if (st != BIA_OK) return st;
+    cudaSetDevice(ctx->device);
+    st = ensure_step_buffers(ctx, cfg, n);
+    if (st != BIA_OK) return st;
+    if (stats) {
+        cudaError_t e = cudaMemsetAsync(ctx->stats.ptr, 0, kNumStats * sizeof(unsigned long long), ctx->stream);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    const int nb = num_blocks32(n);
+    int c0 = 0, c1 = 0;
+    shard_columns(nb, shard, nshards, &c0, &c1);
+    const long long t0 = (long long)c0 * (c0 + 1) / 2, t1 = (long long)c1 * (c1 + 1) / 2;
+    st = enqueue_pairs(ctx, cfg, n, x, y, z, u, v, w, q, t0, t1 - t0);
+    if (st != BIA_OK) return st;
+    ShardReduceArgs R;
+    R.part = cfg->deterministic ? (const double *)ctx->part.ptr : (const double *)ctx->acc.ptr;
+    R.out = sums;
+    R.n = n;
+    R.npad = nb * 32;
+    R.nparts = cfg->deterministic ? nb : 1;
+    R.c0 = c0;
+    R.c1 = c1;
+    bia_shard_reduce_kernel<<<(n + 31) / 32, kReduceThreads, 0, ctx->stream>>>(R);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e);
+    if (stats) return fetch_stats(ctx, stats);
+    return BIA_OK;
+}
+
+int bia_apply_update(bia_context *ctx, int n, double dt, double *x, double *y, double *z, double *u, double *v,
+                     double *w, const double *sums)
+{
+    if (!ctx || n < 1 || !x || !y || !z || !u || !v || !w || !sums) return BIA_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    bia_apply_update_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, dt, x, y, z, u, v, w, sums);
+    return cuda_status(cudaGetLastError());
 }
 
 }  // extern "C"

@@ -155,6 +155,23 @@ int bia_run_host(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
                  double *z, double *u, double *v, double *w, const double *q, int nsteps,
                  bia_stats *stats);
 
+/* Multi-GPU step by shards (the path's exchange is the per-particle sum: one FP64
+   all-reduce of 6n per step).  Shard `shard` of `nshards` owns the pairs (i, j), i < j, whose
+   j lies in columns [c0, c1) of 32-particle blocks; bia_shard_columns gives them (about
+   equal pair counts; no GPU needed).  bia_step_shard solves the shard's pairs on the context's
+   device and writes their sums into the device array sums[6][n] (dX..dW without drift, the
+   state unchanged); the caller adds the shards' sums across GPUs (an NCCL all-reduce) and
+   then calls bia_apply_update, which adds the drift and updates the state
+   (bia/bia.f90:194-204).  The shards of one step partition its pairs, so their sums add up to
+   the whole step's (deterministic mode: the same planes in the same order per shard).  No
+   counterpart in the reference, which runs on one GPU. */
+int bia_shard_columns(int n, int shard, int nshards, int *c0, int *c1);
+int bia_step_shard(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y, double *z,
+                   double *u, double *v, double *w, const double *q, int shard, int nshards,
+                   double *sums, bia_stats *stats);
+int bia_apply_update(bia_context *ctx, int n, double dt, double *x, double *y, double *z, double *u,
+                     double *v, double *w, const double *sums);
+
 /* Allocation-free form of bia_step, for callers that cannot allocate device memory once
    they run (a framework that owns the GPU's memory pool, a real-time loop that must not
    enter the CUDA allocator).  No counterpart in the reference.  The step's scratch is a
@@ -201,6 +218,18 @@ long long bia_ensemble_particles(const bia_ensemble *ens);
 int bia_ensemble_run(bia_context *ctx, bia_ensemble *ens, const bia_config *cfg, double *x,
                      double *y, double *z, double *u, double *v, double *w, const double *q,
                      int nsteps, int use_graph, bia_stats *stats);
+/* Autotuner of the ensemble's pair-kernel launch shape for cfg->method, timed on these
+   systems (1 warm-up and 3 timed launches per shape; only scratch is written, the state is
+   unchanged); the fastest is kept in the ensemble and used by later runs.  Shapes: ALG 0 =
+   8-warp CTAs, 1 = phase-locked 16-warp CTAs (2 per SM), 2 = phase-locked 32-warp CTAs
+   (1 per SM); universal variables 0 = one item per warp, 1 = a persistent grid (2 CTAs per
+   SM); learned 0 / 1 = the persistent list kernel at 1 / 2 CTAs per SM.  Every shape gives
+   bitwise the same results.  variant (optional): the choice (-1 for RKF, one shape); ms
+   (optional, 3 floats): each shape's best time (-1 when not run).  Synchronises the
+   context's stream; not during stream capture.  No counterpart in the reference. */
+int bia_ensemble_autotune(bia_context *ctx, bia_ensemble *ens, const bia_config *cfg, double *x,
+                          double *y, double *z, double *u, double *v, double *w, const double *q,
+                          int *variant, float *ms);
 /* per-system KE and PE (energy[2 s] = sum |v|^2, energy[2 s + 1] = eps_s sum (q_i q_j)/r_ij),
    host array of 2 nsys doubles; synchronises */
 int bia_ensemble_energy(bia_context *ctx, bia_ensemble *ens, const double *x, const double *y,

@@ -127,3 +127,32 @@ def test_ensemble_learned_equals_single_system_steps(cuda):
             assert np.abs(got[:3, off:off + n] - r[:3]).max() <= 1e-12 * scale, n
             off += n
         ens.close()
+
+
+@pytest.mark.parametrize("method", [1, METHOD_UNIVERSAL, 3])
+def test_ensemble_autotune_keeps_results_bitwise(cuda, method):
+    """The ensemble autotuner times each launch shape of the method's pair kernels on the
+    caller's systems without changing the state, keeps the fastest, and a run with the tuned
+    shape is bitwise equal to the untuned run (every shape runs the same per-item
+    arithmetic)."""
+    from bia_3d_gpu_b200 import initial as ini
+    sizes = np.random.default_rng(70).integers(32, 400, 40)
+    states = [ini.plummer(int(n), seed=700 + k)[0] for k, n in enumerate(sizes)]
+    eps = -2.0 / sizes.astype(np.float64)
+    host = np.concatenate(states, axis=1)
+    cfg = default_config(dt=1e-3, method=method)
+    outs = []
+    with BIASolver() as solver:
+        solver.load_heads()
+        for tuned in (False, True):
+            ens = solver.ensemble(sizes, eps)
+            whole = cuda.tensor(host, device="cuda")
+            if tuned:
+                shape, ms = ens.autotune(whole, cfg)
+                assert shape in ens.SHAPES[method] and set(ms) == set(ens.SHAPES[method])
+                assert np.array_equal(whole.cpu().numpy(), host)
+            ens.run(whole, cfg, 3, graph=True, stats=False)
+            solver.stream.synchronize()
+            outs.append(whole.cpu().numpy())
+            ens.close()
+    assert np.array_equal(outs[0], outs[1])
