@@ -452,7 +452,7 @@ class Ensemble:
         return s._finish(st, st_, "bia_ensemble_run")
 
     SHAPES = {1: ("tiles8", "phase16", "phase32"), 2: ("item_per_warp", "persistent"),
-              3: ("list_1_cta_per_sm", "list_2_ctas_per_sm")}
+              3: ("head_1_cta_per_sm", "head_2_ctas_per_sm")}
 
     def autotune(self, state, cfg, q=None):
         """Time the launch shapes of cfg.method's pair kernels on these systems and keep the

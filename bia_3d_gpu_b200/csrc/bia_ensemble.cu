@@ -34,9 +34,10 @@ struct bia_ensemble {
     double *d_part = nullptr;          // partial sums
     double *d_scratch = nullptr;       // [nitems + nparticles] energy scratch
     double *d_energy = nullptr;        // [2 nsys] KE, PE per system
-    // learned step: per-bin list lengths, the bins' lists of items holding learned pairs, 32
-    // pair masks per item
-    unsigned int *d_split = nullptr;   // [16 + kEnsBins nitems + 32 nitems]
+    // learned step: the deferred pairs' rows and the list of items holding them
+    // (bia_learned_block.cuh), one buffer
+    uint8_t *d_split = nullptr;
+    unsigned int rows_cap = 0;
     size_t part_doubles = 0;
     // launch shape chosen by bia_ensemble_autotune per method (index BIA_METHOD_*), -1: the
     // built-in rule
@@ -50,9 +51,6 @@ namespace bia {
 
 constexpr int kEnsWarps = 8;
 constexpr int kEnsThreads = kEnsWarps * 32;
-// the learned step lists its items in bins of floor(log2(learned pairs of the item)), so
-// that the eight items a CTA of the list kernel takes at a time carry similar work
-constexpr int kEnsBins = 11;
 
 struct EnsArgs {
     const double *x, *y, *z, *u, *v, *w, *q;
@@ -65,8 +63,7 @@ struct EnsArgs {
     unsigned long long *stats;
     PairParams P;
     const MlpImage *heads;  // BIA_METHOD_LEARNED
-    unsigned int *wbcount, *wblist;  // learned step: kEnsBins list lengths, lists (nitems each)
-    uint32_t *lmask;                 // and the pair masks of every item
+    LearnedRows R;          // learned step: the deferred pairs' rows and the listed items
 };
 
 // Each warp takes items t = (its global warp index) + k * (warps in the grid), as
@@ -104,13 +101,18 @@ __global__ void __launch_bounds__(kEnsThreads, TileOccupancy<M>::kMinBlocks) ens
 }
 
 // Phase-locked ALG variant of ens_pair_tiles_kernel (see phase_block_solve): CTAs of kW
-// warps, kMinB of them per SM, each warp on one item; bitwise the same results.
+// warps, kMinB of them per SM, each warp on one item, the counters flushed once per CTA as in
+// bia_pair_phase_kernel; bitwise the same results.
 template <int kW, int kMinB>
 __global__ void __launch_bounds__(kW * 32, kMinB) ens_pair_phase_kernel(const EnsArgs A)
 {
     extern __shared__ double phase_smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
+    unsigned long long *slots = reinterpret_cast<unsigned long long *>(phase_smem + kW * kTileSmemDoubles);
+    unsigned long long *wtot = slots + warp * kNumStats;
+    if (lane < kNumStats) wtot[lane] = 0ull;
+    __syncwarp();
     const long long t = (long long)blockIdx.x * kW + warp;
     const bool live = t < A.nitems;
     int s = 0, bi = 0, bj = 0;
@@ -127,10 +129,13 @@ __global__ void __launch_bounds__(kW * 32, kMinB) ens_pair_phase_kernel(const En
     PairCounters cnt;
     phase_block_solve(A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base, q, n, A.eps[s],
                       A.P, bi, bj, lane, live, phase_smem + warp * kTileSmemDoubles, racc, cacc, cnt);
-    if (!live) return;  // warp-uniform; no barrier follows
-    flush_counters(cnt, A.stats, lane);
-    const int nb = (n + 31) / 32;
-    write_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
+    if (live) {  // warp-uniform
+        counters_to_slot(cnt, wtot, lane);
+        const int nb = (n + 31) / 32;
+        write_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
+    }
+    __syncthreads();
+    if (warp == 0) flush_slots(slots, kW, A.stats, lane);
 }
 
 // Once per device (the current one): dynamic shared memory opt-in of the phase-locked
@@ -148,9 +153,9 @@ static int ens_phase_setup()
         int sms = 0;
         bool ok = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess;
         ok = ok && cudaFuncSetAttribute(ens_pair_phase_kernel<32, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        32 * kTileSmemDoubles * (int)sizeof(double)) == cudaSuccess;
+                                        32 * (kTileSmemDoubles + kNumStats) * (int)sizeof(double)) == cudaSuccess;
         ok = ok && cudaFuncSetAttribute(ens_pair_phase_kernel<16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        16 * kTileSmemDoubles * (int)sizeof(double)) == cudaSuccess;
+                                        16 * (kTileSmemDoubles + kNumStats) * (int)sizeof(double)) == cudaSuccess;
         if (!ok) cudaGetLastError();
         sms_of[dev] = ok ? sms : 0;
         done_of[dev] = true;
@@ -158,17 +163,22 @@ static int ens_phase_setup()
     return sms_of[dev];
 }
 
-// Learned step over the item table, first kernel: each item's plain pairs
-// (rest_block_solve, as bia_pair_rest_kernel); items holding pairs in the heads' domain are
-// listed with their masks for ens_pair_learned_list_kernel.
+// Learned step over the item table, first kernel: each item's pairs except the deferred ones
+// (rest_block_solve, rest_block_defer, as bia_pair_rest_kernel), the items holding deferred
+// pairs listed with their rows; the head kernel of the single-system step then evaluates the
+// rows and ens_pair_learned_finish_kernel solves the listed items' deferred pairs.
 __global__ void __launch_bounds__(kEnsThreads, 2) ens_pair_rest_kernel(const EnsArgs A)
 {
-    const unsigned full = 0xffffffffu;
+    extern __shared__ __align__(16) uint8_t ens_rest_smem[];
     const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    double *ws = reinterpret_cast<double *>(ens_rest_smem + warp * kRestWarpBytes);
+    uint32_t *wslots = reinterpret_cast<uint32_t *>(ens_rest_smem + warp * kRestWarpBytes +
+                                                    kTileSmemDoubles * sizeof(double));
     PairCounters tot;
     counters_zero(tot);
     int nblk = 0;
-    for (long long t = (long long)blockIdx.x * kEnsWarps + (threadIdx.x >> 5); t < A.nitems;
+    for (long long t = (long long)blockIdx.x * kEnsWarps + warp; t < A.nitems;
          t += (long long)gridDim.x * kEnsWarps) {  // warp-uniform
         const uint2 it = A.items[t];
         const int s = (int)it.x;
@@ -176,10 +186,11 @@ __global__ void __launch_bounds__(kEnsThreads, 2) ens_pair_rest_kernel(const Ens
         const int base = A.off[s];
         const int n = A.off[s + 1] - base;
         double racc[6], cacc[6];
+        uint32_t mask[kMlpHeads];
         PairCounters cnt;
-        const uint32_t learned = rest_block_solve(A.x + base, A.y + base, A.z + base, A.u + base, A.v + base,
-                                                  A.w + base, A.q ? A.q + base : nullptr, n, A.eps[s], A.P.dt,
-                                                  bi, bj, lane, racc, cacc, cnt);
+        rest_block_solve(A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base,
+                         A.q ? A.q + base : nullptr, n, A.eps[s], A.P.dt, bi, bj, lane, ws, wslots, racc, cacc,
+                         mask, cnt);
         counters_add(tot, cnt);
         if (++nblk == kFlushBlocks) {
             flush_counters(tot, A.stats, lane);
@@ -188,91 +199,66 @@ __global__ void __launch_bounds__(kEnsThreads, 2) ens_pair_rest_kernel(const Ens
         }
         const int nb = (n + 31) / 32;
         write_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
-        const unsigned total = __reduce_add_sync(full, (unsigned)__popc(learned));
-        if (total != 0u) {
-            const int bin = min(kEnsBins - 1, 31 - __clz((int)total));
-            A.lmask[(size_t)t * 32 + lane] = learned;
-            if (lane == 0) {
-                const unsigned int slot = atomicAdd(&A.wbcount[bin], 1u);
-                A.wblist[(size_t)bin * A.nitems + slot] = (unsigned int)t;
-            }
-        }
+        rest_block_defer(A.R, (unsigned int)t, mask, wslots, lane);
     }
     if (nblk > 0) flush_counters(tot, A.stats, lane);
 }
 
-// Learned step, second kernel: persistent CTAs work through the listed items eight at a
-// time (one per warp, of any systems), the heaviest bin first, solve their masked pairs with
-// the learned warp-block and add the sums onto the rest kernel's partials.
-__global__ void __launch_bounds__(kMlpThreads, 2) ens_pair_learned_list_kernel(const EnsArgs A)
+// Learned step over the item table, third kernel: one warp per listed item (persistent 8-warp
+// CTAs), its deferred pairs from their guesses added onto the rest kernel's partials.
+__global__ void __launch_bounds__(kEnsThreads, 2) ens_pair_learned_finish_kernel(const EnsArgs A)
 {
-    extern __shared__ uint8_t ens_list_raw[];
-    const LearnedSmem M = learned_smem(ens_list_raw);
+    __shared__ double s_fin[kTileWarps][kTileSmemDoubles];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    mlp_setup(*M.mlp);
-    uint32_t phase = 0;
-    for (int bin = kEnsBins - 1; bin >= 0; bin--) {
-        const long long count = (long long)A.wbcount[bin];
-        const unsigned int *list = A.wblist + (size_t)bin * A.nitems;
-        for (long long g0 = (long long)blockIdx.x * kLearnedWarps; g0 < count;
-             g0 += (long long)gridDim.x * kLearnedWarps) {
-            const long long e = g0 + warp;
-            const bool live = e < count;
-            int s = 0, bi = 0, bj = 0;
-            uint32_t mask = 0u;
-            if (live) {
-                const unsigned int item = list[e];
-                const uint2 it = A.items[item];
-                s = (int)it.x;
-                bi = (int)(it.y & 0xffffu);
-                bj = (int)(it.y >> 16);
-                mask = A.lmask[(size_t)item * 32 + lane];
-            }
-            const int base = A.off[s];
-            const int n = A.off[s + 1] - base;
-            const LearnedBlockIn B = {A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base,
-                                      A.q ? A.q + base : nullptr, n, A.eps[s], A.P.dt, A.heads};
-            double racc[6], cacc[6];
-            PairCounters cnt;
-            const bool timed_out = learned_block_solve(M, B, bi, bj, lane, live, racc, cacc, cnt, phase, &mask);
-            if (timed_out && threadIdx.x == 0 && !live) atomicAdd(&A.stats[kStatTimeouts], 1ull);
-            if (live) {
-                flush_counters(cnt, A.stats, lane);
-                const int nb = (n + 31) / 32;
-                add_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
-            }
+    const long long count = (long long)*A.R.nlist;
+    PairCounters tot;
+    counters_zero(tot);
+    int nblk = 0;
+    for (long long e = (long long)blockIdx.x * kEnsWarps + warp; e < count;
+         e += (long long)gridDim.x * kEnsWarps) {  // warp-uniform
+        const uint2 it = A.items[A.R.entries[e].x];
+        const int s = (int)it.x;
+        const int bi = (int)(it.y & 0xffffu), bj = (int)(it.y >> 16);
+        const int base = A.off[s];
+        const int n = A.off[s + 1] - base;
+        const LearnedBlockIn B = {A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base,
+                                  A.q ? A.q + base : nullptr, n, A.eps[s], A.P.dt, A.heads};
+        double racc[6], cacc[6];
+        PairCounters cnt;
+        finish_block_solve(A.R, e, B, bi, bj, lane, s_fin[warp], racc, cacc, cnt);
+        counters_add(tot, cnt);
+        if (++nblk == kFlushBlocks) {
+            flush_counters(tot, A.stats, lane);
+            counters_zero(tot);
+            nblk = 0;
         }
+        const int nb = (n + 31) / 32;
+        add_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
     }
-    mlp_teardown(*M.mlp, phase);
+    if (nblk > 0) flush_counters(tot, A.stats, lane);
 }
 
-// Once per device: shared-memory opt-in of the learned ensemble kernels; returns the grid of
-// the persistent list kernel (resident CTAs, at least two per SM), 0 on failure.
+// Once per device: shared-memory opt-in of the ensemble's rest kernel (the head kernel is the
+// single-system step's, set up by bia_learned_head_grid); returns the head kernel's grid
+// (resident CTAs), 0 on failure.
 static int ens_learned_setup()
 {
     constexpr int kMaxDevices = 64;
     static std::mutex mu;
-    static int grid_of[kMaxDevices] = {};
     static bool done_of[kMaxDevices] = {};
+    static bool ok_of[kMaxDevices] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 0;
+    const int hgrid = learned_head_grid();
     std::lock_guard<std::mutex> lk(mu);
     if (!done_of[dev]) {
-        const int bytes = (int)kLearnedSmemBytes;
-        int sms = 0, occ = 0;
-        bool ok = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess;
-        ok = ok && cudaFuncSetAttribute(ens_pair_learned_list_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        bytes) == cudaSuccess;
-        ok = ok && cudaFuncSetAttribute(ens_pair_learned_list_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                        (int)cudaSharedmemCarveoutMaxShared) == cudaSuccess;
-        ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ens_pair_learned_list_kernel, kMlpThreads,
-                                                                 (size_t)bytes) == cudaSuccess;
-        if (!ok) cudaGetLastError();
-        grid_of[dev] = ok ? sms * (occ > 2 ? occ : 2) : 0;
+        ok_of[dev] = cudaFuncSetAttribute(ens_pair_rest_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)kRestSmemBytes) == cudaSuccess;
+        if (!ok_of[dev]) cudaGetLastError();
         done_of[dev] = true;
     }
-    return grid_of[dev];
+    return ok_of[dev] ? hgrid : 0;
 }
 
 struct EnsUpdateArgs {
@@ -379,7 +365,7 @@ __global__ void __launch_bounds__(256) ens_energy_kernel(const double *u, const 
 //                2: phase-locked 32-warp CTAs (1 per SM); built-in rule: 2 from two of its CTAs
 //                per SM up, else 0
 //   universal    0: one item per warp, 1: a persistent grid of 2 CTAs per SM (built-in)
-//   learned      the persistent list kernel with 0: 1 CTA per SM, 1: 2 CTAs per SM (built-in)
+//   learned      the persistent head kernel with 0: 1 CTA per SM, 1: 2 CTAs per SM (built-in)
 // Every shape runs the same per-item arithmetic in the same order: the results are bitwise
 // the same.
 constexpr int kEnsShapes = 3;
@@ -389,22 +375,28 @@ static int ens_pair_launch(bia_context *ctx, bia_ensemble *E, EnsArgs &A, int me
     const unsigned grid = (unsigned)((E->nitems + kEnsWarps - 1) / kEnsWarps);
     cudaStream_t st = ctx->stream;
     if (method == BIA_METHOD_LEARNED) {
-        // the split step of bia_step: the rest kernel, then the list kernel (the same
+        // the split step of bia_step: the rest, head and finish kernels (the same
         // per-warp-block arithmetic, so each system equals its own learned bia_step)
         const int lsetup = ens_learned_setup();
         if (!ctx->heads_loaded) return BIA_ERR_INVALID_ARGUMENT;
         if (lsetup <= 0) return BIA_ERR_CUDA;
-        A.wbcount = E->d_split;
-        A.wblist = E->d_split + 16;
-        A.lmask = E->d_split + 16 + (size_t)kEnsBins * E->nitems;
-        cudaError_t e = cudaMemsetAsync(A.wbcount, 0, kEnsBins * sizeof(unsigned int), st);
+        uint8_t *b = E->d_split;
+        A.R.counts = (unsigned long long *)b;
+        A.R.nlist = (unsigned int *)(b + 16);
+        A.R.entries = (uint4 *)(b + kSplitHeader);
+        A.R.masks = (uint32_t *)(b + kSplitHeader + (size_t)E->nitems * 16);
+        uint32_t *rows = (uint32_t *)(b + kSplitHeader + (size_t)E->nitems * (16 + 64 * sizeof(uint32_t)));
+        A.R.rows_cap = E->rows_cap;
+        A.R.rows[kHeadEll] = rows;
+        A.R.rows[kHeadHyp] = rows + E->rows_cap;
+        cudaError_t e = cudaMemsetAsync(A.R.counts, 0, kSplitHeader, st);
         if (e != cudaSuccess) return cuda_status(e);
-        ens_pair_rest_kernel<<<(unsigned)persistent_grid(grid), kEnsThreads, 0, st>>>(A);
-        const long long need = (E->nitems + kLearnedWarps - 1) / kLearnedWarps;
-        long long cap = lsetup;
-        if (shape == 0 || shape == 1) cap = (long long)device_sm_count() * (shape + 1);
-        const unsigned lgrid = (unsigned)(need < cap ? need : cap);
-        ens_pair_learned_list_kernel<<<lgrid, kMlpThreads, kLearnedSmemBytes, st>>>(A);
+        const unsigned rgrid = (unsigned)persistent_grid(grid);
+        ens_pair_rest_kernel<<<rgrid, kEnsThreads, kRestSmemBytes, st>>>(A);
+        long long hcap = lsetup;
+        if (shape == 0 || shape == 1) hcap = (long long)device_sm_count() * (shape + 1);
+        launch_learned_head(A.R, A.heads, A.stats, (int)hcap, st);
+        ens_pair_learned_finish_kernel<<<rgrid, kEnsThreads, 0, st>>>(A);
         return cuda_status(cudaGetLastError());
     }
     switch (method) {
@@ -420,10 +412,10 @@ static int ens_pair_launch(bia_context *ctx, bia_ensemble *E, EnsArgs &A, int me
         if (sms <= 0) var = 0;
         if (var == 2) {
             ens_pair_phase_kernel<32, 1><<<(unsigned)((E->nitems + 31) / 32), 32 * 32,
-                                            32 * kTileSmemDoubles * sizeof(double), st>>>(A);
+                                            32 * (kTileSmemDoubles + kNumStats) * sizeof(double), st>>>(A);
         } else if (var == 1) {
             ens_pair_phase_kernel<16, 2><<<(unsigned)((E->nitems + 15) / 16), 16 * 32,
-                                            16 * kTileSmemDoubles * sizeof(double), st>>>(A);
+                                            16 * (kTileSmemDoubles + kNumStats) * sizeof(double), st>>>(A);
         } else {
             ens_pair_tiles_kernel<kMethodAlg><<<grid, kEnsThreads, 0, st>>>(A);
         }
@@ -534,7 +526,14 @@ extern "C" int bia_ensemble_create(bia_context *ctx, int nsys, const int *sizes,
     ENS_ALLOC(E->d_part, part);
     ENS_ALLOC(E->d_scratch, nitems);
     ENS_ALLOC(E->d_energy, 2 * nsys);
-    ENS_ALLOC(E->d_split, 16 + (kEnsBins + 32) * nitems);
+    {
+        // rows: up to every pair of the ensemble per head, capped as in the single-system step
+        unsigned long long pairs = 0;
+        for (int s2 = 0; s2 < nsys; s2++) pairs += (unsigned long long)sizes[s2] * (sizes[s2] - 1) / 2;
+        E->rows_cap = (unsigned int)(pairs < (1ull << 27) ? (pairs > 0 ? pairs : 1) : (1ull << 27));
+        ENS_ALLOC(E->d_split, kSplitHeader + (size_t)nitems * (16 + 64 * sizeof(uint32_t)) +
+                                  (size_t)kMlpHeads * E->rows_cap * sizeof(uint32_t));
+    }
 #undef ENS_ALLOC
     if (e == cudaSuccess) e = cudaMemcpy(E->d_off, off.data(), sizeof(int) * (nsys + 1), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(E->d_psys, psys.data(), sizeof(int) * np, cudaMemcpyHostToDevice);

@@ -67,30 +67,59 @@ __device__ __forceinline__ void cta_scan2(MlpSmem &S, int a, int b, int &oa, int
 }
 
 
-// The split learned step's plain part of warp-block (bi, bj) of the system x..w[0, n)
-// (charges q, coupling eps_th): lanes walk the rotation offsets; every pair gets the
-// universal-variable prepare and the fifth-order start (uv_start_fast).  A pair whose start
-// is already exact needs no iteration and is composed here.  Of the others, those inside a
-// head's domain (learned_filter) are left to the learned warp-block, where the head's guess
-// replaces the Newton iterations; the rest run the plain Newton iteration here.  Returns the
-// lane's mask of left pairs (bit k: column (lane + k) mod 32) with the row sums racc and
-// column sums cacc of the solved ones.  The pairs are counted as universal-variable pairs,
-// degenerate ones included, as BIA_METHOD_UNIVERSAL counts them (the exact degenerate test
-// costs 7 % here).
-__device__ __forceinline__ uint32_t rest_block_solve(const double *x, const double *y, const double *z,
-                                                     const double *u, const double *v, const double *w,
-                                                     const double *q, int n, double eps_th, double dt, int bi,
-                                                     int bj, int lane, double racc[6], double cacc[6],
-                                                     PairCounters &cnt)
+// The split learned step in three kernels, shared by the single-system step and the ensemble:
+//  rest    every pair gets the universal-variable prepare and the fifth-order start; a pair
+//          whose start is exact is composed right there.  A pair whose start is not exact and
+//          that lies inside a head's domain (learned_filter, then learned_prepare) is deferred:
+//          its head input goes to the warp's row slot (lane, k) in shared memory.  The other
+//          non-exact pairs run the safeguarded Newton iteration.  After the walk the warp
+//          allocates rows for its deferred pairs in the global row buffer of each head (one
+//          atomic per head and warp-block), writes their inputs there (per lane in ascending
+//          k, lanes in order) and lists the warp-block with its row bases and pair masks.
+//  head    the rows of each head in full 256-row tiles on the tensor cores (mlp_tc.cuh), each
+//          row's guess written over its input.
+//  finish  one warp per listed warp-block: its deferred pairs from their guesses (FP32
+//          correction, FP64 Halley step, composition; the plain solver where the FP64 step
+//          does not settle), their sums added onto the rest kernel's partials.
+// A pair's row holds only that pair's input and guess, and every partial slot is written by
+// the rest kernel and added to by at most one listed warp-block, so neither the order of the
+// rows nor that of the list changes the results.  The rows of a head are capped (rows_cap);
+// a warp-block whose rows do not fit is listed without rows and the finish kernel solves its
+// pairs with the plain solver: only then do the results depend on the order in which
+// warp-blocks took rows.
+struct LearnedRows {
+    uint32_t *rows[kMlpHeads];   // per head (kHeadEll, kHeadHyp): packed BF16 inputs, then FP32 guesses
+    unsigned long long *counts;  // [kMlpHeads] rows taken this step (may run past rows_cap)
+    unsigned int *nlist;         // listed warp-blocks
+    uint4 *entries;              // per listed warp-block: (item, row base ell, row base hyp, 0)
+    uint32_t *masks;             // per listed warp-block: [kMlpHeads][32] lane masks
+    unsigned int rows_cap;
+};
+constexpr unsigned int kNoRows = 0xffffffffu;
+// the buffer's header: the two row counts (u64) and the list length (u32), 32 bytes
+constexpr size_t kSplitHeader = 32;
+
+// Shared memory of a rest-kernel warp: its column slice (kTileSmemDoubles doubles) and 1024
+// row slots (slot lane * 32 + k: the packed head input of the lane's pair at offset k).
+constexpr size_t kRestWarpBytes = kTileSmemDoubles * sizeof(double) + 1024 * sizeof(uint32_t);
+constexpr size_t kRestSmemBytes = kTileWarps * kRestWarpBytes;
+
+// The rest kernel's walk over warp-block (bi, bj) of the system x..w[0, n) (charges q,
+// coupling eps_th), with the column states and sums in the warp's slice ws and the row slots
+// wslots.  Returns the row sums racc, column sums cacc of the pairs solved here, and the
+// lane's masks of deferred pairs per head (bit k: column (lane + k) mod 32).  The pairs
+// solved here are counted as universal-variable pairs, degenerate ones included, as
+// BIA_METHOD_UNIVERSAL counts them.
+__device__ __forceinline__ void rest_block_solve(const double *x, const double *y, const double *z,
+                                                 const double *u, const double *v, const double *w,
+                                                 const double *q, int n, double eps_th, double dt, int bi, int bj,
+                                                 int lane, double *ws, uint32_t *wslots, double racc[6],
+                                                 double cacc[6], uint32_t mask[kMlpHeads], PairCounters &cnt)
 {
-    // column states and sums in the warp's shared slice (as warp_block_solve_uv: slot
-    // (lane + k) mod 32 takes its pairs in ascending k)
-    __shared__ double s_rest[kTileWarps][kTileSmemDoubles];
-    double *ws = s_rest[(threadIdx.x >> 5) % kTileWarps];
     double *wacc = ws + 7 * 32;
     const int i = bi * 32 + lane;
     const bool diag = (bi == bj);
-    uint32_t learned = 0u;
+    mask[kHeadEll] = mask[kHeadHyp] = 0u;
     double si[7];
     {
         double sj[7];
@@ -118,9 +147,17 @@ __device__ __forceinline__ uint32_t rest_block_solve(const double *x, const doub
             if (dt != 0.0) {
                 bool exact;
                 double s = uv_start_fast(p, dt, exact);
+                int kind = kLearnedPlain;
                 if (!exact && learned_filter(p, dt)) {
-                    learned |= 1u << k;
-                } else {
+                    LearnedPair L;
+                    learned_prepare(eps_ij, dt, r, g, L);
+                    kind = L.kind;
+                    if (kind != kLearnedPlain) {
+                        mask[kind == kLearnedHyp ? kHeadHyp : kHeadEll] |= 1u << k;
+                        wslots[lane * 32 + k] = pack_bf16(L.x0, L.x1);
+                    }
+                }
+                if (kind == kLearnedPlain) {
                     double ifp = 0.0;
                     const int it = exact ? 0 : uv_iterate(p, dt, s, &ifp);
                     uv_compose<true>(p, s, r, g, h, exact ? p.ir0 : ifp);
@@ -143,7 +180,57 @@ __device__ __forceinline__ uint32_t rest_block_solve(const double *x, const doub
 #pragma unroll
     for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
     __syncwarp();  // the slice is reused by this warp's next block
-    return learned;
+}
+
+// After rest_block_solve: rows for the warp-block's deferred pairs and its list entry (item:
+// the warp-block's index for the finish kernel).  Every lane of the warp calls it.
+__device__ __forceinline__ void rest_block_defer(const LearnedRows &R, unsigned int item,
+                                                 const uint32_t mask[kMlpHeads], const uint32_t *wslots, int lane)
+{
+    const unsigned full = 0xffffffffu;
+    unsigned int base[kMlpHeads], pre[kMlpHeads], tot[kMlpHeads];
+#pragma unroll
+    for (int hd = 0; hd < kMlpHeads; hd++) {
+        // exclusive prefix of the lanes' counts
+        const unsigned c = (unsigned)__popc(mask[hd]);
+        unsigned inc = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned o = __shfl_up_sync(full, inc, d);
+            if (lane >= d) inc += o;
+        }
+        pre[hd] = inc - c;
+        tot[hd] = __shfl_sync(full, inc, 31);
+    }
+    if (tot[kHeadEll] + tot[kHeadHyp] == 0u) return;  // warp-uniform
+    bool fits = true;
+#pragma unroll
+    for (int hd = 0; hd < kMlpHeads; hd++) {
+        unsigned long long b = 0ull;
+        if (lane == 0 && tot[hd] != 0u) b = atomicAdd(&R.counts[hd], (unsigned long long)tot[hd]);
+        b = __shfl_sync(full, b, 0);
+        if (tot[hd] != 0u && b + tot[hd] > (unsigned long long)R.rows_cap) fits = false;
+        base[hd] = (unsigned int)(b < R.rows_cap ? b : 0ull);
+    }
+    if (fits) {
+#pragma unroll
+        for (int hd = 0; hd < kMlpHeads; hd++) {
+            uint32_t m = mask[hd];
+            unsigned int row = base[hd] + pre[hd];
+            while (m) {
+                const int k = __ffs(m) - 1;
+                m &= m - 1u;
+                R.rows[hd][row++] = wslots[lane * 32 + k];
+            }
+        }
+    }
+    unsigned int e = 0u;
+    if (lane == 0) e = atomicAdd(R.nlist, 1u);
+    e = __shfl_sync(full, e, 0);
+    if (lane == 0)
+        R.entries[e] = make_uint4(item, fits ? base[kHeadEll] : kNoRows, fits ? base[kHeadHyp] : kNoRows, 0u);
+    R.masks[(size_t)e * 64 + lane] = mask[kHeadEll];
+    R.masks[(size_t)e * 64 + 32 + lane] = mask[kHeadHyp];
 }
 
 // The system a warp-block belongs to: particles x..w[0, n) (and charges q), coupling eps_th.
@@ -417,5 +504,135 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
     if (timed_out && threadIdx.x == 0) cnt.timeouts++;
     return timed_out;
 }
+
+// The finish kernel's work on listed warp-block e (item resolved by the caller to the system
+// B and the block (bi, bj)): every deferred pair from its head's guess, with the column
+// states and sums in the warp's slice ws.  Returns the row sums racc and column sums cacc of
+// those pairs only (the caller adds them onto the rest kernel's partials).  Every lane of the
+// warp calls it.
+__device__ __forceinline__ void finish_block_solve(const LearnedRows &R, long long e, const LearnedBlockIn &B,
+                                                   int bi, int bj, int lane, double *ws, double racc[6],
+                                                   double cacc[6], PairCounters &cnt)
+{
+    const unsigned full = 0xffffffffu;
+    double *wacc = ws + 7 * 32;
+    const uint4 ent = R.entries[e];
+    const uint32_t me = R.masks[(size_t)e * 64 + lane], mh = R.masks[(size_t)e * 64 + 32 + lane];
+    double si[7];
+    {
+        double sj[7];
+        load_particle(B.x, B.y, B.z, B.u, B.v, B.w, B.q, B.n, bi * 32 + lane, si);
+        load_particle(B.x, B.y, B.z, B.u, B.v, B.w, B.q, B.n, bj * 32 + lane, sj);
+#pragma unroll
+        for (int c = 0; c < 7; c++) ws[c * 32 + lane] = sj[c];
+#pragma unroll
+        for (int c = 0; c < 6; c++) wacc[c * 32 + lane] = 0.0;
+    }
+    __syncwarp();
+    // the lane's first row of each head: the exclusive prefix of the lanes' counts, as the
+    // rest kernel numbered them
+    unsigned int pre[kMlpHeads];
+#pragma unroll
+    for (int hd = 0; hd < kMlpHeads; hd++) {
+        const unsigned c = (unsigned)__popc(hd == kHeadEll ? me : mh);
+        unsigned inc = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned o = __shfl_up_sync(full, inc, d);
+            if (lane >= d) inc += o;
+        }
+        pre[hd] = inc - c;
+    }
+    const bool have_rows = ent.y != kNoRows;
+#pragma unroll
+    for (int c = 0; c < 6; c++) racc[c] = 0.0;
+    counters_zero(cnt);
+    const bool hq = B.q != nullptr;
+    uint32_t m = mh | me;
+    for (;;) {
+        const bool busy = (m != 0u);
+        const unsigned bm = __ballot_sync(full, busy);
+        if (bm == 0u) break;
+        if (busy) {
+            const int k = __ffs(m) - 1;
+            m &= m - 1u;
+            const bool is_h = (mh >> k) & 1u;
+            const int j = (lane + k) & 31;
+            double r[3], g[3], h[6];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                r[c] = si[c] - ws[c * 32 + j];
+                g[c] = si[3 + c] - ws[(3 + c) * 32 + j];
+            }
+            const double eps_ij = hq ? B.eps_th * si[6] * ws[6 * 32 + j] : B.eps_th;
+            bool done = false;
+            if (have_rows) {
+                const uint32_t below = (1u << k) - 1u;
+                const unsigned int row = is_h ? ent.z + pre[kHeadHyp] + (unsigned)__popc(mh & below)
+                                              : ent.y + pre[kHeadEll] + (unsigned)__popc(me & below);
+                const float yg = __uint_as_float(R.rows[is_h ? kHeadHyp : kHeadEll][row]);
+                LearnedPair L;
+                learned_prepare(eps_ij, B.dt, r, g, L, is_h ? kLearnedHyp : kLearnedEll);
+                bool coarse = true;
+                int fp32_steps = 0;
+                done = learned_finish(L, B.dt, yg, r, g, h, coarse, fp32_steps);
+                cnt.learned++;
+                cnt.learned_fp32 += fp32_steps;
+                if (coarse) cnt.learned_coarse++;
+                if (!done) cnt.learned_fallbacks++;
+            }
+            if (!done) {
+                const int it = uv_halfdisp(eps_ij, B.dt, r, g, h);
+                cnt.it_uv += it;
+                if (it > kUvItMax) cnt.nonconverged++;
+            }
+            cnt.cls[is_h ? kHyperbola : kEllipse]++;
+            count_nonfinite(h, cnt);
+#pragma unroll
+            for (int c = 0; c < 6; c++) racc[c] += h[c];
+            add_column(wacc, j, h, bm, lane);
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
+    __syncwarp();  // the slice is reused by this warp's next block
+}
+
+// The head kernel's pass over the rows of head hd (every thread of the CTA calls it, between
+// mlp_setup and mlp_teardown): 256-row tiles t = blockIdx.x + k gridDim.x of the rows taken
+// (up to rows_cap), each guess written over its row.  Returns false when the tensor-core
+// pipeline timed out (the remaining rows keep their inputs; the step reports the timeout).
+__device__ __forceinline__ bool head_rows_pass(MlpSmem &S, const LearnedRows &R, const MlpImage *heads, int hd,
+                                               uint32_t &phase)
+{
+    const unsigned long long taken = *(volatile unsigned long long *)&R.counts[hd];
+    const unsigned int nrows = taken < R.rows_cap ? (unsigned int)taken : R.rows_cap;
+    const unsigned int ntiles = (nrows + kMlpThreads - 1) / kMlpThreads;
+    if ((unsigned int)blockIdx.x >= ntiles) return true;  // CTA-uniform
+    if (S.head != hd) {
+        __syncthreads();  // every thread has read S.head
+        mlp_load_head(S, heads, hd);
+    }
+    bool ok_all = true;
+    for (unsigned int t = blockIdx.x; t < ntiles && ok_all; t += gridDim.x) {
+        const unsigned int row = t * kMlpThreads + threadIdx.x;
+        const bool valid = row < nrows;
+        const uint32_t x01 = valid ? R.rows[hd][row] : 0u;
+        bool ok;
+        const float y = mlp_eval_cta(S, x01, phase, ok);
+        if (!ok) ok_all = false;
+        if (valid) R.rows[hd][row] = __float_as_uint(ok ? y : __int_as_float(0x7fc00000));
+        ok_all = __syncthreads_and(ok_all ? 1 : 0) != 0;
+    }
+    return ok_all;
+}
+
+// The head kernel of the split learned step (bia_step.cu), shared with the ensemble: its
+// once-per-device set-up (returns the resident grid, 0 on failure) and its launch over the
+// rows of R with `grid` CTAs.
+int learned_head_grid();
+void launch_learned_head(const LearnedRows &R, const MlpImage *heads, unsigned long long *stats, int grid,
+                         cudaStream_t st);
 
 }  // namespace bia

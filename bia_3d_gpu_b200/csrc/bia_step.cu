@@ -51,11 +51,10 @@ struct StepArgs {
     double eps_th;
     PairParams P;
     const MlpImage *heads;  // BIA_METHOD_LEARNED
-    // split learned step: the rest kernel's pair masks (32 words per listed warp-block),
-    // the list of warp-blocks with masked pairs and its length
-    uint32_t *lmask;
-    unsigned int *wblist;
-    unsigned int *wbcount;
+    // split learned step (split = true): the deferred pairs' rows and the list of warp-blocks
+    // holding them (bia_learned_block.cuh)
+    bool split;
+    LearnedRows R;
 };
 
 // Each warp solves warp-blocks t = (its global warp index) + k * (warps in the grid): one
@@ -107,13 +106,22 @@ __global__ void __launch_bounds__(kThreads, TileOccupancy<M>::kMinBlocks) bia_pa
 }
 
 // Phase-locked ALG step kernel (see phase_block_solve): CTAs of kW warps, kMinB of them
-// per SM, each warp on one warp-block.
+// per SM, each warp on one warp-block.  The counters of the CTA's warps are summed in shared
+// memory and flushed with one set of atomics per CTA: flushing per warp-block put ~10 atomics
+// per block on the same 20 addresses from all kW warps at once (the same kernel without
+// counters ran 13 % faster on the Coulomb cube).  (A persistent grid of one CTA per SM, each
+// taking groups in a fixed stride, was slower again: the groups' costs differ, and the
+// hardware's block scheduler balances them better.)
 template <bool kDeterministic, int kW, int kMinB>
 __global__ void __launch_bounds__(kW * 32, kMinB) bia_pair_phase_kernel(const StepArgs A)
 {
     extern __shared__ double phase_smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
+    unsigned long long *slots = reinterpret_cast<unsigned long long *>(phase_smem + kW * kTileSmemDoubles);
+    unsigned long long *wtot = slots + warp * kNumStats;
+    if (lane < kNumStats) wtot[lane] = 0ull;
+    __syncwarp();
     const long long tl = (long long)blockIdx.x * kW + warp;
     const bool live = tl < A.nwb;
     int bi = 0, bj = 0;
@@ -122,24 +130,27 @@ __global__ void __launch_bounds__(kW * 32, kMinB) bia_pair_phase_kernel(const St
     PairCounters cnt;
     phase_block_solve(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P, bi, bj, lane, live,
                       phase_smem + warp * kTileSmemDoubles, racc, cacc, cnt);
-    if (!live) return;  // warp-uniform; no barrier follows
-    flush_counters(cnt, A.stats, lane);
-    const int i = bi * 32 + lane;
-    const int jown = bj * 32 + lane;
-    const size_t plane = (size_t)A.npad;
-    if (kDeterministic) {
-        write_partials(A.part, plane, bi, bj, lane, racc, cacc);
-    } else if (bi == bj) {
+    if (live) {  // warp-uniform
+        counters_to_slot(cnt, wtot, lane);
+        const int i = bi * 32 + lane;
+        const int jown = bj * 32 + lane;
+        const size_t plane = (size_t)A.npad;
+        if (kDeterministic) {
+            write_partials(A.part, plane, bi, bj, lane, racc, cacc);
+        } else if (bi == bj) {
 #pragma unroll
-        for (int c = 0; c < 6; c++)
-            if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c] - cacc[c]);
-    } else {
+            for (int c = 0; c < 6; c++)
+                if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c] - cacc[c]);
+        } else {
 #pragma unroll
-        for (int c = 0; c < 6; c++) {
-            if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c]);
-            if (jown < A.n) atomicAdd(&A.part[c * plane + jown], -cacc[c]);
+            for (int c = 0; c < 6; c++) {
+                if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c]);
+                if (jown < A.n) atomicAdd(&A.part[c * plane + jown], -cacc[c]);
+            }
         }
     }
+    __syncthreads();
+    if (warp == 0) flush_slots(slots, kW, A.stats, lane);
 }
 
 // ALG pair-kernel shapes the autotuner chooses from (bia_context_autotune):
@@ -150,8 +161,9 @@ __global__ void __launch_bounds__(kW * 32, kMinB) bia_pair_phase_kernel(const St
 // else kVarTiles8.
 enum AlgVariant { kVarTiles8 = 0, kVarPhase16 = 1, kVarPhase32 = 2, kVarCount = 3 };
 
+// the warps' slices, then one counter slot of kNumStats u64 per warp
 template <int kW>
-constexpr int phase_smem_bytes() { return kW * kTileSmemDoubles * (int)sizeof(double); }
+constexpr int phase_smem_bytes() { return kW * (kTileSmemDoubles + kNumStats) * (int)sizeof(double); }
 
 // Once per device (the current one): opt the phase-locked kernels in to their dynamic
 // shared memory and read the SM count.  Returns the SM count, 0 when the set-up failed
@@ -311,30 +323,34 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const 
     add_learned_sums<kDeterministic>(A, bi, bj, lane, racc, cacc, true);
 }
 
-// Split learned step, first kernel: every warp-block's plain pairs (rest_block_solve); the
-// pairs in the heads' domain are left as a per-lane mask, and each warp-block with any is
-// appended to the list that bia_pair_learned_list_kernel works through afterwards.
-// Deterministic mode writes every partial slot here; the learned kernel adds onto them.
+// Split learned step, first kernel (rest_block_solve, rest_block_defer): every warp-block's
+// pairs except the deferred ones, whose head inputs go to the rows and whose warp-blocks are
+// listed.  Deterministic mode writes every partial slot here; the finish kernel adds onto
+// them.  Two CTAs per SM (kPersistentCtas): at three the filter spills registers inside the
+// rotation loop.  A persistent grid with the counters flushed per warp, as
+// bia_pair_tiles_kernel; dynamic shared memory: each warp's column slice and row slots.
 template <bool kDeterministic>
-// Two CTAs per SM (kPersistentCtas): at three the filter spills registers inside the
-// rotation loop (measured at n = 32768: 11.2 ms at three, 10.9 ms at two).  A persistent grid
-// with the counters flushed per warp, as bia_pair_tiles_kernel.
 __global__ void __launch_bounds__(kThreads, kPersistentCtas) bia_pair_rest_kernel(const StepArgs A)
 {
-    const unsigned full = 0xffffffffu;
+    extern __shared__ __align__(16) uint8_t rest_smem[];
     const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    double *ws = reinterpret_cast<double *>(rest_smem + warp * kRestWarpBytes);
+    uint32_t *wslots = reinterpret_cast<uint32_t *>(rest_smem + warp * kRestWarpBytes +
+                                                    kTileSmemDoubles * sizeof(double));
     PairCounters tot;
     counters_zero(tot);
     int nblk = 0;
-    for (long long tl = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); tl < A.nwb;
+    for (long long tl = (long long)blockIdx.x * kWarpsPerBlock + warp; tl < A.nwb;
          tl += (long long)gridDim.x * kWarpsPerBlock) {  // warp-uniform
         const long long t = A.t0 + tl;
         int bi, bj;
         warp_block_coords(t, bi, bj);
         double racc[6], cacc[6];
+        uint32_t mask[kMlpHeads];
         PairCounters cnt;
-        const uint32_t learned = rest_block_solve(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P.dt, bi,
-                                                  bj, lane, racc, cacc, cnt);
+        rest_block_solve(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P.dt, bi, bj, lane, ws, wslots, racc,
+                         cacc, mask, cnt);
         counters_add(tot, cnt);
         if (++nblk == kFlushBlocks) {
             flush_counters(tot, A.stats, lane);
@@ -342,55 +358,62 @@ __global__ void __launch_bounds__(kThreads, kPersistentCtas) bia_pair_rest_kerne
             nblk = 0;
         }
         add_learned_sums<kDeterministic>(A, bi, bj, lane, racc, cacc, true);
-        if (__any_sync(full, learned != 0u)) {
-            unsigned int slot = 0;
-            if (lane == 0) slot = atomicAdd(A.wbcount, 1u);
-            slot = __shfl_sync(full, slot, 0);
-            A.lmask[(size_t)slot * 32 + lane] = learned;
-            if (lane == 0) A.wblist[slot] = (unsigned int)t;
-        }
+        rest_block_defer(A.R, (unsigned int)t, mask, wslots, lane);
     }
     if (nblk > 0) flush_counters(tot, A.stats, lane);
 }
 
-// Split learned step, second kernel: persistent CTAs work through the listed warp-blocks,
-// eight at a time (one per warp), solving the masked pairs from the heads' guesses and
-// adding their sums onto the rest kernel's.  The tensor memory is allocated once per CTA.
-template <bool kDeterministic>
-__global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_list_kernel(const StepArgs A)
+// Split learned step, second kernel: the rows of both heads on the tensor cores (persistent
+// CTAs of kMlpThreads, TMEM allocated once per CTA).  A timed-out pipeline is counted; its
+// rows keep their inputs, which the finish kernel's FP64 step rejects (the plain solver
+// takes those pairs).
+__global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_head_kernel(const LearnedRows R,
+                                                                                 const MlpImage *heads,
+                                                                                 unsigned long long *stats)
 {
-    extern __shared__ uint8_t learned_smem_raw[];
-    const LearnedSmem M = learned_smem(learned_smem_raw);
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    const long long count = (long long)*A.wbcount;
-    const LearnedBlockIn B = {A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P.dt, A.heads};
-    mlp_setup(*M.mlp);
+    extern __shared__ uint8_t head_rows_smem[];
+    MlpSmem &S = *reinterpret_cast<MlpSmem *>(((uintptr_t)head_rows_smem + 1023) & ~(uintptr_t)1023);
+    mlp_setup(S);
     uint32_t phase = 0;
-    for (long long g0 = (long long)blockIdx.x * kLearnedWarps; g0 < count;
-         g0 += (long long)gridDim.x * kLearnedWarps) {
-        const long long e = g0 + warp;
-        const bool live = e < count;
-        int bi = 0, bj = 0;
-        uint32_t mask = 0u;
-        if (live) {
-            warp_block_coords((long long)A.wblist[e], bi, bj);
-            mask = A.lmask[(size_t)e * 32 + lane];
-        }
-        double racc[6], cacc[6];
-        PairCounters cnt;
-        const bool timed_out = learned_block_solve(M, B, bi, bj, lane, live, racc, cacc, cnt, phase, &mask);
-        if (timed_out && threadIdx.x == 0 && !live) atomicAdd(&A.stats[kStatTimeouts], 1ull);
-        if (live) {
-            flush_counters(cnt, A.stats, lane);
-            add_learned_sums<kDeterministic>(A, bi, bj, lane, racc, cacc, false);
-        }
-    }
-    mlp_teardown(*M.mlp, phase);
+    bool ok = head_rows_pass(S, R, heads, kHeadHyp, phase);
+    if (ok) ok = head_rows_pass(S, R, heads, kHeadEll, phase);
+    mlp_teardown(S, phase);
+    if (!ok && threadIdx.x == 0) atomicAdd(&stats[kStatTimeouts], 1ull);
 }
 
-// Once per device: dynamic shared memory opt-in of the learned kernels; returns the grid
-// of the persistent list kernel (resident CTAs on the device), 0 on failure.
+// Split learned step, third kernel: one warp per listed warp-block (persistent 8-warp CTAs,
+// no CTA barrier), its deferred pairs from their guesses added onto the partials.
+template <bool kDeterministic>
+__global__ void __launch_bounds__(kThreads, 2) bia_pair_learned_finish_kernel(const StepArgs A)
+{
+    __shared__ double s_fin[kTileWarps][kTileSmemDoubles];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const long long count = (long long)*A.R.nlist;
+    const LearnedBlockIn B = {A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P.dt, A.heads};
+    PairCounters tot;
+    counters_zero(tot);
+    int nblk = 0;
+    for (long long e = (long long)blockIdx.x * kWarpsPerBlock + warp; e < count;
+         e += (long long)gridDim.x * kWarpsPerBlock) {  // warp-uniform
+        int bi, bj;
+        warp_block_coords((long long)A.R.entries[e].x, bi, bj);
+        double racc[6], cacc[6];
+        PairCounters cnt;
+        finish_block_solve(A.R, e, B, bi, bj, lane, s_fin[warp], racc, cacc, cnt);
+        counters_add(tot, cnt);
+        if (++nblk == kFlushBlocks) {
+            flush_counters(tot, A.stats, lane);
+            counters_zero(tot);
+            nblk = 0;
+        }
+        add_learned_sums<kDeterministic>(A, bi, bj, lane, racc, cacc, false);
+    }
+    if (nblk > 0) flush_counters(tot, A.stats, lane);
+}
+
+// Once per device: dynamic shared memory opt-in of the learned kernels; returns the grid of
+// the persistent head kernel (resident CTAs on the device), 0 on failure.
 static int learned_kernel_setup()
 {
     constexpr int kMaxDevices = 64;
@@ -402,24 +425,26 @@ static int learned_kernel_setup()
     std::lock_guard<std::mutex> lk(mu);
     if (!done_of[dev]) {
         const int bytes = (int)kLearnedSmemBytes;
+        const int hbytes = (int)(1024 + sizeof(MlpSmem));
         int sms = 0, occ = 0;
         bool ok = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess;
         ok = ok && cudaFuncSetAttribute(bia_pair_learned_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         bytes) == cudaSuccess;
         ok = ok && cudaFuncSetAttribute(bia_pair_learned_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         bytes) == cudaSuccess;
-        ok = ok && cudaFuncSetAttribute(bia_pair_learned_list_kernel<true>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
-        ok = ok && cudaFuncSetAttribute(bia_pair_learned_list_kernel<false>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(bia_pair_rest_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)kRestSmemBytes) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(bia_pair_rest_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)kRestSmemBytes) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(bia_pair_learned_head_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        hbytes) == cudaSuccess;
         // the largest shared-memory carveout, so that the occupancy query sees what the
         // launch gets (without it the query assumes the default split: 1 CTA per SM)
-        for (const void *f : {(const void *)bia_pair_learned_list_kernel<true>,
-                              (const void *)bia_pair_learned_list_kernel<false>})
-            ok = ok && cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                            (int)cudaSharedmemCarveoutMaxShared) == cudaSuccess;
-        ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bia_pair_learned_list_kernel<true>, kMlpThreads,
-                                                                 (size_t)bytes) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute((const void *)bia_pair_learned_head_kernel,
+                                        cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        (int)cudaSharedmemCarveoutMaxShared) == cudaSuccess;
+        ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bia_pair_learned_head_kernel, kMlpThreads,
+                                                                 (size_t)hbytes) == cudaSuccess;
         if (!ok) cudaGetLastError();
         // at least the launch bound's two CTAs per SM: CTAs beyond the resident ones wait
         // for a slot, so a low answer costs nothing but a short queue
@@ -429,37 +454,62 @@ static int learned_kernel_setup()
     return grid_of[dev];
 }
 
-// The learned step's pair launches: one kernel, or (A.lmask set) the rest kernel and the
-// persistent list kernel.
+int learned_head_grid() { return learned_kernel_setup(); }
+
+void launch_learned_head(const LearnedRows &R, const MlpImage *heads, unsigned long long *stats, int grid,
+                         cudaStream_t st)
+{
+    bia_pair_learned_head_kernel<<<grid, kMlpThreads, 1024 + sizeof(MlpSmem), st>>>(R, heads, stats);
+}
+
+// The learned step's pair launches: one kernel, or (A.split) the rest, head and finish
+// kernels.
 template <bool kDeterministic>
 static int launch_pair_learned(const StepArgs &A, cudaStream_t st)
 {
     const int lgrid = learned_kernel_setup();
     if (lgrid <= 0) return BIA_ERR_CUDA;
-    if (!A.lmask) {
+    if (!A.split) {
         const long long grid = (A.nwb + kLearnedWarps - 1) / kLearnedWarps;
         bia_pair_learned_kernel<kDeterministic><<<(unsigned)grid, kMlpThreads, kLearnedSmemBytes, st>>>(A);
         return BIA_OK;
     }
-    if (cudaMemsetAsync(A.wbcount, 0, sizeof(unsigned int), st) != cudaSuccess) return BIA_ERR_CUDA;
+    // the row counts of both heads and the list length start at zero
+    if (cudaMemsetAsync(A.R.counts, 0, kSplitHeader, st) != cudaSuccess) return BIA_ERR_CUDA;
     const long long rgrid = persistent_grid((A.nwb + kWarpsPerBlock - 1) / kWarpsPerBlock);
-    bia_pair_rest_kernel<kDeterministic><<<(unsigned)rgrid, kThreads, 0, st>>>(A);
-    const long long need = (A.nwb + kLearnedWarps - 1) / kLearnedWarps;
-    const int grid = (int)(need < lgrid ? need : lgrid);
-    bia_pair_learned_list_kernel<kDeterministic><<<grid, kMlpThreads, kLearnedSmemBytes, st>>>(A);
+    bia_pair_rest_kernel<kDeterministic><<<(unsigned)rgrid, kThreads, kRestSmemBytes, st>>>(A);
+    launch_learned_head(A.R, A.heads, A.stats, lgrid, st);
+    bia_pair_learned_finish_kernel<kDeterministic><<<(unsigned)rgrid, kThreads, 0, st>>>(A);
     return BIA_OK;
 }
 
-// The split learned step's buffer: the list length (16 bytes), the list (nwb words) and the
-// masks (32 words per listed warp-block).
-static size_t split_buffer_bytes(long long nwb) { return 16 + (size_t)nwb * 33 * sizeof(uint32_t); }
+// The split learned step's buffer: the row counts and list length (kSplitHeader bytes), the
+// list entries (16 bytes per warp-block), the pair masks (2 x 32 words per warp-block) and the
+// rows of both heads (4 bytes each, up to kRowsCap per head: 1 GB in all at the cap).
+constexpr unsigned int kRowsCap = 1u << 27;
+static unsigned int rows_cap(long long nwb)
+{
+    const unsigned long long pairs = (unsigned long long)nwb * 1024ull;
+    return pairs < kRowsCap ? (unsigned int)pairs : kRowsCap;
+}
+static size_t split_buffer_bytes(long long nwb)
+{
+    return kSplitHeader + (size_t)nwb * (16 + 64 * sizeof(uint32_t)) +
+           (size_t)kMlpHeads * rows_cap(nwb) * sizeof(uint32_t);
+}
 
 static void split_buffer_carve(void *base, long long nwb, StepArgs &A)
 {
     uint8_t *b = (uint8_t *)base;
-    A.wbcount = (unsigned int *)b;
-    A.wblist = (unsigned int *)(b + 16);
-    A.lmask = (uint32_t *)(b + 16 + (size_t)nwb * sizeof(uint32_t));
+    A.split = true;
+    A.R.counts = (unsigned long long *)b;
+    A.R.nlist = (unsigned int *)(b + 16);
+    A.R.entries = (uint4 *)(b + kSplitHeader);
+    A.R.masks = (uint32_t *)(b + kSplitHeader + (size_t)nwb * 16);
+    uint32_t *rows = (uint32_t *)(b + kSplitHeader + (size_t)nwb * (16 + 64 * sizeof(uint32_t)));
+    A.R.rows_cap = rows_cap(nwb);
+    A.R.rows[kHeadEll] = rows;
+    A.R.rows[kHeadHyp] = rows + A.R.rows_cap;
 }
 
 // The learned step splits (plain pairs in the rest kernel, learned pairs in the list
@@ -622,6 +672,7 @@ static int enqueue_pairs(bia_context *ctx, const bia_config *cfg, int n, double 
         split = (lt >= 0) ? (lt == 1 && ctx->lmask.ptr) : learned_split(all);
     }
     if (split) split_buffer_carve(ctx->lmask.ptr, all, A);
+    else A.split = false;
     if (learned && !ctx->heads_loaded) return BIA_ERR_INVALID_ARGUMENT;
     if (A.nwb == 0) {  // an empty shard: nothing to launch (the accumulators are cleared)
         if (!cfg->deterministic)
@@ -890,11 +941,11 @@ int bia_context_autotune(bia_context *ctx, const bia_config *cfg, int n, double 
     A.P.dt = cfg->dt; A.P.err = cfg->err; A.P.relerr = cfg->rkf_relerr; A.P.abserr = cfg->rkf_abserr;
     A.P.itr = cfg->itr; A.P.method = cfg->method;
     A.heads = (const MlpImage *)ctx->heads.ptr;
-    A.lmask = nullptr;
+    A.split = false;
     const int det = cfg->deterministic ? 1 : 0;
     A.part = det ? (double *)ctx->part.ptr : (double *)ctx->acc.ptr;
     const bool learned = cfg->method == BIA_METHOD_LEARNED;
-    if (learned) {  // layouts: 0 one kernel, 1 split (the rest kernel, then the list kernel)
+    if (learned) {  // layouts: 0 one kernel, 1 split (the rest, head and finish kernels)
         e = ctx->lmask.reserve(split_buffer_bytes(A.nwb));
         if (e != cudaSuccess) return set_last_error(cuda_status(e));
     }
@@ -915,7 +966,7 @@ int bia_context_autotune(bia_context *ctx, const bia_config *cfg, int n, double 
             if (e == cudaSuccess) e = cudaEventRecord(ev[0], ctx->stream);
             int lst = BIA_OK;
             if (learned) {
-                A.lmask = nullptr;
+                A.split = false;
                 if (var == 1) split_buffer_carve(ctx->lmask.ptr, A.nwb, A);
                 lst = det ? launch_pair_learned<true>(A, ctx->stream) : launch_pair_learned<false>(A, ctx->stream);
             } else if (det) {

@@ -208,7 +208,6 @@ __device__ __forceinline__ void warp_block_solve_compact(const double *x, const 
 #endif
 constexpr int kPhaseWarps = BIA_PHASE_WARPS > 0 ? BIA_PHASE_WARPS : 8;
 constexpr int kPhaseMinBlocks = BIA_PHASE_MIN_BLOCKS;
-constexpr int kPhaseSmemBytes = kPhaseWarps * kTileSmemDoubles * (int)sizeof(double);
 
 __device__ __forceinline__ void phase_block_solve(const double *x, const double *y, const double *z,
                                                   const double *u, const double *v, const double *w,
@@ -287,6 +286,31 @@ __device__ __forceinline__ void warp_block_solve_uv(const double *x, const doubl
 #pragma unroll
     for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
     __syncwarp();  // the slice is reused by this warp's next block
+}
+
+// The phase-locked kernels' counters: a warp-block's counters summed over the warp into the
+// warp's slot wtot[kNumStats] in shared memory (lane 0); after a CTA barrier one warp adds
+// the CTA's slots up and flushes them with one set of atomics (flush_slots).
+__device__ __forceinline__ void counters_to_slot(const PairCounters &c, unsigned long long *wtot, int lane)
+{
+    const unsigned full = 0xffffffffu;
+    int vals[kNumStats] = {c.cls[0], c.cls[1], c.cls[2], c.cls[3], c.cls[4], c.cls[5],
+                           c.it_hyp, c.it_ell, c.it_par, c.it_uv, c.rkf_steps,
+                           c.nonconverged, c.bracket_exits, c.fallbacks, c.nonfinite,
+                           c.learned, c.learned_fallbacks, c.learned_coarse, c.timeouts, c.learned_fp32};
+#pragma unroll
+    for (int k = 0; k < kNumStats; k++) {
+        const int s = __reduce_add_sync(full, vals[k]);
+        if (lane == 0 && s != 0) wtot[k] += (unsigned long long)s;
+    }
+}
+__device__ __forceinline__ void flush_slots(const unsigned long long *slots, int nwarps, unsigned long long *stats,
+                                            int lane)
+{
+    if (lane >= kNumStats) return;
+    unsigned long long sum = 0ull;
+    for (int w = 0; w < nwarps; w++) sum += slots[w * kNumStats + lane];
+    if (sum != 0ull) atomicAdd(&stats[lane], sum);
 }
 
 // Running sums of a warp's counters over the blocks it solves (persistent kernels flush

@@ -29,6 +29,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "bia_internal.cuh"
@@ -571,17 +572,23 @@ struct bia_trainer {
 
 namespace {
 
+// Once per device (the current one): the training kernel's dynamic shared-memory opt-in.
 int trainer_setup_kernel()
 {
-    static bool done = false;
-    static int ok = 0;
-    if (!done) {
-        ok = cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kTrainSmemBytes) == cudaSuccess;
-        if (!ok) cudaGetLastError();
-        done = true;
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static bool done_of[kMaxDevices] = {};
+    static bool ok_of[kMaxDevices] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 0;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!done_of[dev]) {
+        ok_of[dev] = cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)kTrainSmemBytes) == cudaSuccess;
+        if (!ok_of[dev]) cudaGetLastError();
+        done_of[dev] = true;
     }
-    return ok;
+    return ok_of[dev] ? 1 : 0;
 }
 
 void trainer_free(bia_trainer *t)

@@ -102,8 +102,9 @@ int bia_context_destroy(bia_context *ctx);
    and floor(log2 n) in the context, which later steps of that size then use.
    Shapes: 0 = 8-warp CTAs, 1 = phase-locked 16-warp CTAs (2 per SM), 2 = phase-locked
    32-warp CTAs (1 per SM).  BIA_METHOD_LEARNED: 0 = one kernel, 1 = split (the plain pairs
-   in a universal-variable kernel that lists the warp-blocks holding learned pairs, then a
-   persistent kernel over that list; the untuned default at every size).  variant (optional) receives the
+   in a universal-variable kernel that defers the learned pairs' head inputs to rows and lists
+   their warp-blocks, a persistent kernel that evaluates the rows on the tensor cores, and one
+   that finishes the listed warp-blocks; the untuned default at every size).  variant (optional) receives the
    choice, ms (optional, 3 floats) the best time of each candidate (-1 when not run).  RKF
    and universal variables have one shape: variant = -1.
    Synchronises the context's stream; not during stream capture.  No counterpart in the
@@ -223,7 +224,8 @@ int bia_ensemble_run(bia_context *ctx, bia_ensemble *ens, const bia_config *cfg,
    unchanged); the fastest is kept in the ensemble and used by later runs.  Shapes: ALG 0 =
    8-warp CTAs, 1 = phase-locked 16-warp CTAs (2 per SM), 2 = phase-locked 32-warp CTAs
    (1 per SM); universal variables 0 = one item per warp, 1 = a persistent grid (2 CTAs per
-   SM); learned 0 / 1 = the persistent list kernel at 1 / 2 CTAs per SM.  Every shape gives
+   SM); learned 0 / 1 = the persistent head kernel (the deferred pairs' rows on the tensor
+   cores) at 1 / 2 CTAs per SM.  Every shape gives
    bitwise the same results.  variant (optional): the choice (-1 for RKF, one shape); ms
    (optional, 3 floats): each shape's best time (-1 when not run).  Synchronises the
    context's stream; not during stream capture.  No counterpart in the reference. */
@@ -245,7 +247,8 @@ int bia_ensemble_energy(bia_context *ctx, bia_ensemble *ens, const double *x, co
    operands, FP32 accumulation in tensor memory) and Adam on the device; results are the
    same for the same seed.  Parameters (FP32, bia_trainer_param_count() of them) are ordered
    W1[64][2], b1[64], W2[64][64], b2[64], W3[64][64], b3[64], w4[64], b4 (weights
-   output-major). */
+   output-major).  The trainer works on the context's device and on the stream the context
+   had when the trainer was created; every call synchronises that stream. */
 typedef struct bia_trainer bia_trainer;
 int bia_trainer_create(bia_context *ctx, int head, long long nsamples, unsigned long long seed,
                        bia_trainer **trainer);
