@@ -77,12 +77,11 @@ METHODS = {"rkf": 0, "alg": 1, "universal": 2, "learned": 3}
 # kernel, from one ncu capture at n = 16384 of the same workload and method, scaled by the
 # pairs per launch (both the partial sums and any local-memory traffic grow with the pairs):
 #   (workload, method, learned layout) -> (pairs in the capture, bytes in the capture)
-# The split learned step is its two kernels (the rest kernel writes every partial slot, the
-# list kernel reads and writes back the slots of the warp-blocks it solves).
+# The learned step's dominant kernel is the rest kernel (it writes every partial slot; the head
+# and finish kernels move under 1 MB at this size on this workload).
 TRAFFIC = {
-    ("plummer_32768", 3, "split"): (16384 * 16383 // 2, (1.255e6 + 354.301e6) + (256.467e6 + 196.120e6)),
-    ("coulomb_cube_32768", 3, "split"): (16384 * 16383 // 2, (1.048e6 + 360.475e6) + (421.979e6 + 353.333e6)),
-    ("coulomb_cube_32768", 1, None): (16384 * 16383 // 2, 100.488e6 + 3169.538e6),  # phase-locked ALG
+    ("plummer_32768", 3, "split"): (16384 * 16383 // 2, 0.912e6 + 343.940e6),
+    ("coulomb_cube_32768", 1, None): (16384 * 16383 // 2, 34.942e6 + 3184.887e6),  # phase-locked ALG
 }
 
 
@@ -112,6 +111,7 @@ def parse():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="plummer_32768")
     ap.add_argument("--n", type=int, default=None, help="override the particle count")
+    ap.add_argument("--dt", type=float, default=None, help="override the workload's step length")
     ap.add_argument("--method", choices=("learned", "alg", "rkf", "universal"), default="learned")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--systems", type=int, default=4096)
@@ -382,7 +382,7 @@ def run_ensemble(args, rank, world, local):
                        "parallelism": f"replicas x{world}", "autotuned": main_r["autotuned"]},
             "forms": {k: {kk: vv for kk, vv in v.items() if kk != "stats"} for k, v in res.items()},
             "energy_drift": main_r["energy_drift"],
-            "clocks": clocks, "gpu_launches": (3 if method == 3 else 2) * steps,
+            "clocks": clocks, "gpu_launches": (4 if method == 3 else 2) * steps,
             "stats": main_r["stats"]}
         if "learned" in res:
             best = min(v["ms_per_step"] for k, v in res.items() if k in ("alg", "universal"))
@@ -552,6 +552,10 @@ def error_vs_oracle(solver, cfg, d_init, d_q, state, eps, q, dt, nsel=16, nquad=
         "pos_max_err_over_max_x": float(np.abs(got[:, :3] - ref[:, :3]).max() / np.abs(state[:3]).max()),
         "vel_max_err_over_max_v": float(np.abs(got[:, 3:] - ref[:, 3:]).max() / np.abs(state[3:]).max()),
         "interaction_dx_rel_err_vs_exact": rel(got[:nquad, :3] - drift, refq[:, :3] - drift),
+        # dX = U dt + interaction is stored in FP64, so the interaction part is resolved to
+        # half an ulp of dX, not better: an error of 0 means below this
+        "interaction_dx_fp64_resolution": float(np.linalg.norm(np.spacing(refq[:, :3]) / 2)
+                                                / np.linalg.norm(refq[:, :3] - drift)),
         "dv_rel_err_vs_exact": rel(got[:nquad, 3:], refq[:, 3:]),
         "fp64_oracle_interaction_dx_rel_err_vs_exact": rel(ref[:nquad, :3] - drift, refq[:, :3] - drift),
         "fp64_oracle_dv_rel_err_vs_exact": rel(ref[:nquad, 3:], refq[:, 3:]),
@@ -581,6 +585,8 @@ def main():
     dist = _init_dist(world)
 
     state, eps, q, dt, steps_cfg = initial.make(args.workload, n=args.n)
+    if args.dt is not None:
+        dt = args.dt
     n = state.shape[1]
     pairs = n * (n - 1) // 2
     steps = args.steps if args.steps is not None else steps_cfg
@@ -649,7 +655,8 @@ def main():
     else:  # the library's rule: the learned step splits at every size
         split = method == 3
     if method == 3:
-        kernel_name = ("bia_pair_rest_kernel<true> + bia_pair_learned_list_kernel<true> (one timed interval)"
+        kernel_name = ("bia_pair_rest_kernel<true> + bia_pair_learned_head_kernel + "
+                       "bia_pair_learned_finish_kernel<true> (one timed interval)"
                        if split else "bia_pair_learned_kernel<true>")
     elif method == 1 and tuned is not None:
         kernel_name = {"tiles8": "bia_pair_tiles_kernel<true, 1>", "phase16": "bia_pair_phase_kernel<true, 16, 2>",
@@ -665,12 +672,12 @@ def main():
     achieved = per_launch_flops / per_launch_s / 1e12
     traffic = None
     tkey = (args.workload, method, ("split" if split else "one_kernel") if method == 3 else None)
-    if args.n is None and tkey in TRAFFIC:
+    if args.n is None and args.dt is None and tkey in TRAFFIC:
         tp, tb = TRAFFIC[tkey]
         traffic = tb * pairs / tp
     roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak if peak else None, "traffic": traffic,
-                "traffic_note": "ncu capture of the same kernel and workload at n = 16384, "
+                "traffic_note": "ncu capture of the dominant kernel on the same workload at n = 16384, "
                                 "scaled by pairs per launch" if traffic else None,
                 "algorithmic_bytes_per_launch": nb_blocks * 6 * n * 8 + 6 * n * 8,
                 "peak_source": "measured live: bia_measure_fp64_peak DFMA loop on this GPU",
@@ -745,7 +752,7 @@ def main():
                                          "its Fortran build (README.md:43)"}}
 
     extras = None
-    if rank == 0 and world == 1 and not args.no_extras and args.n is None:
+    if rank == 0 and world == 1 and not args.no_extras and args.n is None and args.dt is None:
         extras = run_extras(solver, timer, args)
 
     if dist is not None:
@@ -766,9 +773,10 @@ def main():
                                         "device copy; the e2e loop copies it into the host buffer)",
                                   autotuned=tuned, shard=shard),
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-            # pair kernel(s) and the reduction per step; a shard's reduction is two launches
-            # (the shard's sums, then the update after the all-reduce)
-            "gpu_launches": ((3 if split else 2) + (1 if shard else 0)) * steps,
+            # pair kernels (the split learned step: rest, head, finish) and the reduction per
+            # step; a shard's reduction is two launches (the shard's sums, then the update
+            # after the all-reduce)
+            "gpu_launches": ((4 if split else 2) + (1 if shard else 0)) * steps,
             "learned_vs_best_plain": learned_vs_best_plain,
             "error_vs_oracle": errors,
             "plain_fp64": plain, "universal": universal,
@@ -844,8 +852,9 @@ def run_extras(solver, timer, args):
     out = {}
     dev = timer.dev
 
-    def forms(name, entries, steps, warmup):
-        s, eps, q, dt, _ = initial.make(name)
+    def forms(name, entries, steps, warmup, dt=None):
+        s, eps, q, dt_cfg, _ = initial.make(name)
+        dt = dt_cfg if dt is None else dt
         n = s.shape[1]
         pairs = n * (n - 1) // 2
         d_init = torch.tensor(s, device=dev)
@@ -868,8 +877,7 @@ def run_extras(solver, timer, args):
         ("rkf_rel_1e-12", 0, {"rkf_relerr": 1e-12, "rkf_abserr": 1e-16}),
         ("rkf_reference_tol_0_1e-16", 0, {})], steps=3, warmup=3)
     out["coulomb_cube_32768"]["learned_long_step_dt_1e-3"] = forms(
-        "coulomb_cube_32768", [("learned", 3, {"dt": 1e-3}), ("universal", 2, {"dt": 1e-3})],
-        steps=3, warmup=3)
+        "coulomb_cube_32768", [("learned", 3, {}), ("universal", 2, {})], steps=3, warmup=3, dt=1e-3)
     out["cold_ball_131072"] = forms("cold_ball_131072", [("alg", 1, {}), ("universal", 2, {}),
                                                          ("learned", 3, {})], steps=3, warmup=3)
     out["gravity_ball_1332"] = forms("gravity_ball_1332", [("alg", 1, {}), ("universal", 2, {}),

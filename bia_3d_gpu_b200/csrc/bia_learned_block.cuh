@@ -9,12 +9,11 @@
 
 namespace bia {
 
-// A learned CTA: 8 warps, one warp-block each, two CTAs per SM, in three phases.
+// The one-kernel learned form: a CTA of 8 warps, one warp-block each, two CTAs per SM, in
+// three phases (the split step below spreads the same work over three kernels).
 //  1. Each lane classifies its pairs (hyperbolic head, elliptic head, plain) and writes the
 //     head input of each learned pair (packed BF16) into the pair's own row slot
-//     (warp, lane, k) in shared memory.  With a pair mask from the split step's rest
-//     kernel only the masked pairs are classified (and solved); the others are the rest
-//     kernel's.
+//     (warp, lane, k) in shared memory.
 //  2. A CTA scan of the per-lane counts numbers the learned pairs of each head in thread
 //     and bit order; the CTA evaluates each head on its pairs in full 256-row blocks on
 //     the tensor cores (mlp_tc.cuh), each thread finding its row's slot from the scan, and
@@ -263,12 +262,10 @@ __device__ __forceinline__ LearnedSmem learned_smem(uint8_t *raw)
 // CTA's mlp_setup and mlp_teardown; phase is the MMA barrier's phase, carried across
 // calls.  Returns the row sums racc (particle 32 bi + lane), the column sums cacc (particle
 // 32 bj + lane; the caller writes -cacc) and the counters; true when the tensor-core
-// pipeline timed out.  mask (split step, may be null): this lane's pairs to solve (bit k:
-// column (lane + k) mod 32); without it every pair of the block is solved here.
+// pipeline timed out.
 __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const LearnedBlockIn &B, int bi, int bj,
                                                     int lane, bool live, double racc[6], double cacc[6],
-                                                    PairCounters &cnt, uint32_t &phase,
-                                                    const uint32_t *mask = nullptr)
+                                                    PairCounters &cnt, uint32_t &phase)
 {
     MlpSmem &S = *M.mlp;
     const int warp = threadIdx.x >> 5;
@@ -297,24 +294,7 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
 
     // 1. classification and the head inputs
     unsigned mh = 0u, me = 0u, mr = 0u;
-    if (live && mask) {
-        unsigned m = *mask;
-        while (m) {
-            const int k = __ffs(m) - 1;
-            m &= m - 1u;
-            const int src = (lane + k) & 31;
-            const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
-            const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
-            const double eps_ij = hq ? B.eps_th * si[6] * ws[6 * 32 + src] : B.eps_th;
-            LearnedPair L;
-            learned_prepare(eps_ij, dt, r, g, L);
-            const unsigned bit = 1u << k;
-            if (L.kind != kLearnedPlain) myrows[k] = pack_bf16(L.x0, L.x1);
-            if (L.kind == kLearnedHyp) mh |= bit;
-            else if (L.kind == kLearnedEll) me |= bit;
-            else mr |= bit;
-        }
-    } else if (live) {
+    if (live) {
         const int k0 = diag ? 1 : 0, k1 = diag ? 16 : 31;
         for (int k = k0; k <= k1; k++) {
             const int src = (lane + k) & 31;
@@ -393,9 +373,8 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
     __syncwarp();
 
     // 3. learned pairs from their guesses, per warp.  A warp without learned pairs walks the
-    // rotation offsets instead (all its pairs plain; column sums by shuffle, no shared adds);
-    // with a mask the few plain pairs go through the per-lane loop below
-    const bool warp_learned = mask != nullptr || __any_sync(0xffffffffu, (mh | me) != 0u);
+    // rotation offsets instead (all its pairs plain; column sums by shuffle, no shared adds)
+    const bool warp_learned = __any_sync(0xffffffffu, (mh | me) != 0u);
     if (!warp_learned) {
         const unsigned full = 0xffffffffu;
 #pragma unroll

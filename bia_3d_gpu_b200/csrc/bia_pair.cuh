@@ -742,6 +742,16 @@ static __device__ __noinline__ int rkf_pair(double eps_th, double xe, double rel
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void stumpff(double x, double c[4])
 {
+    if (fabs(x) <= 1e-6) {
+        // three terms: the next ones, x^3/8! and x^3/9!, are below 3e-23
+        const double c2 = 0.5 - x * (1.0 / 24 - x * (1.0 / 720));
+        const double c3 = 1.0 / 6 - x * (1.0 / 120 - x * (1.0 / 5040));
+        c[0] = 1.0 - x * c2;
+        c[1] = 1.0 - x * c3;
+        c[2] = c2;
+        c[3] = c3;
+        return;
+    }
     if (fabs(x) <= 1e-2) {
         // the first five terms: the next ones, x^5/12! and x^5/13!, are below 2e-19
         const double c2 = 0.5 - x * (1.0 / 24 - x * (1.0 / 720 - x * (1.0 / 40320 - x * (1.0 / 3628800))));
@@ -960,14 +970,17 @@ __device__ __forceinline__ void uv_compose(const UvPair &p, double s, const doub
     } else {
         irr = (irr_hint != 0.0 && fabs(e) <= 1e-8) ? fma(irr_hint, e, irr_hint) : 1.0 / rr;
     }
-    const double fm1 = -p.mu * s2c2 * p.ir0;
-    const double gmdt = -p.mu * s3c3;
-    const double fdot = -p.mu * s * c[1] * (irr * p.ir0);
-    const double gdm1 = -p.mu * s2c2 * irr;
+    // the half-displacement's factor 1/2 is taken into the coefficients: scaling by a power of
+    // two is exact, so h is the same as (f - 1) r + (g - dt) v halved afterwards, at four
+    // multiplications instead of six
+    const double fm1 = -0.5 * p.mu * s2c2 * p.ir0;
+    const double gmdt = -0.5 * p.mu * s3c3;
+    const double fdot = -0.5 * p.mu * s * c[1] * (irr * p.ir0);
+    const double gdm1 = -0.5 * p.mu * s2c2 * irr;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        h[k] = (fm1 * r[k] + gmdt * g[k]) * 0.5;
-        h[3 + k] = (fdot * r[k] + gdm1 * g[k]) * 0.5;
+        h[k] = fm1 * r[k] + gmdt * g[k];
+        h[3 + k] = fdot * r[k] + gdm1 * g[k];
     }
 }
 

@@ -743,12 +743,13 @@ void shard_columns(int nb, int shard, int nshards, int *c0, int *c1)
 struct ShardReduceArgs {
     const double *part;
     double *out;  // [6][n]
-    int n, npad, nparts, c0, c1;
+    int n, npad, c0, c1;
+    bool atomic;  // part is the atomic-mode accumulator (one plane, the shard's sums only)
 };
 
 // out[c][p] = the shard's partial planes of particle p summed in ascending plane order
-// (deterministic), or the atomic accumulator (nparts = 1): one warp per component per 32
-// particles, as bia_reduce_update_kernel.
+// (deterministic), or the atomic accumulator: one warp per component per 32 particles, as
+// bia_reduce_update_kernel.
 __global__ void __launch_bounds__(kReduceThreads) bia_shard_reduce_kernel(const ShardReduceArgs A)
 {
     const int lane = threadIdx.x & 31;
@@ -759,7 +760,7 @@ __global__ void __launch_bounds__(kReduceThreads) bia_shard_reduce_kernel(const 
     const double *src = A.part + (size_t)c * plane + p;
     const size_t step = 6 * plane;
     double sum = 0.0;
-    if (A.nparts == 1) {
+    if (A.atomic) {
         sum = src[0];
     } else {
         const int b = p / 32;
@@ -1215,7 +1216,7 @@ int bia_step_shard(bia_context *ctx, const bia_config *cfg, int n, double *x, do
     R.out = sums;
     R.n = n;
     R.npad = nb * 32;
-    R.nparts = cfg->deterministic ? nb : 1;
+    R.atomic = !cfg->deterministic;
     R.c0 = c0;
     R.c1 = c1;
     bia_shard_reduce_kernel<<<(n + 31) / 32, kReduceThreads, 0, ctx->stream>>>(R);

@@ -218,3 +218,21 @@ def test_learned_long_step_full_size(cuda):
     ex, ev = interaction_errors(got[:6], refq, s, sel[:6], dt)
     print(f"coulomb dt=1e-3 learned: {st['learned']} learned pairs, interaction dX rel err {ex:.2e}, dV {ev:.2e}")
     assert ex <= 1e-10 and ev <= 1e-10
+
+
+def test_rkf_full_size_sampled_particles(cuda):
+    """The reference's per-pair RKF45 mode (bia/find_dXYUV_RKF.f90, its tolerances) on
+    coulomb_cube_32768: 24 sampled particles against the oracle's RKF pair sums, to 1e-12
+    of the state, and momentum from the antisymmetry."""
+    from bia_3d_gpu_b200 import METHOD_RKF
+    s, eps, q, dt, _ = initial.make("coulomb_cube_32768")
+    n = s.shape[1]
+    new, disp, st = one_step(cuda, s, eps, dt, q, method=METHOD_RKF)
+    assert st["rkf"] + st["degenerate"] == n * (n - 1) // 2 and st["nonfinite"] == 0
+    sel = np.random.default_rng(19).choice(n, 24, replace=False)
+    ref = oracle.particle_disp(s, eps, dt, sel, q=q, method=0)
+    got = disp[:, sel].T
+    assert np.abs(got[:, :3] - ref[:, :3]).max() <= 1e-12 * np.abs(s[:3]).max()
+    assert np.abs(got[:, 3:] - ref[:, 3:]).max() <= 1e-12 * np.abs(s[3:]).max()
+    kick = disp[3:].sum(axis=1)
+    assert np.abs(kick).max() <= 1e-12 * np.abs(disp[3:]).sum(axis=1).max()

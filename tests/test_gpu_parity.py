@@ -351,3 +351,51 @@ def test_bia_driver_reproduces_reference_record(cuda, golden, golden_ic, tmp_pat
     line = (tmp_path / "BIA_10^0.0001332").read_text().splitlines()[0]
     vals = [float(line[23 + 24 * k:23 + 24 * (k + 1)]) for k in range(6)]
     assert np.abs(np.array(vals) - golden["bia_p1"][1:]).max() <= 1e-13
+
+
+def test_universal_solver_against_reference_equations_near_unit_eccentricity(cuda):
+    """The universal-variable solver (every pair of BIA_METHOD_UNIVERSAL and of the learned
+    form) against the reference's own conic equations (bia/find_hyperbola.f90,
+    bia/find_ellipse.f90) evaluated in quad precision, on attractive pairs drawn in
+    0.1 < |e^2 - 1| < 0.3: there ALG still takes the reference's equations and they are well
+    conditioned, so the quad oracle is their exact step.  One 2-particle system per pair, as an
+    ensemble; steps long enough to move the pairs through a good part of their orbits."""
+    from bia_3d_gpu_b200 import METHOD_UNIVERSAL
+    rng = np.random.default_rng(77)
+    eps, dt = -1.0, 0.3
+    pairs = []
+    while len(pairs) < 200:
+        r = rng.standard_normal(3)
+        r *= rng.uniform(0.5, 2.0) / np.linalg.norm(r)
+        g = rng.standard_normal(3) * rng.uniform(0.2, 2.0)
+        rm = np.linalg.norm(r)
+        E = g @ g + 2 * eps / rm
+        L = np.cross(r, g)
+        e2m1 = E * (L @ L) / eps ** 2
+        if 0.1 < abs(e2m1) < 0.3:
+            pairs.append((r, g))
+    states = []
+    for r, g in pairs:
+        states.append(np.array([[r[0] / 2, -r[0] / 2], [r[1] / 2, -r[1] / 2], [r[2] / 2, -r[2] / 2],
+                                [g[0] / 2, -g[0] / 2], [g[1] / 2, -g[1] / 2], [g[2] / 2, -g[2] / 2]]))
+    host = np.concatenate(states, axis=1)
+    whole = cuda.tensor(host, device="cuda")
+    with BIASolver() as solver:
+        ens = solver.ensemble([2] * len(pairs), [eps] * len(pairs))
+        st = ens.run(whole, default_config(dt=dt, method=METHOD_UNIVERSAL), 1, graph=False)
+        solver.stream.synchronize()
+        ens.close()
+    got = whole.cpu().numpy()
+    assert st["nonfinite"] == 0 and st["nonconverged"] == 0
+    worst = 0.0
+    for k, (r, g) in enumerate(pairs):
+        d = got[:, 2 * k] - host[:, 2 * k]
+        h = d.copy()
+        h[:3] -= host[3:, 2 * k] * dt  # the interaction part of particle i's displacement
+        ref, rst = oracle.pair_halfdisp(r, g, eps, dt, method=1, quad=True)
+        assert rst["hyperbola"] + rst["ellipse"] == 1  # the reference's equations, not the universal path
+        worst = max(worst, np.linalg.norm(h[:3] - ref[:3]) / np.linalg.norm(ref[:3]),
+                    np.linalg.norm(h[3:] - ref[3:]) / np.linalg.norm(ref[3:]))
+    print(f"universal solver vs the reference's equations in quad, 200 pairs at 0.1 < |e^2-1| < 0.3: "
+          f"worst relative error {worst:.2e}")
+    assert worst <= 1e-12

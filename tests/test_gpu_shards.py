@@ -38,3 +38,25 @@ def test_shards_add_up_to_the_step(cuda, method, nshards, det):
         assert np.array_equal(a, b)
     ref, _, _ = oracle.bia_step(s, eps, dt, q=q, method=1 if method != METHOD_UNIVERSAL else 2)
     assert rel_err(b[:3], ref[:3]) <= 1e-12 and rel_err(b[3:], ref[3:]) <= 1e-12
+
+
+@pytest.mark.parametrize("n", [2, 33, 97])
+def test_shards_of_ragged_sizes(cuda, n):
+    """More shards than 32-particle columns (empty shards) and partial blocks: the shards'
+    sums still add up to the step."""
+    s, eps, q = initial.coulomb_cube(n, seed=93 + n, dmin=1e-2)
+    cfg = default_config(eps_th=eps, dt=1e-5, method=METHOD_ALG)
+    qt = cuda.tensor(q, device="cuda")
+    whole = cuda.tensor(s, device="cuda")
+    parts = cuda.tensor(s, device="cuda")
+    with BIASolver() as solver:
+        solver.step(whole, cfg, q=qt, stats=False)
+        total = cuda.zeros_like(parts)
+        sums = cuda.empty_like(parts)
+        for r in range(5):
+            solver.step_shard(parts, cfg, r, 5, sums, q=qt)
+            total += sums
+        solver.apply_update(parts, 1e-5, total)
+        solver.stream.synchronize()
+    a, b = whole.cpu().numpy(), parts.cpu().numpy()
+    assert rel_err(b[:3], a[:3]) <= 1e-14 and rel_err(b[3:], a[3:]) <= 1e-14
