@@ -144,10 +144,9 @@ __device__ __forceinline__ void rest_block_solve(const double *x, const double *
             const double eps_ij = q ? eps_th * si[6] * ws[6 * 32 + src] : eps_th;
             const UvPair p = uv_prepare(eps_ij, r, g);
             if (dt != 0.0) {
-                bool exact;
-                double s = uv_start_fast(p, dt, exact);
+                const UvSeries sq = uv_series(p, dt);
                 int kind = kLearnedPlain;
-                if (!exact && learned_filter(p, dt)) {
+                if (!sq.exact && learned_filter(p, dt)) {
                     LearnedPair L;
                     learned_prepare(eps_ij, dt, r, g, L);
                     kind = L.kind;
@@ -157,9 +156,15 @@ __device__ __forceinline__ void rest_block_solve(const double *x, const double *
                     }
                 }
                 if (kind == kLearnedPlain) {
-                    double ifp = 0.0;
-                    const int it = exact ? 0 : uv_iterate(p, dt, s, &ifp);
-                    uv_compose<true>(p, s, r, g, h, exact ? p.ir0 : ifp);
+                    int it = 0;
+                    if (sq.exact) {
+                        uv_compose_series(p, sq, dt, r, g, h);
+                    } else {
+                        double s = uv_series_start(sq);
+                        double ifp = 0.0;
+                        it = uv_iterate(p, dt, s, &ifp);
+                        uv_compose<true>(p, s, r, g, h, ifp);
+                    }
                     cnt.it_uv += it;
                     if (it > kUvItMax) cnt.nonconverged++;
                     cnt.cls[kUniversal]++;
@@ -306,9 +311,7 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
                 int kind = kLearnedPlain;
                 if (learned_candidate(eps_ij, dt, r, g)) {
                     // the split step's routing: a pair whose fifth-order start is exact stays plain
-                    bool exact;
-                    uv_start_fast(uv_prepare(eps_ij, r, g), dt, exact);
-                    if (!exact) {
+                    if (!uv_series(uv_prepare(eps_ij, r, g), dt).exact) {
                         LearnedPair L;
                         learned_prepare(eps_ij, dt, r, g, L);
                         kind = L.kind;

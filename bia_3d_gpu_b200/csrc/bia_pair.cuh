@@ -821,71 +821,103 @@ __device__ __forceinline__ double uv_start(const UvPair &p, double dt)
     return (s > 0.0) ? s : x;
 }
 
-// Fifth-order start (uv_start_fast, the universal-variable method and the split learned
-// step's plain pairs): the series reversion of the universal Kepler equation
+// Fifth-order start of the universal-variable method and the split learned step's plain
+// pairs, in dimensionless form.  The universal Kepler equation
 //   t = b1 s + b2 s^2 + b3 s^3 + b4 s^4 + b5 s^5 + O(s^6),
 //   b1 = r0, b2 = sig/2, b3 = (mu - beta r0)/6, b4 = -sig beta/24, b5 = beta (beta r0 - mu)/120
-// (the Stumpff series of r0 s c1 + sig s^2 c2 + mu s^3 c3), inverted with the Lagrange
+// (the Stumpff series of r0 s c1 + sig s^2 c2 + mu s^3 c3) is inverted with the Lagrange
 // reversion coefficients (Abramowitz and Stegun 3.6.25):
 //   a1 = 1/b1, a2 = -b2/b1^3, a3 = (2 b2^2 - b1 b3)/b1^5, a4 = (5 b1 b2 b3 - b1^2 b4 - 5 b2^3)/b1^7,
 //   a5 = (6 b1^2 b2 b4 + 3 b1^2 b3^2 + 14 b2^4 - b1^3 b5 - 21 b1 b2^2 b3)/b1^9,
 //   s = a1 t + a2 t^2 + a3 t^3 + a4 t^4 + a5 t^5 + O(t^6).
-// When every |a_k t^(k-1)| <= Q^(k-1) a1 with Q = 3e-4 (the step is that small against the
-// pair's time scales), the fifth-order sum is returned with exact_out = true: its truncation is
-// below 1.1e-17 relative, a tenth of an FP64 ulp (checked in extended precision against the
-// solved equation on 12000 attractive and repulsive pairs drawn around that boundary), so no
-// Newton correction is needed.  Otherwise the
-// third-order sum (error O((dt/T)^3), one Newton correction below the 1e-10 acceptance at
-// small steps) is returned with exact_out = false.  The ALG kernels keep uv_start: changing
-// the code they inline changes how the compiler contracts their own FP64 expressions.
-// Every product and sum is written out (fma, __dmul_rn, __dsub_rn) so that each kernel
-// that inlines this computes the same bits and takes the same branch: the ensemble's
-// systems equal their own steps bit for bit.
-__device__ __forceinline__ double uv_start_fast(const UvPair &p, double dt, bool &exact_out)
+// With x = dt/r0, y = sig dt/(2 r0^2), m = mu/r0, z = (m - beta) x^2/6 and w = beta x^2 the
+// relative terms c_k = a_(k+1) dt^k / a1 are
+//   c1 = -y, c2 = 2y^2 - z, c3 = y (5z + w/12 - 5y^2),
+//   c4 = y^2 (14y^2 - 21z - w/2) + z (3z + w/20),
+// and s = x S with S = 1 + c1 + c2 + c3 + c4 (about 25 FP64 operations instead of 65 for the
+// same sum from the a_k).  When every |c_k| <= Q^k with Q = 3e-4 (the step is that small
+// against the pair's time scales) the sum is exact: its truncation is below 1.1e-17
+// relative, a tenth of an FP64 ulp (checked in extended precision against the solved equation
+// on 12000 attractive and repulsive pairs drawn around that boundary), so no Newton
+// correction runs and uv_compose_series composes the half-displacement from S.  Otherwise
+// uv_series_start gives the third-order sum x (1 + c1 + c2) (error O((dt/T)^3), one Newton
+// correction below the 1e-10 acceptance at small steps).  The ALG kernels keep uv_start:
+// changing the code they inline changes how the compiler contracts their own FP64
+// expressions.  Every product and sum is written out (fma, __dmul_rn) so that each kernel
+// that inlines this computes the same bits and takes the same branch: the ensemble's systems
+// equal their own steps bit for bit.
+struct UvSeries {
+    double x, y, x2, w, c2;
+    double mh;  // -m/2
+    double S;   // s = x S where exact
+    bool exact;
+};
+
+__device__ __forceinline__ UvSeries uv_series(const UvPair &p, double dt)
 {
-    const double r0 = p.r0, ir0 = p.ir0;
-    const double ir2 = __dmul_rn(ir0, ir0);
-    const double h = 0.5 * p.sig;  // exact
-    const double br = __dmul_rn(p.beta, r0);
-    const double b3 = __dmul_rn(__dsub_rn(p.mu, br), 1.0 / 6.0);
-    const double a1 = ir0;
-    const double a2 = __dmul_rn(-h, __dmul_rn(ir0, ir2));
-    const double hh = __dmul_rn(h, h);
-    const double a3 = __dmul_rn(fma(2.0, hh, -__dmul_rn(r0, b3)), __dmul_rn(__dmul_rn(ir2, ir2), ir0));
-    const double t = dt;
-    const double s3 = __dmul_rn(t, fma(t, fma(t, a3, a2), a1));
-    bool *exact = &exact_out;
-    {
-        const double b4 = __dmul_rn(__dmul_rn(-h, p.beta), 1.0 / 12.0);
-        const double b5 = __dmul_rn(__dmul_rn(p.beta, __dsub_rn(br, p.mu)), 1.0 / 120.0);
-        const double r02 = __dmul_rn(r0, r0);
-        const double ir7 = __dmul_rn(__dmul_rn(__dmul_rn(ir2, ir2), ir2), ir0);
-        // a4 = (5 r0 h b3 - r0^2 b4 - 5 h^3) / r0^7
-        const double n4 = fma(5.0 * r0, __dmul_rn(h, b3), -fma(r02, b4, __dmul_rn(5.0 * hh, h)));
-        const double a4 = __dmul_rn(n4, ir7);
-        // a5 = (6 r0^2 h b4 + 3 r0^2 b3^2 + 14 h^4 - r0^3 b5 - 21 r0 h^2 b3) / r0^9
-        double n5 = __dmul_rn(__dmul_rn(6.0 * r02, h), b4);
-        n5 = fma(3.0 * r02, __dmul_rn(b3, b3), n5);
-        n5 = fma(14.0 * hh, hh, n5);
-        n5 = fma(-__dmul_rn(r02, r0), b5, n5);
-        n5 = fma(-21.0 * r0, __dmul_rn(hh, b3), n5);
-        const double a5 = __dmul_rn(n5, __dmul_rn(ir7, ir2));
-        constexpr double Q = 3e-4;
-        const double t2 = __dmul_rn(t, t);
-        const bool small = fabs(__dmul_rn(a2, t)) <= Q * a1 && fabs(__dmul_rn(a3, t2)) <= (Q * Q) * a1 &&
-                           fabs(__dmul_rn(a4, __dmul_rn(t2, t))) <= (Q * Q * Q) * a1 &&
-                           fabs(__dmul_rn(a5, __dmul_rn(t2, t2))) <= (Q * Q * Q * Q) * a1;
-        *exact = false;
-        if (small) {
-            const double s5 = __dmul_rn(t, fma(t, fma(t, fma(t, fma(t, a5, a4), a3), a2), a1));
-            if (s5 > 0.0) {
-                *exact = true;
-                return s5;
-            }
-        }
+    UvSeries q;
+    q.x = __dmul_rn(dt, p.ir0);
+    const double m = __dmul_rn(p.mu, p.ir0);
+    q.mh = -0.5 * m;
+    q.y = __dmul_rn(__dmul_rn(0.5 * p.sig, p.ir0), q.x);
+    q.x2 = __dmul_rn(q.x, q.x);
+    q.w = __dmul_rn(p.beta, q.x2);
+    const double y = q.y, w = q.w;
+    const double z = __dmul_rn(__dsub_rn(m, p.beta), __dmul_rn(q.x2, 1.0 / 6.0));
+    const double y2 = __dmul_rn(y, y);
+    q.c2 = fma(2.0 * y, y, -z);
+    const double c3 = __dmul_rn(y, fma(-5.0, y2, fma(w, 1.0 / 12.0, 5.0 * z)));
+    const double c4 = fma(z, fma(3.0, z, __dmul_rn(w, 0.05)), __dmul_rn(y2, fma(14.0, y2, fma(-21.0, z, -0.5 * w))));
+    constexpr double Q = 3e-4;
+    const bool small = fabs(y) <= Q && fabs(q.c2) <= Q * Q && fabs(c3) <= Q * Q * Q && fabs(c4) <= Q * Q * Q * Q;
+    q.S = 1.0 + (q.c2 - y + (c3 + c4));
+    q.exact = small && __dmul_rn(q.x, q.S) > 0.0;
+    return q;
+}
+
+// The third-order start for a pair whose series is not exact (uv_iterate corrects it).
+__device__ __forceinline__ double uv_series_start(const UvSeries &q)
+{
+    const double s3 = __dmul_rn(q.x, 1.0 + (q.c2 - q.y));
+    return (s3 > 0.0) ? s3 : q.x;
+}
+
+// Half-displacement of an exact series pair: the coefficients of uv_compose in the series'
+// variables.  With K = -m x^2/2 (= -mu dt^2/(2 r0^3)), A = S^2 c2(w S^2), B = S^3 c3(w S^2)
+// and rho = r0/r(s):
+//   (f - 1)/2 = K A,  (g - dt)/2 = K dt B,  (g' - 1)/2 = K A rho,  f'/2 = -(m/2)(x/r0) S c1 rho,
+// and r(s)/r0 = 1 + d with d = -w S^2 c2 + 2 y S c1 - 2 K A (r(s) = r0 c0 + sig s c1 +
+// mu s^2 c2 and c0 = 1 - beta s^2 c2), formed without cancellation.  rho is the alternating
+// series of 1/(1 + d) to d^6 where |d| <= 1e-3 (truncation below 1e-21), else a division.
+// The factor 1/2 of the half-displacement is inside K (a power of two: the same bits).
+__device__ __forceinline__ void uv_compose_series(const UvPair &p, const UvSeries &q, double dt, const double r[3],
+                                                  const double g[3], double h[6])
+{
+    const double S = q.S;
+    const double S2 = __dmul_rn(S, S);
+    const double arg = __dmul_rn(q.w, S2);
+    double c[4];
+    stumpff(arg, c);
+    const double A = __dmul_rn(S2, c[2]);
+    const double B = __dmul_rn(__dmul_rn(S2, S), c[3]);
+    const double K = __dmul_rn(q.mh, q.x2);
+    const double fm1 = __dmul_rn(K, A);
+    const double gmdt = __dmul_rn(__dmul_rn(K, dt), B);
+    const double d = fma(-arg, c[2], fma(__dmul_rn(2.0 * q.y, S), c[1], -2.0 * fm1));
+    double rho;
+    if (fabs(d) <= 1e-3) {
+        const double nd = -d;
+        rho = fma(nd, fma(nd, fma(nd, fma(nd, fma(nd, fma(nd, 1.0, 1.0), 1.0), 1.0), 1.0), 1.0), 1.0);
+    } else {
+        rho = 1.0 / (1.0 + d);
     }
-    const double x = __dmul_rn(dt, ir0);
-    return (s3 > 0.0) ? s3 : x;
+    const double gdm1 = __dmul_rn(fm1, rho);
+    const double fdot = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(q.mh, __dmul_rn(q.x, p.ir0)), S), c[1]), rho);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        h[k] = fma(fm1, r[k], __dmul_rn(gmdt, g[k]));
+        h[3 + k] = fma(fdot, r[k], __dmul_rn(gdm1, g[k]));
+    }
 }
 
 // Safeguarded Newton on F(s) = t(s) - dt, F' = r(s) > 0, with the bracket [lo, hi]
@@ -947,8 +979,8 @@ __device__ __forceinline__ double uv_halley_step(const UvPair &p, double dt, dou
 // functions (no cancellation at small s).  irr_hint (optional, 0: none): an approximation
 // of 1/r(s), such as uv_iterate's last 1/F'; within 1e-8 of it one Newton-Raphson step for
 // the reciprocal (x + x (1 - r x)) gives 1/r(s) to ~1e-16, else 1/r(s) is divided out.
-// kTwoSteps (the universal-variable method and the split step's plain pairs, which pass
-// 1/r0 when no Newton iteration ran): two Newton-Raphson steps from a hint within 1e-4
+// kTwoSteps (the universal-variable method and the split step's plain pairs after Newton
+// iterations, the learned finish): two Newton-Raphson steps from a hint within 1e-4
 // (error e^4 <= 1e-16); the ALG kernels keep the one-step form.
 template <bool kTwoSteps = false>
 __device__ __forceinline__ void uv_compose(const UvPair &p, double s, const double r[3], const double g[3],
@@ -1007,11 +1039,15 @@ __device__ __forceinline__ int uv_halfdisp_fast(double eps_th, double dt, const 
     for (int k = 0; k < 6; k++) h[k] = 0.0;
     if (dt == 0.0) return 0;
     const UvPair p = uv_prepare(eps_th, r, g);
-    bool exact;
-    double s = uv_start_fast(p, dt, exact);
+    const UvSeries q = uv_series(p, dt);
+    if (q.exact) {
+        uv_compose_series(p, q, dt, r, g, h);
+        return 0;
+    }
+    double s = uv_series_start(q);
     double ifp = 0.0;
-    const int it = exact ? 0 : uv_iterate(p, dt, s, &ifp);
-    uv_compose<true>(p, s, r, g, h, exact ? p.ir0 : ifp);
+    const int it = uv_iterate(p, dt, s, &ifp);
+    uv_compose<true>(p, s, r, g, h, ifp);
     return it;
 }
 

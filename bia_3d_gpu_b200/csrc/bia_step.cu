@@ -1162,8 +1162,13 @@ int bia_run_host(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
     if (e != cudaSuccess) return cuda_status(e);
     double *d = (double *)ctx->state.ptr;
     double *host[6] = {x, y, z, u, v, w};
-    for (int k = 0; k < 6; k++) {
-        e = cudaMemcpyAsync(d + (size_t)k * n, host[k], n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+    // six arrays back to back in host memory (a [6][n] state) move in one copy each way
+    bool packed = true;
+    for (int k = 1; k < 6; k++) packed = packed && host[k] == x + (size_t)k * n;
+    const int ncopies = packed ? 1 : 6;
+    const size_t copy_bytes = (packed ? 6 : 1) * (size_t)n * sizeof(double);
+    for (int k = 0; k < ncopies; k++) {
+        e = cudaMemcpyAsync(d + (size_t)k * n, host[k], copy_bytes, cudaMemcpyHostToDevice, ctx->stream);
         if (e != cudaSuccess) return cuda_status(e);
     }
     const double *dq = nullptr;
@@ -1176,8 +1181,8 @@ int bia_run_host(bia_context *ctx, const bia_config *cfg, int n, double *x, doub
                  d + 5 * (size_t)n, dq, nsteps, 1, stats);
     if (st != BIA_OK && st != BIA_ERR_NONFINITE) return st;
     int st2 = st;
-    for (int k = 0; k < 6; k++) {
-        e = cudaMemcpyAsync(host[k], d + (size_t)k * n, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    for (int k = 0; k < ncopies; k++) {
+        e = cudaMemcpyAsync(host[k], d + (size_t)k * n, copy_bytes, cudaMemcpyDeviceToHost, ctx->stream);
         if (e != cudaSuccess) return cuda_status(e);
     }
     e = cudaStreamSynchronize(ctx->stream);
