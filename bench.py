@@ -62,11 +62,12 @@ FLOPS = {
     "ellipse": (447, 47),      # per pair, per Kepler Newton step
     "parabola": (429, 76),     # per pair, per Barker Newton step
     "rkf": (147, 758),         # per pair, per accepted RKF45 step (3 Fehlberg stages sets)
-    # universal variables (this library's solver, not the reference's): prepare 20, fifth-order
-    # start with its exactness test 76, composition 66 per pair, 43 per Newton iteration (almost
-    # none at the benchmark steps), with the five-term Stumpff series that every pair of the
-    # benchmark workloads takes (|beta s^2| <= 1e-2)
-    "universal": (162, 43),
+    # universal variables (this library's solver, not the reference's), counted from the
+    # dimensionless series form every exact pair takes: differences 6, prepare 20 (|r|^2,
+    # r.g, |g|^2, rsqrt as sqrt + division, beta), series with its exactness test 41,
+    # composition with the three-term Stumpff series and the series of r0/r 63, accumulation
+    # 12 per pair; 43 per Newton iteration (almost none at the benchmark steps)
+    "universal": (142, 43),
     "learned": (330, 0),       # per learned pair: elements, FP64 Halley step, composition
 }
 # BF16 tensor-core flops per learned pair: 2 x (16 x 64 + 64 x 64 + 64 x 64) multiply-adds
@@ -80,7 +81,7 @@ METHODS = {"rkf": 0, "alg": 1, "universal": 2, "learned": 3}
 # The learned step's dominant kernel is the rest kernel (it writes every partial slot; the head
 # and finish kernels move under 1 MB at this size on this workload).
 TRAFFIC = {
-    ("plummer_32768", 3, "split"): (16384 * 16383 // 2, 0.912e6 + 343.940e6),
+    ("plummer_32768", 3, "split"): (16384 * 16383 // 2, 1.200e6 + 344.538e6),
     ("coulomb_cube_32768", 1, None): (16384 * 16383 // 2, 34.942e6 + 3184.887e6),  # phase-locked ALG
 }
 
