@@ -226,7 +226,8 @@ __global__ void __launch_bounds__(kEnsThreads, 2) ens_pair_learned_finish_kernel
                                   A.q ? A.q + base : nullptr, n, A.eps[s], A.P.dt, A.heads};
         double racc[6], cacc[6];
         PairCounters cnt;
-        finish_block_solve(A.R, e, B, bi, bj, lane, s_fin[warp], racc, cacc, cnt);
+        bool row_hit, col_hit;
+        finish_block_solve(A.R, e, B, bi, bj, lane, s_fin[warp], racc, cacc, cnt, row_hit, col_hit);
         counters_add(tot, cnt);
         if (++nblk == kFlushBlocks) {
             flush_counters(tot, A.stats, lane);
@@ -234,7 +235,7 @@ __global__ void __launch_bounds__(kEnsThreads, 2) ens_pair_learned_finish_kernel
             nblk = 0;
         }
         const int nb = (n + 31) / 32;
-        add_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc);
+        add_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc, row_hit, col_hit);
     }
     if (nblk > 0) flush_counters(tot, A.stats, lane);
 }

@@ -494,12 +494,17 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
 // warp calls it.
 __device__ __forceinline__ void finish_block_solve(const LearnedRows &R, long long e, const LearnedBlockIn &B,
                                                    int bi, int bj, int lane, double *ws, double racc[6],
-                                                   double cacc[6], PairCounters &cnt)
+                                                   double cacc[6], PairCounters &cnt, bool &row_hit,
+                                                   bool &col_hit)
 {
     const unsigned full = 0xffffffffu;
     double *wacc = ws + 7 * 32;
     const uint4 ent = R.entries[e];
     const uint32_t me = R.masks[(size_t)e * 64 + lane], mh = R.masks[(size_t)e * 64 + 32 + lane];
+    // the rows and columns this block's listed pairs touch (bit k of a lane's mask: column
+    // (lane + k) mod 32, so the mask rotated left by the lane is the lane's column set)
+    row_hit = (me | mh) != 0u;
+    col_hit = (__reduce_or_sync(full, __funnelshift_l(me | mh, me | mh, lane)) >> lane) & 1u;
     double si[7];
     {
         double sj[7];

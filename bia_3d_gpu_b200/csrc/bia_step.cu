@@ -273,26 +273,32 @@ static void launch_pair_tiles(const StepArgs &A, long long grid, cudaStream_t st
 }
 
 // Adds a learned warp-block's sums onto the partials (deterministic: the rest kernel wrote
-// every slot first) or into the accumulators; assign: write the slots instead.
+// every slot first) or into the accumulators; assign: write the slots instead.  With
+// assign == false only the slots the added sums touch are read and written: row_hit (this
+// lane's row has a pair among them) and col_hit (this lane's column does); the others would
+// add zero, so the sums are bitwise the same.
 template <bool kDeterministic>
 __device__ __forceinline__ void add_learned_sums(const StepArgs &A, int bi, int bj, int lane, const double racc[6],
-                                                 const double cacc[6], bool assign)
+                                                 const double cacc[6], bool assign, bool row_hit = true,
+                                                 bool col_hit = true)
 {
     const int i = bi * 32 + lane;
     const int jown = bj * 32 + lane;
     const size_t plane = (size_t)A.npad;
     if (kDeterministic) {
         if (assign) write_partials(A.part, plane, bi, bj, lane, racc, cacc);
-        else add_partials(A.part, plane, bi, bj, lane, racc, cacc);
+        else add_partials(A.part, plane, bi, bj, lane, racc, cacc, row_hit, col_hit);
     } else if (bi == bj) {
+        if (row_hit || col_hit) {
 #pragma unroll
-        for (int c = 0; c < 6; c++)
-            if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c] - cacc[c]);
+            for (int c = 0; c < 6; c++)
+                if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c] - cacc[c]);
+        }
     } else {
 #pragma unroll
         for (int c = 0; c < 6; c++) {
-            if (i < A.n) atomicAdd(&A.part[c * plane + i], racc[c]);
-            if (jown < A.n) atomicAdd(&A.part[c * plane + jown], -cacc[c]);
+            if (row_hit && i < A.n) atomicAdd(&A.part[c * plane + i], racc[c]);
+            if (col_hit && jown < A.n) atomicAdd(&A.part[c * plane + jown], -cacc[c]);
         }
     }
 }
@@ -329,8 +335,17 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_kernel(const 
 // them.  Two CTAs per SM (kPersistentCtas): at three the filter spills registers inside the
 // rotation loop.  A persistent grid with the counters flushed per warp, as
 // bia_pair_tiles_kernel; dynamic shared memory: each warp's column slice and row slots.
+// Warps per CTA of the rest kernel.  At 112 registers the register file would hold 18 warps
+// per SM, but CTAs of 9 (96 registers, small spills) or 10 warps (92 registers) are slower:
+// 6.45 and 6.50 against 5.61 ms for the learned pair kernels on plummer_32768.
+#ifndef BIA_REST_WARPS
+#define BIA_REST_WARPS 8
+#endif
+constexpr int kRestWarps = BIA_REST_WARPS;
+constexpr size_t kRestKernelSmemBytes = kRestWarps * kRestWarpBytes;
+
 template <bool kDeterministic>
-__global__ void __launch_bounds__(kThreads, kPersistentCtas) bia_pair_rest_kernel(const StepArgs A)
+__global__ void __launch_bounds__(kRestWarps * 32, kPersistentCtas) bia_pair_rest_kernel(const StepArgs A)
 {
     extern __shared__ __align__(16) uint8_t rest_smem[];
     const int lane = threadIdx.x & 31;
@@ -341,8 +356,8 @@ __global__ void __launch_bounds__(kThreads, kPersistentCtas) bia_pair_rest_kerne
     PairCounters tot;
     counters_zero(tot);
     int nblk = 0;
-    for (long long tl = (long long)blockIdx.x * kWarpsPerBlock + warp; tl < A.nwb;
-         tl += (long long)gridDim.x * kWarpsPerBlock) {  // warp-uniform
+    for (long long tl = (long long)blockIdx.x * kRestWarps + warp; tl < A.nwb;
+         tl += (long long)gridDim.x * kRestWarps) {  // warp-uniform
         const long long t = A.t0 + tl;
         int bi, bj;
         warp_block_coords(t, bi, bj);
@@ -400,14 +415,15 @@ __global__ void __launch_bounds__(kThreads, 2) bia_pair_learned_finish_kernel(co
         warp_block_coords((long long)A.R.entries[e].x, bi, bj);
         double racc[6], cacc[6];
         PairCounters cnt;
-        finish_block_solve(A.R, e, B, bi, bj, lane, s_fin[warp], racc, cacc, cnt);
+        bool row_hit, col_hit;
+        finish_block_solve(A.R, e, B, bi, bj, lane, s_fin[warp], racc, cacc, cnt, row_hit, col_hit);
         counters_add(tot, cnt);
         if (++nblk == kFlushBlocks) {
             flush_counters(tot, A.stats, lane);
             counters_zero(tot);
             nblk = 0;
         }
-        add_learned_sums<kDeterministic>(A, bi, bj, lane, racc, cacc, false);
+        add_learned_sums<kDeterministic>(A, bi, bj, lane, racc, cacc, false, row_hit, col_hit);
     }
     if (nblk > 0) flush_counters(tot, A.stats, lane);
 }
@@ -433,9 +449,9 @@ static int learned_kernel_setup()
         ok = ok && cudaFuncSetAttribute(bia_pair_learned_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         bytes) == cudaSuccess;
         ok = ok && cudaFuncSetAttribute(bia_pair_rest_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kRestSmemBytes) == cudaSuccess;
+                                        (int)kRestKernelSmemBytes) == cudaSuccess;
         ok = ok && cudaFuncSetAttribute(bia_pair_rest_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kRestSmemBytes) == cudaSuccess;
+                                        (int)kRestKernelSmemBytes) == cudaSuccess;
         ok = ok && cudaFuncSetAttribute(bia_pair_learned_head_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         hbytes) == cudaSuccess;
         // the largest shared-memory carveout, so that the occupancy query sees what the
@@ -476,10 +492,11 @@ static int launch_pair_learned(const StepArgs &A, cudaStream_t st)
     }
     // the row counts of both heads and the list length start at zero
     if (cudaMemsetAsync(A.R.counts, 0, kSplitHeader, st) != cudaSuccess) return BIA_ERR_CUDA;
-    const long long rgrid = persistent_grid((A.nwb + kWarpsPerBlock - 1) / kWarpsPerBlock);
-    bia_pair_rest_kernel<kDeterministic><<<(unsigned)rgrid, kThreads, kRestSmemBytes, st>>>(A);
+    const long long rgrid = persistent_grid((A.nwb + kRestWarps - 1) / kRestWarps);
+    bia_pair_rest_kernel<kDeterministic><<<(unsigned)rgrid, kRestWarps * 32, kRestKernelSmemBytes, st>>>(A);
     launch_learned_head(A.R, A.heads, A.stats, lgrid, st);
-    bia_pair_learned_finish_kernel<kDeterministic><<<(unsigned)rgrid, kThreads, 0, st>>>(A);
+    const long long fgrid = persistent_grid((A.nwb + kWarpsPerBlock - 1) / kWarpsPerBlock);
+    bia_pair_learned_finish_kernel<kDeterministic><<<(unsigned)fgrid, kThreads, 0, st>>>(A);
     return BIA_OK;
 }
 

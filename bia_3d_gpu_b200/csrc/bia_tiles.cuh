@@ -403,23 +403,29 @@ __device__ __forceinline__ void write_partials(double *part, size_t plane, int b
 }
 
 // The same slots as write_partials, added onto instead of written (a second kernel's share
-// of the same warp-block).
+// of the same warp-block).  row_hit / col_hit false: this lane's row / column sum is zero
+// and its slot is left alone (adding zero would not change it).
 __device__ __forceinline__ void add_partials(double *part, size_t plane, int bi, int bj, int lane,
-                                             const double racc[6], const double cacc[6])
+                                             const double racc[6], const double cacc[6], bool row_hit = true,
+                                             bool col_hit = true)
 {
     const int i = bi * 32 + lane;
     const int j = bj * 32 + lane;
     if (bi == bj) {
+        if (!row_hit && !col_hit) return;
         double *dst = part + (size_t)bi * 6 * plane;
 #pragma unroll
         for (int c = 0; c < 6; c++) dst[c * plane + i] += racc[c] - cacc[c];
     } else {
         double *drow = part + (size_t)bj * 6 * plane;
         double *dcol = part + (size_t)bi * 6 * plane;
+        if (row_hit) {
 #pragma unroll
-        for (int c = 0; c < 6; c++) {
-            drow[c * plane + i] += racc[c];
-            dcol[c * plane + j] -= cacc[c];
+            for (int c = 0; c < 6; c++) drow[c * plane + i] += racc[c];
+        }
+        if (col_hit) {
+#pragma unroll
+            for (int c = 0; c < 6; c++) dcol[c * plane + j] -= cacc[c];
         }
     }
 }
