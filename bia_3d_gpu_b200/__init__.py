@@ -328,6 +328,16 @@ class BIASolver:
                  else ("tiles8", "phase16", "phase32"))
         return var.value, {names[k]: float(ms[k]) for k in range(3) if ms[k] >= 0}
 
+    def set_shape(self, method, n, shape, deterministic=True):
+        """Pin the pair-kernel shape of `method` (ALG: "tiles8", "phase16", "phase32";
+        learned: "one_kernel", "split"; None: the default rule) for sizes in n's
+        floor(log2 n) bucket, as autotune would store it."""
+        names = (("one_kernel", "split") if method == capi.METHOD_LEARNED
+                 else ("tiles8", "phase16", "phase32"))
+        var = -1 if shape is None else names.index(shape)
+        capi.check(capi.lib().bia_context_set_shape(self._ctx, int(method), int(bool(deterministic)), int(n), var),
+                   "bia_context_set_shape")
+
     def load_heads(self, path=None):
         """Load the learned heads (learned_heads.bin) for METHOD_LEARNED steps."""
         blob = open(path or HEADS_PATH, "rb").read()

@@ -119,6 +119,8 @@ def lib():
     L.bia_context_autotune.argtypes = ([_V, ctypes.POINTER(BiaConfig), _I] + [_V] * 7 +
                                        [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)])
     L.bia_context_autotune.restype = _I
+    L.bia_context_set_shape.argtypes = [_V, _I, _I, _I, _I]
+    L.bia_context_set_shape.restype = _I
     L.bia_selftest_wait_timeout.argtypes = [_V]
     L.bia_selftest_wait_timeout.restype = _I
     L.bia_context_set_heads.argtypes = [_V, ctypes.c_char_p, ctypes.c_size_t]
@@ -188,7 +190,7 @@ EXPORTED_SYMBOLS = ("bia_config_default", "bia_context_create", "bia_context_des
                     "bia_measure_fp64_peak", "bia_context_stats", "bia_dim_integrate", "rkf_c_",
                     "bia_ensemble_create", "bia_ensemble_destroy", "bia_ensemble_particles",
                     "bia_ensemble_run", "bia_ensemble_energy", "bia_ensemble_autotune",
-                    "bia_context_set_heads", "bia_learned_head_eval", "bia_context_autotune",
+                    "bia_context_set_heads", "bia_learned_head_eval", "bia_context_autotune", "bia_context_set_shape",
                     "bia_selftest_wait_timeout", "bia_step_noalloc",
                     "bia_shard_columns", "bia_step_shard", "bia_apply_update",
                     "bia_trainer_create", "bia_trainer_destroy", "bia_trainer_param_count",

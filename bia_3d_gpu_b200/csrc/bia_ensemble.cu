@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(kW * 32, kMinB) ens_pair_phase_kernel(const En
     extern __shared__ double phase_smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    unsigned long long *slots = reinterpret_cast<unsigned long long *>(phase_smem + kW * kTileSmemDoubles);
+    unsigned long long *slots = reinterpret_cast<unsigned long long *>(phase_smem + kW * kPhaseSliceDoubles);
     unsigned long long *wtot = slots + warp * kNumStats;
     if (lane < kNumStats) wtot[lane] = 0ull;
     __syncwarp();
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(kW * 32, kMinB) ens_pair_phase_kernel(const En
     double racc[6], cacc[6];
     PairCounters cnt;
     phase_block_solve(A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base, q, n, A.eps[s],
-                      A.P, bi, bj, lane, live, phase_smem + warp * kTileSmemDoubles, racc, cacc, cnt);
+                      A.P, bi, bj, lane, live, phase_smem + warp * kPhaseSliceDoubles, racc, cacc, cnt);
     if (live) {  // warp-uniform
         counters_to_slot(cnt, wtot, lane);
         const int nb = (n + 31) / 32;
@@ -153,9 +153,9 @@ static int ens_phase_setup()
         int sms = 0;
         bool ok = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess;
         ok = ok && cudaFuncSetAttribute(ens_pair_phase_kernel<32, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        32 * (kTileSmemDoubles + kNumStats) * (int)sizeof(double)) == cudaSuccess;
+                                        32 * (kPhaseSliceDoubles + kNumStats) * (int)sizeof(double)) == cudaSuccess;
         ok = ok && cudaFuncSetAttribute(ens_pair_phase_kernel<16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        16 * (kTileSmemDoubles + kNumStats) * (int)sizeof(double)) == cudaSuccess;
+                                        16 * (kPhaseSliceDoubles + kNumStats) * (int)sizeof(double)) == cudaSuccess;
         if (!ok) cudaGetLastError();
         sms_of[dev] = ok ? sms : 0;
         done_of[dev] = true;
@@ -413,10 +413,10 @@ static int ens_pair_launch(bia_context *ctx, bia_ensemble *E, EnsArgs &A, int me
         if (sms <= 0) var = 0;
         if (var == 2) {
             ens_pair_phase_kernel<32, 1><<<(unsigned)((E->nitems + 31) / 32), 32 * 32,
-                                            32 * (kTileSmemDoubles + kNumStats) * sizeof(double), st>>>(A);
+                                            32 * (kPhaseSliceDoubles + kNumStats) * sizeof(double), st>>>(A);
         } else if (var == 1) {
             ens_pair_phase_kernel<16, 2><<<(unsigned)((E->nitems + 15) / 16), 16 * 32,
-                                            16 * (kTileSmemDoubles + kNumStats) * sizeof(double), st>>>(A);
+                                            16 * (kPhaseSliceDoubles + kNumStats) * sizeof(double), st>>>(A);
         } else {
             ens_pair_tiles_kernel<kMethodAlg><<<grid, kEnsThreads, 0, st>>>(A);
         }

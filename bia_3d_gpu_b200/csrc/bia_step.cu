@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(kW * 32, kMinB) bia_pair_phase_kernel(const St
     extern __shared__ double phase_smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    unsigned long long *slots = reinterpret_cast<unsigned long long *>(phase_smem + kW * kTileSmemDoubles);
+    unsigned long long *slots = reinterpret_cast<unsigned long long *>(phase_smem + kW * kPhaseSliceDoubles);
     unsigned long long *wtot = slots + warp * kNumStats;
     if (lane < kNumStats) wtot[lane] = 0ull;
     __syncwarp();
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(kW * 32, kMinB) bia_pair_phase_kernel(const St
     double racc[6], cacc[6];
     PairCounters cnt;
     phase_block_solve(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P, bi, bj, lane, live,
-                      phase_smem + warp * kTileSmemDoubles, racc, cacc, cnt);
+                      phase_smem + warp * kPhaseSliceDoubles, racc, cacc, cnt);
     if (live) {  // warp-uniform
         counters_to_slot(cnt, wtot, lane);
         const int i = bi * 32 + lane;
@@ -163,7 +163,7 @@ enum AlgVariant { kVarTiles8 = 0, kVarPhase16 = 1, kVarPhase32 = 2, kVarCount = 
 
 // the warps' slices, then one counter slot of kNumStats u64 per warp
 template <int kW>
-constexpr int phase_smem_bytes() { return kW * (kTileSmemDoubles + kNumStats) * (int)sizeof(double); }
+constexpr int phase_smem_bytes() { return kW * (kPhaseSliceDoubles + kNumStats) * (int)sizeof(double); }
 
 // Once per device (the current one): opt the phase-locked kernels in to their dynamic
 // shared memory and read the SM count.  Returns the SM count, 0 when the set-up failed
@@ -1016,6 +1016,22 @@ int bia_context_autotune(bia_context *ctx, const bia_config *cfg, int n, double 
     if (learned) ctx->learned_tuned[det][ilog2_bucket(n)] = best;
     else ctx->alg_tuned[det][ilog2_bucket(n)] = best;
     if (variant) *variant = best;
+    return set_last_error(BIA_OK);
+}
+
+int bia_context_set_shape(bia_context *ctx, int method, int deterministic, int n, int variant)
+{
+    if (!ctx || n < 1) return set_last_error(BIA_ERR_INVALID_ARGUMENT);
+    const int det = deterministic ? 1 : 0;
+    if (method == BIA_METHOD_ALG) {
+        if (variant < -1 || variant >= kVarCount) return set_last_error(BIA_ERR_INVALID_ARGUMENT);
+        ctx->alg_tuned[det][ilog2_bucket(n)] = variant;
+    } else if (method == BIA_METHOD_LEARNED) {
+        if (variant < -1 || variant > 1) return set_last_error(BIA_ERR_INVALID_ARGUMENT);
+        ctx->learned_tuned[det][ilog2_bucket(n)] = variant;
+    } else {
+        return set_last_error(BIA_ERR_INVALID_ARGUMENT);  // one shape only
+    }
     return set_last_error(BIA_OK);
 }
 

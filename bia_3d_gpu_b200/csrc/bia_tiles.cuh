@@ -126,6 +126,94 @@ __device__ __forceinline__ void compact_class_loop(unsigned m, const double si[7
     }
 }
 
+// Balanced class loop of the phase-locked kernels.  The class's pairs of the warp-block are
+// enumerated round by round: round r holds the r-th pair (in bit order) of every lane that
+// has more than r of them, lanes in order.  Turn t takes entries 32 t .. 32 t + 31 of that
+// enumeration, one per lane.  Full rounds are exactly the compact loop's turns (lane l solves
+// its own pair); the tail rounds, in which only some lanes still have pairs, are packed
+// together, so the loop takes ceil(pairs / 32) turns instead of the largest per-lane count
+// (on the mixed-class Coulomb cube the compact loop's turns cost about 1.5x the balanced
+// ones).  The solving lane is no longer the row's lane, so the row states rs and the row
+// sums racs live in the warp's shared slice, and lanes that hit the same row or the same
+// column in one turn add in lane order.  Every row then takes its pairs in rank order and
+// every column in (round, lane) order: the compact loop's orders, so the sums are bitwise the
+// compact loop's.
+template <int C>
+__device__ __forceinline__ void balanced_class_loop(unsigned m, const double *rs, double *racs, const double *ws,
+                                                    double *wacc, int lane, bool has_q, double eps_th,
+                                                    const PairParams &P, PairCounters &cnt)
+{
+    const unsigned full = 0xffffffffu;
+    const unsigned lt = (1u << lane) - 1u;
+    const int total = (int)__reduce_add_sync(full, (unsigned)__popc(m));
+    int rbase = 0;                          // enumeration index of the current round's first pair
+    unsigned cur = m;                       // this lane's pairs not in a finished round
+    unsigned rm = __ballot_sync(full, cur != 0u);  // lanes of the current round
+    for (int base = 0; base < total; base += 32) {
+        const int q = base + lane;
+        int o = -1, k = 0;
+        while (rm != 0u) {  // the rounds this turn covers (warp-uniform)
+            const int nr = __popc(rm);
+            const int idx = q - rbase;
+            const bool here = idx >= 0 && idx < nr;
+            const int src = here ? (int)__fns(rm, 0, idx + 1) : 0;
+            const int kk = __shfl_sync(full, __ffs(cur) - 1, src);  // the owner's pair of this round
+            if (here) {
+                o = src;
+                k = kk;
+            }
+            if (rbase + nr > base + 32) break;  // the round goes on in the next turn
+            rbase += nr;
+            if ((rm >> lane) & 1u) cur &= cur - 1u;
+            rm = __ballot_sync(full, cur != 0u);
+        }
+        const bool busy = o >= 0;
+        const unsigned bm = __ballot_sync(full, busy);
+        if (busy) {
+            const int j = (o + k) & 31;
+            double si[7], sc[7];
+#pragma unroll
+            for (int c = 0; c < 7; c++) {
+                si[c] = rs[c * 32 + o];
+                sc[c] = ws[c * 32 + j];
+            }
+            const double r[3] = {si[0] - sc[0], si[1] - sc[1], si[2] - sc[2]};
+            const double g[3] = {si[3] - sc[3], si[4] - sc[4], si[5] - sc[5]};
+            const double eps_ij = has_q ? eps_th * si[6] * sc[6] : eps_th;
+            double h[6];
+            if (C == kClsUv) {
+                alg_rare_pair(P, eps_ij, r, g, h, cnt, alg_classify(eps_ij, r, g));
+            } else {
+                alg_conic_pair<C>(P, eps_ij, r, g, h, cnt);
+            }
+            {
+                const unsigned grp = __match_any_sync(bm, o);
+                const int rank = __popc(grp & lt);
+                const int turns = (int)__reduce_max_sync(bm, (unsigned)__popc(grp));
+                for (int t = 0; t < turns; t++) {
+                    if (rank == t) {
+#pragma unroll
+                        for (int c = 0; c < 6; c++) racs[c * 32 + o] += h[c];
+                    }
+                    __syncwarp(bm);
+                }
+            }
+            {
+                const unsigned grp = __match_any_sync(bm, j);
+                const int rank = __popc(grp & lt);
+                const int turns = (int)__reduce_max_sync(bm, (unsigned)__popc(grp));
+                for (int t = 0; t < turns; t++) {
+                    if (rank == t) {
+#pragma unroll
+                        for (int c = 0; c < 6; c++) wacc[c * 32 + j] += h[c];
+                    }
+                    __syncwarp(bm);
+                }
+            }
+        }
+    }
+}
+
 // Loads of a compacted warp-block and classification of its pairs: the column states go
 // to the warp's shared slice ws (sums zeroed), si receives the row particle, and the class
 // masks (bit k: the pair with column (lane + k) mod 32) are returned in mh, me, mr.
@@ -196,10 +284,12 @@ __device__ __forceinline__ void warp_block_solve_compact(const double *x, const 
 // (barrier) the rare classes, so the SM fetches one solver's instructions at a time: the
 // mixed-class ALG step is bound by instruction fetch when the warps of one SM sit in
 // different solvers (measured on B200, Coulomb N = 32768: 218 ms per step with 8-warp
-// CTAs, 122 ms phase-locked with 32 warps).  Same per-block arithmetic and order as
-// warp_block_solve_compact, so the results are bitwise equal.  Every thread of the CTA
-// must call it (warps without a block pass live = false); ws is the warp's slice of
-// kTileSmemDoubles doubles.
+// CTAs, 122 ms phase-locked with 32 warps).  The class loops are the balanced ones
+// (balanced_class_loop), with the same per-block arithmetic and order as
+// warp_block_solve_compact, so the results are bitwise equal.  Every thread of the CTA must
+// call it (warps without a block pass live = false); ws is the warp's slice of
+// kPhaseSliceDoubles doubles: column states [7][32], column sums [6][32], row states
+// [7][32], row sums [6][32].
 #ifndef BIA_PHASE_WARPS
 #define BIA_PHASE_WARPS 32  // 0: never use the phase-locked kernels
 #endif
@@ -207,6 +297,7 @@ __device__ __forceinline__ void warp_block_solve_compact(const double *x, const 
 #define BIA_PHASE_MIN_BLOCKS 1
 #endif
 constexpr int kPhaseWarps = BIA_PHASE_WARPS > 0 ? BIA_PHASE_WARPS : 8;
+constexpr int kPhaseSliceDoubles = kTileSmemDoubles + 13 * 32;
 constexpr int kPhaseMinBlocks = BIA_PHASE_MIN_BLOCKS;
 
 __device__ __forceinline__ void phase_block_solve(const double *x, const double *y, const double *z,
@@ -215,22 +306,31 @@ __device__ __forceinline__ void phase_block_solve(const double *x, const double 
                                                   int bi, int bj, int lane, bool live, double *ws,
                                                   double racc[6], double cacc[6], PairCounters &cnt)
 {
-    double si[7];
     unsigned mh, me, mr;
     counters_zero(cnt);
+    double *rs = ws + kTileSmemDoubles;
+    double *racs = rs + 7 * 32;
+    {
+        double si[7];
+        compact_prepare(x, y, z, u, v, w, q, n, eps_th, bi, bj, lane, live, ws, si, mh, me, mr);
 #pragma unroll
-    for (int c = 0; c < 6; c++) racc[c] = 0.0;
-    compact_prepare(x, y, z, u, v, w, q, n, eps_th, bi, bj, lane, live, ws, si, mh, me, mr);
+        for (int c = 0; c < 7; c++) rs[c * 32 + lane] = si[c];
+#pragma unroll
+        for (int c = 0; c < 6; c++) racs[c * 32 + lane] = 0.0;
+    }
     const bool hq = q != nullptr;
     __syncthreads();
-    compact_class_loop<kClsHyp>(mh, si, ws, ws + 7 * 32, lane, hq, eps_th, P, racc, cnt);
+    balanced_class_loop<kClsHyp>(mh, rs, racs, ws, ws + 7 * 32, lane, hq, eps_th, P, cnt);
     __syncthreads();
-    compact_class_loop<kClsEll>(me, si, ws, ws + 7 * 32, lane, hq, eps_th, P, racc, cnt);
+    balanced_class_loop<kClsEll>(me, rs, racs, ws, ws + 7 * 32, lane, hq, eps_th, P, cnt);
     __syncthreads();
-    compact_class_loop<kClsUv>(mr, si, ws, ws + 7 * 32, lane, hq, eps_th, P, racc, cnt);
+    balanced_class_loop<kClsUv>(mr, rs, racs, ws, ws + 7 * 32, lane, hq, eps_th, P, cnt);
     __syncwarp();
 #pragma unroll
-    for (int c = 0; c < 6; c++) cacc[c] = ws[(7 + c) * 32 + lane];
+    for (int c = 0; c < 6; c++) {
+        racc[c] = racs[c * 32 + lane];
+        cacc[c] = ws[(7 + c) * 32 + lane];
+    }
 }
 
 // Universal-variable warp-block: lanes walk the rotation offsets as in warp_block_solve,

@@ -112,6 +112,12 @@ int bia_context_destroy(bia_context *ctx);
 int bia_context_autotune(bia_context *ctx, const bia_config *cfg, int n, double *x, double *y,
                          double *z, double *u, double *v, double *w, const double *q,
                          int *variant, float *ms);
+/* Pins the pair-kernel shape that later steps of this context take for `method`
+   (BIA_METHOD_ALG or BIA_METHOD_LEARNED), reduction mode `deterministic` and sizes in n's
+   floor(log2 n) bucket: what bia_context_autotune stores, for a caller that keeps an earlier
+   tuning result; variant -1 restores the default rule.  The shapes of a method compute
+   bitwise the same results.  No counterpart in the reference. */
+int bia_context_set_shape(bia_context *ctx, int method, int deterministic, int n, int variant);
 /* Self-test of the device-side bounded waits: a kernel waits on an mbarrier that nothing
    completes, gives up after its limit and reports it; returns BIA_ERR_DEVICE_TIMEOUT (the
    expected answer) and leaves the context usable.  No counterpart in the reference. */

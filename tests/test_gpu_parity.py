@@ -319,6 +319,36 @@ def test_autotune_picks_a_shape_and_keeps_results(cuda):
     assert cuda.equal(a, b)
 
 
+@pytest.mark.parametrize("det", [True, False])
+def test_alg_shapes_are_bitwise_equal_on_mixed_classes(cuda, det):
+    """The three ALG pair-kernel shapes give bitwise the same step on a system of mixed
+    classes (hyperbolae, ellipses, near-unit eccentricity): 8-warp CTAs with per-lane class
+    loops, and phase-locked 16- and 32-warp CTAs whose class loops pack the lanes' last pairs
+    of a class into shared turns (each row and each column still adds its pairs in the same
+    order).  Atomic mode is compared to rounding.  The step matches the oracle."""
+    n = 3000
+    s, eps, q = initial.coulomb_cube(n, seed=31)
+    cfg = default_config(eps_th=eps, dt=1e-5)
+    cfg.deterministic = 1 if det else 0
+    outs = []
+    with BIASolver() as solver:
+        qt = cuda.tensor(q, device="cuda")
+        for shape in ("tiles8", "phase16", "phase32"):
+            solver.set_shape(METHOD_ALG, n, shape, deterministic=det)
+            t = cuda.tensor(s, device="cuda")
+            st = solver.step(t, cfg, q=qt)
+            assert st["hyperbola"] > 0 and st["ellipse"] > 0 and st["universal"] > 0
+            outs.append(t.cpu().numpy())
+        solver.set_shape(METHOD_ALG, n, None, deterministic=det)
+    for o in outs[1:]:
+        if det:
+            assert np.array_equal(outs[0], o)
+        else:
+            assert rel_err(o, outs[0]) <= 1e-15
+    ref, _, _ = oracle.bia_step(s, eps, 1e-5, q=q)
+    assert_parity(outs[0], ref)
+
+
 def test_bounded_device_wait_reports_timeout(cuda):
     """A device-side wait that nothing completes gives up after its limit and the step API
     reports BIA_ERR_DEVICE_TIMEOUT; the context then runs a normal step."""
