@@ -204,40 +204,80 @@ __global__ void __launch_bounds__(kEnsThreads, 2) ens_pair_rest_kernel(const Ens
     if (nblk > 0) flush_counters(tot, A.stats, lane);
 }
 
-// Learned step over the item table, third kernel: one warp per listed item (persistent 8-warp
-// CTAs), its deferred pairs from their guesses added onto the rest kernel's partials.
+// Learned step over the item table, third kernel (persistent 8-warp CTAs): a dense or
+// diagonal item finished by one warp, then the sparse ones in chunks of 32 list entries and
+// batches of 32 pairs, as bia_pair_learned_finish_kernel (each system bitwise its own step).
 __global__ void __launch_bounds__(kEnsThreads, 2) ens_pair_learned_finish_kernel(const EnsArgs A)
 {
     __shared__ double s_fin[kTileWarps][kTileSmemDoubles];
+    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const long long count = (long long)*A.R.nlist;
     PairCounters tot;
     counters_zero(tot);
-    int nblk = 0;
+    int nchunk = 0;
+    // the system, block and partials of list entry e
+    auto resolve_entry = [&](long long e) {
+        const uint2 it = A.items[A.R.entries[e].x];
+        const int s = (int)it.x;
+        const int base = A.off[s];
+        const int n = A.off[s + 1] - base;
+        FinishBlock F;
+        F.B = {A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base,
+               A.q ? A.q + base : nullptr, n, A.eps[s], A.P.dt, A.heads};
+        F.bi = (int)(it.y & 0xffffu);
+        F.bj = (int)(it.y >> 16);
+        F.part = A.part + A.part_off[s];
+        F.plane = (size_t)((n + 31) / 32) * 32;
+        return F;
+    };
+    // 1. the dense and diagonal items, one per warp
     for (long long e = (long long)blockIdx.x * kEnsWarps + warp; e < count;
          e += (long long)gridDim.x * kEnsWarps) {  // warp-uniform
         const uint2 it = A.items[A.R.entries[e].x];
-        const int s = (int)it.x;
-        const int bi = (int)(it.y & 0xffffu), bj = (int)(it.y >> 16);
-        const int base = A.off[s];
-        const int n = A.off[s + 1] - base;
-        const LearnedBlockIn B = {A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base,
-                                  A.q ? A.q + base : nullptr, n, A.eps[s], A.P.dt, A.heads};
+        if ((it.y & 0xffffu) != (it.y >> 16) && A.R.entries[e].w <= (unsigned)kBatchPairs) continue;
+        const FinishBlock F = resolve_entry(e);
         double racc[6], cacc[6];
         PairCounters cnt;
         bool row_hit, col_hit;
-        finish_block_solve(A.R, e, B, bi, bj, lane, s_fin[warp], racc, cacc, cnt, row_hit, col_hit);
+        finish_block_solve(A.R, e, F.B, F.bi, F.bj, lane, s_fin[warp], racc, cacc, cnt, row_hit, col_hit);
         counters_add(tot, cnt);
-        if (++nblk == kFlushBlocks) {
+        if (++nchunk == kFlushBlocks) {
             flush_counters(tot, A.stats, lane);
             counters_zero(tot);
-            nblk = 0;
+            nchunk = 0;
         }
-        const int nb = (n + 31) / 32;
-        add_partials(A.part + A.part_off[s], (size_t)nb * 32, bi, bj, lane, racc, cacc, row_hit, col_hit);
+        add_partials(F.part, F.plane, F.bi, F.bj, lane, racc, cacc, row_hit, col_hit);
     }
-    if (nblk > 0) flush_counters(tot, A.stats, lane);
+    // 2. the sparse ones, batched per chunk of list entries (up to 32 per warp, fewer when the
+    // list is short)
+    const long long nwarps = (long long)gridDim.x * kEnsWarps;
+    const long long chunk = count >= 32 * nwarps ? 32 : (count + nwarps - 1) / nwarps;
+    for (long long c0 = ((long long)blockIdx.x * kEnsWarps + warp) * chunk; c0 < count;
+         c0 += nwarps * chunk) {  // warp-uniform
+        const long long e = c0 + lane;
+        const bool valid = lane < chunk && e < count;
+        unsigned int npairs = 0u;
+        bool sparse = false;
+        if (valid) {
+            npairs = A.R.entries[e].w;
+            const uint2 it = A.items[A.R.entries[e].x];
+            sparse = (it.y & 0xffffu) != (it.y >> 16) && npairs <= (unsigned)kBatchPairs;
+        }
+        if (__ballot_sync(full, sparse) == 0u) continue;
+        auto resolve = [&](int l) { return resolve_entry(c0 + l); };
+        PairCounters cnt;
+        counters_zero(cnt);
+        finish_batches<true>(A.R, c0, sparse, npairs, lane, resolve, cnt);
+        counters_add(tot, cnt);
+        if (++nchunk == kFlushBlocks) {
+            flush_counters(tot, A.stats, lane);
+            counters_zero(tot);
+            nchunk = 0;
+        }
+    }
+    if (nchunk > 0) flush_counters(tot, A.stats, lane);
 }
 
 // Once per device: shared-memory opt-in of the ensemble's rest kernel (the head kernel is the
@@ -386,7 +426,8 @@ static int ens_pair_launch(bia_context *ctx, bia_ensemble *E, EnsArgs &A, int me
         A.R.nlist = (unsigned int *)(b + 16);
         A.R.entries = (uint4 *)(b + kSplitHeader);
         A.R.masks = (uint32_t *)(b + kSplitHeader + (size_t)E->nitems * 16);
-        uint32_t *rows = (uint32_t *)(b + kSplitHeader + (size_t)E->nitems * (16 + 64 * sizeof(uint32_t)));
+        A.R.pairs = (uint2 *)(b + kSplitHeader + (size_t)E->nitems * (16 + 64 * sizeof(uint32_t)));
+        uint32_t *rows = (uint32_t *)(b + kSplitHeader + (size_t)E->nitems * kListBytesPerBlock);
         A.R.rows_cap = E->rows_cap;
         A.R.rows[kHeadEll] = rows;
         A.R.rows[kHeadHyp] = rows + E->rows_cap;
@@ -532,7 +573,7 @@ extern "C" int bia_ensemble_create(bia_context *ctx, int nsys, const int *sizes,
         unsigned long long pairs = 0;
         for (int s2 = 0; s2 < nsys; s2++) pairs += (unsigned long long)sizes[s2] * (sizes[s2] - 1) / 2;
         E->rows_cap = (unsigned int)(pairs < (1ull << 27) ? (pairs > 0 ? pairs : 1) : (1ull << 27));
-        ENS_ALLOC(E->d_split, kSplitHeader + (size_t)nitems * (16 + 64 * sizeof(uint32_t)) +
+        ENS_ALLOC(E->d_split, kSplitHeader + (size_t)nitems * kListBytesPerBlock +
                                   (size_t)kMlpHeads * E->rows_cap * sizeof(uint32_t));
     }
 #undef ENS_ALLOC

@@ -90,11 +90,18 @@ struct LearnedRows {
     uint32_t *rows[kMlpHeads];   // per head (kHeadEll, kHeadHyp): packed BF16 inputs, then FP32 guesses
     unsigned long long *counts;  // [kMlpHeads] rows taken this step (may run past rows_cap)
     unsigned int *nlist;         // listed warp-blocks
-    uint4 *entries;              // per listed warp-block: (item, row base ell, row base hyp, 0)
+    uint4 *entries;              // per listed warp-block: (item, row base ell, row base hyp, pairs)
     uint32_t *masks;             // per listed warp-block: [kMlpHeads][32] lane masks
+    uint2 *pairs;                // per listed warp-block with at most kBatchPairs pairs: [kBatchPairs]
+                                 // (row or kNoRows, lane | k << 5 | head << 10) in solve order
     unsigned int rows_cap;
 };
 constexpr unsigned int kNoRows = 0xffffffffu;
+// A listed warp-block with at most this many deferred pairs (and off the diagonal) is
+// finished in a batch with other such blocks, one pair per lane.
+constexpr int kBatchPairs = 32;
+// list bytes per warp-block: the entry, the masks, the pair descriptors
+constexpr size_t kListBytesPerBlock = 16 + 64 * sizeof(uint32_t) + kBatchPairs * sizeof(uint2);
 // the buffer's header: the two row counts (u64) and the list length (u32), 32 bytes
 constexpr size_t kSplitHeader = 32;
 
@@ -231,10 +238,33 @@ __device__ __forceinline__ void rest_block_defer(const LearnedRows &R, unsigned 
     unsigned int e = 0u;
     if (lane == 0) e = atomicAdd(R.nlist, 1u);
     e = __shfl_sync(full, e, 0);
+    const unsigned int npairs = tot[kHeadEll] + tot[kHeadHyp];
     if (lane == 0)
-        R.entries[e] = make_uint4(item, fits ? base[kHeadEll] : kNoRows, fits ? base[kHeadHyp] : kNoRows, 0u);
+        R.entries[e] = make_uint4(item, fits ? base[kHeadEll] : kNoRows, fits ? base[kHeadHyp] : kNoRows, npairs);
     R.masks[(size_t)e * 64 + lane] = mask[kHeadEll];
     R.masks[(size_t)e * 64 + 32 + lane] = mask[kHeadHyp];
+    if (npairs <= (unsigned)kBatchPairs) {
+        // the pairs in the order the per-block finish solves them: round r holds the r-th pair
+        // (in k order) of every lane with more than r, lanes in order
+        const uint32_t both = mask[kHeadEll] | mask[kHeadHyp];
+        uint32_t left = both;
+        unsigned int at = 0u;
+        for (;;) {
+            const unsigned rm = __ballot_sync(full, left != 0u);
+            if (rm == 0u) break;
+            if (left) {
+                const int k = __ffs(left) - 1;
+                left &= left - 1u;
+                const int hd = ((mask[kHeadHyp] >> k) & 1u) ? kHeadHyp : kHeadEll;
+                const unsigned int row =
+                    fits ? base[hd] + pre[hd] + (unsigned)__popc(mask[hd] & ((1u << k) - 1u)) : kNoRows;
+                const unsigned int pos = at + (unsigned)__popc(rm & ((1u << lane) - 1u));
+                R.pairs[(size_t)e * kBatchPairs + pos] = make_uint2(row, (unsigned)lane | ((unsigned)k << 5) |
+                                                                              ((unsigned)hd << 10));
+            }
+            at += (unsigned)__popc(rm);
+        }
+    }
 }
 
 // The system a warp-block belongs to: particles x..w[0, n) (and charges q), coupling eps_th.
@@ -487,6 +517,55 @@ __device__ __forceinline__ bool learned_block_solve(const LearnedSmem &M, const 
     return timed_out;
 }
 
+// One deferred pair (row state si, column state sc) from its head's guess in row `row` of
+// head is_h (kNoRows: no row, the plain solver): the FP32 correction and FP64 step, or the
+// plain universal-variable solver where the guess does not settle; counted in cnt.
+__device__ __forceinline__ void finish_pair(const LearnedRows &R, const LearnedBlockIn &B, const double si[7],
+                                            const double sc[7], bool is_h, unsigned int row, double h[6],
+                                            PairCounters &cnt)
+{
+    double r[3], g[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        r[c] = si[c] - sc[c];
+        g[c] = si[3 + c] - sc[3 + c];
+    }
+    const double eps_ij = B.q ? B.eps_th * si[6] * sc[6] : B.eps_th;
+    bool done = false;
+    if (row != kNoRows) {
+        const float yg = __uint_as_float(R.rows[is_h ? kHeadHyp : kHeadEll][row]);
+        LearnedPair L;
+        learned_prepare(eps_ij, B.dt, r, g, L, is_h ? kLearnedHyp : kLearnedEll);
+        bool coarse = true;
+        int fp32_steps = 0;
+        done = learned_finish(L, B.dt, yg, r, g, h, coarse, fp32_steps);
+        cnt.learned++;
+        cnt.learned_fp32 += fp32_steps;
+        if (coarse) cnt.learned_coarse++;
+        if (!done) cnt.learned_fallbacks++;
+    }
+    if (!done) {
+        const int it = uv_halfdisp(eps_ij, B.dt, r, g, h);
+        cnt.it_uv += it;
+        if (it > kUvItMax) cnt.nonconverged++;
+    }
+    cnt.cls[is_h ? kHyperbola : kEllipse]++;
+    count_nonfinite(h, cnt);
+}
+
+// finish_pair for the batched path, compiled once per file: the per-block path inlines
+// finish_pair into its own loop, and the compiler may contract the FP64 expressions of an
+// inlined copy differently in different places (so the single-system and the ensemble
+// kernels, whose batched paths differ around the call, would not give the same bits); one
+// out-of-line body gives every kernel the same bits for a batched pair.  Batched pairs are
+// few (at most kBatchPairs per warp-block), so the call costs little.
+static __device__ __noinline__ void finish_pair_batched(const LearnedRows &R, const LearnedBlockIn &B,
+                                                        const double si[7], const double sc[7], bool is_h,
+                                                        unsigned int row, double h[6], PairCounters &cnt)
+{
+    finish_pair(R, B, si, sc, is_h, row, h, cnt);
+}
+
 // The finish kernel's work on listed warp-block e (item resolved by the caller to the system
 // B and the block (bi, bj)): every deferred pair from its head's guess, with the column
 // states and sums in the warp's slice ws.  Returns the row sums racc and column sums cacc of
@@ -534,7 +613,6 @@ __device__ __forceinline__ void finish_block_solve(const LearnedRows &R, long lo
 #pragma unroll
     for (int c = 0; c < 6; c++) racc[c] = 0.0;
     counters_zero(cnt);
-    const bool hq = B.q != nullptr;
     uint32_t m = mh | me;
     for (;;) {
         const bool busy = (m != 0u);
@@ -545,36 +623,16 @@ __device__ __forceinline__ void finish_block_solve(const LearnedRows &R, long lo
             m &= m - 1u;
             const bool is_h = (mh >> k) & 1u;
             const int j = (lane + k) & 31;
-            double r[3], g[3], h[6];
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                r[c] = si[c] - ws[c * 32 + j];
-                g[c] = si[3 + c] - ws[(3 + c) * 32 + j];
-            }
-            const double eps_ij = hq ? B.eps_th * si[6] * ws[6 * 32 + j] : B.eps_th;
-            bool done = false;
+            unsigned int row = kNoRows;
             if (have_rows) {
                 const uint32_t below = (1u << k) - 1u;
-                const unsigned int row = is_h ? ent.z + pre[kHeadHyp] + (unsigned)__popc(mh & below)
-                                              : ent.y + pre[kHeadEll] + (unsigned)__popc(me & below);
-                const float yg = __uint_as_float(R.rows[is_h ? kHeadHyp : kHeadEll][row]);
-                LearnedPair L;
-                learned_prepare(eps_ij, B.dt, r, g, L, is_h ? kLearnedHyp : kLearnedEll);
-                bool coarse = true;
-                int fp32_steps = 0;
-                done = learned_finish(L, B.dt, yg, r, g, h, coarse, fp32_steps);
-                cnt.learned++;
-                cnt.learned_fp32 += fp32_steps;
-                if (coarse) cnt.learned_coarse++;
-                if (!done) cnt.learned_fallbacks++;
+                row = is_h ? ent.z + pre[kHeadHyp] + (unsigned)__popc(mh & below)
+                           : ent.y + pre[kHeadEll] + (unsigned)__popc(me & below);
             }
-            if (!done) {
-                const int it = uv_halfdisp(eps_ij, B.dt, r, g, h);
-                cnt.it_uv += it;
-                if (it > kUvItMax) cnt.nonconverged++;
-            }
-            cnt.cls[is_h ? kHyperbola : kEllipse]++;
-            count_nonfinite(h, cnt);
+            double sc[7], h[6];
+#pragma unroll
+            for (int c = 0; c < 7; c++) sc[c] = ws[c * 32 + j];
+            finish_pair(R, B, si, sc, is_h, row, h, cnt);
 #pragma unroll
             for (int c = 0; c < 6; c++) racc[c] += h[c];
             add_column(wacc, j, h, bm, lane);
@@ -584,6 +642,100 @@ __device__ __forceinline__ void finish_block_solve(const LearnedRows &R, long lo
 #pragma unroll
     for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
     __syncwarp();  // the slice is reused by this warp's next block
+}
+
+// A listed warp-block as the batched finish sees it: its system, its block and where its
+// partial slots live (deterministic: part[m][6][plane]; atomic: one accumulator plane).
+struct FinishBlock {
+    LearnedBlockIn B;
+    int bi, bj;
+    double *part;
+    size_t plane;
+};
+
+// Batched finish of the sparse listed warp-blocks among the 32 list entries of a chunk (lane
+// l holds entry l: sparse says whether it is one of them, npairs its deferred pairs).  The
+// sparse blocks' pairs are laid end to end and taken 32 at a time, one per lane, each block
+// whole within one batch.  A block's pairs sit in the per-block finish's solve order (its
+// descriptors), and its row and column sums are added in lane order from zero and then onto
+// the slots once, as the per-block finish adds them; which blocks share a batch does not
+// change any block's sums, so the step stays deterministic.  resolve(l) gives the
+// FinishBlock of the chunk's entry l.  Every lane of the warp calls it.
+template <bool kDeterministic, class Resolve>
+__device__ __forceinline__ void finish_batches(const LearnedRows &R, long long first_entry, bool sparse,
+                                               unsigned int npairs, int lane, const Resolve &resolve,
+                                               PairCounters &cnt)
+{
+    const unsigned full = 0xffffffffu;
+    const int c = sparse ? (int)npairs : 0;
+    int incl = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int o = __shfl_up_sync(full, incl, d);
+        if (lane >= d) incl += o;
+    }
+    const int total = __shfl_sync(full, incl, 31);
+    int done = 0;
+    while (done < total) {  // warp-uniform
+        // this batch: the blocks whose pairs end within done + 32
+        const unsigned bm = __ballot_sync(full, c > 0 && incl > done && incl <= done + kBatchPairs);
+        const int upto = __shfl_sync(full, incl, 31 - __clz(bm));
+        const int qp = done + lane;
+        const bool act = qp < upto;
+        // the block of pair qp: the first lane whose prefix passes it
+        int lo = 0, hi = 31;
+#pragma unroll
+        for (int it = 0; it < 5; it++) {
+            const int mid = (lo + hi) >> 1;
+            if (__shfl_sync(full, incl, mid) > qp) hi = mid;
+            else lo = mid + 1;
+        }
+        const int own = lo;
+        const int own_start = __shfl_sync(full, incl - c, own);
+        double h[6] = {0, 0, 0, 0, 0, 0};
+        unsigned int row_key = 0u, col_key = 0u;
+        int l = 0, j = 0;
+        FinishBlock F{};
+        if (act) {
+            F = resolve(own);
+            const uint2 d = R.pairs[(size_t)(first_entry + own) * kBatchPairs + (qp - own_start)];
+            l = (int)(d.y & 31u);
+            const int k = (int)((d.y >> 5) & 31u);
+            const bool is_h = ((d.y >> 10) & 1u) == (unsigned)kHeadHyp;
+            j = (l + k) & 31;
+            double si[7], sc[7];
+            load_particle(F.B.x, F.B.y, F.B.z, F.B.u, F.B.v, F.B.w, F.B.q, F.B.n, F.bi * 32 + l, si);
+            load_particle(F.B.x, F.B.y, F.B.z, F.B.u, F.B.v, F.B.w, F.B.q, F.B.n, F.bj * 32 + j, sc);
+            finish_pair_batched(R, F.B, si, sc, is_h, d.x, h, cnt);
+            row_key = ((unsigned)own << 6) | (unsigned)l;
+            col_key = ((unsigned)own << 6) | 32u | (unsigned)j;
+        }
+        const unsigned am = __ballot_sync(full, act);
+        if (act) {
+#pragma unroll
+            for (int pass = 0; pass < 2; pass++) {
+                const unsigned grp = __match_any_sync(am, pass == 0 ? row_key : col_key);
+                double sum[6] = {0, 0, 0, 0, 0, 0};
+                for (unsigned m = grp; m; m &= m - 1u) {  // members in lane order (grp-uniform)
+                    const int src = __ffs(m) - 1;
+#pragma unroll
+                    for (int cc = 0; cc < 6; cc++) sum[cc] += __shfl_sync(grp, h[cc], src);
+                }
+                if (lane == 31 - __clz(grp)) {  // the group's last lane adds the sum once
+                    const int p = pass == 0 ? F.bi * 32 + l : F.bj * 32 + j;
+                    const size_t m0 = kDeterministic ? (size_t)(pass == 0 ? F.bj : F.bi) * 6 * F.plane : 0;
+#pragma unroll
+                    for (int cc = 0; cc < 6; cc++) {
+                        double *slot = F.part + m0 + (size_t)cc * F.plane + p;
+                        const double v = pass == 0 ? sum[cc] : -sum[cc];
+                        if (kDeterministic) *slot += v;
+                        else atomicAdd(slot, v);
+                    }
+                }
+            }
+        }
+        done = upto;
+    }
 }
 
 // The head kernel's pass over the rows of head hd (every thread of the CTA calls it, between

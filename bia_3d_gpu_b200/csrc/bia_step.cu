@@ -396,36 +396,79 @@ __global__ void __launch_bounds__(kMlpThreads, 2) bia_pair_learned_head_kernel(c
     if (!ok && threadIdx.x == 0) atomicAdd(&stats[kStatTimeouts], 1ull);
 }
 
-// Split learned step, third kernel: one warp per listed warp-block (persistent 8-warp CTAs,
-// no CTA barrier), its deferred pairs from their guesses added onto the partials.
+// Split learned step, third kernel (persistent 8-warp CTAs, no CTA barrier).  A warp-block
+// with many deferred pairs (or on the diagonal) is finished by one warp, one lane per row, the
+// list entries spread over the warps one at a time; the others, with at most kBatchPairs
+// pairs, are then taken in chunks of 32 list entries, laid end to end and finished 32 pairs
+// at a time (finish_batches).  Whether a block is batched depends on the block alone, so
+// the step stays deterministic.  (With one warp per warp-block, the Coulomb cube's ~3e5
+// listed blocks of one or two pairs each kept a warp for a whole solve per block: 1.0 ms per
+// step.)
+
 template <bool kDeterministic>
 __global__ void __launch_bounds__(kThreads, 2) bia_pair_learned_finish_kernel(const StepArgs A)
 {
     __shared__ double s_fin[kTileWarps][kTileSmemDoubles];
+    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const long long count = (long long)*A.R.nlist;
     const LearnedBlockIn B = {A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P.dt, A.heads};
     PairCounters tot;
     counters_zero(tot);
-    int nblk = 0;
+    int nflush = 0;
+    // 1. the dense and diagonal warp-blocks, one per warp
     for (long long e = (long long)blockIdx.x * kWarpsPerBlock + warp; e < count;
          e += (long long)gridDim.x * kWarpsPerBlock) {  // warp-uniform
+        const uint4 ent = A.R.entries[e];
         int bi, bj;
-        warp_block_coords((long long)A.R.entries[e].x, bi, bj);
+        warp_block_coords((long long)ent.x, bi, bj);
+        if (bi != bj && ent.w <= (unsigned)kBatchPairs) continue;  // batched below
         double racc[6], cacc[6];
         PairCounters cnt;
         bool row_hit, col_hit;
         finish_block_solve(A.R, e, B, bi, bj, lane, s_fin[warp], racc, cacc, cnt, row_hit, col_hit);
         counters_add(tot, cnt);
-        if (++nblk == kFlushBlocks) {
+        if (++nflush == kFlushBlocks) {
             flush_counters(tot, A.stats, lane);
             counters_zero(tot);
-            nblk = 0;
+            nflush = 0;
         }
         add_learned_sums<kDeterministic>(A, bi, bj, lane, racc, cacc, false, row_hit, col_hit);
     }
-    if (nblk > 0) flush_counters(tot, A.stats, lane);
+    // 2. the sparse ones, batched per chunk of list entries: up to 32 per warp, fewer when the
+    // list is short, so that every warp has a chunk (a block's sums do not depend on the blocks
+    // batched with it)
+    const long long nwarps = (long long)gridDim.x * kWarpsPerBlock;
+    const long long chunk = count >= 32 * nwarps ? 32 : (count + nwarps - 1) / nwarps;
+    for (long long c0 = ((long long)blockIdx.x * kWarpsPerBlock + warp) * chunk; c0 < count;
+         c0 += nwarps * chunk) {  // warp-uniform
+        const long long e = c0 + lane;
+        const bool valid = lane < chunk && e < count;
+        const uint4 ent = valid ? A.R.entries[e] : make_uint4(0u, 0u, 0u, 0u);
+        int bi = 0, bj = 0;
+        if (valid) warp_block_coords((long long)ent.x, bi, bj);
+        const bool sparse = valid && bi != bj && ent.w <= (unsigned)kBatchPairs;
+        if (__ballot_sync(full, sparse) == 0u) continue;
+        auto resolve = [&](int l) {
+            FinishBlock F;
+            F.B = B;
+            warp_block_coords((long long)A.R.entries[c0 + l].x, F.bi, F.bj);
+            F.part = A.part;
+            F.plane = (size_t)A.npad;
+            return F;
+        };
+        PairCounters cnt;
+        counters_zero(cnt);
+        finish_batches<kDeterministic>(A.R, c0, sparse, ent.w, lane, resolve, cnt);
+        counters_add(tot, cnt);
+        if (++nflush == kFlushBlocks) {
+            flush_counters(tot, A.stats, lane);
+            counters_zero(tot);
+            nflush = 0;
+        }
+    }
+    if (nflush > 0) flush_counters(tot, A.stats, lane);
 }
 
 // Once per device: dynamic shared memory opt-in of the learned kernels; returns the grid of
@@ -511,8 +554,7 @@ static unsigned int rows_cap(long long nwb)
 }
 static size_t split_buffer_bytes(long long nwb)
 {
-    return kSplitHeader + (size_t)nwb * (16 + 64 * sizeof(uint32_t)) +
-           (size_t)kMlpHeads * rows_cap(nwb) * sizeof(uint32_t);
+    return kSplitHeader + (size_t)nwb * kListBytesPerBlock + (size_t)kMlpHeads * rows_cap(nwb) * sizeof(uint32_t);
 }
 
 static void split_buffer_carve(void *base, long long nwb, StepArgs &A)
@@ -523,7 +565,8 @@ static void split_buffer_carve(void *base, long long nwb, StepArgs &A)
     A.R.nlist = (unsigned int *)(b + 16);
     A.R.entries = (uint4 *)(b + kSplitHeader);
     A.R.masks = (uint32_t *)(b + kSplitHeader + (size_t)nwb * 16);
-    uint32_t *rows = (uint32_t *)(b + kSplitHeader + (size_t)nwb * (16 + 64 * sizeof(uint32_t)));
+    A.R.pairs = (uint2 *)(b + kSplitHeader + (size_t)nwb * (16 + 64 * sizeof(uint32_t)));
+    uint32_t *rows = (uint32_t *)(b + kSplitHeader + (size_t)nwb * kListBytesPerBlock);
     A.R.rows_cap = rows_cap(nwb);
     A.R.rows[kHeadEll] = rows;
     A.R.rows[kHeadHyp] = rows + A.R.rows_cap;

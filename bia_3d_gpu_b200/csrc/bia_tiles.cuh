@@ -146,26 +146,43 @@ __device__ __forceinline__ void balanced_class_loop(unsigned m, const double *rs
     const unsigned full = 0xffffffffu;
     const unsigned lt = (1u << lane) - 1u;
     const int total = (int)__reduce_add_sync(full, (unsigned)__popc(m));
+    const int most = (int)__reduce_max_sync(full, (unsigned)__popc(m));
+    // packing saves turns only when the busiest lane has more than ceil(total / 32) pairs;
+    // otherwise (every round full, as on an all-hyperbolic system) each lane solves its own
+    // pairs in order and adds its own row directly: the same schedule and sums.  (The
+    // per-lane loop with rows in registers as a second copy of the solver here spilled more
+    // and was slower on the mixed classes.)
+    const bool packed = most * 32 > total + 31;  // warp-uniform
+    const int nturns = packed ? (total + 31) / 32 : most;
     int rbase = 0;                          // enumeration index of the current round's first pair
     unsigned cur = m;                       // this lane's pairs not in a finished round
     unsigned rm = __ballot_sync(full, cur != 0u);  // lanes of the current round
-    for (int base = 0; base < total; base += 32) {
-        const int q = base + lane;
+    for (int turn = 0; turn < nturns; turn++) {
         int o = -1, k = 0;
-        while (rm != 0u) {  // the rounds this turn covers (warp-uniform)
-            const int nr = __popc(rm);
-            const int idx = q - rbase;
-            const bool here = idx >= 0 && idx < nr;
-            const int src = here ? (int)__fns(rm, 0, idx + 1) : 0;
-            const int kk = __shfl_sync(full, __ffs(cur) - 1, src);  // the owner's pair of this round
-            if (here) {
-                o = src;
-                k = kk;
+        if (!packed) {
+            if (cur) {
+                o = lane;
+                k = __ffs(cur) - 1;
+                cur &= cur - 1u;
             }
-            if (rbase + nr > base + 32) break;  // the round goes on in the next turn
-            rbase += nr;
-            if ((rm >> lane) & 1u) cur &= cur - 1u;
-            rm = __ballot_sync(full, cur != 0u);
+        } else {
+            const int base = turn * 32;
+            const int q = base + lane;
+            while (rm != 0u) {  // the rounds this turn covers (warp-uniform)
+                const int nr = __popc(rm);
+                const int idx = q - rbase;
+                const bool here = idx >= 0 && idx < nr;
+                const int src = here ? (int)__fns(rm, 0, idx + 1) : 0;
+                const int kk = __shfl_sync(full, __ffs(cur) - 1, src);  // the owner's pair of this round
+                if (here) {
+                    o = src;
+                    k = kk;
+                }
+                if (rbase + nr > base + 32) break;  // the round goes on in the next turn
+                rbase += nr;
+                if ((rm >> lane) & 1u) cur &= cur - 1u;
+                rm = __ballot_sync(full, cur != 0u);
+            }
         }
         const bool busy = o >= 0;
         const unsigned bm = __ballot_sync(full, busy);
@@ -186,7 +203,10 @@ __device__ __forceinline__ void balanced_class_loop(unsigned m, const double *rs
             } else {
                 alg_conic_pair<C>(P, eps_ij, r, g, h, cnt);
             }
-            {
+            if (!packed) {  // the lane's own row
+#pragma unroll
+                for (int c = 0; c < 6; c++) racs[c * 32 + o] += h[c];
+            } else {
                 const unsigned grp = __match_any_sync(bm, o);
                 const int rank = __popc(grp & lt);
                 const int turns = (int)__reduce_max_sync(bm, (unsigned)__popc(grp));
