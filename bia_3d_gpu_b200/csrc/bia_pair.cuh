@@ -871,7 +871,7 @@ __device__ __forceinline__ UvSeries uv_series(const UvPair &p, double dt)
     constexpr double Q = 3e-4;
     const bool small = fabs(y) <= Q && fabs(q.c2) <= Q * Q && fabs(c3) <= Q * Q * Q && fabs(c4) <= Q * Q * Q * Q;
     q.S = 1.0 + (q.c2 - y + (c3 + c4));
-    q.exact = small && __dmul_rn(q.x, q.S) > 0.0;
+    q.exact = small && q.S > 0.0 && dt > 0.0;  // s = x S > 0
     return q;
 }
 
@@ -888,7 +888,8 @@ __device__ __forceinline__ double uv_series_start(const UvSeries &q)
 //   (f - 1)/2 = K A,  (g - dt)/2 = K dt B,  (g' - 1)/2 = K A rho,  f'/2 = -(m/2)(x/r0) S c1 rho,
 // and r(s)/r0 = 1 + d with d = -w S^2 c2 + 2 y S c1 - 2 K A (r(s) = r0 c0 + sig s c1 +
 // mu s^2 c2 and c0 = 1 - beta s^2 c2), formed without cancellation.  rho is the alternating
-// series of 1/(1 + d) to d^6 where |d| <= 1e-3 (truncation below 1e-21), else a division.
+// series of 1/(1 + d) to d^5 where |d| <= 1e-3 (truncation below 1e-18), else a division.
+// f'/2 is formed as (K/dt) S c1 rho (K/dt = -(m/2) x/r0) with 1/dt taken once.
 // The factor 1/2 of the half-displacement is inside K (a power of two: the same bits).
 __device__ __forceinline__ void uv_compose_series(const UvPair &p, const UvSeries &q, double dt, const double r[3],
                                                   const double g[3], double h[6])
@@ -907,12 +908,12 @@ __device__ __forceinline__ void uv_compose_series(const UvPair &p, const UvSerie
     double rho;
     if (fabs(d) <= 1e-3) {
         const double nd = -d;
-        rho = fma(nd, fma(nd, fma(nd, fma(nd, fma(nd, fma(nd, 1.0, 1.0), 1.0), 1.0), 1.0), 1.0), 1.0);
+        rho = fma(nd, fma(nd, fma(nd, fma(nd, fma(nd, 1.0, 1.0), 1.0), 1.0), 1.0), 1.0);
     } else {
         rho = 1.0 / (1.0 + d);
     }
     const double gdm1 = __dmul_rn(fm1, rho);
-    const double fdot = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(q.mh, __dmul_rn(q.x, p.ir0)), S), c[1]), rho);
+    const double fdot = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(K, 1.0 / dt), S), c[1]), rho);
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         h[k] = fma(fm1, r[k], __dmul_rn(gmdt, g[k]));
