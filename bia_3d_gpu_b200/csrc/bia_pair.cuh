@@ -889,7 +889,7 @@ __device__ __forceinline__ double uv_series_start(const UvSeries &q)
 // and r(s)/r0 = 1 + d with d = -w S^2 c2 + 2 y S c1 - 2 K A (r(s) = r0 c0 + sig s c1 +
 // mu s^2 c2 and c0 = 1 - beta s^2 c2), formed without cancellation.  rho is the alternating
 // series of 1/(1 + d) to d^5 where |d| <= 1e-3 (truncation below 1e-18), else a division.
-// f'/2 is formed as (K/dt) S c1 rho (K/dt = -(m/2) x/r0) with 1/dt taken once.
+// f'/2 is formed as (K/dt) S c1 rho (K/dt = -(m/2) x/r0; 1/dt is the same for every pair).
 // The factor 1/2 of the half-displacement is inside K (a power of two: the same bits).
 __device__ __forceinline__ void uv_compose_series(const UvPair &p, const UvSeries &q, double dt, const double r[3],
                                                   const double g[3], double h[6])
