@@ -608,7 +608,7 @@ def main():
     if (method == 1 or (method != 1 and not args.no_plain)) and not args.no_autotune:
         cfg_alg = default_config(eps_th=eps, dt=dt, method=1)
         var, tms = solver.autotune(d_state, cfg_alg, q=d_q)
-        tuned = {"alg_shape": ("tiles8", "phase16", "phase32")[var], "ms": tms}
+        tuned = {"alg_shape": ("tiles8", "phase32_lane", "phase32")[var], "ms": tms}
     if method == 3 and not args.no_autotune:
         lvar, lms = solver.autotune(d_state, cfg, q=d_q)
         tuned = dict(tuned or {}, learned_layout=("one_kernel", "split")[lvar], learned_ms=lms)
@@ -663,8 +663,9 @@ def main():
                        "bia_pair_learned_finish_kernel<true> (one timed interval)"
                        if split else "bia_pair_learned_kernel<true>")
     elif method == 1 and tuned is not None:
-        kernel_name = {"tiles8": "bia_pair_tiles_kernel<true, 1>", "phase16": "bia_pair_phase_kernel<true, 16, 2>",
-                       "phase32": "bia_pair_phase_kernel<true, 32, 1>"}[tuned["alg_shape"]]
+        kernel_name = {"tiles8": "bia_pair_tiles_kernel<true, 1>",
+                       "phase32_lane": "bia_pair_phase_kernel<true, 32, 1, false>",
+                       "phase32": "bia_pair_phase_kernel<true, 32, 1, true>"}[tuned["alg_shape"]]
     elif method == 1 and (nwb + 31) // 32 >= 2 * sms:
         kernel_name = "bia_pair_phase_kernel<true, 32, 1>"
     else:

@@ -325,15 +325,15 @@ class BIASolver:
         self._leave(cur)
         capi.check(st, "bia_context_autotune")
         names = (("one_kernel", "split", "-") if cfg.method == capi.METHOD_LEARNED
-                 else ("tiles8", "phase16", "phase32"))
+                 else ("tiles8", "phase32_lane", "phase32"))
         return var.value, {names[k]: float(ms[k]) for k in range(3) if ms[k] >= 0}
 
     def set_shape(self, method, n, shape, deterministic=True):
-        """Pin the pair-kernel shape of `method` (ALG: "tiles8", "phase16", "phase32";
+        """Pin the pair-kernel shape of `method` (ALG: "tiles8", "phase32_lane", "phase32";
         learned: "one_kernel", "split"; None: the default rule) for sizes in n's
         floor(log2 n) bucket, as autotune would store it."""
         names = (("one_kernel", "split") if method == capi.METHOD_LEARNED
-                 else ("tiles8", "phase16", "phase32"))
+                 else ("tiles8", "phase32_lane", "phase32"))
         var = -1 if shape is None else names.index(shape)
         capi.check(capi.lib().bia_context_set_shape(self._ctx, int(method), int(bool(deterministic)), int(n), var),
                    "bia_context_set_shape")
@@ -461,7 +461,7 @@ class Ensemble:
             return None
         return s._finish(st, st_, "bia_ensemble_run")
 
-    SHAPES = {1: ("tiles8", "phase16", "phase32"), 2: ("item_per_warp", "persistent"),
+    SHAPES = {1: ("tiles8", "phase32_lane", "phase32"), 2: ("item_per_warp", "persistent"),
               3: ("head_1_cta_per_sm", "head_2_ctas_per_sm")}
 
     def autotune(self, state, cfg, q=None):

@@ -103,13 +103,13 @@ __global__ void __launch_bounds__(kEnsThreads, TileOccupancy<M>::kMinBlocks) ens
 // Phase-locked ALG variant of ens_pair_tiles_kernel (see phase_block_solve): CTAs of kW
 // warps, kMinB of them per SM, each warp on one item, the counters flushed once per CTA as in
 // bia_pair_phase_kernel; bitwise the same results.
-template <int kW, int kMinB>
+template <int kW, int kMinB, bool kBalanced = true>
 __global__ void __launch_bounds__(kW * 32, kMinB) ens_pair_phase_kernel(const EnsArgs A)
 {
     extern __shared__ double phase_smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    unsigned long long *slots = reinterpret_cast<unsigned long long *>(phase_smem + kW * kPhaseSliceDoubles);
+    unsigned long long *slots = reinterpret_cast<unsigned long long *>(phase_smem + kW * phase_slice_doubles<kBalanced>());
     unsigned long long *wtot = slots + warp * kNumStats;
     if (lane < kNumStats) wtot[lane] = 0ull;
     __syncwarp();
@@ -127,8 +127,9 @@ __global__ void __launch_bounds__(kW * 32, kMinB) ens_pair_phase_kernel(const En
     const double *q = A.q ? A.q + base : nullptr;
     double racc[6], cacc[6];
     PairCounters cnt;
-    phase_block_solve(A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base, q, n, A.eps[s],
-                      A.P, bi, bj, lane, live, phase_smem + warp * kPhaseSliceDoubles, racc, cacc, cnt);
+    phase_block_solve<kBalanced>(A.x + base, A.y + base, A.z + base, A.u + base, A.v + base, A.w + base, q, n,
+                                 A.eps[s],
+                      A.P, bi, bj, lane, live, phase_smem + warp * phase_slice_doubles<kBalanced>(), racc, cacc, cnt);
     if (live) {  // warp-uniform
         counters_to_slot(cnt, wtot, lane);
         const int nb = (n + 31) / 32;
@@ -154,8 +155,8 @@ static int ens_phase_setup()
         bool ok = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess;
         ok = ok && cudaFuncSetAttribute(ens_pair_phase_kernel<32, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         32 * (kPhaseSliceDoubles + kNumStats) * (int)sizeof(double)) == cudaSuccess;
-        ok = ok && cudaFuncSetAttribute(ens_pair_phase_kernel<16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        16 * (kPhaseSliceDoubles + kNumStats) * (int)sizeof(double)) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(ens_pair_phase_kernel<32, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        32 * (kTileSmemDoubles + kNumStats) * (int)sizeof(double)) == cudaSuccess;
         if (!ok) cudaGetLastError();
         sms_of[dev] = ok ? sms : 0;
         done_of[dev] = true;
@@ -402,9 +403,9 @@ __global__ void __launch_bounds__(256) ens_energy_kernel(const double *u, const 
 }
 
 // Launch shapes of the ensemble's pair kernels (bia_ensemble_autotune chooses among them):
-//   ALG          0: 8-warp CTAs (ens_pair_tiles_kernel), 1: phase-locked 16-warp CTAs (2 per SM),
-//                2: phase-locked 32-warp CTAs (1 per SM); built-in rule: 2 from two of its CTAs
-//                per SM up, else 0
+//   ALG          0: 8-warp CTAs (ens_pair_tiles_kernel), 1: phase-locked 32-warp CTAs (1 per
+//                SM) with per-lane class loops, 2: the same with the balanced class loops;
+//                built-in rule: 2 from two of its CTAs per SM up, else 0
 //   universal    0: one item per warp, 1: a persistent grid of 2 CTAs per SM (built-in)
 //   learned      the persistent head kernel with 0: 1 CTA per SM, 1: 2 CTAs per SM (built-in)
 // Every shape runs the same per-item arithmetic in the same order: the results are bitwise
@@ -456,8 +457,8 @@ static int ens_pair_launch(bia_context *ctx, bia_ensemble *E, EnsArgs &A, int me
             ens_pair_phase_kernel<32, 1><<<(unsigned)((E->nitems + 31) / 32), 32 * 32,
                                             32 * (kPhaseSliceDoubles + kNumStats) * sizeof(double), st>>>(A);
         } else if (var == 1) {
-            ens_pair_phase_kernel<16, 2><<<(unsigned)((E->nitems + 15) / 16), 16 * 32,
-                                            16 * (kPhaseSliceDoubles + kNumStats) * sizeof(double), st>>>(A);
+            ens_pair_phase_kernel<32, 1, false><<<(unsigned)((E->nitems + 31) / 32), 32 * 32,
+                                                   32 * (kTileSmemDoubles + kNumStats) * sizeof(double), st>>>(A);
         } else {
             ens_pair_tiles_kernel<kMethodAlg><<<grid, kEnsThreads, 0, st>>>(A);
         }

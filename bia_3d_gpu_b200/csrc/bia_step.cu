@@ -112,13 +112,13 @@ __global__ void __launch_bounds__(kThreads, TileOccupancy<M>::kMinBlocks) bia_pa
 // counters ran 13 % faster on the Coulomb cube).  (A persistent grid of one CTA per SM, each
 // taking groups in a fixed stride, was slower again: the groups' costs differ, and the
 // hardware's block scheduler balances them better.)
-template <bool kDeterministic, int kW, int kMinB>
+template <bool kDeterministic, int kW, int kMinB, bool kBalanced = true>
 __global__ void __launch_bounds__(kW * 32, kMinB) bia_pair_phase_kernel(const StepArgs A)
 {
     extern __shared__ double phase_smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    unsigned long long *slots = reinterpret_cast<unsigned long long *>(phase_smem + kW * kPhaseSliceDoubles);
+    unsigned long long *slots = reinterpret_cast<unsigned long long *>(phase_smem + kW * phase_slice_doubles<kBalanced>());
     unsigned long long *wtot = slots + warp * kNumStats;
     if (lane < kNumStats) wtot[lane] = 0ull;
     __syncwarp();
@@ -128,8 +128,8 @@ __global__ void __launch_bounds__(kW * 32, kMinB) bia_pair_phase_kernel(const St
     if (live) warp_block_coords(A.t0 + tl, bi, bj);
     double racc[6], cacc[6];
     PairCounters cnt;
-    phase_block_solve(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P, bi, bj, lane, live,
-                      phase_smem + warp * kPhaseSliceDoubles, racc, cacc, cnt);
+    phase_block_solve<kBalanced>(A.x, A.y, A.z, A.u, A.v, A.w, A.q, A.n, A.eps_th, A.P, bi, bj, lane, live,
+                      phase_smem + warp * phase_slice_doubles<kBalanced>(), racc, cacc, cnt);
     if (live) {  // warp-uniform
         counters_to_slot(cnt, wtot, lane);
         const int i = bi * 32 + lane;
@@ -155,15 +155,22 @@ __global__ void __launch_bounds__(kW * 32, kMinB) bia_pair_phase_kernel(const St
 
 // ALG pair-kernel shapes the autotuner chooses from (bia_context_autotune):
 //   kVarTiles8    8-warp CTAs, per-warp class phases (bia_pair_tiles_kernel)
-//   kVarPhase16   phase-locked CTAs of 16 warps, 2 per SM (64 registers)
-//   kVarPhase32   phase-locked CTAs of 32 warps, 1 per SM (64 registers)
+//   kVarPhase32Lane phase-locked CTAs of 32 warps, 1 per SM, per-lane class loops (rows in
+//                 registers: all-hyperbolic systems, where packing saves no turn)
+//   kVarPhase32   phase-locked CTAs of 32 warps, 1 per SM (64 registers), balanced class
+//                 loops (mixed classes)
+// (CTAs of 16 warps, 2 per SM, were never the fastest: Plummer 72.6, Coulomb 111 ms against
+// 70.9 and 82.7 ms for kVarPhase32 at n = 32768.)  All shapes give bitwise the same step.
 // Without a tuned entry the step takes kVarPhase32 when it gives at least two CTAs per SM,
 // else kVarTiles8.
-enum AlgVariant { kVarTiles8 = 0, kVarPhase16 = 1, kVarPhase32 = 2, kVarCount = 3 };
+enum AlgVariant { kVarTiles8 = 0, kVarPhase32Lane = 1, kVarPhase32 = 2, kVarCount = 3 };
 
 // the warps' slices, then one counter slot of kNumStats u64 per warp
-template <int kW>
-constexpr int phase_smem_bytes() { return kW * (kPhaseSliceDoubles + kNumStats) * (int)sizeof(double); }
+template <int kW, bool kBalanced = true>
+constexpr int phase_smem_bytes()
+{
+    return kW * (phase_slice_doubles<kBalanced>() + kNumStats) * (int)sizeof(double);
+}
 
 // Once per device (the current one): opt the phase-locked kernels in to their dynamic
 // shared memory and read the SM count.  Returns the SM count, 0 when the set-up failed
@@ -184,10 +191,10 @@ static int phase_kernel_setup()
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, phase_smem_bytes<32>()) == cudaSuccess;
         ok = ok && cudaFuncSetAttribute(bia_pair_phase_kernel<false, 32, 1>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, phase_smem_bytes<32>()) == cudaSuccess;
-        ok = ok && cudaFuncSetAttribute(bia_pair_phase_kernel<true, 16, 2>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, phase_smem_bytes<16>()) == cudaSuccess;
-        ok = ok && cudaFuncSetAttribute(bia_pair_phase_kernel<false, 16, 2>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, phase_smem_bytes<16>()) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(bia_pair_phase_kernel<true, 32, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        phase_smem_bytes<32, false>()) == cudaSuccess;
+        ok = ok && cudaFuncSetAttribute(bia_pair_phase_kernel<false, 32, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        phase_smem_bytes<32, false>()) == cudaSuccess;
         if (!ok) cudaGetLastError();  // clear; the 8-warp kernel is used instead
         sms_of[dev] = ok ? sms : 0;
         done_of[dev] = true;
@@ -252,9 +259,9 @@ static void launch_pair_tiles(const StepArgs &A, long long grid, cudaStream_t st
                 <<<(unsigned)((A.nwb + 31) / 32), 32 * 32, phase_smem_bytes<32>(), st>>>(A);
             return;
         }
-        if (var == kVarPhase16) {
-            bia_pair_phase_kernel<kDeterministic, 16, 2>
-                <<<(unsigned)((A.nwb + 15) / 16), 16 * 32, phase_smem_bytes<16>(), st>>>(A);
+        if (var == kVarPhase32Lane) {
+            bia_pair_phase_kernel<kDeterministic, 32, 1, false>
+                <<<(unsigned)((A.nwb + 31) / 32), 32 * 32, phase_smem_bytes<32, false>(), st>>>(A);
             return;
         }
     }

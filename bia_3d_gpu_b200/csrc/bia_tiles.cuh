@@ -304,9 +304,10 @@ __device__ __forceinline__ void warp_block_solve_compact(const double *x, const 
 // (barrier) the rare classes, so the SM fetches one solver's instructions at a time: the
 // mixed-class ALG step is bound by instruction fetch when the warps of one SM sit in
 // different solvers (measured on B200, Coulomb N = 32768: 218 ms per step with 8-warp
-// CTAs, 122 ms phase-locked with 32 warps).  The class loops are the balanced ones
-// (balanced_class_loop), with the same per-block arithmetic and order as
-// warp_block_solve_compact, so the results are bitwise equal.  Every thread of the CTA must
+// CTAs, 122 ms phase-locked with 32 warps).  kBalanced: the balanced class loops
+// (balanced_class_loop; mixed classes), else the per-lane loops of warp_block_solve_compact
+// with the row in registers (all-hyperbolic systems); both have the per-block arithmetic and
+// order of warp_block_solve_compact, so the results are bitwise equal.  Every thread of the CTA must
 // call it (warps without a block pass live = false); ws is the warp's slice of
 // kPhaseSliceDoubles doubles: column states [7][32], column sums [6][32], row states
 // [7][32], row sums [6][32].
@@ -318,8 +319,14 @@ __device__ __forceinline__ void warp_block_solve_compact(const double *x, const 
 #endif
 constexpr int kPhaseWarps = BIA_PHASE_WARPS > 0 ? BIA_PHASE_WARPS : 8;
 constexpr int kPhaseSliceDoubles = kTileSmemDoubles + 13 * 32;
+// a phase-locked warp's slice: the balanced loops add the rows to the column slice; the
+// per-lane loops keep the rows in registers and leave the rest of the SM's on-chip memory to
+// L1, which caches their register spills
+template <bool kBalanced>
+__host__ __device__ constexpr int phase_slice_doubles() { return kBalanced ? kPhaseSliceDoubles : kTileSmemDoubles; }
 constexpr int kPhaseMinBlocks = BIA_PHASE_MIN_BLOCKS;
 
+template <bool kBalanced = true>
 __device__ __forceinline__ void phase_block_solve(const double *x, const double *y, const double *z,
                                                   const double *u, const double *v, const double *w,
                                                   const double *q, int n, double eps_th, const PairParams &P,
@@ -328,6 +335,23 @@ __device__ __forceinline__ void phase_block_solve(const double *x, const double 
 {
     unsigned mh, me, mr;
     counters_zero(cnt);
+    const bool hq = q != nullptr;
+    if (!kBalanced) {  // the per-lane class loops, row state and row sums in registers
+        double si[7];
+#pragma unroll
+        for (int c = 0; c < 6; c++) racc[c] = 0.0;
+        compact_prepare(x, y, z, u, v, w, q, n, eps_th, bi, bj, lane, live, ws, si, mh, me, mr);
+        __syncthreads();
+        compact_class_loop<kClsHyp>(mh, si, ws, ws + 7 * 32, lane, hq, eps_th, P, racc, cnt);
+        __syncthreads();
+        compact_class_loop<kClsEll>(me, si, ws, ws + 7 * 32, lane, hq, eps_th, P, racc, cnt);
+        __syncthreads();
+        compact_class_loop<kClsUv>(mr, si, ws, ws + 7 * 32, lane, hq, eps_th, P, racc, cnt);
+        __syncwarp();
+#pragma unroll
+        for (int c = 0; c < 6; c++) cacc[c] = ws[(7 + c) * 32 + lane];
+        return;
+    }
     double *rs = ws + kTileSmemDoubles;
     double *racs = rs + 7 * 32;
     {
@@ -338,7 +362,6 @@ __device__ __forceinline__ void phase_block_solve(const double *x, const double 
 #pragma unroll
         for (int c = 0; c < 6; c++) racs[c * 32 + lane] = 0.0;
     }
-    const bool hq = q != nullptr;
     __syncthreads();
     balanced_class_loop<kClsHyp>(mh, rs, racs, ws, ws + 7 * 32, lane, hq, eps_th, P, cnt);
     __syncthreads();

@@ -100,8 +100,9 @@ int bia_context_destroy(bia_context *ctx);
 /* Autotuner: times the ALG pair-kernel shapes on this device state (the timed launches
    write only scratch; the state is unchanged) and keeps the fastest for this reduction mode
    and floor(log2 n) in the context, which later steps of that size then use.
-   Shapes: 0 = 8-warp CTAs, 1 = phase-locked 16-warp CTAs (2 per SM), 2 = phase-locked
-   32-warp CTAs (1 per SM).  BIA_METHOD_LEARNED: 0 = one kernel, 1 = split (the plain pairs
+   Shapes: 0 = 8-warp CTAs, 1 = phase-locked 32-warp CTAs (1 per SM) with per-lane class
+   loops, 2 = the same with the balanced class loops (mixed classes; the default from two of
+   its CTAs per SM up).  BIA_METHOD_LEARNED: 0 = one kernel, 1 = split (the plain pairs
    in a universal-variable kernel that defers the learned pairs' head inputs to rows and lists
    their warp-blocks, a persistent kernel that evaluates the rows on the tensor cores, and one
    that finishes the listed warp-blocks; the untuned default at every size).  variant (optional) receives the
@@ -228,8 +229,8 @@ int bia_ensemble_run(bia_context *ctx, bia_ensemble *ens, const bia_config *cfg,
 /* Autotuner of the ensemble's pair-kernel launch shape for cfg->method, timed on these
    systems (1 warm-up and 3 timed launches per shape; only scratch is written, the state is
    unchanged); the fastest is kept in the ensemble and used by later runs.  Shapes: ALG 0 =
-   8-warp CTAs, 1 = phase-locked 16-warp CTAs (2 per SM), 2 = phase-locked 32-warp CTAs
-   (1 per SM); universal variables 0 = one item per warp, 1 = a persistent grid (2 CTAs per
+   8-warp CTAs, 1 = phase-locked 32-warp CTAs (1 per SM) with per-lane class loops, 2 = the
+   same with the balanced class loops; universal variables 0 = one item per warp, 1 = a persistent grid (2 CTAs per
    SM); learned 0 / 1 = the persistent head kernel (the deferred pairs' rows on the tensor
    cores) at 1 / 2 CTAs per SM.  Every shape gives
    bitwise the same results.  variant (optional): the choice (-1 for RKF, one shape); ms

@@ -312,7 +312,7 @@ def test_autotune_picks_a_shape_and_keeps_results(cuda):
         var, ms = solver.autotune(t, cfg, q=qt)
         assert cuda.equal(t, cuda.tensor(s, device="cuda"))   # state untouched
         assert var in (0, 1, 2) and len(ms) == 3 and all(v > 0 for v in ms.values())
-        assert min(ms, key=ms.get) == ("tiles8", "phase16", "phase32")[var]
+        assert min(ms, key=ms.get) == ("tiles8", "phase32_lane", "phase32")[var]
         b = t.clone()
         st = solver.step(b, cfg, q=qt)
         assert st["hyperbola"] + st["ellipse"] + st["universal"] + st["parabola"] + st["degenerate"] == 8192 * 8191 // 2
@@ -333,7 +333,7 @@ def test_alg_shapes_are_bitwise_equal_on_mixed_classes(cuda, det):
     outs = []
     with BIASolver() as solver:
         qt = cuda.tensor(q, device="cuda")
-        for shape in ("tiles8", "phase16", "phase32"):
+        for shape in ("tiles8", "phase32_lane", "phase32"):
             solver.set_shape(METHOD_ALG, n, shape, deterministic=det)
             t = cuda.tensor(s, device="cuda")
             st = solver.step(t, cfg, q=qt)
