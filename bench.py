@@ -868,9 +868,16 @@ def run_extras(solver, timer, args):
         for label, m, kw in entries:
             fdt = kw.pop("dt", dt)
             c = default_config(eps_th=eps, dt=fdt, method=m, **kw)
+            tuned = None
+            if m == 1 and not args.no_autotune:
+                # the context keeps one ALG shape per size: tune it on this workload's state
+                var, _ = solver.autotune(d_init, c, q=d_q)
+                tuned = ("tiles8", "phase32_lane", "phase32")[var]
             ms, _, st, _ = timer.time(d_init, c, d_q, steps, warmup)
             res[label] = {"ms_per_step": ms / steps, "pair_updates_per_s": steps * pairs / (ms * 1e-3),
                           "newton_iterations": newton_per_pair(st, m), "nonfinite": st["nonfinite"]}
+            if tuned:
+                res[label]["alg_shape"] = tuned
             if fdt != dt:
                 res[label]["dt"] = fdt
             if m == 0:
