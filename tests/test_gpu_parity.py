@@ -349,6 +349,29 @@ def test_alg_shapes_are_bitwise_equal_on_mixed_classes(cuda, det):
     assert_parity(outs[0], ref)
 
 
+def test_set_shape_validates_and_pins(cuda):
+    """bia_context_set_shape refuses shapes out of range and methods with one shape, and a
+    pinned shape (or the default restored) gives the same step bitwise."""
+    from bia_3d_gpu_b200 import capi
+    s, eps, q = initial.coulomb_cube(600, seed=32)
+    cfg = default_config(eps_th=eps, dt=1e-5)
+    outs = []
+    with BIASolver() as solver:
+        lib = capi.lib()
+        assert lib.bia_context_set_shape(solver._ctx, METHOD_ALG, 1, 600, 3) == capi.BIA_ERR_INVALID_ARGUMENT
+        assert lib.bia_context_set_shape(solver._ctx, METHOD_ALG, 1, 600, -2) == capi.BIA_ERR_INVALID_ARGUMENT
+        assert lib.bia_context_set_shape(solver._ctx, METHOD_UNIVERSAL, 1, 600, 0) == capi.BIA_ERR_INVALID_ARGUMENT
+        assert lib.bia_context_set_shape(solver._ctx, METHOD_ALG, 1, 0, 0) == capi.BIA_ERR_INVALID_ARGUMENT
+        assert lib.bia_context_set_shape(None, METHOD_ALG, 1, 600, 0) == capi.BIA_ERR_INVALID_ARGUMENT
+        qt = cuda.tensor(q, device="cuda")
+        for shape in (None, "phase32_lane", None):
+            solver.set_shape(METHOD_ALG, 600, shape)
+            t = cuda.tensor(s, device="cuda")
+            solver.step(t, cfg, q=qt, stats=False)
+            outs.append(t.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+
+
 def test_bounded_device_wait_reports_timeout(cuda):
     """A device-side wait that nothing completes gives up after its limit and the step API
     reports BIA_ERR_DEVICE_TIMEOUT; the context then runs a normal step."""
