@@ -82,7 +82,7 @@ METHODS = {"rkf": 0, "alg": 1, "universal": 2, "learned": 3}
 # The learned step's dominant kernel is the rest kernel (it writes every partial slot; the head
 # and finish kernels move under 1 MB at this size on this workload).
 TRAFFIC = {
-    ("plummer_32768", 3, "split"): (16384 * 16383 // 2, 1.200e6 + 344.538e6),
+    ("plummer_32768", 3, "split"): (16384 * 16383 // 2, 1.049e6 + 345.274e6),
     ("coulomb_cube_32768", 1, None): (16384 * 16383 // 2, 3.880e6 + 2105.114e6),  # phase-locked ALG
 }
 
