@@ -25,7 +25,18 @@ namespace bia {
 #ifndef BIA_UV_MIN_BLOCKS
 #define BIA_UV_MIN_BLOCKS 2  // 3 spills in the rotation loop: 9.4 ms vs 8.6 ms at n = 32768
 #endif
+// RKF45: the shared-memory column walk at two CTAs per SM (128 registers; 600 B of spills
+// around the out-of-line pair integrator) measured 184 ms per Coulomb step at n = 32768
+// against 245 ms for the shuffle walk at one CTA per SM (222 registers) and 194 ms for the
+// shuffle walk at two; bitwise the same sums.
+#ifndef BIA_RKF_MIN_BLOCKS
+#define BIA_RKF_MIN_BLOCKS 2
+#endif
+#ifndef BIA_RKF_SMEM
+#define BIA_RKF_SMEM 1  // RKF walks with the column slice in shared memory
+#endif
 template <int M> struct TileOccupancy { static constexpr int kMinBlocks = 1; };
+template <> struct TileOccupancy<kMethodRkf> { static constexpr int kMinBlocks = BIA_RKF_MIN_BLOCKS; };
 template <> struct TileOccupancy<kMethodAlg> { static constexpr int kMinBlocks = BIA_ALG_MIN_BLOCKS; };
 template <> struct TileOccupancy<kMethodUniversal> { static constexpr int kMinBlocks = BIA_UV_MIN_BLOCKS; };
 
@@ -382,6 +393,7 @@ __device__ __forceinline__ void phase_block_solve(const double *x, const double 
 // a different slot on every lane, so the slots take their pairs in ascending k, the order
 // of the shuffle walk: the sums are bitwise the same.  Measured at n = 32768: 6.48 ms
 // against 6.79 ms for the shuffle walk (100 instead of 118 registers, no shuffles).
+template <int M = kMethodUniversal>
 __device__ __forceinline__ void warp_block_solve_uv(const double *x, const double *y, const double *z,
                                                     const double *u, const double *v, const double *w,
                                                     const double *q, int n, double eps_th, const PairParams &P,
@@ -417,7 +429,7 @@ __device__ __forceinline__ void warp_block_solve_uv(const double *x, const doubl
             const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
             const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
             const double eps_ij = q ? eps_th * si[6] * ws[6 * 32 + src] : eps_th;
-            pair_halfdisp<kMethodUniversal>(P, eps_ij, r, g, h, cnt);
+            pair_halfdisp<M>(P, eps_ij, r, g, h, cnt);
         }
 #pragma unroll
         for (int c = 0; c < 6; c++) {
@@ -484,8 +496,8 @@ __device__ __forceinline__ void warp_block_solve(const double *x, const double *
         warp_block_solve_compact(x, y, z, u, v, w, q, n, eps_th, P, bi, bj, lane, racc, cacc, cnt);
         return;
     }
-    if (M == kMethodUniversal) {
-        warp_block_solve_uv(x, y, z, u, v, w, q, n, eps_th, P, bi, bj, lane, racc, cacc, cnt);
+    if (M == kMethodUniversal || (M == kMethodRkf && BIA_RKF_SMEM)) {
+        warp_block_solve_uv<M>(x, y, z, u, v, w, q, n, eps_th, P, bi, bj, lane, racc, cacc, cnt);
         return;
     }
     const unsigned full = 0xffffffffu;
