@@ -679,6 +679,7 @@ __device__ __forceinline__ void finish_batches(const LearnedRows &R, long long f
     while (done < total) {  // warp-uniform
         // this batch: the blocks whose pairs end within done + 32
         const unsigned bm = __ballot_sync(full, c > 0 && incl > done && incl <= done + kBatchPairs);
+        if (bm == 0u) break;  // not reached: the next block's pairs always fit a batch
         const int upto = __shfl_sync(full, incl, 31 - __clz(bm));
         const int qp = done + lane;
         const bool act = qp < upto;
