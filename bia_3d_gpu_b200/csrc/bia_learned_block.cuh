@@ -77,9 +77,11 @@ __device__ __forceinline__ void cta_scan2(MlpSmem &S, int a, int b, int &oa, int
 //          k, lanes in order) and lists the warp-block with its row bases and pair masks.
 //  head    the rows of each head in full 256-row tiles on the tensor cores (mlp_tc.cuh), each
 //          row's guess written over its input.
-//  finish  one warp per listed warp-block: its deferred pairs from their guesses (FP32
-//          correction, FP64 Halley step, composition; the plain solver where the FP64 step
-//          does not settle), their sums added onto the rest kernel's partials.
+//  finish  the deferred pairs from their guesses (FP32 correction, FP64 Halley step,
+//          composition; the plain solver where the FP64 step does not settle), their sums
+//          added onto the rest kernel's partials: a listed warp-block with many pairs (or on
+//          the diagonal) by one warp, the others batched 32 pairs at a time from the pair
+//          descriptors the rest kernel wrote for them (finish_batches).
 // A pair's row holds only that pair's input and guess, and every partial slot is written by
 // the rest kernel and added to by at most one listed warp-block, so neither the order of the
 // rows nor that of the list changes the results.  The rows of a head are capped (rows_cap);
