@@ -121,10 +121,11 @@ def test_learned_needs_heads(cuda):
 @pytest.mark.parametrize("dt", [1e-5, 1e-3])
 def test_learned_split_step_matches_oracle(cuda, dt):
     """The split learned step at n = 6000 (the plain pairs in the rest kernel, which lists
-    the warp-blocks holding learned pairs; those in the list kernel, added onto the same
-    partials): sampled particles against the oracle's full pair sums, and momentum from the
-    antisymmetry.  At dt = 1e-5 almost every start is exact and the list is short; at
-    dt = 1e-3 ~45 % of the pairs are listed."""
+    the warp-blocks holding learned pairs; the head kernel's guesses; the finish kernel, which
+    adds the learned pairs onto the same partials): sampled particles against the oracle's
+    full pair sums, and momentum from the antisymmetry.  At dt = 1e-5 almost every series is
+    exact and the listed blocks hold one or two pairs each (the batched finish); at dt = 1e-3
+    ~45 % of the pairs are listed (the per-block finish)."""
     s, eps, q = initial.coulomb_cube(6000, seed=36)
     t = cuda.tensor(s, device="cuda")
     qt = cuda.tensor(q, device="cuda")
