@@ -12,14 +12,14 @@ from bia_3d_gpu_b200 import (METHOD_ALG, METHOD_LEARNED, METHOD_UNIVERSAL, BIASo
 pytestmark = pytest.mark.gpu
 
 
-def one_step(cuda, s, eps, dt, q=None, method=METHOD_ALG):
+def one_step(cuda, s, eps, dt, q=None, method=METHOD_ALG, **cfg_kw):
     t = cuda.tensor(s, device="cuda")
     qt = cuda.tensor(q, device="cuda") if q is not None else None
     d = cuda.zeros_like(t)
     with BIASolver() as solver:
         if method == METHOD_LEARNED:
             solver.load_heads()
-        st = solver.step(t, default_config(eps_th=eps, dt=dt, method=method), q=qt, disp=d)
+        st = solver.step(t, default_config(eps_th=eps, dt=dt, method=method, **cfg_kw), q=qt, disp=d)
     return t.cpu().numpy(), d.cpu().numpy(), st
 
 
@@ -220,17 +220,19 @@ def test_learned_long_step_full_size(cuda):
     assert ex <= 1e-10 and ev <= 1e-10
 
 
-def test_rkf_full_size_sampled_particles(cuda):
-    """The reference's per-pair RKF45 mode (bia/find_dXYUV_RKF.f90, its tolerances) on
-    coulomb_cube_32768: 24 sampled particles against the oracle's RKF pair sums, to 1e-12
-    of the state, and momentum from the antisymmetry."""
+@pytest.mark.parametrize("relerr", [0.0, 1e-12])
+def test_rkf_full_size_sampled_particles(cuda, relerr):
+    """The reference's per-pair RKF45 mode (bia/find_dXYUV_RKF.f90) on coulomb_cube_32768, at
+    its tolerances (rel 0, abs 1e-16) and at rel 1e-12: 24 sampled particles against the
+    oracle's RKF pair sums at the same tolerances, to 1e-12 of the state, and momentum from
+    the antisymmetry."""
     from bia_3d_gpu_b200 import METHOD_RKF
     s, eps, q, dt, _ = initial.make("coulomb_cube_32768")
     n = s.shape[1]
-    new, disp, st = one_step(cuda, s, eps, dt, q, method=METHOD_RKF)
+    new, disp, st = one_step(cuda, s, eps, dt, q, method=METHOD_RKF, rkf_relerr=relerr, rkf_abserr=1e-16)
     assert st["rkf"] + st["degenerate"] == n * (n - 1) // 2 and st["nonfinite"] == 0
     sel = np.random.default_rng(19).choice(n, 24, replace=False)
-    ref = oracle.particle_disp(s, eps, dt, sel, q=q, method=0)
+    ref = oracle.particle_disp(s, eps, dt, sel, q=q, method=0, relerr=relerr, abserr=1e-16)
     got = disp[:, sel].T
     assert np.abs(got[:, :3] - ref[:, :3]).max() <= 1e-12 * np.abs(s[:3]).max()
     assert np.abs(got[:, 3:] - ref[:, 3:]).max() <= 1e-12 * np.abs(s[3:]).max()
