@@ -16,9 +16,9 @@
 
 namespace bia {
 
-// Resident CTAs per SM each method's kernel is compiled for (register budget
-// 65536 / (256 threads * blocks)): ALG 3 and universal 3 (<= 85 registers), measured
-// fastest on the mixed-class Coulomb workload.
+// Resident CTAs per SM each method's 8-warp kernel is compiled for (register budget
+// 65536 / (256 threads * blocks)): ALG 3 (<= 85 registers, measured fastest on the
+// mixed-class Coulomb workload), universal variables 2 and RKF45 2 (<= 128).
 #ifndef BIA_ALG_MIN_BLOCKS
 #define BIA_ALG_MIN_BLOCKS 3
 #endif
