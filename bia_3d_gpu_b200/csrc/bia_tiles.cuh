@@ -310,7 +310,7 @@ __device__ __forceinline__ void warp_block_solve_compact(const double *x, const 
     __syncwarp();  // the slice is reused by this warp's next block
 }
 
-// Phase-locked CTAs: kPhaseWarps warps, one warp-block each.  After the classification
+// Phase-locked CTAs (32 warps, one warp-block each).  After the classification
 // every warp of the CTA runs the hyperbola loop, then (barrier) the ellipse loop, then
 // (barrier) the rare classes, so the SM fetches one solver's instructions at a time: the
 // mixed-class ALG step is bound by instruction fetch when the warps of one SM sit in
@@ -318,24 +318,19 @@ __device__ __forceinline__ void warp_block_solve_compact(const double *x, const 
 // CTAs, 122 ms phase-locked with 32 warps).  kBalanced: the balanced class loops
 // (balanced_class_loop; mixed classes), else the per-lane loops of warp_block_solve_compact
 // with the row in registers (all-hyperbolic systems); both have the per-block arithmetic and
-// order of warp_block_solve_compact, so the results are bitwise equal.  Every thread of the CTA must
-// call it (warps without a block pass live = false); ws is the warp's slice of
-// kPhaseSliceDoubles doubles: column states [7][32], column sums [6][32], row states
-// [7][32], row sums [6][32].
+// order of warp_block_solve_compact, so the results are bitwise equal.  Every thread of the
+// CTA must call it (warps without a block pass live = false); ws is the warp's slice of
+// phase_slice_doubles<kBalanced>() doubles: column states [7][32], column sums [6][32], and
+// for the balanced loops row states [7][32] and row sums [6][32].
 #ifndef BIA_PHASE_WARPS
 #define BIA_PHASE_WARPS 32  // 0: never use the phase-locked kernels
 #endif
-#ifndef BIA_PHASE_MIN_BLOCKS
-#define BIA_PHASE_MIN_BLOCKS 1
-#endif
-constexpr int kPhaseWarps = BIA_PHASE_WARPS > 0 ? BIA_PHASE_WARPS : 8;
 constexpr int kPhaseSliceDoubles = kTileSmemDoubles + 13 * 32;
 // a phase-locked warp's slice: the balanced loops add the rows to the column slice; the
 // per-lane loops keep the rows in registers and leave the rest of the SM's on-chip memory to
 // L1, which caches their register spills
 template <bool kBalanced>
 __host__ __device__ constexpr int phase_slice_doubles() { return kBalanced ? kPhaseSliceDoubles : kTileSmemDoubles; }
-constexpr int kPhaseMinBlocks = BIA_PHASE_MIN_BLOCKS;
 
 template <bool kBalanced = true>
 __device__ __forceinline__ void phase_block_solve(const double *x, const double *y, const double *z,
