@@ -233,23 +233,33 @@ __global__ void __launch_bounds__(kEnsThreads, 2) ens_pair_learned_finish_kernel
         F.plane = (size_t)((n + 31) / 32) * 32;
         return F;
     };
-    // 1. the dense and diagonal items, one per warp
-    for (long long e = (long long)blockIdx.x * kEnsWarps + warp; e < count;
-         e += (long long)gridDim.x * kEnsWarps) {  // warp-uniform
-        const uint2 it = A.items[A.R.entries[e].x];
-        if ((it.y & 0xffffu) != (it.y >> 16) && A.R.entries[e].w <= (unsigned)kBatchPairs) continue;
-        const FinishBlock F = resolve_entry(e);
-        double racc[6], cacc[6];
-        PairCounters cnt;
-        bool row_hit, col_hit;
-        finish_block_solve(A.R, e, F.B, F.bi, F.bj, lane, s_fin[warp], racc, cacc, cnt, row_hit, col_hit);
-        counters_add(tot, cnt);
-        if (++nchunk == kFlushBlocks) {
-            flush_counters(tot, A.stats, lane);
-            counters_zero(tot);
-            nchunk = 0;
+    // 1. the dense and diagonal items, the list entries spread over the warps one at a time,
+    // read 32 at a time with one load per lane
+    const long long gw = (long long)blockIdx.x * kEnsWarps + warp;
+    const long long stride = (long long)gridDim.x * kEnsWarps;
+    for (long long k0 = 0; gw + k0 * stride < count; k0 += 32) {  // warp-uniform
+        const long long el = gw + (k0 + lane) * stride;
+        bool dense = false;
+        if (el < count) {
+            const uint4 ent = A.R.entries[el];
+            const uint2 it = A.items[ent.x];
+            dense = !((it.y & 0xffffu) != (it.y >> 16) && ent.w <= (unsigned)kBatchPairs);
         }
-        add_partials(F.part, F.plane, F.bi, F.bj, lane, racc, cacc, row_hit, col_hit);
+        for (unsigned dm = __ballot_sync(full, dense); dm; dm &= dm - 1u) {
+            const long long e = gw + (k0 + (__ffs(dm) - 1)) * stride;
+            const FinishBlock F = resolve_entry(e);
+            double racc[6], cacc[6];
+            PairCounters cnt;
+            bool row_hit, col_hit;
+            finish_block_solve(A.R, e, F.B, F.bi, F.bj, lane, s_fin[warp], racc, cacc, cnt, row_hit, col_hit);
+            counters_add(tot, cnt);
+            if (++nchunk == kFlushBlocks) {
+                flush_counters(tot, A.stats, lane);
+                counters_zero(tot);
+                nchunk = 0;
+            }
+            add_partials(F.part, F.plane, F.bi, F.bj, lane, racc, cacc, row_hit, col_hit);
+        }
     }
     // 2. the sparse ones, batched per chunk of list entries (up to 32 per warp, fewer when the
     // list is short)

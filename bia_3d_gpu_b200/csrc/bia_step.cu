@@ -424,24 +424,36 @@ __global__ void __launch_bounds__(kThreads, 2) bia_pair_learned_finish_kernel(co
     PairCounters tot;
     counters_zero(tot);
     int nflush = 0;
-    // 1. the dense and diagonal warp-blocks, one per warp
-    for (long long e = (long long)blockIdx.x * kWarpsPerBlock + warp; e < count;
-         e += (long long)gridDim.x * kWarpsPerBlock) {  // warp-uniform
-        const uint4 ent = A.R.entries[e];
-        int bi, bj;
-        warp_block_coords((long long)ent.x, bi, bj);
-        if (bi != bj && ent.w <= (unsigned)kBatchPairs) continue;  // batched below
-        double racc[6], cacc[6];
-        PairCounters cnt;
-        bool row_hit, col_hit;
-        finish_block_solve(A.R, e, B, bi, bj, lane, s_fin[warp], racc, cacc, cnt, row_hit, col_hit);
-        counters_add(tot, cnt);
-        if (++nflush == kFlushBlocks) {
-            flush_counters(tot, A.stats, lane);
-            counters_zero(tot);
-            nflush = 0;
+    // 1. the dense and diagonal warp-blocks, the list entries spread over the warps one at a
+    // time; a warp reads its next 32 entries with one load per lane (not one dependent load
+    // per entry) and finishes the dense ones among them in order
+    const long long gw = (long long)blockIdx.x * kWarpsPerBlock + warp;
+    const long long stride = (long long)gridDim.x * kWarpsPerBlock;
+    for (long long k0 = 0; gw + k0 * stride < count; k0 += 32) {  // warp-uniform
+        const long long el = gw + (k0 + lane) * stride;
+        bool dense = false;
+        int lbi = 0, lbj = 0;
+        if (el < count) {
+            const uint4 ent = A.R.entries[el];
+            warp_block_coords((long long)ent.x, lbi, lbj);
+            dense = !(lbi != lbj && ent.w <= (unsigned)kBatchPairs);  // else batched below
         }
-        add_learned_sums<kDeterministic>(A, bi, bj, lane, racc, cacc, false, row_hit, col_hit);
+        for (unsigned dm = __ballot_sync(full, dense); dm; dm &= dm - 1u) {
+            const int src = __ffs(dm) - 1;
+            const long long e = gw + (k0 + src) * stride;
+            const int bi = __shfl_sync(full, lbi, src), bj = __shfl_sync(full, lbj, src);
+            double racc[6], cacc[6];
+            PairCounters cnt;
+            bool row_hit, col_hit;
+            finish_block_solve(A.R, e, B, bi, bj, lane, s_fin[warp], racc, cacc, cnt, row_hit, col_hit);
+            counters_add(tot, cnt);
+            if (++nflush == kFlushBlocks) {
+                flush_counters(tot, A.stats, lane);
+                counters_zero(tot);
+                nflush = 0;
+            }
+            add_learned_sums<kDeterministic>(A, bi, bj, lane, racc, cacc, false, row_hit, col_hit);
+        }
     }
     // 2. the sparse ones, batched per chunk of list entries: up to 32 per warp, fewer when the
     // list is short, so that every warp has a chunk (a block's sums do not depend on the blocks
