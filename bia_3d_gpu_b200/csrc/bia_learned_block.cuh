@@ -112,6 +112,60 @@ constexpr size_t kSplitHeader = 32;
 constexpr size_t kRestWarpBytes = kTileSmemDoubles * sizeof(double) + 1024 * sizeof(uint32_t);
 constexpr size_t kRestSmemBytes = kTileWarps * kRestWarpBytes;
 
+// One pair of the rest kernel's walk: the universal-variable prepare and series; a non-exact
+// pair inside a head's domain is deferred (returns its head, L holds its head input), any
+// other is solved here (returns kLearnedPlain, h and its Newton iterations in it).
+__device__ __forceinline__ int rest_pair(double eps_ij, double dt, const double r[3], const double g[3],
+                                         double h[6], LearnedPair &L, int &it)
+{
+    it = 0;
+    const UvPair p = uv_prepare(eps_ij, r, g);
+    if (dt == 0.0) return kLearnedPlain;  // h stays zero
+    const UvSeries sq = uv_series(p, dt);
+    if (!sq.exact && learned_filter(p, dt)) {
+        learned_prepare(eps_ij, dt, r, g, L);
+        if (L.kind != kLearnedPlain) return L.kind;
+    }
+    if (sq.exact) {
+        uv_compose_series(p, sq, dt, r, g, h);
+    } else {
+        double s = uv_series_start(sq);
+        double ifp = 0.0;
+        it = uv_iterate(p, dt, s, &ifp);
+        uv_compose<true>(p, s, r, g, h, ifp);
+    }
+    return kLearnedPlain;
+}
+
+// The non-finite pairs solved in a rest-kernel warp-block whose sums came out non-finite
+// (rare): this lane's pairs solved again, the plain ones counted one by one (the deferred
+// ones are counted where they are finished).  Out of line, so that the walk carries no copy.
+static __device__ __noinline__ int rest_block_recount(const double *si, const double *ws, bool hq, double eps_th,
+                                                      double dt, int i, int n, int bj, int lane)
+{
+    const bool diag = (i / 32 == bj);
+    const int k0 = diag ? 1 : 0, k1 = diag ? 16 : 31;
+    int bad = 0;
+    for (int k = k0; k <= k1; k++) {
+        const int src = (lane + k) & 31;
+        if ((!diag || k < 16 || lane < 16) && i < n && bj * 32 + src < n) {
+            const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
+            const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
+            const double eps_ij = hq ? eps_th * si[6] * ws[6 * 32 + src] : eps_th;
+            double h[6] = {0, 0, 0, 0, 0, 0};
+            LearnedPair L;
+            int it;
+            if (rest_pair(eps_ij, dt, r, g, h, L, it) == kLearnedPlain) {
+                PairCounters scratch;
+                counters_zero(scratch);
+                count_nonfinite(h, scratch);
+                bad += scratch.nonfinite;
+            }
+        }
+    }
+    return bad;
+}
+
 // The rest kernel's walk over warp-block (bi, bj) of the system x..w[0, n) (charges q,
 // coupling eps_th), with the column states and sums in the warp's slice ws and the row slots
 // wslots.  Returns the row sums racc, column sums cacc of the pairs solved here, and the
@@ -151,35 +205,15 @@ __device__ __forceinline__ void rest_block_solve(const double *x, const double *
             const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
             const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
             const double eps_ij = q ? eps_th * si[6] * ws[6 * 32 + src] : eps_th;
-            const UvPair p = uv_prepare(eps_ij, r, g);
-            if (dt != 0.0) {
-                const UvSeries sq = uv_series(p, dt);
-                int kind = kLearnedPlain;
-                if (!sq.exact && learned_filter(p, dt)) {
-                    LearnedPair L;
-                    learned_prepare(eps_ij, dt, r, g, L);
-                    kind = L.kind;
-                    if (kind != kLearnedPlain) {
-                        mask[kind == kLearnedHyp ? kHeadHyp : kHeadEll] |= 1u << k;
-                        wslots[lane * 32 + k] = pack_bf16(L.x0, L.x1);
-                    }
-                }
-                if (kind == kLearnedPlain) {
-                    int it = 0;
-                    if (sq.exact) {
-                        uv_compose_series(p, sq, dt, r, g, h);
-                    } else {
-                        double s = uv_series_start(sq);
-                        double ifp = 0.0;
-                        it = uv_iterate(p, dt, s, &ifp);
-                        uv_compose<true>(p, s, r, g, h, ifp);
-                    }
-                    cnt.it_uv += it;
-                    if (it > kUvItMax) cnt.nonconverged++;
-                    cnt.cls[kUniversal]++;
-                    count_nonfinite(h, cnt);
-                }
+            LearnedPair L;
+            int it;
+            const int kind = rest_pair(eps_ij, dt, r, g, h, L, it);
+            if (kind != kLearnedPlain) {
+                mask[kind == kLearnedHyp ? kHeadHyp : kHeadEll] |= 1u << k;
+                wslots[lane * 32 + k] = pack_bf16(L.x0, L.x1);
             } else {
+                cnt.it_uv += it;
+                if (it > kUvItMax) cnt.nonconverged++;
                 cnt.cls[kUniversal]++;
             }
         }
@@ -192,6 +226,12 @@ __device__ __forceinline__ void rest_block_solve(const double *x, const double *
     }
 #pragma unroll
     for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
+    if (__any_sync(0xffffffffu, !sums_finite(racc, cacc))) {
+        double sic[7];  // a copy: passing si itself would keep it in memory for the whole walk
+#pragma unroll
+        for (int c = 0; c < 7; c++) sic[c] = si[c];
+        cnt.nonfinite += rest_block_recount(sic, ws, q != nullptr, eps_th, dt, i, n, bj, lane);
+    }
     __syncwarp();  // the slice is reused by this warp's next block
 }
 

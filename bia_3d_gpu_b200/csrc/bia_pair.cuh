@@ -1169,7 +1169,10 @@ __device__ __forceinline__ void alg_rare_pair(const PairParams &P, double eps_ij
     }
 }
 
-template <int M>
+// kCountNonfinite false (universal variables and RKF45 only): the caller counts the
+// non-finite half-displacements itself (once per warp-block from its sums, see
+// warp_block_solve_uv).
+template <int M, bool kCountNonfinite = true>
 __device__ __forceinline__ void pair_halfdisp(const PairParams &P, double eps_ij, const double r[3],
                                               const double g[3], double h[6], PairCounters &cnt)
 {
@@ -1178,7 +1181,7 @@ __device__ __forceinline__ void pair_halfdisp(const PairParams &P, double eps_ij
         cnt.it_uv += it;
         if (it > kUvItMax) cnt.nonconverged++;
         cnt.cls[kUniversal]++;
-        count_nonfinite(h, cnt);
+        if (kCountNonfinite) count_nonfinite(h, cnt);
     } else if (M == kMethodAlg) {
         const int c = alg_classify(eps_ij, r, g);
         if (c == kClsUv || c == kClsDeg) {
@@ -1217,8 +1220,19 @@ __device__ __forceinline__ void pair_halfdisp(const PairParams &P, double eps_ij
         cnt.rkf_steps += nacc;
         if (fabs(error) > P.err) cnt.nonconverged++;
         compose_halfdisp(P, g, e_xi, e_eta, YZ, YN, h);
-        count_nonfinite(h, cnt);
+        if (kCountNonfinite) count_nonfinite(h, cnt);
     }
+}
+
+// A warp-block's sums are finite exactly when every half-displacement added into them is (a
+// NaN stays NaN and an infinity stays infinite or turns NaN), so the walks test the lane's
+// row and column sums once per block instead of each pair.
+__device__ __forceinline__ bool sums_finite(const double racc[6], const double cacc[6])
+{
+    bool ok = true;
+#pragma unroll
+    for (int c = 0; c < 6; c++) ok = ok && isfinite(racc[c]) && isfinite(cacc[c]);
+    return ok;
 }
 
 }  // namespace bia

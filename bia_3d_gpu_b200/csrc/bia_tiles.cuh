@@ -388,6 +388,31 @@ __device__ __forceinline__ void phase_block_solve(const double *x, const double 
 // a different slot on every lane, so the slots take their pairs in ascending k, the order
 // of the shuffle walk: the sums are bitwise the same.  Measured at n = 32768: 6.48 ms
 // against 6.79 ms for the shuffle walk (100 instead of 118 registers, no shuffles).
+// The non-finite pairs of a warp-block whose sums came out non-finite (rare): this lane's
+// pairs solved again, counted one by one.  Out of line, so that the walk carries no copy.
+template <int M>
+static __device__ __noinline__ int uv_block_recount(const PairParams &P, const double *si, const double *ws,
+                                                    bool hq, double eps_th, int i, int n, int bj, int lane)
+{
+    const bool diag = (i / 32 == bj);
+    const int k0 = diag ? 1 : 0, k1 = diag ? 16 : 31;
+    int bad = 0;
+    for (int k = k0; k <= k1; k++) {
+        const int src = (lane + k) & 31;
+        if ((!diag || k < 16 || lane < 16) && i < n && bj * 32 + src < n) {
+            const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
+            const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
+            const double eps_ij = hq ? eps_th * si[6] * ws[6 * 32 + src] : eps_th;
+            double h[6];
+            PairCounters scratch;
+            counters_zero(scratch);
+            pair_halfdisp<M, true>(P, eps_ij, r, g, h, scratch);
+            bad += scratch.nonfinite;
+        }
+    }
+    return bad;
+}
+
 template <int M = kMethodUniversal>
 __device__ __forceinline__ void warp_block_solve_uv(const double *x, const double *y, const double *z,
                                                     const double *u, const double *v, const double *w,
@@ -395,6 +420,9 @@ __device__ __forceinline__ void warp_block_solve_uv(const double *x, const doubl
                                                     int bi, int bj, int lane, double racc[6], double cacc[6],
                                                     PairCounters &cnt)
 {
+    // universal variables: the non-finite pairs counted from the block's sums (one test per
+    // block instead of six per pair); RKF45 pairs are costly enough to keep the per-pair count
+    constexpr bool kBlockCheck = (M == kMethodUniversal);
     __shared__ double s_uv[kTileWarps][kTileSmemDoubles];
     double *ws = s_uv[(threadIdx.x >> 5) % kTileWarps];
     double *wacc = ws + 7 * 32;
@@ -424,7 +452,7 @@ __device__ __forceinline__ void warp_block_solve_uv(const double *x, const doubl
             const double r[3] = {si[0] - ws[0 * 32 + src], si[1] - ws[1 * 32 + src], si[2] - ws[2 * 32 + src]};
             const double g[3] = {si[3] - ws[3 * 32 + src], si[4] - ws[4 * 32 + src], si[5] - ws[5 * 32 + src]};
             const double eps_ij = q ? eps_th * si[6] * ws[6 * 32 + src] : eps_th;
-            pair_halfdisp<M>(P, eps_ij, r, g, h, cnt);
+            pair_halfdisp<M, !kBlockCheck>(P, eps_ij, r, g, h, cnt);
         }
 #pragma unroll
         for (int c = 0; c < 6; c++) {
@@ -435,6 +463,12 @@ __device__ __forceinline__ void warp_block_solve_uv(const double *x, const doubl
     }
 #pragma unroll
     for (int c = 0; c < 6; c++) cacc[c] = wacc[c * 32 + lane];
+    if (kBlockCheck && __any_sync(0xffffffffu, !sums_finite(racc, cacc))) {
+        double sic[7];  // a copy: passing si itself would keep it in memory for the whole walk
+#pragma unroll
+        for (int c = 0; c < 7; c++) sic[c] = si[c];
+        cnt.nonfinite += uv_block_recount<M>(P, sic, ws, q != nullptr, eps_th, i, n, bj, lane);
+    }
     __syncwarp();  // the slice is reused by this warp's next block
 }
 

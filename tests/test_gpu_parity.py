@@ -234,6 +234,20 @@ def test_nonfinite_input_is_reported(cuda):
     assert st["nonfinite"] >= 39
 
 
+@pytest.mark.parametrize("method", [METHOD_UNIVERSAL, METHOD_RKF, 3])
+def test_nonfinite_pairs_counted_exactly(cuda, method):
+    """The universal-variable, RKF45 and learned walks test each warp-block's sums instead of
+    each pair and count the pairs again only where a sum is not finite: one NaN particle
+    among 40 gives exactly its 39 pairs."""
+    s, eps = initial.gravity_ball(40, seed=30)
+    s[0, 5] = np.nan
+    t = cuda.tensor(s, device="cuda")
+    with BIASolver() as solver:
+        solver.load_heads()
+        st = solver.step(t, default_config(eps_th=eps, dt=1e-4, method=method))
+    assert st["nonfinite"] == 39
+
+
 def test_invalid_arguments_raise(cuda):
     from bia_3d_gpu_b200 import BiaError
     t = cuda.zeros((6, 8), dtype=cuda.float64, device="cuda")
